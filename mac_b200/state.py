@@ -1,0 +1,225 @@
+"""Host-side state container for the sparse brick grid.
+
+A state mirrors one Mac world: the chunk grid of ``src/ChunkHashTable.h:22-160``
+with 8^3 chunks (called bricks here), every cell's two staggered speed buffers and
+acceleration (``src/Data_Chunk_Speed.h:13-15``), pressure, material
+(``src/Data_CellType_Fluid_Air_Solid_Inflow.h:24``), no-delete mark, const-face
+bits (``src/Data_Grid_Speed.h:54-59``), layer and solver id, plus the particle
+list (``src/TableContainerList.h:24-25``) and the timing data
+(``src/Data_Timing_Time.h:7-9``).
+
+All 512 cells of a live brick are kept, existing or not: the reference keeps the
+data of erased cells of a live chunk and reuses it when ``operator[]`` re-creates
+the cell (``src/ChunkHashTable.tpp:62-87``).
+
+The binary file layout is the one documented in ``oracle/state_format.h`` (the
+tests exchange states with the checkers through it).
+"""
+from __future__ import annotations
+
+import dataclasses
+import struct
+
+import numpy as np
+
+BRICK = 8
+BRICK_CELLS = 512
+AIR, FLUID, SOLID, INFLOW = 0, 1, 2, 3
+FLAG_CONST = (1, 2, 4)
+FLAG_NODELETE = 8
+
+_HDR = struct.Struct("<8sqq3d6dii Q ii136x")
+assert _HDR.size == 256
+
+CELL_F64 = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
+
+
+@dataclasses.dataclass
+class Params:
+    """World parameters (spacing, CFL factor, dt clamp, gravity, layer depth)."""
+    h: tuple = (0.05, 0.05, 0.05)
+    t: float = 0.0
+    dt: float = 0.0
+    cfl_factor: float = 0.5
+    dt_min: float = 0.0
+    dt_max: float = 0.1
+    gravity: float = -9.81
+    gravity_axis: int = 3
+    layer_max: int = 4
+    step: int = 0
+    interp_symmetric: int = 1
+
+
+@dataclasses.dataclass
+class State:
+    params: Params
+    keys: np.ndarray          # (nb, 3) int32 brick keys
+    exists: np.ndarray        # (nb, 512) uint8
+    f64: dict                 # name -> (nb, 512) float64, names in CELL_F64
+    flags: np.ndarray         # (nb, 512) uint8
+    type: np.ndarray          # (nb, 512) uint8
+    layer: np.ndarray         # (nb, 512) int32
+    id: np.ndarray            # (nb, 512) int32
+    pos: np.ndarray           # (np, 3) float64
+
+    @property
+    def nbricks(self) -> int:
+        return int(self.keys.shape[0])
+
+    @property
+    def nparticles(self) -> int:
+        return int(self.pos.shape[0])
+
+    # ------------------------------------------------------------------ io
+    def write(self, path: str) -> None:
+        pr = self.params
+        hdr = _HDR.pack(b"MACST001", self.nbricks, self.nparticles, *pr.h, pr.t, pr.dt,
+                        pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
+                        pr.layer_max, pr.step, pr.interp_symmetric, 0)
+        with open(path, "wb") as f:
+            f.write(hdr)
+            f.write(np.ascontiguousarray(self.keys, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(self.exists, dtype="u1").tobytes())
+            for n in CELL_F64:
+                f.write(np.ascontiguousarray(self.f64[n], dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(self.flags, dtype="u1").tobytes())
+            f.write(np.ascontiguousarray(self.type, dtype="u1").tobytes())
+            f.write(np.ascontiguousarray(self.layer, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(self.id, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(self.pos, dtype="<f8").tobytes())
+
+    @staticmethod
+    def read(path: str) -> "State":
+        with open(path, "rb") as f:
+            buf = f.read()
+        (magic, nb, npart, h0, h1, h2, t, dt, cfl, dtmin, dtmax, g, gax, lmax, step, isym,
+         _r) = _HDR.unpack_from(buf, 0)
+        if magic != b"MACST001":
+            raise ValueError(f"{path}: not a state file")
+        off = _HDR.size
+        nc = nb * BRICK_CELLS
+
+        def take(dtype, count, shape):
+            nonlocal off
+            a = np.frombuffer(buf, dtype=dtype, count=count, offset=off).reshape(shape).copy()
+            off += a.nbytes
+            return a
+
+        keys = take("<i4", nb * 3, (nb, 3))
+        exists = take("u1", nc, (nb, BRICK_CELLS))
+        f64 = {n: take("<f8", nc, (nb, BRICK_CELLS)) for n in CELL_F64}
+        flags = take("u1", nc, (nb, BRICK_CELLS))
+        typ = take("u1", nc, (nb, BRICK_CELLS))
+        layer = take("<i4", nc, (nb, BRICK_CELLS))
+        ids = take("<i4", nc, (nb, BRICK_CELLS))
+        pos = take("<f8", npart * 3, (npart, 3))
+        params = Params(h=(h0, h1, h2), t=t, dt=dt, cfl_factor=cfl, dt_min=dtmin, dt_max=dtmax,
+                        gravity=g, gravity_axis=gax, layer_max=lmax, step=step,
+                        interp_symmetric=isym)
+        return State(params, keys, exists, f64, flags, typ, layer, ids, pos)
+
+    # ------------------------------------------------------------- queries
+    def cell_keys(self) -> np.ndarray:
+        """(nb, 512, 3) integer cell keys of every slot."""
+        o = np.arange(BRICK_CELLS)
+        local = np.stack([o % 8, (o // 8) % 8, o // 64], axis=-1)
+        return self.keys[:, None, :].astype(np.int64) * BRICK + local[None, :, :]
+
+    def fluid_cells(self) -> int:
+        ex = self.exists.astype(bool)
+        return int(np.count_nonzero(ex & ((self.type == FLUID) | (self.type == INFLOW))))
+
+    def sorted(self) -> "State":
+        """Bricks in (z, y, x) key order (the canonical order of state files)."""
+        order = np.lexsort((self.keys[:, 0], self.keys[:, 1], self.keys[:, 2]))
+        return State(self.params, self.keys[order], self.exists[order],
+                     {n: v[order] for n, v in self.f64.items()}, self.flags[order],
+                     self.type[order], self.layer[order], self.id[order], self.pos)
+
+
+def from_cells(params: Params, keys, typ, flags, u, pos=None) -> State:
+    """Builds a state from a list of existing cells (an experiment's ``main()``
+    creates them one by one with ``grid[v]``: ``test/TestJetDEau_Basic.cpp:273-284``).
+    ``keys`` (n,3) int, ``typ``/``flags`` (n,) uint8, ``u`` (n,3) float64 speed 0;
+    later duplicates of a key override earlier ones."""
+    keys = np.asarray(keys, dtype=np.int64).reshape(-1, 3)
+    n = keys.shape[0]
+    bk = np.floor_divide(keys, BRICK)
+    ub, inv = np.unique(bk, axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    order = np.lexsort((ub[:, 0], ub[:, 1], ub[:, 2]))
+    rank = np.empty_like(order)
+    rank[order] = np.arange(len(order))
+    ub = ub[order]
+    bidx = rank[inv]
+    loc = keys - bk * BRICK
+    off = loc[:, 0] + 8 * loc[:, 1] + 64 * loc[:, 2]
+    st = empty_state(params, ub.astype(np.int32))
+    st.exists[bidx, off] = 1
+    st.type[bidx, off] = np.asarray(typ, dtype=np.uint8).reshape(n)
+    st.flags[bidx, off] = np.asarray(flags, dtype=np.uint8).reshape(n)
+    u = np.asarray(u, dtype=np.float64).reshape(n, 3)
+    st.f64["u0x"][bidx, off] = u[:, 0]
+    st.f64["u0y"][bidx, off] = u[:, 1]
+    st.f64["u0z"][bidx, off] = u[:, 2]
+    if pos is not None:
+        st.pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    return st
+
+
+def _box(x0, x1, y0, y1, z0, z1):
+    z, y, x = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1),
+                          indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=-1)
+
+
+def empty_state(params: Params, keys: np.ndarray) -> State:
+    nb = keys.shape[0]
+    z = lambda dt: np.zeros((nb, BRICK_CELLS), dtype=dt)
+    return State(params, keys.astype(np.int32), z(np.uint8), {n: z(np.float64) for n in CELL_F64},
+                 z(np.uint8), z(np.uint8), np.full((nb, BRICK_CELLS), -1, np.int32),
+                 np.full((nb, BRICK_CELLS), -1, np.int32), np.zeros((0, 3), np.float64))
+
+
+def jet_world(nx=32, ny=32, nz=64, h=0.05, r_inflow=4.0, w_inflow=1.0, pool_depth=0,
+              layer_max=4, cfl=0.5, dt_max=0.1, particles_per_cell=8, seed=1) -> State:
+    """Vertical water jet in a walled box (the jet experiments' setup, with solid
+    side walls and floor): cells 0..nx-1 x 0..ny-1 x 0..nz-1 are open, the walls
+    at x,y = -1 / n and the floor at z = -1 are Solid, a disc of radius
+    ``r_inflow`` cells centred on the floor is Inflow with a const face speed
+    ``w_inflow`` (``test/Jet3.cpp:448-470`` builds its inflow the same way).
+    ``pool_depth`` > 0 fills z < pool_depth with fluid particles at
+    ``particles_per_cell`` jittered particles per cell (seeded)."""
+    pr = Params(h=(h, h, h), cfl_factor=cfl, dt_max=dt_max, layer_max=layer_max)
+    walls = [
+        _box(-1, -1, -1, ny, -1, nz - 1), _box(nx, nx, -1, ny, -1, nz - 1),
+        _box(0, nx - 1, -1, -1, -1, nz - 1), _box(0, nx - 1, ny, ny, -1, nz - 1),
+        _box(0, nx - 1, 0, ny - 1, -1, -1),
+    ]
+    wk = np.concatenate(walls, axis=0)
+    fl = _box(0, nx - 1, 0, ny - 1, 0, 0)
+    cx, cy = (nx - 1) / 2.0, (ny - 1) / 2.0
+    disc = fl[(fl[:, 0] - cx) ** 2 + (fl[:, 1] - cy) ** 2 <= r_inflow ** 2]
+    keys = np.concatenate([wk, disc], axis=0)
+    typ = np.concatenate([np.full(len(wk), SOLID, np.uint8), np.full(len(disc), INFLOW, np.uint8)])
+    flags = np.concatenate([np.zeros(len(wk), np.uint8), np.full(len(disc), FLAG_CONST[2], np.uint8)])
+    u = np.zeros((len(keys), 3))
+    u[len(wk):, 2] = w_inflow
+    pos = None
+    if pool_depth > 0:
+        pos = pool_particles(nx, ny, pool_depth, h, particles_per_cell, seed)
+    return from_cells(pr, keys, typ, flags, u, pos)
+
+
+def pool_particles(nx, ny, depth, h, ppc=8, seed=1):
+    """Jittered 2x2x2 lattice (offsets +-h/4 plus uniform jitter in (-h/4, h/4))
+    in every cell of the slab 0..nx-1 x 0..ny-1 x 0..depth-1."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(np.arange(depth), np.arange(ny), np.arange(nx), indexing="ij")
+    base = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=-1).astype(np.float64)
+    out = []
+    for s in range(ppc):
+        o = np.array([0.25 if (s >> i) & 1 else -0.25 for i in range(3)])
+        j = (rng.random(base.shape) - 0.5) * 0.499
+        out.append((base + o + j) * h)
+    return np.concatenate(out, axis=0)

@@ -1,0 +1,1048 @@
+/* CPU restatement of Mac's per-timestep hot path (test infrastructure only).
+ *
+ * This is the oracle the CUDA path is checked against. It restates, in plain
+ * C, the algorithms the reference composes in test/TestJetDEau_Basic.cpp:433-446
+ * (pipeline A): topology rebuild, CFL time step, gravity + first-order upwind
+ * convection, SSP-RK2 with two pressure projections, air-layer velocity
+ * extrapolation and RK4 particle moves through the staggered trilinear field.
+ * Every function cites the reference lines it follows. Arithmetic is written
+ * in the reference's operation order (contraction off) so that non-solver
+ * results agree bit for bit with the reference compiled from its own headers
+ * (oracle/_ref/mac_ref, built by oracle/Makefile); the linear solve is FP64
+ * Jacobi-CG to a relative residual of 1e-14 (the reference's Umfpack LU,
+ * src/Policy_Solve_Linear_Umfpack.h:23-70, is not installed here).
+ *
+ * Only the tests, the smoke check and bench.py's CPU-baseline leg may load this
+ * library, and only as a checker or a reported baseline.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "state_format.h"
+
+typedef struct {
+  int32_t key[3];
+  uint8_t exists[512];
+  double u[2][3][512];
+  double acc[3][512];
+  double p[512];
+  uint8_t flags[512];
+  uint8_t type[512];
+  int32_t layer[512];
+  int32_t id[512];
+  int32_t mark[512]; /* scratch */
+} brick_t;
+
+typedef struct {
+  mac_state_header hdr;
+  double h[3], ih[3];
+  brick_t** b;
+  int64_t nb, capb;
+  int64_t* hkeys; /* open addressing table: packed key, -1 empty */
+  int32_t* hval;
+  int64_t hcap;
+  double* pos;
+  int64_t np, capp;
+  uint64_t seed;
+  /* statistics */
+  int64_t invalid_reads, created_cells, cg_iters;
+  double max_div, last_relres;
+} world_t;
+
+/* ------------------------------------------------------------------ grid */
+static int64_t pack_key(int x, int y, int z) {
+  return ((int64_t)(uint32_t)(x + (1 << 20)) & 0x1FFFFF) |
+         (((int64_t)(uint32_t)(y + (1 << 20)) & 0x1FFFFF) << 21) |
+         (((int64_t)(uint32_t)(z + (1 << 20)) & 0x1FFFFF) << 42);
+}
+
+static uint64_t hmix(uint64_t k) {
+  k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+  return k;
+}
+
+static void hash_rebuild(world_t* w) {
+  int64_t need = 64;
+  while (need < 4 * (w->nb + 1)) need <<= 1;
+  if (need != w->hcap) {
+    free(w->hkeys); free(w->hval);
+    w->hcap = need;
+    w->hkeys = (int64_t*)malloc(sizeof(int64_t) * need);
+    w->hval = (int32_t*)malloc(sizeof(int32_t) * need);
+  }
+  for (int64_t i = 0; i < w->hcap; ++i) w->hkeys[i] = -1;
+  for (int64_t i = 0; i < w->nb; ++i) {
+    int64_t k = pack_key(w->b[i]->key[0], w->b[i]->key[1], w->b[i]->key[2]);
+    uint64_t s = hmix((uint64_t)k) & (uint64_t)(w->hcap - 1);
+    while (w->hkeys[s] != -1) s = (s + 1) & (uint64_t)(w->hcap - 1);
+    w->hkeys[s] = k;
+    w->hval[s] = (int32_t)i;
+  }
+}
+
+static int64_t brick_find(const world_t* w, int bx, int by, int bz) {
+  int64_t k = pack_key(bx, by, bz);
+  uint64_t s = hmix((uint64_t)k) & (uint64_t)(w->hcap - 1);
+  while (w->hkeys[s] != -1) {
+    if (w->hkeys[s] == k) return w->hval[s];
+    s = (s + 1) & (uint64_t)(w->hcap - 1);
+  }
+  return -1;
+}
+
+/* Floor division of a cell key by the chunk edge (src/ChunkHashTable.tpp:180-196). */
+static int fdiv8(int v) { return v >= 0 ? v / 8 : (v + 1) / 8 - 1; }
+/* Offset x + 8y + 64z inside the chunk (src/Offset.h:14-24). */
+static int offs(int x, int y, int z) { return (x & 7) + 8 * (y & 7) + 64 * (z & 7); }
+
+static void brick_prototype(brick_t* b, int bx, int by, int bz) {
+  memset(b, 0, sizeof(*b));
+  b->key[0] = bx; b->key[1] = by; b->key[2] = bz;
+  for (int o = 0; o < 512; ++o) { b->layer[o] = -1; b->id[o] = -1; }
+}
+
+static int64_t brick_create(world_t* w, int bx, int by, int bz) {
+  if (w->nb == w->capb) {
+    w->capb = w->capb ? 2 * w->capb : 64;
+    w->b = (brick_t**)realloc(w->b, sizeof(brick_t*) * w->capb);
+  }
+  brick_t* b = (brick_t*)malloc(sizeof(brick_t));
+  brick_prototype(b, bx, by, bz);
+  w->b[w->nb] = b;
+  ++w->nb;
+  if (4 * (w->nb + 1) > w->hcap) hash_rebuild(w);
+  else {
+    int64_t k = pack_key(bx, by, bz);
+    uint64_t s = hmix((uint64_t)k) & (uint64_t)(w->hcap - 1);
+    while (w->hkeys[s] != -1) s = (s + 1) & (uint64_t)(w->hcap - 1);
+    w->hkeys[s] = k;
+    w->hval[s] = (int32_t)(w->nb - 1);
+  }
+  return w->nb - 1;
+}
+
+typedef struct { int64_t b; int o; } cell_t;
+
+/* Lookup without creation; b = -1 when the chunk does not exist. */
+static cell_t cell_at(const world_t* w, int x, int y, int z) {
+  cell_t c;
+  c.b = brick_find(w, fdiv8(x), fdiv8(y), fdiv8(z));
+  c.o = offs(x, y, z);
+  return c;
+}
+
+static int cell_valid(const world_t* w, cell_t c) { return c.b >= 0 && w->b[c.b]->exists[c.o]; }
+
+/* grid[key]: creates the chunk (from the prototype) and sets the existence bit
+ * (src/ChunkHashTable.tpp:62-87). Data of a re-created cell is whatever the
+ * chunk held. */
+static cell_t cell_get(world_t* w, int x, int y, int z) {
+  cell_t c = cell_at(w, x, y, z);
+  if (c.b < 0) c.b = brick_create(w, fdiv8(x), fdiv8(y), fdiv8(z));
+  if (!w->b[c.b]->exists[c.o]) ++w->created_cells;
+  w->b[c.b]->exists[c.o] = 1;
+  return c;
+}
+
+#define B(c) (w->b[(c).b])
+static void key_of(const world_t* w, int64_t bi, int o, int k[3]) {
+  k[0] = w->b[bi]->key[0] * 8 + (o & 7);
+  k[1] = w->b[bi]->key[1] * 8 + ((o >> 3) & 7);
+  k[2] = w->b[bi]->key[2] * 8 + (o >> 6);
+}
+
+/* Neighbour read helpers: a read of a cell that does not exist would
+ * dereference a null chunk in the reference (src/Offset_Base_Neighbour.h:14-33);
+ * here it returns the stored value (0 for a missing chunk) and is counted. */
+static double rd_u(world_t* w, int ib, int i, const int k[3], int dx, int dy, int dz) {
+  cell_t c = cell_at(w, k[0] + dx, k[1] + dy, k[2] + dz);
+  if (!cell_valid(w, c)) ++w->invalid_reads;
+  return c.b >= 0 ? B(c)->u[ib][i][c.o] : 0.0;
+}
+static double rd_p(world_t* w, const int k[3], int dx, int dy, int dz) {
+  cell_t c = cell_at(w, k[0] + dx, k[1] + dy, k[2] + dz);
+  if (!cell_valid(w, c)) ++w->invalid_reads;
+  return c.b >= 0 ? B(c)->p[c.o] : 0.0;
+}
+
+static int is_fluid(uint8_t t) { return t == MAC_FLUID || t == MAC_INFLOW; }
+/* Data_CellType_Domain_Fluid: in domain <=> GetIsFluid (src/Data_CellType_Domain_Fluid.h:59-62). */
+static int in_domain(uint8_t t) { return is_fluid(t); }
+/* Sticky setters (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:141-157). */
+static uint8_t set_air(uint8_t t) { return t == MAC_FLUID ? MAC_AIR : t; }
+static uint8_t set_fluid(uint8_t t) { return t == MAC_AIR ? MAC_FLUID : t; }
+
+/* Data_Grid_Speed::Set(i, v, force) (src/Data_Grid_Speed.tpp:19-26): the three
+ * buffers of a cell share its const bits (src/Data_Chunk_Speed.h:99-123). */
+static void set_u(brick_t* b, double* arr, int o, int i, double v, int force) {
+  if (force || !(b->flags[o] & (1u << i))) arr[o] = v;
+}
+
+/* ------------------------------------------------------------- topology */
+/* src/Algorithms_Initialize_MacCell.h:15-21 */
+static void alg_initialize(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o)
+      if (w->b[bi]->exists[o]) w->b[bi]->layer[o] = -1;
+}
+
+/* Policy_Particle_To_Key::GetKeyFromParticle (src/Policy_Particle_To_Key.h:24-35). */
+static void particle_key(const world_t* w, const double* pos, int k[3]) {
+  for (int i = 0; i < 3; ++i) k[i] = (int)lround(pos[i] * w->ih[i]);
+}
+
+/* src/Algorithms_Layer_Initial_With_Particle.h:26-30 */
+static void alg_layer_initial(world_t* w) {
+  for (int64_t q = 0; q < w->np; ++q) {
+    int k[3];
+    particle_key(w, w->pos + 3 * q, k);
+    cell_t c = cell_get(w, k[0], k[1], k[2]);
+    B(c)->layer[c.o] = 0;
+    B(c)->type[c.o] = set_fluid(B(c)->type[c.o]);
+  }
+}
+
+static void add_particle(world_t* w, const double p[3]) {
+  if (w->np == w->capp) {
+    w->capp = w->capp ? 2 * w->capp : 1024;
+    w->pos = (double*)realloc(w->pos, sizeof(double) * 3 * w->capp);
+  }
+  memcpy(w->pos + 3 * w->np, p, sizeof(double) * 3);
+  ++w->np;
+}
+
+/* src/Algorithms_Create_Fluid_Particle.h:25-33 with
+ * Policy_Is_Inbound_Filling_Layer_CellType (src/Policy_Is_Inbound_Filling_Layer_CellType.h:16-19)
+ * and the 8-jittered-particles refill. */
+static void alg_create_fluid(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o] || b->type[o] != MAC_INFLOW || b->layer[o] != -1) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      for (int s = 0; s < 8; ++s) {
+        double p[3];
+        mac_jitter8_position(w->seed, k[0], k[1], k[2], s, w->h[0], w->h[1], w->h[2], p);
+        add_particle(w, p);
+      }
+      b->layer[o] = 0;
+      b->type[o] = set_fluid(b->type[o]);
+    }
+  }
+}
+
+static const int DIRS[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+
+typedef struct { int* k; int64_t n, cap; } keylist;
+static void kl_push(keylist* l, const int k[3]) {
+  if (l->n == l->cap) { l->cap = l->cap ? 2 * l->cap : 256; l->k = (int*)realloc(l->k, sizeof(int) * 3 * l->cap); }
+  memcpy(l->k + 3 * l->n, k, sizeof(int) * 3);
+  ++l->n;
+}
+
+static int empty_or_invalid(world_t* w, int x, int y, int z) {
+  cell_t c = cell_at(w, x, y, z);
+  return !cell_valid(w, c) || B(c)->layer[c.o] == -1;
+}
+
+/* src/Algorithms_Update_CellType_Layer.h:22-89 */
+static void alg_update_layer(world_t* w) {
+  keylist s = {0}, s2 = {0};
+  int lmax = w->hdr.layer_max;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      if (!w->b[bi]->exists[o] || w->b[bi]->layer[o] != 0) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      for (int d = 0; d < 6; ++d)
+        if (empty_or_invalid(w, k[0] + DIRS[d][0], k[1] + DIRS[d][1], k[2] + DIRS[d][2])) {
+          kl_push(&s, k);
+          break;
+        }
+    }
+  for (int lay = 1; lay <= lmax; ++lay) {
+    for (int64_t q = 0; q < s.n; ++q) {
+      int* k = s.k + 3 * q;
+      for (int d = 0; d < 6; ++d) {
+        int x = k[0] + DIRS[d][0], y = k[1] + DIRS[d][1], z = k[2] + DIRS[d][2];
+        if (empty_or_invalid(w, x, y, z)) {
+          cell_t c = cell_get(w, x, y, z);
+          B(c)->layer[c.o] = lay;
+          B(c)->type[c.o] = set_air(B(c)->type[c.o]);
+          int kk[3] = {x, y, z};
+          kl_push(&s2, kk);
+        }
+      }
+    }
+    keylist t = s; s = s2; s2 = t; s2.n = 0;
+  }
+  for (int64_t q = 0; q < s.n; ++q) {
+    int* k = s.k + 3 * q;
+    for (int i = 0; i < 3; ++i) {
+      int x = k[0] + (i == 0), y = k[1] + (i == 1), z = k[2] + (i == 2);
+      if (empty_or_invalid(w, x, y, z)) {
+        cell_t c = cell_get(w, x, y, z);
+        B(c)->layer[c.o] = lmax + 1;
+        B(c)->type[c.o] = set_air(B(c)->type[c.o]);
+      }
+    }
+  }
+  free(s.k); free(s2.k);
+}
+
+/* src/Algorithms_Delete_MacCell.h:22-44 and chunk freeing in erase
+ * (src/ChunkHashTable.tpp:132-147). */
+static void alg_delete(world_t* w) {
+  int64_t keep = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    int any = 0;
+    for (int o = 0; o < 512; ++o) {
+      if (b->exists[o] && b->layer[o] == -1 && !(b->flags[o] & MAC_FLAG_NODELETE)) b->exists[o] = 0;
+      any |= b->exists[o];
+    }
+    if (any) w->b[keep++] = b;
+    else free(b);
+  }
+  w->nb = keep;
+  hash_rebuild(w);
+}
+
+/* src/Algorithms_Calculate_Time_Step.h:41-62 and src/Policy_CheckDT.h:16-29 */
+static void alg_dt(world_t* w) {
+  double mx = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      if (!b->exists[o] || !is_fluid(b->type[o])) continue;
+      double t = 0;
+      for (int i = 0; i < 3; ++i) {
+        double v = b->u[0][i][o] * w->ih[i];
+        t += v * v;
+      }
+      if (t > mx) mx = t;
+    }
+  double dt = 1 / sqrt(mx) * w->hdr.cfl_factor;
+  if (dt < w->hdr.dt_min) dt = w->hdr.dt_min;
+  else if (dt > w->hdr.dt_max) dt = w->hdr.dt_max;
+  w->hdr.dt = dt;
+}
+
+/* ------------------------------------------------------------- advection */
+/* Policy_Gravity::NeedToApply / ApplyGravity (src/Policy_Gravity.h:14-45). */
+static void alg_gravity(world_t* w, int ib) {
+  (void)ib;
+  int ax = w->hdr.gravity_axis - 1;
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o]) continue;
+      int apply = 0;
+      if (is_fluid(b->type[o])) apply = 1;
+      else if (b->layer[o] != -1) {
+        int k[3];
+        key_of(w, bi, o, k);
+        k[ax] -= 1;
+        cell_t n = cell_at(w, k[0], k[1], k[2]);
+        apply = cell_valid(w, n) && is_fluid(B(n)->type[n.o]);
+      }
+      if (apply) set_u(b, b->acc[ax], o, ax, b->acc[ax][o] + w->hdr.gravity, 0);
+    }
+  }
+}
+
+/* Policy_Convection_Apply_If::Get_If_Apply_Convection(neigh, i)
+ * (src/Policy_Convection_Apply_If.h:41-61). */
+static int conv_apply(world_t* w, int64_t bi, int o, int i) {
+  brick_t* b = w->b[bi];
+  if (is_fluid(b->type[o])) return 1;
+  if (b->layer[o] == -1) return 0;
+  int k[3];
+  key_of(w, bi, o, k);
+  k[i] -= 1;
+  cell_t n = cell_at(w, k[0], k[1], k[2]);
+  if (!cell_valid(w, n)) return 0;
+  return is_fluid(B(n)->type[n.o]);
+}
+
+/* Get_Speed_At_Bound (src/Policy_Speed_Interpolation_Linear_Symmetric.h:120-127). */
+static double speed_at_bound(world_t* w, int ib, const int k[3], int i, int j) {
+  if (i == j) return rd_u(w, ib, j, k, 0, 0, 0);
+  int ej[3] = {0, 0, 0}, ei[3] = {0, 0, 0};
+  ej[j] = 1; ei[i] = 1;
+  double a = rd_u(w, ib, j, k, 0, 0, 0);
+  double b = rd_u(w, ib, j, k, ej[0], ej[1], ej[2]);
+  double c = rd_u(w, ib, j, k, -ei[0], -ei[1], -ei[2]);
+  double d = rd_u(w, ib, j, k, ej[0] - ei[0], ej[1] - ei[1], ej[2] - ei[2]);
+  return 0.25 * (((a + b) + c) + d);
+}
+
+/* Policy_Upwind_1_Order::Get_Convection_Element / Get_Convection_Speed
+ * (src/Policy_Upwind_1_Order.h:18-38,58-66). */
+static double convection_speed(world_t* w, int ib, const int k[3], int i) {
+  double ret = 0;
+  for (int j = 0; j < 3; ++j) {
+    double U = speed_at_bound(w, ib, k, i, j);
+    int e[3] = {0, 0, 0};
+    e[j] = 1;
+    double U1 = rd_u(w, ib, i, k, 0, 0, 0), U2;
+    if (U > 0) {
+      U2 = rd_u(w, ib, i, k, -e[0], -e[1], -e[2]);
+      U *= (U1 - U2) * w->ih[j];
+    } else {
+      U2 = rd_u(w, ib, i, k, e[0], e[1], e[2]);
+      U *= (U2 - U1) * w->ih[j];
+    }
+    ret -= U;
+  }
+  return ret;
+}
+
+/* src/Algorithms_Convection.h:24-33 */
+static void alg_convection(world_t* w, int ib) {
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o]) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      for (int i = 0; i < 3; ++i)
+        if (conv_apply(w, bi, o, i)) set_u(b, b->acc[i], o, i, b->acc[i][o] + convection_speed(w, ib, k, i), 0);
+    }
+  }
+}
+
+static void acc_zero(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o)
+      if (w->b[bi]->exists[o])
+        for (int i = 0; i < 3; ++i) w->b[bi]->acc[i][o] = 0.0;
+}
+
+/* ------------------------------------------------------------- pressure */
+typedef struct {
+  int64_t n;
+  int64_t* rowptr;
+  int64_t* col;
+  double* val;
+  double* diag;
+  int64_t* bi; /* cell of each unknown */
+  int* o;
+} csr_t;
+
+static void csr_free(csr_t* A) { free(A->rowptr); free(A->col); free(A->val); free(A->diag); free(A->bi); free(A->o); memset(A, 0, sizeof(*A)); }
+
+/* Von Neumann face test: GetIsConstantInterface_Impl(neigh, dim, sign)
+ * (src/Data_CellType_Interface_Constant.h:45-61). */
+static int neumann(world_t* w, cell_t c, cell_t n, int i, int s) {
+  if (!cell_valid(w, n)) return 0;
+  return s > 0 ? (B(n)->flags[n.o] >> i) & 1 : (B(c)->flags[c.o] >> i) & 1;
+}
+
+/* Assembly of the ghost-fluid 7-point matrix (src/Algorithms_Solve_Pressure.h:44-157):
+ * diag -= 1/h^2 per face, += 1/h^2 back on a valid Neumann face, off-diagonal
+ * +1/h^2 to a valid in-domain neighbour; anything else is Dirichlet p = 0.
+ * Unknowns are numbered in brick order rather than by the reference's BFS; the
+ * solution of the system does not depend on the numbering. */
+static void assemble(world_t* w, csr_t* A) {
+  memset(A, 0, sizeof(*A));
+  int64_t n = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      b->id[o] = -1;
+      if (b->exists[o] && in_domain(b->type[o])) b->id[o] = (int32_t)n++;
+    }
+  A->n = n;
+  A->rowptr = (int64_t*)calloc(n + 1, 8);
+  A->col = (int64_t*)malloc(sizeof(int64_t) * (6 * n + 1));
+  A->val = (double*)malloc(sizeof(double) * (6 * n + 1));
+  A->diag = (double*)malloc(sizeof(double) * (n + 1));
+  A->bi = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  A->o = (int*)malloc(sizeof(int) * (n + 1));
+  int64_t nnz = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      if (b->id[o] < 0) continue;
+      int64_t r = b->id[o];
+      A->bi[r] = bi; A->o[r] = o;
+      int k[3];
+      key_of(w, bi, o, k);
+      cell_t c = {bi, o};
+      double diag = 0;
+      for (int i = 0; i < 3; ++i)
+        for (int s = -1; s <= 1; s += 2) {
+          double h2 = w->ih[i] * w->ih[i];
+          diag -= h2;
+          cell_t nb = cell_at(w, k[0] + s * (i == 0), k[1] + s * (i == 1), k[2] + s * (i == 2));
+          if (!cell_valid(w, nb)) continue;
+          if (neumann(w, c, nb, i, s)) diag += h2;
+          else if (in_domain(B(nb)->type[nb.o])) {
+            A->col[nnz] = B(nb)->id[nb.o];
+            A->val[nnz] = h2;
+            ++nnz;
+          }
+        }
+      A->diag[r] = diag;
+      A->rowptr[r + 1] = nnz;
+    }
+}
+
+/* y = A x */
+static void spmv(const csr_t* A, const double* x, double* y) {
+  for (int64_t r = 0; r < A->n; ++r) {
+    double s = A->diag[r] * x[r];
+    for (int64_t k = A->rowptr[r]; k < A->rowptr[r + 1]; ++k) s += A->val[k] * x[A->col[k]];
+    y[r] = s;
+  }
+}
+
+static double g_rtol = 1e-14;
+
+/* FP64 Jacobi-preconditioned CG on -A (SPD), standing in for the LU solve. */
+static void solve(world_t* w, const csr_t* A, const double* b, double* x) {
+  int64_t n = A->n;
+  double *r = (double*)malloc(8 * (n + 1)), *z = (double*)malloc(8 * (n + 1)),
+         *p = (double*)malloc(8 * (n + 1)), *q = (double*)malloc(8 * (n + 1));
+  double bn = 0;
+  for (int64_t i = 0; i < n; ++i) { x[i] = 0; r[i] = -b[i]; bn += b[i] * b[i]; }
+  bn = sqrt(bn);
+  w->last_relres = 0;
+  if (bn > 0) {
+    double rz = 0;
+    for (int64_t i = 0; i < n; ++i) { z[i] = r[i] / -A->diag[i]; p[i] = z[i]; rz += r[i] * z[i]; }
+    for (int it = 0; it < 200000; ++it) {
+      spmv(A, p, q);
+      double pq = 0;
+      for (int64_t i = 0; i < n; ++i) { q[i] = -q[i]; pq += p[i] * q[i]; }
+      double a = rz / pq, rn = 0;
+      for (int64_t i = 0; i < n; ++i) { x[i] += a * p[i]; r[i] -= a * q[i]; rn += r[i] * r[i]; }
+      ++w->cg_iters;
+      w->last_relres = sqrt(rn) / bn;
+      if (sqrt(rn) <= g_rtol * bn) break;
+      double rz2 = 0;
+      for (int64_t i = 0; i < n; ++i) { z[i] = r[i] / -A->diag[i]; rz2 += r[i] * z[i]; }
+      double be = rz2 / rz;
+      rz = rz2;
+      for (int64_t i = 0; i < n; ++i) p[i] = z[i] + be * p[i];
+    }
+  }
+  free(r); free(z); free(p); free(q);
+}
+
+/* Policy_Divergence::Get_Divergence (src/Policy_Divergence.h:20-29). */
+static double divergence(world_t* w, int ib, const int k[3]) {
+  double ret = 0;
+  for (int i = 0; i < 3; ++i) {
+    ret -= rd_u(w, ib, i, k, 0, 0, 0) * w->ih[i];
+    ret += rd_u(w, ib, i, k, i == 0, i == 1, i == 2) * w->ih[i];
+  }
+  return ret;
+}
+
+/* Policy_Pressure_If_Correction::Get_Pressure_If_Correction(neigh, i)
+ * (src/Policy_Pressure_If_Correction.h:33-49). */
+static int correction_applies(world_t* w, int64_t bi, int o, int i) {
+  if (in_domain(w->b[bi]->type[o])) return 1;
+  int k[3];
+  key_of(w, bi, o, k);
+  k[i] -= 1;
+  cell_t n = cell_at(w, k[0], k[1], k[2]);
+  if (!cell_valid(w, n)) return 0;
+  return in_domain(B(n)->type[n.o]);
+}
+
+/* Algorithms_Solve_Pressure::Divergence_Projection (src/Algorithms_Solve_Pressure.h:168-222)
+ * on speed buffer ib with an already assembled system. */
+static void project_with(world_t* w, const csr_t* A, int ib) {
+  int64_t n = A->n;
+  double* b = (double*)malloc(8 * (n + 1));
+  double* x = (double*)malloc(8 * (n + 1));
+  for (int64_t r = 0; r < n; ++r) {
+    int k[3];
+    key_of(w, A->bi[r], A->o[r], k);
+    b[r] = divergence(w, ib, k);
+  }
+  solve(w, A, b, x);
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* br = w->b[bi];
+      if (!br->exists[o]) continue;
+      br->p[o] = in_domain(br->type[o]) ? x[br->id[o]] : 0.0;
+    }
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* br = w->b[bi];
+      if (!br->exists[o]) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      for (int i = 0; i < 3; ++i)
+        if (correction_applies(w, bi, o, i)) {
+          /* Policy_Gradiant::Get_Gradiant(neigh, i) (src/Policy_Gradiant.h:32-37) */
+          double g = br->p[o] * w->ih[i];
+          g -= rd_p(w, k, -(i == 0), -(i == 1), -(i == 2)) * w->ih[i];
+          set_u(br, br->u[ib][i], o, i, br->u[ib][i][o] - g, 0);
+        }
+    }
+  w->max_div = 0;
+  for (int64_t r = 0; r < n; ++r) {
+    int k[3];
+    key_of(w, A->bi[r], A->o[r], k);
+    double d = fabs(divergence(w, ib, k));
+    if (d > w->max_div) w->max_div = d;
+  }
+  free(b); free(x);
+}
+
+/* src/Algorithms_RungeKutta_RK2_TVD.h:20-66 with Policy = Algorithms<Gravity,
+ * Convection> + Algorithms_Solve_Pressure. */
+static void alg_rk2(world_t* w) {
+  csr_t A;
+  assemble(w, &A);
+  double dt = w->hdr.dt;
+  acc_zero(w);
+  alg_gravity(w, 0);
+  alg_convection(w, 0);
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      if (!b->exists[o]) continue;
+      for (int i = 0; i < 3; ++i) b->u[1][i][o] = b->u[0][i][o] + b->acc[i][o] * dt;
+    }
+  acc_zero(w);
+  project_with(w, &A, 1);
+  alg_gravity(w, 1);
+  alg_convection(w, 1);
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      if (!b->exists[o]) continue;
+      for (int i = 0; i < 3; ++i) {
+        double v = 0.5 * b->u[0][i][o] + 0.5 * b->u[1][i][o] + 0.5 * b->acc[i][o] * dt;
+        set_u(b, b->u[0][i], o, i, v, 0);
+      }
+    }
+  project_with(w, &A, 0);
+  csr_free(&A);
+}
+
+/* Algorithms_Do_Pressure::Do (src/Algorithms_Do_Pressure.h:16-21) on speed 0. */
+static void alg_project(world_t* w) {
+  csr_t A;
+  assemble(w, &A);
+  project_with(w, &A, 0);
+  csr_free(&A);
+}
+
+/* ---------------------------------------------------------- extrapolation */
+static int lay_of(world_t* w, int x, int y, int z, int* valid) {
+  cell_t c = cell_at(w, x, y, z);
+  *valid = cell_valid(w, c) && B(c)->layer[c.o] != -1;
+  return *valid ? B(c)->layer[c.o] : -1;
+}
+
+/* Algorithms_Extrapolate::Do (src/Algorithms_Extrapolate.h:25-233): level by
+ * level, each face between a layer-lay cell and a cell of layer >= lay (or a
+ * missing one on the minus side) gets the mean of the parallel or collinear
+ * faces that touch a lower layer. n == 0 yields 0/0 as in the reference. */
+static void alg_extrapolate(world_t* w) {
+  keylist set = {0}, set2 = {0};
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) {
+      brick_t* b = w->b[bi];
+      if (b->exists[o]) b->mark[o] = 0;
+      if (b->exists[o] && b->layer[o] == 1) {
+        int k[3];
+        key_of(w, bi, o, k);
+        kl_push(&set, k);
+      }
+    }
+  int lay = 1;
+  int gen = 1;
+  while (1) {
+    ++gen;
+    for (int64_t q = 0; q < set.n; ++q) {
+      int* K = set.k + 3 * q;
+      for (int i = 0; i < 3; ++i) {
+        int e[3] = {i == 0, i == 1, i == 2};
+        int v2, v3, v4;
+        /* +1 direction: face u_i(neigh2) with neigh2 = K + e_i */
+        int l2 = lay_of(w, K[0] + e[0], K[1] + e[1], K[2] + e[2], &v2);
+        if (v2 && l2 >= lay) {
+          if (l2 > lay) {
+            cell_t c2 = cell_at(w, K[0] + e[0], K[1] + e[1], K[2] + e[2]);
+            if (B(c2)->mark[c2.o] != gen) {
+              B(c2)->mark[c2.o] = gen;
+              int kk[3] = {K[0] + e[0], K[1] + e[1], K[2] + e[2]};
+              kl_push(&set2, kk);
+            }
+          }
+          int n = 0;
+          double val = 0;
+          for (int j = 0; j < 3; ++j) {
+            int f[3] = {j == 0, j == 1, j == 2};
+            for (int s2 = -1; s2 <= 1; s2 += 2) {
+              if (s2 == -1 && j == i) {
+                int l3 = lay_of(w, K[0] - e[0], K[1] - e[1], K[2] - e[2], &v3);
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, i, K, 0, 0, 0); }
+              } else if (s2 == 1 && j == i) {
+                int l3 = lay_of(w, K[0] + 2 * e[0], K[1] + 2 * e[1], K[2] + 2 * e[2], &v3);
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, i, K, 2 * e[0], 2 * e[1], 2 * e[2]); }
+              } else {
+                int d3[3] = {e[0] + s2 * f[0], e[1] + s2 * f[1], e[2] + s2 * f[2]};
+                int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
+                int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
+                int l4 = lay_of(w, K[0] + d4[0], K[1] + d4[1], K[2] + d4[2], &v4);
+                if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d3[0], d3[1], d3[2]); }
+              }
+            }
+          }
+          cell_t c2 = cell_at(w, K[0] + e[0], K[1] + e[1], K[2] + e[2]);
+          set_u(B(c2), B(c2)->u[0][i], c2.o, i, val / n, 0);
+        }
+        /* -1 direction: face u_i(neigh) with neigh2 = K - e_i */
+        l2 = lay_of(w, K[0] - e[0], K[1] - e[1], K[2] - e[2], &v2);
+        cell_t c = cell_at(w, K[0], K[1], K[2]);
+        if (v2) {
+          if (l2 >= lay) {
+            if (l2 > lay) {
+              cell_t c2 = cell_at(w, K[0] - e[0], K[1] - e[1], K[2] - e[2]);
+              if (B(c2)->mark[c2.o] != gen) {
+                B(c2)->mark[c2.o] = gen;
+                int kk[3] = {K[0] - e[0], K[1] - e[1], K[2] - e[2]};
+                kl_push(&set2, kk);
+              }
+            }
+            int n = 0;
+            double val = 0;
+            for (int j = 0; j < 3; ++j) {
+              int f[3] = {j == 0, j == 1, j == 2};
+              for (int s2 = -1; s2 <= 1; s2 += 2) {
+                if (s2 == 1 && j == i) {
+                  int l3 = lay_of(w, K[0] + f[0], K[1] + f[1], K[2] + f[2], &v3);
+                  if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, f[0], f[1], f[2]); }
+                } else if (s2 == -1 && j == i) {
+                  int l3 = lay_of(w, K[0] - 2 * f[0], K[1] - 2 * f[1], K[2] - 2 * f[2], &v3);
+                  if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, -f[0], -f[1], -f[2]); }
+                } else {
+                  int d3[3] = {-e[0] + s2 * f[0], -e[1] + s2 * f[1], -e[2] + s2 * f[2]};
+                  int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
+                  int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
+                  int l4 = lay_of(w, K[0] + d4[0], K[1] + d4[1], K[2] + d4[2], &v4);
+                  if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d4[0], d4[1], d4[2]); }
+                }
+              }
+            }
+            set_u(B(c), B(c)->u[0][i], c.o, i, val / n, 0);
+          }
+        } else {
+          int n = 0;
+          double val = 0;
+          for (int j = 0; j < 3; ++j) {
+            int f[3] = {j == 0, j == 1, j == 2};
+            for (int s2 = -1; s2 <= 1; s2 += 2) {
+              if (s2 == 1 && j == i) {
+                int l3 = lay_of(w, K[0] + f[0], K[1] + f[1], K[2] + f[2], &v3);
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, f[0], f[1], f[2]); }
+              } else if (s2 == -1 && j == i) {
+              } else {
+                int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
+                int l4 = lay_of(w, K[0] + d4[0], K[1] + d4[1], K[2] + d4[2], &v4);
+                if (v4) {
+                  int d3[3] = {d4[0] - e[0], d4[1] - e[1], d4[2] - e[2]};
+                  int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
+                  if (v3 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d4[0], d4[1], d4[2]); }
+                }
+              }
+            }
+          }
+          set_u(B(c), B(c)->u[0][i], c.o, i, val / n, 0);
+        }
+      }
+    }
+    keylist t = set; set = set2; set2 = t; set2.n = 0;
+    ++lay;
+    if (set.n == 0) break;
+  }
+  free(set.k); free(set2.k);
+}
+
+/* ------------------------------------------------------------- particles */
+/* Speed read through grid[key] semantics: the interpolation's m_grid[key]
+ * creates the base cell (src/Policy_Speed_Interpolation_Linear_Symmetric.h:115). */
+static double interp_rec(world_t* w, const double* d, int i, const int k[3], int comp, int sym) {
+  double w0, w1;
+  if (sym && i == comp) { w0 = 0.5 - d[i]; w1 = 0.5 + d[i]; }
+  else { w0 = 1 - d[i]; w1 = d[i]; }
+  int k1[3] = {k[0] + (i == 0), k[1] + (i == 1), k[2] + (i == 2)};
+  if (i < 2) return w0 * interp_rec(w, d, i + 1, k, comp, sym) + w1 * interp_rec(w, d, i + 1, k1, comp, sym);
+  return w0 * rd_u(w, 0, comp, k, 0, 0, 0) + w1 * rd_u(w, 0, comp, k1, 0, 0, 0);
+}
+
+/* Get_Speed of Policy_Speed_Interpolation_Linear_Symmetric
+ * (src/Policy_Speed_Interpolation_Linear_Symmetric.h:79-119) when sym != 0,
+ * of Policy_Speed_Interpolation_Linear (src/Policy_Speed_Interpolation_Linear.h:64-106)
+ * otherwise. */
+static void get_speed(world_t* w, const double pos[3], double out[3], int sym) {
+  double pd[3];
+  int k0[3];
+  for (int i = 0; i < 3; ++i) {
+    pd[i] = pos[i] * w->ih[i];
+    k0[i] = (int)lround(pd[i]);
+    pd[i] -= k0[i];
+  }
+  for (int k = 0; k < 3; ++k) {
+    if (!sym) pd[k] += 0.5;
+    int key[3];
+    double d2[3];
+    for (int j = 0; j < 3; ++j) {
+      if (j != k && pd[j] < 0) { key[j] = k0[j] - 1; d2[j] = 1 + pd[j]; }
+      else { key[j] = k0[j]; d2[j] = pd[j]; }
+    }
+    cell_get(w, key[0], key[1], key[2]);
+    out[k] = interp_rec(w, d2, 0, key, k, sym);
+    if (!sym) pd[k] -= 0.5;
+  }
+}
+
+/* Algorithms_Move_Particles::Do (src/Algorithms_Move_Particles.h:29-32) with
+ * Policy_Advance_Ode_RungeKutta::AdvanceSolveODE (src/Policy_Advance_ODE_RungeKutta.h:15-27). */
+static void alg_move(world_t* w, int sym) {
+  double dt = w->hdr.dt;
+  for (int64_t q = 0; q < w->np; ++q) {
+    double* pos = w->pos + 3 * q;
+    double res[3], k[3], a[3], v[3];
+    for (int i = 0; i < 3; ++i) res[i] = pos[i];
+    get_speed(w, pos, v, sym);
+    for (int i = 0; i < 3; ++i) { k[i] = dt * v[i]; res[i] += (1. / 6.) * k[i]; }
+    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
+    get_speed(w, a, v, sym);
+    for (int i = 0; i < 3; ++i) { k[i] = dt * v[i]; res[i] += (1. / 3.) * k[i]; }
+    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
+    get_speed(w, a, v, sym);
+    for (int i = 0; i < 3; ++i) { k[i] = dt * v[i]; res[i] += (1. / 3.) * k[i]; }
+    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i];
+    get_speed(w, a, v, sym);
+    for (int i = 0; i < 3; ++i) { k[i] = dt * v[i]; res[i] += (1. / 6.) * k[i]; }
+    for (int i = 0; i < 3; ++i) pos[i] = res[i];
+  }
+}
+
+/* ---------------------------------------------------------- setup passes */
+/* src/Algorithms_Solid_To_Const.h:32-58 */
+static void alg_solid_to_const(world_t* w) {
+  keylist s = {0};
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o)
+      if (w->b[bi]->exists[o] && w->b[bi]->type[o] == MAC_SOLID) {
+        int k[3];
+        key_of(w, bi, o, k);
+        kl_push(&s, k);
+      }
+  for (int64_t q = s.n - 1; q >= 0; --q) {
+    int* k = s.k + 3 * q;
+    cell_t c = cell_get(w, k[0], k[1], k[2]);
+    B(c)->flags[c.o] |= MAC_FLAG_NODELETE;
+    B(c)->p[c.o] = 0;
+    for (int i = 0; i < 3; ++i) {
+      c = cell_get(w, k[0], k[1], k[2]);
+      set_u(B(c), B(c)->u[0][i], c.o, i, 0.0, 0);
+      B(c)->flags[c.o] |= (uint8_t)(1u << i);
+      cell_t n = cell_get(w, k[0] + (i == 0), k[1] + (i == 1), k[2] + (i == 2));
+      B(n)->flags[n.o] |= MAC_FLAG_NODELETE;
+      for (int j = 0; j < 3; ++j) set_u(B(n), B(n)->u[0][j], n.o, j, 0.0, 0);
+      B(n)->p[n.o] = 0;
+      B(n)->flags[n.o] |= (uint8_t)(1u << i);
+    }
+  }
+  free(s.k);
+}
+
+/* src/Algorithms_Speed_Constant_Mirror.h:22-70 */
+static void alg_mirror(world_t* w) {
+  keylist s = {0};
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o)
+      if (w->b[bi]->exists[o] && (w->b[bi]->flags[o] & 7)) {
+        int k[3];
+        key_of(w, bi, o, k);
+        kl_push(&s, k);
+      }
+  for (int64_t q = 0; q < s.n; ++q) {
+    int* k = s.k + 3 * q;
+    for (int i = 0; i < 3; ++i) {
+      cell_t n = cell_get(w, k[0] + (i == 0), k[1] + (i == 1), k[2] + (i == 2));
+      for (int j = 0; j < 3; ++j) set_u(B(n), B(n)->u[0][j], n.o, j, 0.0, 0);
+    }
+  }
+  for (int64_t q = 0; q < s.n; ++q) {
+    int* k = s.k + 3 * q;
+    for (int i = 0; i < 3; ++i) {
+      cell_t n = cell_get(w, k[0] + (i == 0), k[1] + (i == 1), k[2] + (i == 2));
+      cell_t c = cell_get(w, k[0], k[1], k[2]);
+      if ((B(c)->flags[c.o] >> i) & 1) set_u(B(n), B(n)->u[0][i], n.o, i, B(c)->u[0][i][c.o], 0);
+    }
+  }
+  free(s.k);
+}
+
+/* --------------------------------------------------------------- driver */
+static world_t* world_from_file(const mac_state_file* st) {
+  world_t* w = (world_t*)calloc(1, sizeof(world_t));
+  w->hdr = st->hdr;
+  for (int i = 0; i < 3; ++i) { w->h[i] = st->hdr.h[i]; w->ih[i] = 1 / st->hdr.h[i]; }
+  w->seed = st->hdr.step;
+  hash_rebuild(w);
+  for (int64_t c = 0; c < st->hdr.nchunks; ++c) {
+    int64_t bi = brick_create(w, st->keys[3 * c], st->keys[3 * c + 1], st->keys[3 * c + 2]);
+    brick_t* b = w->b[bi];
+    size_t base = (size_t)c * 512;
+    memcpy(b->exists, st->exists + base, 512);
+    for (int k = 0; k < 2; ++k)
+      for (int i = 0; i < 3; ++i) memcpy(b->u[k][i], st->u[k][i] + base, 512 * 8);
+    for (int i = 0; i < 3; ++i) memcpy(b->acc[i], st->acc[i] + base, 512 * 8);
+    memcpy(b->p, st->p + base, 512 * 8);
+    memcpy(b->flags, st->flags + base, 512);
+    memcpy(b->type, st->type + base, 512);
+    memcpy(b->layer, st->layer + base, 512 * 4);
+    memcpy(b->id, st->id + base, 512 * 4);
+  }
+  for (int64_t q = 0; q < st->hdr.nparticles; ++q) add_particle(w, st->pos + 3 * q);
+  return w;
+}
+
+static int cmp_keys(const void* a, const void* b) {
+  const brick_t* x = *(brick_t* const*)a;
+  const brick_t* y = *(brick_t* const*)b;
+  for (int i = 2; i >= 0; --i)
+    if (x->key[i] != y->key[i]) return x->key[i] < y->key[i] ? -1 : 1;
+  return 0;
+}
+
+static void world_to_file(world_t* w, mac_state_file* st) {
+  qsort(w->b, (size_t)w->nb, sizeof(brick_t*), cmp_keys);
+  hash_rebuild(w);
+  mac_state_alloc(st, w->nb, w->np);
+  st->hdr = w->hdr;
+  st->hdr.nchunks = w->nb;
+  st->hdr.nparticles = w->np;
+  st->hdr.step = w->seed;
+  for (int64_t c = 0; c < w->nb; ++c) {
+    brick_t* b = w->b[c];
+    size_t base = (size_t)c * 512;
+    memcpy(st->keys + 3 * c, b->key, 12);
+    memcpy(st->exists + base, b->exists, 512);
+    for (int k = 0; k < 2; ++k)
+      for (int i = 0; i < 3; ++i) memcpy(st->u[k][i] + base, b->u[k][i], 512 * 8);
+    for (int i = 0; i < 3; ++i) memcpy(st->acc[i] + base, b->acc[i], 512 * 8);
+    memcpy(st->p + base, b->p, 512 * 8);
+    memcpy(st->flags + base, b->flags, 512);
+    memcpy(st->type + base, b->type, 512);
+    memcpy(st->layer + base, b->layer, 512 * 4);
+    memcpy(st->id + base, b->id, 512 * 4);
+  }
+  memcpy(st->pos, w->pos, (size_t)w->np * 24);
+}
+
+static void world_free(world_t* w) {
+  for (int64_t i = 0; i < w->nb; ++i) free(w->b[i]);
+  free(w->b); free(w->hkeys); free(w->hval); free(w->pos); free(w);
+}
+
+static int64_t fluid_count(world_t* w) {
+  int64_t n = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) n += w->b[bi]->exists[o] && is_fluid(w->b[bi]->type[o]);
+  return n;
+}
+
+static void topology(world_t* w) {
+  alg_initialize(w);
+  alg_layer_initial(w);
+  alg_create_fluid(w);
+  alg_update_layer(w);
+  alg_delete(w);
+  alg_dt(w);
+}
+
+/* One named stage (same names as oracle/_ref/mac_ref) n times. Returns 0 on
+ * success; stats[] receives invalid reads, created cells, CG iterations, the
+ * last relative residual, the max |div| after the last projection and the
+ * accumulated fluid cell-steps. */
+int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, int n, double rtol,
+                   double* stats) {
+  mac_state_file st;
+  if (mac_state_read(in_path, &st) != 0) return -1;
+  world_t* w = world_from_file(&st);
+  mac_state_free(&st);
+  if (rtol > 0) g_rtol = rtol;
+  int64_t fcs = 0;
+  int sym = w->hdr.interp_symmetric != 0;
+  for (int r = 0; r < n; ++r) {
+    if (!strcmp(cmd, "firstinit")) {
+      alg_solid_to_const(w);
+      alg_mirror(w);
+      alg_initialize(w);
+      alg_create_fluid(w);
+      alg_layer_initial(w);
+      alg_update_layer(w);
+      alg_delete(w);
+      alg_extrapolate(w);
+    } else if (!strcmp(cmd, "step") || !strcmp(cmd, "bench")) {
+      ++w->seed;
+      topology(w);
+      alg_rk2(w);
+      alg_extrapolate(w);
+      alg_move(w, sym);
+      w->hdr.t += w->hdr.dt;
+      fcs += fluid_count(w);
+    } else if (!strcmp(cmd, "topology")) {
+      ++w->seed;
+      topology(w);
+    } else if (!strcmp(cmd, "forces")) {
+      acc_zero(w);
+      alg_gravity(w, 0);
+      alg_convection(w, 0);
+    } else if (!strcmp(cmd, "ode")) {
+      alg_rk2(w);
+    } else if (!strcmp(cmd, "project")) {
+      alg_project(w);
+    } else if (!strcmp(cmd, "extrapolate")) {
+      alg_extrapolate(w);
+    } else if (!strcmp(cmd, "move")) {
+      alg_move(w, 1);
+    } else if (!strcmp(cmd, "movelin")) {
+      alg_move(w, 0);
+    } else {
+      world_free(w);
+      return -2;
+    }
+  }
+  if (stats) {
+    stats[0] = (double)w->invalid_reads;
+    stats[1] = (double)w->created_cells;
+    stats[2] = (double)w->cg_iters;
+    stats[3] = w->last_relres;
+    stats[4] = w->max_div;
+    stats[5] = (double)fcs;
+  }
+  int rc = 0;
+  if (out_path && out_path[0]) {
+    world_to_file(w, &st);
+    rc = mac_state_write(out_path, &st);
+    mac_state_free(&st);
+  }
+  world_free(w);
+  return rc;
+}
+
+/* The jitter function, exported so the tests can compare it with the device's. */
+void mac_oracle_jitter8(uint64_t seed, int kx, int ky, int kz, int s, double hx, double hy,
+                        double hz, double* out) {
+  mac_jitter8_position(seed, kx, ky, kz, s, hx, hy, hz, out);
+}

@@ -1,0 +1,80 @@
+"""Python access to the checkers (test infrastructure only).
+
+* ``run_oracle`` drives the C restatement (``libmac_oracle.so``).
+* ``run_ref`` drives the reference's own code compiled from its headers
+  (``_ref/mac_ref``), when that binary was built.
+
+Both exchange states through the file format of ``state_format.h``.
+Only the tests, the smoke check and bench.py's CPU-baseline leg use this.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libmac_oracle.so")
+REF = os.path.join(HERE, "_ref", "mac_ref")
+
+_lib = None
+
+
+def build(quiet: bool = True) -> None:
+    """Builds the restatement (and the reference runner when the reference
+    sources are present)."""
+    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+        _lib.mac_oracle_run.restype = ctypes.c_int
+        _lib.mac_oracle_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                        ctypes.c_int, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_double)]
+        _lib.mac_oracle_jitter8.restype = None
+        _lib.mac_oracle_jitter8.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double,
+                                            ctypes.POINTER(ctypes.c_double)]
+    return _lib
+
+
+def run_oracle(cmd: str, in_path: str, out_path: str, n: int = 1, rtol: float = 1e-14) -> dict:
+    """Runs stage ``cmd`` ``n`` times on the state in ``in_path``."""
+    stats = (ctypes.c_double * 8)()
+    rc = lib().mac_oracle_run(in_path.encode(), (out_path or "").encode(), cmd.encode(), n, rtol,
+                              stats)
+    if rc != 0:
+        raise RuntimeError(f"oracle {cmd} failed ({rc})")
+    return {"invalid_reads": stats[0], "created_cells": stats[1], "cg_iters": stats[2],
+            "relres": stats[3], "max_div": stats[4], "fluid_cell_steps": stats[5]}
+
+
+def jitter8(seed, k, s, h):
+    out = (ctypes.c_double * 3)()
+    lib().mac_oracle_jitter8(seed, int(k[0]), int(k[1]), int(k[2]), int(s), h[0], h[1], h[2], out)
+    return [out[0], out[1], out[2]]
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF)
+
+
+def run_ref(cmd: str, in_path: str, out_path: str, arg=None, timeout: float = 600.0) -> str:
+    """Runs the reference's own code on a state (``cmd`` as in ``ref_world.cpp``)."""
+    args = [REF, cmd, in_path, out_path]
+    if arg is not None:
+        args.append(str(arg))
+    out = subprocess.run(args, capture_output=True, text=True, timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"mac_ref {cmd} failed: {out.stderr}")
+    return out.stdout
