@@ -1,0 +1,163 @@
+/* C-ABI of the B200 implementation of Mac's per-timestep fluid hot path.
+ *
+ * Plain C types only: a host program (or the C++ policy wrappers in
+ * include/mac_gpu/) hands the world over through mac_host_state, runs the
+ * reference's algorithms on the device, and reads the world back. Each entry
+ * point replaces one reference algorithm or policy; the comment above it names
+ * the reference interface (file:line, relative to the reference repository).
+ *
+ * Every function returns MAC_OK (0) or a negative MAC_ERR_* status; nothing
+ * aborts. A context owns one CUDA stream and its device memory; calls on one
+ * context must not overlap (not thread-safe per context).
+ */
+#ifndef MAC_GPU_H
+#define MAC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MAC_OK = 0,
+  MAC_ERR_INVALID = -1,       /* bad argument or state */
+  MAC_ERR_CUDA = -2,          /* a CUDA call failed */
+  MAC_ERR_CAPACITY = -3,      /* brick pool, particle array or hash table full */
+  MAC_ERR_NOT_CONVERGED = -4, /* iterative solve hit max_iters */
+  MAC_ERR_NO_DEVICE = -5,     /* no CUDA device */
+  MAC_ERR_OUT_OF_MEMORY = -6,
+  MAC_ERR_TIMEOUT = -7
+};
+
+/* Pressure solver of the projection. */
+enum {
+  MAC_SOLVER_MGPCG_FP64 = 0,  /* plain form: FP64 multigrid-preconditioned CG */
+  MAC_SOLVER_MGPCG_MIXED = 1, /* FP32 multigrid inside FP64 CG */
+  MAC_SOLVER_CG_FP64 = 2      /* Jacobi-preconditioned CG (reference for the others) */
+};
+
+/* Cell materials, as Data_CellType_Fluid_Air_Solid_Inflow::MaterialToInt
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:3-18). */
+enum { MAC_CELL_AIR = 0, MAC_CELL_FLUID = 1, MAC_CELL_SOLID = 2, MAC_CELL_INFLOW = 3 };
+/* Per-cell flag bits: const faces x/y/z (src/Data_Grid_Speed.h:54-59) and the
+ * no-delete mark (src/Data_CellType_Fluid_Air_Solid_Inflow.h:331-338). */
+enum { MAC_FLAG_CONST_X = 1, MAC_FLAG_CONST_Y = 2, MAC_FLAG_CONST_Z = 4, MAC_FLAG_NODELETE = 8 };
+
+#define MAC_BRICK_EDGE 8
+#define MAC_BRICK_CELLS 512
+
+typedef struct {
+  double h[3];          /* cell spacing (Data_Grid_Base_Spacing::m_h) */
+  double cfl_factor;    /* Data_Timing_Time::m_factor */
+  double dt_min, dt_max;/* Policy_CheckDT(min, max) */
+  double gravity;       /* Policy_Gravity(g, axis) */
+  int32_t gravity_axis; /* 1..3 */
+  int32_t layer_max;    /* Policy_Layer_Max */
+  int32_t interp_symmetric; /* 1: Policy_Speed_Interpolation_Linear_Symmetric, 0: _Linear */
+  int32_t solver;       /* MAC_SOLVER_* */
+  double rtol;          /* relative residual target of the projection solve */
+  int32_t max_iters;
+  int32_t warm_start;   /* 1: start the solve from the last pressure */
+  int64_t max_bricks;   /* device brick pool capacity (8^3 cells each) */
+  int64_t max_particles;
+  int32_t device;
+  int32_t div_check;    /* 1: compute max |div| after each projection */
+} mac_params;
+
+/* Host view of a world, arrays owned by the caller. Brick b holds cells
+ * key = 8*keys[b] + (x, y, z), slot x + 8y + 64z (src/Offset.h:14-24). All 512
+ * slots of a live brick are carried, existing or not: the reference keeps the
+ * data of erased cells of a live chunk (src/ChunkHashTable.tpp:62-87,132-147). */
+typedef struct {
+  int64_t nbricks, nparticles;
+  int32_t* keys;        /* [nbricks][3] */
+  uint8_t* exists;      /* [nbricks*512] */
+  double* u[2][3];      /* two speed buffers (src/Data_Chunk_Speed.h:13) */
+  double* acc[3];       /* acceleration buffer */
+  double* p;            /* pressure */
+  uint8_t* flags;       /* MAC_FLAG_* */
+  uint8_t* type;        /* MAC_CELL_* */
+  int32_t* layer;       /* -1 empty */
+  double* pos;          /* [nparticles][3] */
+  double t, dt;
+  uint64_t step;        /* refill seed counter */
+} mac_host_state;
+
+typedef struct {
+  int32_t iterations;   /* CG iterations of the last solve */
+  int32_t solves;
+  double relres;        /* final relative residual of the last solve */
+  double max_div;       /* max |div u| over domain cells after the last projection */
+  int64_t fluid_cells;  /* fluid + inflow cells after the last topology rebuild */
+  int64_t unknowns;     /* in-domain cells of the last system */
+  int64_t live_bricks;
+  int64_t particles;
+  int64_t total_iterations; /* accumulated over the context's life */
+} mac_stats;
+
+/* ---- context ---- */
+void mac_default_params(mac_params* p);
+int mac_ctx_create(const mac_params* p, void** ctx);
+int mac_ctx_destroy(void* ctx);
+int mac_get_stats(void* ctx, mac_stats* out);
+const char* mac_error_string(int code);
+
+/* ---- state transfer (host <-> device), cf. the chunk grid src/ChunkHashTable.h:22-160 ---- */
+int mac_upload_state(void* ctx, const mac_host_state* s);
+int mac_query_sizes(void* ctx, int64_t* nbricks, int64_t* nparticles);
+int mac_download_state(void* ctx, mac_host_state* s);
+
+/* ---- topology rebuild: Algorithms<Initialize_MacCell, Layer_Initial_With_Particle,
+ *      Create_Fluid_Particle, Update_CellType_Layer, Delete_MacCell, Calculate_Time_Step>
+ *      (test/TestJetDEau_Basic.cpp:325-326) ---- */
+/* src/Algorithms_Initialize_MacCell.h:15-21 */
+int mac_initialize_maccell(void* ctx);
+/* src/Algorithms_Layer_Initial_With_Particle.h:20-34 + Policy_Particle_To_Key (src/Policy_Particle_To_Key.h:24-35) */
+int mac_layer_initial_with_particle(void* ctx);
+/* src/Algorithms_Create_Fluid_Particle.h:19-33 (8 jittered particles per refilled inflow cell) */
+int mac_create_fluid_particle(void* ctx);
+/* src/Algorithms_Update_CellType_Layer.h:22-89 */
+int mac_update_celltype_layer(void* ctx);
+/* src/Algorithms_Delete_MacCell.h:22-44 */
+int mac_delete_maccell(void* ctx);
+/* src/Algorithms_Calculate_Time_Step.h:35-66 + Policy_CheckDT (src/Policy_CheckDT.h:16-29) */
+int mac_calculate_time_step(void* ctx, double* dt);
+/* The whole init sequence above, in the reference's order. Increments the refill seed first. */
+int mac_topology_rebuild(void* ctx);
+
+/* ---- advection and projection ---- */
+/* acc = 0; Algorithms_Gravity + Algorithms_Convection with Policy_Upwind_1_Order on speed buffer
+ * ispeed (src/Algorithms_Gravity.h:15-28, src/Algorithms_Convection.h:18-37) */
+int mac_forces(void* ctx, int ispeed);
+/* Algorithms_Do_Pressure::Do on speed buffer ispeed: Init_Iteration + Divergence_Projection +
+ * End_Iteration of Algorithms_Solve_Pressure (src/Algorithms_Do_Pressure.h:16-21,
+ * src/Algorithms_Solve_Pressure.h:44-222) */
+int mac_pressure_project(void* ctx, int ispeed);
+/* Algorithms_RungeKutta_RK2_TVD::Do with Policy = Algorithms<Gravity, Convection> +
+ * Algorithms_Solve_Pressure (src/Algorithms_RungeKutta_RK2_TVD.h:20-66) */
+int mac_rk2tvd(void* ctx);
+/* src/Algorithms_Extrapolate.h:25-233 */
+int mac_extrapolate(void* ctx);
+/* Algorithms_Move_Particles + Policy_Advance_Ode_RungeKutta + Get_Speed
+ * (src/Algorithms_Move_Particles.h:22-36, src/Policy_Advance_ODE_RungeKutta.h:14-27,
+ * src/Policy_Speed_Interpolation_Linear_Symmetric.h:79-119 or src/Policy_Speed_Interpolation_Linear.h:64-106) */
+int mac_move_particles(void* ctx);
+/* One full step of test/TestJetDEau_Basic.cpp:434-441: topology rebuild, RK2-TVD,
+ * extrapolation, particle move, t += dt. */
+int mac_step(void* ctx);
+/* Synchronises the context's stream. */
+int mac_sync(void* ctx);
+
+/* ---- drop-in linear solver: the Policy_Solve_Linear_Umfpack member functions
+ * (src/Policy_Solve_Linear_Umfpack.h:28-70) over the CSC arrays the reference assembles
+ * in Algorithms_Solve_Pressure::Init_Iteration (src/Algorithms_Solve_Pressure.h:52-152).
+ * The matrix is symmetric and negative definite; solved by FP64 Jacobi-PCG on the device. ---- */
+int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value);
+int mac_csc_solve(void* ctx, int n, const double* b, double* x);
+int mac_csc_clean(void* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,224 @@
+// Device-side data model of the brick grid and the context shared by the kernels.
+//
+// The reference's sparse chunk grid (src/ChunkHashTable.h:22-160: an
+// unordered_map from chunk key to an 8^3 chunk of SoA arrays with an existence
+// bitset) becomes:
+//   * a pool of bricks; brick b owns cells [b*512, b*512+512), slot x+8y+64z,
+//   * an open-addressing hash table from packed brick key to pool index,
+//     rebuilt after every topology pass,
+//   * a compact list of live bricks and a free list,
+//   * a 27-entry neighbour table per live brick (the reference links chunks to
+//     their 2*DIM neighbours: src/Hook_Neighbour_List_key.h:97-120).
+// Per-cell fields are SoA arrays over the pool. Existence and layer share one
+// signed byte `lay`: -2 = cell does not exist, -1 = exists with an empty layer,
+// >= 0 = layer. The reference keeps a separate bit and leaves the layer of an
+// erased cell stale; that stale layer is never read before it is rewritten
+// (every re-creation path sets the layer), so folding the two is exact and lets
+// one byte store publish both at once.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mac_gpu.h"
+
+namespace mac {
+
+constexpr int kBrick = 8;
+constexpr int kCells = 512;
+constexpr int kNbr = 27;
+constexpr int kSelf = 13;
+constexpr int8_t kMissing = -2;
+constexpr int8_t kEmpty = -1;
+constexpr uint64_t kEmptyKey = ~0ull;
+constexpr int32_t kPending = -2;
+constexpr int kLevels = 4;  // brick-local multigrid levels: 8^3, 4^3, 2^3, 1 cell per brick
+
+enum ErrBits : int {
+  kErrBricks = 1,
+  kErrParticles = 2,
+  kErrHash = 4,
+  kErrPending = 8,
+};
+
+// Field indices of the FP64 per-cell block.
+enum F64 : int { U0X = 0, U0Y, U0Z, U1X, U1Y, U1Z, AX, AY, AZ, PRES, NF64 };
+
+struct Scalars {
+  int32_t nlive;
+  int32_t nlive_new;
+  int32_t nfree;
+  int32_t nnew;       // newly inserted hash slots waiting for a brick
+  int32_t npending;   // particles waiting for their brick
+  int32_t err;
+  int64_t np;
+  double dt;
+  double t;
+  unsigned long long cfl_bits;  // max over fluid cells of sum (u_i/h_i)^2, as ordered bits
+  unsigned long long div_bits;  // max |div| after a projection, as ordered bits
+  int64_t nfluid;
+  int64_t nunknown;
+  // CG scalars
+  double rz, rz_new, pq, rr, bnorm2, alpha, beta;
+  int32_t done;
+  int32_t iters;
+  int32_t bbox[6];    // brick key bounds of the live set (min xyz, max xyz)
+  unsigned long long bad_reads;  // particles whose stencil touched a missing cell
+};
+
+struct Params {
+  double h[3], ih[3], ih2[3];
+  double cfl, dt_min, dt_max, g;
+  int gaxis;     // 0..2
+  int layer_max;
+  int interp_sym;
+};
+
+struct Ctx {
+  mac_params prm;
+  Params dp;
+  cudaStream_t stream = nullptr;
+  int64_t cap_bricks = 0, cap_particles = 0, hcap = 0, cap_pending = 0;
+  uint64_t seed = 0;
+  int own_device = 0;
+
+  // brick pool
+  int* bkey = nullptr;        // [cap][3]
+  int8_t* lay = nullptr;      // [cap*512]
+  uint8_t* type = nullptr;    // [cap*512]
+  uint8_t* flags = nullptr;   // [cap*512]
+  double* f64 = nullptr;      // [NF64][cap*512]
+  int* nbr = nullptr;         // [cap][27]
+  int* blist = nullptr;       // live bricks (current)
+  int* blist2 = nullptr;      // scratch for compaction
+  int* freelist = nullptr;
+  uint8_t* alive = nullptr;   // [cap] per-brick flag
+  // hash
+  unsigned long long* hkeys = nullptr;
+  int* hval = nullptr;
+  int* newslots = nullptr;    // [cap]
+  // particles (SoA)
+  double* px = nullptr;
+  double* py = nullptr;
+  double* pz = nullptr;
+  int64_t* pending = nullptr; // particle indices waiting for a brick
+  // pressure system and solver
+  uint16_t* fmask = nullptr;  // [cap*512] face classes of the level-0 operator
+  double* x = nullptr;        // solution (pressure in domain)
+  double* b = nullptr;        // right-hand side
+  double* r = nullptr;
+  double* z = nullptr;
+  double* pd = nullptr;       // search direction
+  double* q = nullptr;
+  double* partial = nullptr;  // per-block partial sums
+  int64_t npartial = 0;
+  // multigrid (T = double or float storage, chosen by the solver)
+  void* mg_e[kLevels] = {};   // correction
+  void* mg_e2[kLevels] = {};  // ping-pong
+  void* mg_r[kLevels] = {};   // level residual (levels >= 1)
+  void* mg_w[kLevels] = {};   // [4][cells]: left-face weights x,y,z and Dirichlet diagonal
+  void* mg_dinv[kLevels] = {};
+  int mg_float = 0;
+  // scalars
+  Scalars* ds = nullptr;      // device
+  Scalars* hs = nullptr;      // pinned host mirror
+  int nlive_host = 0;
+  int64_t np_host = 0;
+  mac_stats stats{};
+  bool system_ready = false;
+  // drop-in CSC solver
+  int csc_n = 0;
+  int* csc_off = nullptr;
+  int* csc_ind = nullptr;
+  double* csc_val = nullptr;
+  double* csc_vec = nullptr;   // [6][n]
+};
+
+// ---------------------------------------------------------------- helpers
+__host__ __device__ inline unsigned long long pack_key(int x, int y, int z) {
+  return ((unsigned long long)((uint32_t)(x + (1 << 20)) & 0x1FFFFFu)) |
+         ((unsigned long long)((uint32_t)(y + (1 << 20)) & 0x1FFFFFu) << 21) |
+         ((unsigned long long)((uint32_t)(z + (1 << 20)) & 0x1FFFFFu) << 42);
+}
+__host__ __device__ inline void unpack_key(unsigned long long k, int* x, int* y, int* z) {
+  *x = (int)(k & 0x1FFFFFu) - (1 << 20);
+  *y = (int)((k >> 21) & 0x1FFFFFu) - (1 << 20);
+  *z = (int)((k >> 42) & 0x1FFFFFu) - (1 << 20);
+}
+__host__ __device__ inline unsigned long long hmix(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return k;
+}
+// Floor division by the brick edge (src/ChunkHashTable.tpp:180-196).
+__host__ __device__ inline int fdiv8(int v) { return v >= 0 ? v >> 3 : -((-v + 7) >> 3); }
+
+__device__ inline int hash_find(const unsigned long long* __restrict__ hk, const int* __restrict__ hv,
+                                int64_t hcap, unsigned long long key) {
+  unsigned long long s = hmix(key) & (unsigned long long)(hcap - 1);
+  for (int64_t probe = 0; probe < hcap; ++probe) {
+    unsigned long long k = hk[s];
+    if (k == key) return hv[s];
+    if (k == kEmptyKey) return -1;
+    s = (s + 1) & (unsigned long long)(hcap - 1);
+  }
+  return -1;
+}
+
+// Neighbour table index of brick offset (dx,dy,dz) in {-1,0,1}^3.
+__host__ __device__ inline int nbr_index(int dx, int dy, int dz) { return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1); }
+
+// Cell (brick, slot) of the cell at local coordinates (x,y,z) of brick `b`
+// where the coordinates may leave [0,D) by at most D (one brick). Returns -1
+// brick when the neighbour brick is not live.
+template <int D>
+__device__ inline int nb_brick(const int* __restrict__ nbr, int b, int x, int y, int z) {
+  int dx = x < 0 ? -1 : (x >= D ? 1 : 0);
+  int dy = y < 0 ? -1 : (y >= D ? 1 : 0);
+  int dz = z < 0 ? -1 : (z >= D ? 1 : 0);
+  if ((dx | dy | dz) == 0) return b;
+  return nbr[(size_t)b * kNbr + nbr_index(dx, dy, dz)];
+}
+template <int D>
+__device__ inline int wrap(int v) { return v < 0 ? v + D : (v >= D ? v - D : v); }
+template <int D>
+__device__ inline int slot(int x, int y, int z) { return x + D * y + D * D * z; }
+
+__device__ inline bool is_fluid(uint8_t t) { return t == MAC_CELL_FLUID || t == MAC_CELL_INFLOW; }
+
+// Ordered-bits max for non-negative doubles.
+__device__ inline void atomic_max_nonneg(unsigned long long* a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+inline int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// ------------------------------------------------------------- launchers
+// Implemented in the .cu files; all enqueue on ctx->stream.
+int check(cudaError_t e);
+int topology_rebuild(Ctx* c, bool first_init_order);
+int topo_initialize(Ctx* c);
+int topo_layer_initial(Ctx* c);
+int topo_create_fluid(Ctx* c);
+int topo_update_layer(Ctx* c);
+int topo_delete(Ctx* c);
+int topo_dt(Ctx* c);
+int topo_finish(Ctx* c);
+int rebuild_index(Ctx* c);
+int read_scalars(Ctx* c);
+int forces(Ctx* c, int ib);
+int rk2tvd(Ctx* c);
+int project(Ctx* c, int ib);
+int setup_system(Ctx* c);
+int extrapolate(Ctx* c);
+int move_particles(Ctx* c);
+int alloc_solver(Ctx* c);
+void free_solver(Ctx* c);
+
+}  // namespace mac

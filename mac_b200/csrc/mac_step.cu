@@ -1,0 +1,281 @@
+// Step orchestration and the stage entry points of the C-ABI, plus the
+// drop-in CSC linear solver (the Policy_Solve_Linear_* member functions).
+#include <cmath>
+#include <cstring>
+
+#include "mac_internal.cuh"
+
+namespace mac {
+
+int rk_stage(Ctx* c, int stage);
+
+// Algorithms_RungeKutta_RK2_TVD::Do (src/Algorithms_RungeKutta_RK2_TVD.h:20-66):
+// Init_Iteration (system set-up) once, stage 1 into speed 1, projection of
+// speed 1, stage 2 back into speed 0, projection of speed 0.
+int rk2tvd(Ctx* c) {
+  int rc = setup_system(c);
+  if (rc) return rc;
+  if ((rc = rk_stage(c, 1))) return rc;
+  int s1 = project(c, 1);
+  if (s1 && s1 != MAC_ERR_NOT_CONVERGED) return s1;
+  if ((rc = rk_stage(c, 2))) return rc;
+  int s2 = project(c, 0);
+  if (s2) return s2;
+  return s1;
+}
+
+__global__ void k_advance_time(Scalars* ds) { ds->t += ds->dt; }
+
+// One step of test/TestJetDEau_Basic.cpp:434-441.
+static int step(Ctx* c) {
+  int rc = topology_rebuild(c, false);
+  if (rc) return rc;
+  int ode = rk2tvd(c);
+  if (ode && ode != MAC_ERR_NOT_CONVERGED) return ode;
+  if ((rc = extrapolate(c))) return rc;
+  if ((rc = move_particles(c))) return rc;
+  k_advance_time<<<1, 1, 0, c->stream>>>(c->ds);
+  rc = check(cudaGetLastError());
+  return rc ? rc : ode;
+}
+
+// ------------------------------------------------------- drop-in CSC solver
+// The reference's assembled matrix is symmetric, so its CSC arrays read as CSR
+// rows: y_j = sum_k value[k] * x[indice[k]] over column j.
+__global__ void k_csc_spmv(int n, const int* __restrict__ off, const int* __restrict__ ind,
+                           const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                           double* partial_dot, const double* __restrict__ pdot) {
+  double acc = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int k = off[j]; k < off[j + 1]; ++k) s += val[k] * x[ind[k]];
+    s = -s;  // M = -A
+    y[j] = s;
+    acc += pdot[j] * s;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(partial_dot, acc);
+}
+
+__global__ void k_csc_diag(int n, const int* __restrict__ off, const int* __restrict__ ind,
+                           const double* __restrict__ val, double* dinv) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    double d = 0;
+    for (int k = off[j]; k < off[j + 1]; ++k)
+      if (ind[k] == j) d = -val[k];
+    dinv[j] = d != 0 ? 1.0 / d : 0.0;
+  }
+}
+
+// mode 0: r = -b, x = 0, z = dinv r, p = z, scal[0] += r.z, scal[1] += b.b
+// mode 1: x += a p, r -= a q, scal[2] += r.r
+// mode 2: z = dinv r, scal[0] += r.z
+// mode 3: p = z + beta p
+__global__ void k_csc_vec(int n, int mode, const double* b, double* x, double* r, double* z, double* p,
+                          const double* q, const double* dinv, double* scal, double a) {
+  double s0 = 0, s1 = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (mode == 0) {
+      double rv = -b[j];
+      r[j] = rv;
+      x[j] = 0;
+      double zv = dinv[j] * rv;
+      z[j] = zv;
+      p[j] = zv;
+      s0 += rv * zv;
+      s1 += b[j] * b[j];
+    } else if (mode == 1) {
+      x[j] += a * p[j];
+      double rv = r[j] - a * q[j];
+      r[j] = rv;
+      s0 += rv * rv;
+    } else if (mode == 2) {
+      double zv = dinv[j] * r[j];
+      z[j] = zv;
+      s0 += r[j] * zv;
+    } else {
+      p[j] = z[j] + a * p[j];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_down_sync(0xffffffffu, s0, o);
+    s1 += __shfl_down_sync(0xffffffffu, s1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (mode == 0) {
+      atomicAdd(scal + 0, s0);
+      atomicAdd(scal + 1, s1);
+    } else if (mode == 1) {
+      atomicAdd(scal + 2, s0);
+    } else if (mode == 2) {
+      atomicAdd(scal + 0, s0);
+    }
+  }
+}
+
+static int csc_solve(Ctx* c, const double* hb, double* hx) {
+  int n = c->csc_n;
+  if (n <= 0) return MAC_OK;
+  cudaStream_t st = c->stream;
+  double* v = c->csc_vec;
+  double *b = v, *x = v + n, *r = v + 2 * (size_t)n, *z = v + 3 * (size_t)n, *p = v + 4 * (size_t)n,
+         *q = v + 5 * (size_t)n, *dinv = v + 6 * (size_t)n, *scal = v + 7 * (size_t)n;
+  int g = grid_for(n, 256);
+  if (g > 1184) g = 1184;
+  int rc = check(cudaMemcpyAsync(b, hb, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+  if (rc) return rc;
+  k_csc_diag<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, dinv);
+  cudaMemsetAsync(scal, 0, 8 * 8, st);
+  k_csc_vec<<<g, 256, 0, st>>>(n, 0, b, x, r, z, p, q, dinv, scal, 0);
+  double hs[8];
+  cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  double rz = hs[0], bb = hs[1];
+  double rtol = c->prm.rtol;
+  int it = 0;
+  double rr = bb;
+  while (bb > 0 && it < c->prm.max_iters) {
+    cudaMemsetAsync(scal, 0, 64, st);
+    k_csc_spmv<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, p, q, scal + 3, p);
+    cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    double alpha = rz / hs[3];
+    k_csc_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, z, p, q, dinv, scal, alpha);
+    k_csc_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, z, p, q, dinv, scal, 0);
+    cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
+    if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    ++it;
+    rr = hs[2];
+    if (rr <= rtol * rtol * bb) break;
+    double beta = hs[0] / rz;
+    rz = hs[0];
+    k_csc_vec<<<g, 256, 0, st>>>(n, 3, b, x, r, z, p, q, dinv, scal, beta);
+  }
+  if ((rc = check(cudaMemcpyAsync(hx, x, 8 * (size_t)n, cudaMemcpyDeviceToHost, st)))) return rc;
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  c->stats.iterations = it;
+  c->stats.total_iterations += it;
+  c->stats.solves += 1;
+  c->stats.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+  c->stats.unknowns = n;
+  return (bb > 0 && !(rr <= rtol * rtol * bb)) ? MAC_ERR_NOT_CONVERGED : MAC_OK;
+}
+
+}  // namespace mac
+
+using mac::Ctx;
+
+#define CTX_OR_FAIL()                        \
+  Ctx* c = (Ctx*)ctx;                        \
+  if (!c) return MAC_ERR_INVALID;            \
+  cudaSetDevice(c->prm.device)
+
+extern "C" {
+
+int mac_initialize_maccell(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::topo_initialize(c);
+}
+int mac_layer_initial_with_particle(void* ctx) {
+  CTX_OR_FAIL();
+  int rc = mac::topo_layer_initial(c);
+  return rc ? rc : mac::read_scalars(c);
+}
+int mac_create_fluid_particle(void* ctx) {
+  CTX_OR_FAIL();
+  int rc = mac::topo_create_fluid(c);
+  return rc ? rc : mac::read_scalars(c);
+}
+int mac_update_celltype_layer(void* ctx) {
+  CTX_OR_FAIL();
+  int rc = mac::topo_update_layer(c);
+  return rc ? rc : mac::read_scalars(c);
+}
+int mac_delete_maccell(void* ctx) {
+  CTX_OR_FAIL();
+  int rc = mac::topo_delete(c);
+  return rc ? rc : mac::read_scalars(c);
+}
+int mac_calculate_time_step(void* ctx, double* dt) {
+  CTX_OR_FAIL();
+  int rc = mac::topo_dt(c);
+  if (rc) return rc;
+  rc = mac::topo_finish(c);
+  if (dt) *dt = c->hs->dt;
+  return rc;
+}
+int mac_topology_rebuild(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::topology_rebuild(c, false);
+}
+int mac_forces(void* ctx, int ispeed) {
+  CTX_OR_FAIL();
+  if (ispeed < 0 || ispeed > 1) return MAC_ERR_INVALID;
+  return mac::forces(c, ispeed);
+}
+int mac_pressure_project(void* ctx, int ispeed) {
+  CTX_OR_FAIL();
+  if (ispeed < 0 || ispeed > 1) return MAC_ERR_INVALID;
+  int rc = mac::setup_system(c);
+  return rc ? rc : mac::project(c, ispeed);
+}
+int mac_rk2tvd(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::rk2tvd(c);
+}
+int mac_extrapolate(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::extrapolate(c);
+}
+int mac_move_particles(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::move_particles(c);
+}
+int mac_step(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::step(c);
+}
+
+int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value) {
+  CTX_OR_FAIL();
+  if (n < 0 || (n > 0 && (!offset || !indice || !value))) return MAC_ERR_INVALID;
+  mac_csc_clean(ctx);
+  if (n == 0) return MAC_OK;
+  int nnz = offset[n];
+  int rc = mac::check(cudaMalloc((void**)&c->csc_off, 4 * (size_t)(n + 1)));
+  if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_ind, 4 * (size_t)(nnz ? nnz : 1)));
+  if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_val, 8 * (size_t)(nnz ? nnz : 1)));
+  if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_vec, 8 * (size_t)(7 * (size_t)n + 8)));
+  if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_off, offset, 4 * (size_t)(n + 1), cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_ind, indice, 4 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_val, value, 8 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = mac::check(cudaStreamSynchronize(c->stream));
+  if (rc) {
+    mac_csc_clean(ctx);
+    return rc;
+  }
+  c->csc_n = n;
+  return MAC_OK;
+}
+
+int mac_csc_solve(void* ctx, int n, const double* b, double* x) {
+  CTX_OR_FAIL();
+  if (n != c->csc_n || (n > 0 && (!b || !x))) return MAC_ERR_INVALID;
+  return mac::csc_solve(c, b, x);
+}
+
+int mac_csc_clean(void* ctx) {
+  CTX_OR_FAIL();
+  cudaFree(c->csc_off);
+  cudaFree(c->csc_ind);
+  cudaFree(c->csc_val);
+  cudaFree(c->csc_vec);
+  c->csc_off = nullptr;
+  c->csc_ind = nullptr;
+  c->csc_val = nullptr;
+  c->csc_vec = nullptr;
+  c->csc_n = 0;
+  return MAC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+"""Python host binding of the C-ABI in include/mac_gpu.h (libmac_gpu.so).
+
+The device library is the product; this module only moves numpy states across
+the boundary and names the reference algorithms each call stands in for. It
+fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .state import BRICK_CELLS, CELL_F64, Params, State
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmac_gpu.so")
+
+MAC_OK = 0
+ERRORS = {-1: "invalid", -2: "cuda", -3: "capacity", -4: "not converged", -5: "no device",
+          -6: "out of memory", -7: "timeout"}
+SOLVERS = {"mgpcg64": 0, "mixed": 1, "cg64": 2}
+
+
+class MacError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
+        self.code = code
+
+
+class mac_params(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_double * 3), ("cfl_factor", ctypes.c_double), ("dt_min", ctypes.c_double),
+                ("dt_max", ctypes.c_double), ("gravity", ctypes.c_double), ("gravity_axis", ctypes.c_int32),
+                ("layer_max", ctypes.c_int32), ("interp_symmetric", ctypes.c_int32), ("solver", ctypes.c_int32),
+                ("rtol", ctypes.c_double), ("max_iters", ctypes.c_int32), ("warm_start", ctypes.c_int32),
+                ("max_bricks", ctypes.c_int64), ("max_particles", ctypes.c_int64), ("device", ctypes.c_int32),
+                ("div_check", ctypes.c_int32)]
+
+
+_P = ctypes.POINTER
+
+
+class mac_host_state(ctypes.Structure):
+    _fields_ = [("nbricks", ctypes.c_int64), ("nparticles", ctypes.c_int64), ("keys", _P(ctypes.c_int32)),
+                ("exists", _P(ctypes.c_uint8)), ("u", (_P(ctypes.c_double) * 3) * 2), ("acc", _P(ctypes.c_double) * 3),
+                ("p", _P(ctypes.c_double)), ("flags", _P(ctypes.c_uint8)), ("type", _P(ctypes.c_uint8)),
+                ("layer", _P(ctypes.c_int32)), ("pos", _P(ctypes.c_double)), ("t", ctypes.c_double),
+                ("dt", ctypes.c_double), ("step", ctypes.c_uint64)]
+
+
+class mac_stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("solves", ctypes.c_int32), ("relres", ctypes.c_double),
+                ("max_div", ctypes.c_double), ("fluid_cells", ctypes.c_int64), ("unknowns", ctypes.c_int64),
+                ("live_bricks", ctypes.c_int64), ("particles", ctypes.c_int64),
+                ("total_iterations", ctypes.c_int64)]
+
+
+EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_stats", "mac_error_string",
+           "mac_upload_state", "mac_query_sizes", "mac_download_state", "mac_initialize_maccell",
+           "mac_layer_initial_with_particle", "mac_create_fluid_particle", "mac_update_celltype_layer",
+           "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
+           "mac_pressure_project", "mac_rk2tvd", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
+           "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean"]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads libmac_gpu.so; raises if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m mac_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.mac_default_params.argtypes = [_P(mac_params)]
+    lib.mac_default_params.restype = None
+    lib.mac_ctx_create.argtypes = [_P(mac_params), _P(vp)]
+    lib.mac_ctx_destroy.argtypes = [vp]
+    lib.mac_get_stats.argtypes = [vp, _P(mac_stats)]
+    lib.mac_error_string.argtypes = [ctypes.c_int]
+    lib.mac_error_string.restype = ctypes.c_char_p
+    lib.mac_upload_state.argtypes = [vp, _P(mac_host_state)]
+    lib.mac_query_sizes.argtypes = [vp, _P(ctypes.c_int64), _P(ctypes.c_int64)]
+    lib.mac_download_state.argtypes = [vp, _P(mac_host_state)]
+    for n in ["mac_initialize_maccell", "mac_layer_initial_with_particle", "mac_create_fluid_particle",
+              "mac_update_celltype_layer", "mac_delete_maccell", "mac_topology_rebuild", "mac_rk2tvd",
+              "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync", "mac_csc_clean"]:
+        getattr(lib, n).argtypes = [vp]
+    lib.mac_calculate_time_step.argtypes = [vp, _P(ctypes.c_double)]
+    lib.mac_forces.argtypes = [vp, ctypes.c_int]
+    lib.mac_pressure_project.argtypes = [vp, ctypes.c_int]
+    lib.mac_csc_factorize.argtypes = [vp, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_double)]
+    lib.mac_csc_solve.argtypes = [vp, ctypes.c_int, _P(ctypes.c_double), _P(ctypes.c_double)]
+    _lib = lib
+    return lib
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(_P(ct))
+
+
+def make_params(pr: Params, max_bricks: int, max_particles: int, solver="mgpcg64", rtol=1e-8, max_iters=500,
+                warm_start=False, device=0, div_check=True) -> mac_params:
+    p = mac_params()
+    load().mac_default_params(ctypes.byref(p))
+    for i in range(3):
+        p.h[i] = pr.h[i]
+    p.cfl_factor = pr.cfl_factor
+    p.dt_min = pr.dt_min
+    p.dt_max = pr.dt_max
+    p.gravity = pr.gravity
+    p.gravity_axis = pr.gravity_axis
+    p.layer_max = pr.layer_max
+    p.interp_symmetric = pr.interp_symmetric
+    p.solver = SOLVERS[solver]
+    p.rtol = rtol
+    p.max_iters = max_iters
+    p.warm_start = int(warm_start)
+    p.max_bricks = int(max_bricks)
+    p.max_particles = int(max_particles)
+    p.device = device
+    p.div_check = int(div_check)
+    return p
+
+
+class HostState:
+    """Host arrays laid out as mac_host_state expects (optionally in pinned memory)."""
+
+    def __init__(self, nbricks: int, nparticles: int, pinned: bool = False):
+        nc = nbricks * BRICK_CELLS
+        if pinned:
+            import torch
+            alloc = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()
+            f64 = lambda n: alloc(n, torch.float64)
+            u8 = lambda n: alloc(n, torch.uint8)
+            i32 = lambda n: alloc(n, torch.int32)
+        else:
+            f64 = lambda n: np.empty(n, np.float64)
+            u8 = lambda n: np.empty(n, np.uint8)
+            i32 = lambda n: np.empty(n, np.int32)
+        self.nbricks, self.nparticles = nbricks, nparticles
+        self.keys = i32(3 * max(nbricks, 1))
+        self.exists = u8(max(nc, 1))
+        self.f64 = {n: f64(max(nc, 1)) for n in CELL_F64}
+        self.flags = u8(max(nc, 1))
+        self.type = u8(max(nc, 1))
+        self.layer = i32(max(nc, 1))
+        self.pos = f64(3 * max(nparticles, 1))
+        self.t = self.dt = 0.0
+        self.step = 0
+
+    def fill(self, s: State) -> "HostState":
+        nb, nc = s.nbricks, s.nbricks * BRICK_CELLS
+        self.keys[:3 * nb] = s.keys.reshape(-1)
+        self.exists[:nc] = s.exists.reshape(-1)
+        for n in CELL_F64:
+            self.f64[n][:nc] = s.f64[n].reshape(-1)
+        self.flags[:nc] = s.flags.reshape(-1)
+        self.type[:nc] = s.type.reshape(-1)
+        self.layer[:nc] = s.layer.reshape(-1)
+        self.pos[:3 * s.nparticles] = s.pos.reshape(-1)
+        self.nbricks, self.nparticles = nb, s.nparticles
+        self.t, self.dt, self.step = s.params.t, s.params.dt, s.params.step
+        return self
+
+    def c_struct(self) -> mac_host_state:
+        h = mac_host_state()
+        h.nbricks, h.nparticles = self.nbricks, self.nparticles
+        h.keys = _ptr(self.keys, ctypes.c_int32)
+        h.exists = _ptr(self.exists, ctypes.c_uint8)
+        for b in range(2):
+            for i in range(3):
+                h.u[b][i] = _ptr(self.f64[CELL_F64[3 * b + i]], ctypes.c_double)
+        for i in range(3):
+            h.acc[i] = _ptr(self.f64[CELL_F64[6 + i]], ctypes.c_double)
+        h.p = _ptr(self.f64["p"], ctypes.c_double)
+        h.flags = _ptr(self.flags, ctypes.c_uint8)
+        h.type = _ptr(self.type, ctypes.c_uint8)
+        h.layer = _ptr(self.layer, ctypes.c_int32)
+        h.pos = _ptr(self.pos, ctypes.c_double)
+        h.t, h.dt, h.step = self.t, self.dt, self.step
+        return h
+
+    def to_state(self, params: Params) -> State:
+        nb, nc, npart = self.nbricks, self.nbricks * BRICK_CELLS, self.nparticles
+        shp = (nb, BRICK_CELLS)
+        pr = Params(**{**params.__dict__})
+        pr.t, pr.dt, pr.step = self.t, self.dt, self.step
+        return State(pr, self.keys[:3 * nb].reshape(nb, 3).copy(), self.exists[:nc].reshape(shp).copy(),
+                     {n: self.f64[n][:nc].reshape(shp).copy() for n in CELL_F64},
+                     self.flags[:nc].reshape(shp).copy(), self.type[:nc].reshape(shp).copy(),
+                     self.layer[:nc].reshape(shp).copy(), np.full(shp, -1, np.int32),
+                     self.pos[:3 * npart].reshape(npart, 3).copy()).sorted()
+
+
+class Context:
+    """One device context (one CUDA stream, its own device memory)."""
+
+    def __init__(self, params: Params, max_bricks=4096, max_particles=1 << 20, **kw):
+        self.lib = load()
+        self.params = params
+        self.cp = make_params(params, max_bricks, max_particles, **kw)
+        h = ctypes.c_void_p()
+        self._check(self.lib.mac_ctx_create(ctypes.byref(self.cp), ctypes.byref(h)), "mac_ctx_create")
+        self.h = h
+
+    def _check(self, rc, what, allow=()):
+        if rc != MAC_OK and rc not in allow:
+            raise MacError(rc, what)
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mac_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- transfer
+    def upload(self, s: State, host: HostState | None = None):
+        host = host or HostState(s.nbricks, s.nparticles).fill(s)
+        self._host_in = host
+        st = host.c_struct()
+        self._check(self.lib.mac_upload_state(self.h, ctypes.byref(st)), "mac_upload_state")
+
+    def sizes(self):
+        nb, npart = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.mac_query_sizes(self.h, ctypes.byref(nb), ctypes.byref(npart)), "mac_query_sizes")
+        return nb.value, npart.value
+
+    def download(self, host: HostState | None = None) -> State:
+        nb, npart = self.sizes()
+        if host is None or host.nbricks < nb or len(host.pos) < 3 * npart:
+            host = HostState(nb, npart)
+        host.nbricks, host.nparticles = nb, npart
+        st = host.c_struct()
+        self._check(self.lib.mac_download_state(self.h, ctypes.byref(st)), "mac_download_state")
+        host.nbricks, host.nparticles = st.nbricks, st.nparticles
+        host.t, host.dt, host.step = st.t, st.dt, st.step
+        return host.to_state(self.params)
+
+    def stats(self) -> dict:
+        s = mac_stats()
+        self._check(self.lib.mac_get_stats(self.h, ctypes.byref(s)), "mac_get_stats")
+        return {k: getattr(s, k) for k, _ in mac_stats._fields_}
+
+    # ---- the reference algorithms
+    def topology(self):
+        return self._check(self.lib.mac_topology_rebuild(self.h), "mac_topology_rebuild")
+
+    def first_init_topology(self):
+        """Initialize_MacCell, Create_Fluid_Particle, Layer_Initial_With_Particle,
+        Update_CellType_Layer, Delete_MacCell in the first-init order
+        (test/TestJetDEau_Basic.cpp:329-330)."""
+        for n in ["mac_initialize_maccell", "mac_create_fluid_particle", "mac_layer_initial_with_particle",
+                  "mac_update_celltype_layer", "mac_delete_maccell"]:
+            self._check(getattr(self.lib, n)(self.h), n)
+
+    def dt(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.lib.mac_calculate_time_step(self.h, ctypes.byref(v)), "mac_calculate_time_step")
+        return v.value
+
+    def forces(self, ispeed=0):
+        return self._check(self.lib.mac_forces(self.h, ispeed), "mac_forces")
+
+    def project(self, ispeed=0, allow_not_converged=False):
+        return self._check(self.lib.mac_pressure_project(self.h, ispeed), "mac_pressure_project",
+                           allow=(-4,) if allow_not_converged else ())
+
+    def rk2tvd(self, allow_not_converged=False):
+        return self._check(self.lib.mac_rk2tvd(self.h), "mac_rk2tvd", allow=(-4,) if allow_not_converged else ())
+
+    def extrapolate(self):
+        return self._check(self.lib.mac_extrapolate(self.h), "mac_extrapolate")
+
+    def move(self):
+        return self._check(self.lib.mac_move_particles(self.h), "mac_move_particles")
+
+    def step(self, allow_not_converged=False):
+        return self._check(self.lib.mac_step(self.h), "mac_step", allow=(-4,) if allow_not_converged else ())
+
+    def sync(self):
+        return self._check(self.lib.mac_sync(self.h), "mac_sync")
+
+    # ---- drop-in CSC solver
+    def csc_solve(self, offset, indice, value, b):
+        off = np.ascontiguousarray(offset, dtype=np.int32)
+        ind = np.ascontiguousarray(indice, dtype=np.int32)
+        val = np.ascontiguousarray(value, dtype=np.float64)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        n = len(off) - 1
+        x = np.zeros(n, np.float64)
+        self._check(self.lib.mac_csc_factorize(self.h, n, _ptr(off, ctypes.c_int), _ptr(ind, ctypes.c_int),
+                                               _ptr(val, ctypes.c_double)), "mac_csc_factorize")
+        self._check(self.lib.mac_csc_solve(self.h, n, _ptr(bb, ctypes.c_double), _ptr(x, ctypes.c_double)),
+                    "mac_csc_solve")
+        self._check(self.lib.mac_csc_clean(self.h), "mac_csc_clean")
+        return x

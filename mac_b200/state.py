@@ -118,6 +118,28 @@ class State:
                         interp_symmetric=isym)
         return State(params, keys, exists, f64, flags, typ, layer, ids, pos)
 
+    def save_npz(self, path: str) -> None:
+        """Compressed copy (used for the committed fixtures)."""
+        pr = self.params
+        hdr = np.array([*pr.h, pr.t, pr.dt, pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
+                        pr.layer_max, pr.step, pr.interp_symmetric], dtype=np.float64)
+        np.savez_compressed(path, hdr=hdr, keys=self.keys, exists=self.exists, flags=self.flags, type=self.type,
+                            layer=self.layer, id=self.id, pos=self.pos, **self.f64)
+
+    @staticmethod
+    def load_npz(path: str) -> "State":
+        z = np.load(path)
+        h = z["hdr"]
+        pr = Params(h=(h[0], h[1], h[2]), t=h[3], dt=h[4], cfl_factor=h[5], dt_min=h[6], dt_max=h[7],
+                    gravity=h[8], gravity_axis=int(h[9]), layer_max=int(h[10]), step=int(h[11]),
+                    interp_symmetric=int(h[12]))
+        return State(pr, z["keys"], z["exists"], {n: z[n] for n in CELL_F64}, z["flags"], z["type"], z["layer"],
+                     z["id"], z["pos"])
+
+    @staticmethod
+    def load(path: str) -> "State":
+        return State.load_npz(path) if path.endswith(".npz") else State.read(path)
+
     # ------------------------------------------------------------- queries
     def cell_keys(self) -> np.ndarray:
         """(nb, 512, 3) integer cell keys of every slot."""

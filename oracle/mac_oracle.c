@@ -993,6 +993,9 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
       alg_update_layer(w);
       alg_delete(w);
       alg_extrapolate(w);
+    } else if (!strcmp(cmd, "setup")) {
+      alg_solid_to_const(w);
+      alg_mirror(w);
     } else if (!strcmp(cmd, "step") || !strcmp(cmd, "bench")) {
       ++w->seed;
       topology(w);

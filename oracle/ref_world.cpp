@@ -479,6 +479,9 @@ static int run(int argc, char** argv) {
   for (int r = 0; r < nrep; ++r) {
     if (cmd == "firstinit") {
       m_alg_first_init.Do();
+    } else if (cmd == "setup") {
+      m_alg_solid.Do();
+      m_alg_mirror.Do();
     } else if (cmd == "step" || cmd == "bench") {
       ++g_refill_seed;
       m_alg_init.Do();

@@ -1,0 +1,69 @@
+"""Generates the committed golden fixtures from the reference's own code.
+
+Run here, where the reference sources exist (oracle/Makefile builds
+oracle/_ref/mac_ref from them). The outputs are compressed states of the
+32x32x64 vertical-jet world (h = 0.05, inflow radius 4 at w = 1, LayerMax 4,
+CFL 0.5) produced by the unmodified reference algorithms:
+
+  c1_setup.npz         world as built (walls, inflow), before any pass
+  c1_ref_setup.npz     after Solid_To_Const + Speed_Constant_Mirror
+  c1_ref_s0.npz        after the reference's first init
+  c1_ref_s30.npz       after 30 steps
+  c1_ref_t30.npz       c1_ref_s30 after the per-step init (topology + dt)
+  c1_ref_t30_<stage>.npz  c1_ref_t30 after one stage: forces, ode, project,
+                       extrapolate, move, movelin
+  c1_ref_s31.npz       one full step from c1_ref_s30
+  c1_ref_s60.npz       after 60 steps from c1_ref_s0
+  c1_ref_t30_csc.bin   the CSC system the reference assembled for the projection
+                       of c1_ref_t30 (n, nnz, offset, indice, value, b, x)
+
+Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from mac_b200.state import State, jet_world  # noqa: E402
+import oracle  # noqa: E402
+
+STAGES = ["forces", "ode", "project", "extrapolate", "move", "movelin"]
+
+
+def main():
+    oracle.build()
+    if not oracle.have_ref():
+        raise SystemExit("oracle/_ref/mac_ref is not built (reference sources missing)")
+    tmp = tempfile.mkdtemp()
+    t = lambda n: os.path.join(tmp, n + ".state")
+    out = lambda n: os.path.join(HERE, n + ".npz")
+    s = jet_world()
+    s.write(t("setup"))
+    s.save_npz(out("c1_setup"))
+    oracle.run_ref("setup", t("setup"), t("rsetup"))
+    State.read(t("rsetup")).save_npz(out("c1_ref_setup"))
+    oracle.run_ref("firstinit", t("setup"), t("s0"))
+    State.read(t("s0")).save_npz(out("c1_ref_s0"))
+    oracle.run_ref("step", t("s0"), t("s30"), 30)
+    State.read(t("s30")).save_npz(out("c1_ref_s30"))
+    oracle.run_ref("step", t("s30"), t("s31"), 1)
+    State.read(t("s31")).save_npz(out("c1_ref_s31"))
+    oracle.run_ref("step", t("s30"), t("s60"), 30)
+    State.read(t("s60")).save_npz(out("c1_ref_s60"))
+    oracle.run_ref("topology", t("s30"), t("t30"))
+    State.read(t("t30")).save_npz(out("c1_ref_t30"))
+    for st in STAGES:
+        oracle.run_ref(st, t("t30"), t("t30_" + st))
+        State.read(t("t30_" + st)).save_npz(out("c1_ref_t30_" + st))
+    oracle.run_ref("csc", t("t30"), t("junk"), os.path.join(HERE, "c1_ref_t30_csc.bin"))
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
