@@ -1,0 +1,390 @@
+"""Benchmark: fluid cell-steps/s of the full Mac step at Poisson relative residual 1e-8.
+
+Workload (default): the 256x256x512 vertical jet (h = 0.01 m, inflow radius 24
+cells at w = 2.0 m/s, gravity -9.81 z, solid side walls and floor, LayerMax 4,
+CFL 0.5) in a synthetic spun-up state: a pool of depth 122 cells (~8.0M fluid
+cells) with 8 jittered particles per fluid cell (~64M particles). Each step is
+the reference's whole step (test/TestJetDEau_Basic.cpp:434-441): topology
+rebuild, CFL time step, RK2-TVD with gravity + upwind convection and two
+pressure projections (plain FP64 MG-PCG at relative residual 1e-8), air-layer
+extrapolation, RK4 particle move.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own code (compiled from its headers into
+oracle/_ref/mac_ref; its solver stand-in is FP64 Jacobi-CG at 1e-8) on the
+host cores, one single-threaded process per core, each on a bounded sub-box of
+the same jet.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fluid cell-steps/s at Poisson rel-resid 1e-8 (full advect+project step)"
+UNIT = "cell-steps/s"
+
+WORKLOADS = {
+    # name: (nx, ny, nz, h, r_inflow, w_inflow, pool_depth, dt_max, max_bricks, max_particles)
+    "jet256": (256, 256, 512, 0.01, 24.0, 2.0, 122, 0.01, 40000, 80_000_000),
+    "jet128": (128, 128, 256, 0.01, 24.0, 2.0, 61, 0.01, 8000, 12_000_000),
+    "jet32": (32, 32, 64, 0.05, 4.0, 1.0, 0, 0.1, 1024, 1 << 20),
+}
+# Bounded sample of the jet for the CPU arms: a sub-box with the same spacing,
+# inflow and pool fraction.
+CPU_SAMPLE = (48, 48, 96, 0.01, 12.0, 2.0, 23, 0.01)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ world
+def make_world(name):
+    from mac_b200.state import jet_world
+    nx, ny, nz, h, r, w, depth, dt_max = WORKLOADS[name][:8]
+    return jet_world(nx, ny, nz, h=h, r_inflow=r, w_inflow=w, pool_depth=depth, dt_max=dt_max, seed=1)
+
+
+def sample_world():
+    from mac_b200.state import jet_world
+    nx, ny, nz, h, r, w, depth, dt_max = CPU_SAMPLE
+    return jet_world(nx, ny, nz, h=h, r_inflow=r, w_inflow=w, pool_depth=depth, dt_max=dt_max, seed=1)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU arms
+def _ref_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "mac_ref")
+    return p if os.path.exists(p) else None
+
+
+def cpu_reference_run(steps, procs, tmpdir):
+    """Runs the reference's own code (or, when it was not built, the oracle port)
+    on `procs` independent replicas of the bounded sample, `steps` steps each,
+    concurrently; returns (fluid cell-steps/s, kind, seconds, fluid_cell_steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    s = sample_world()
+    setup = os.path.join(tmpdir, "sample_setup.state")
+    s.write(setup)
+    init = os.path.join(tmpdir, "sample_s0.state")
+    ref = _ref_binary()
+    kind = "reference" if ref else "port"
+    env = dict(os.environ, MAC_REF_RTOL="1e-8")
+    if ref:
+        subprocess.run([ref, "firstinit", setup, init], check=True, capture_output=True, env=env)
+        cmds = [[ref, "bench", init, os.path.join(tmpdir, f"out{i}.state"), str(steps)] for i in range(procs)]
+        t0 = time.perf_counter()
+        ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env) for c in cmds]
+        outs = [p.communicate() for p in ps]
+        wall = time.perf_counter() - t0
+        fcs = 0
+        secs = 0.0
+        for o, _e in outs:
+            d = json.loads(o.strip().splitlines()[-1])
+            fcs += d["fluid_cell_steps"]
+            secs = max(secs, d["seconds"])
+        return fcs / secs, kind, secs, fcs, wall
+    oracle.run_oracle("firstinit", setup, init)
+    t0 = time.perf_counter()
+    st = oracle.run_oracle("bench", init, "", steps, 1e-8)
+    secs = time.perf_counter() - t0
+    return st["fluid_cell_steps"] / secs, kind, secs, st["fluid_cell_steps"], secs
+
+
+def sample_desc(steps, procs):
+    nx, ny, nz, h, r, w, depth, _ = CPU_SAMPLE
+    return (f"{procs} concurrent single-thread replica(s) of a {nx}x{ny}x{nz} sub-box of the same jet "
+            f"(h={h}, inflow r={r:g} at w={w}, pool depth {depth}), {steps} steps each after the first init, "
+            f"solver stand-in FP64 Jacobi-CG at rel-resid 1e-8")
+
+
+# ------------------------------------------------------------- our arm
+def roofline_models(ctx_stats, prof, np_count, n_exist):
+    """Achieved GB/s per phase from algorithmic bytes (every array element a
+    kernel must touch, read or written once) over the measured event times."""
+    unk = ctx_stats["unknowns"]
+    models = {
+        # phase: (bytes per launch, description)
+        "move": (48.0 * np_count, "48 B per particle (read + write 3 FP64 positions)"),
+        "spmv": (18.0 * unk, "18 B per unknown (read p 8, face mask 2, write q 8)"),
+        "forces": (75.0 * n_exist, "75 B per existing cell (mean of stage 1: 51, stage 2: 99)"),
+        "gradient": (67.0 * n_exist, "67 B per existing cell (x 8, flags 3, p 8, u read+write 48)"),
+        "divergence": (42.0 * unk, "42 B per unknown (u 24, mask 2, rhs 8, x 8)"),
+    }
+    out = {}
+    for ph, (nbytes, desc) in models.items():
+        ms, n = prof.get(ph, (0.0, 0))
+        if n:
+            out[ph] = {"ms_total": ms, "launches": n, "avg_ms": ms / n,
+                       "gbs": nbytes / (ms / n * 1e-3) / 1e9, "bytes_per_launch": nbytes, "model": desc}
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from mac_b200.gpu import Context, HostState
+    from mac_b200.world import first_init
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.workload]
+    t0 = time.perf_counter()
+    s = make_world(args.workload)
+    log(f"[rank {rank}] world built in {time.perf_counter() - t0:.1f}s: {s.nbricks} bricks, {s.nparticles} particles")
+    ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
+                  device=dev, div_check=True)
+    t0 = time.perf_counter()
+    first_init(ctx, s)
+    ctx.sync()
+    log(f"[rank {rank}] first init {time.perf_counter() - t0:.1f}s")
+    del s
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+
+    for _ in range(args.warmup):
+        ctx.step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.profile()  # reset
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    l0 = ctx.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    fluid_steps = 0
+    iters = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.step()
+        st = ctx.stats()
+        fluid_steps += st["fluid_cells"]
+        iters.append(st["iterations"])
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launches() - l0
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    st = ctx.stats()
+    sec = ms / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([sec], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        n = torch.tensor([float(fluid_steps)], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        total_fluid_steps = float(n.item())
+    else:
+        total_fluid_steps = float(fluid_steps)
+    value = total_fluid_steps / sec
+
+    # e2e through the C-ABI with pinned host buffers: upload, step, download per step
+    nb, npart = ctx.sizes()
+    host = HostState(int(nb * 1.1) + 64, int(npart * 1.02) + 4096, pinned=True)
+    ctx.download(host)
+    e2e_steps = max(1, min(args.steps, 3))
+    bi = bo = 0
+    f2 = 0
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(e2e_steps):
+        bi += host.nbytes()
+        ctx.upload(None, host)
+        ctx.step()
+        f2 += ctx.stats()["fluid_cells"]
+        ctx.download(host)
+        bo += host.nbytes()
+    a1.record(stream)
+    a1.synchronize()
+    e2e_sec = a0.elapsed_time(a1) / 1e3
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_sec], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+        n = torch.tensor([float(f2)], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        f2 = float(n.item())
+    e2e = {"value": f2 / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": bi // e2e_steps,
+           "d2h_bytes_per_step": bo // e2e_steps, "steps": e2e_steps}
+
+    n_exist = int(st["live_bricks"] * 512)  # upper bound of existing cells (slots of live bricks)
+    rl = roofline_models(st, prof, st["particles"], n_exist)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(rl, key=lambda k: rl[k]["ms_total"]) if rl else None
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(dom)
+    except (OSError, ValueError):
+        pass
+    roofline = None
+    if dom:
+        r = rl[dom]
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(r["gbs"], 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(r["gbs"] / peak, 4), "peak_source": peak_src,
+                    "traffic": traffic, "bytes_per_launch": r["bytes_per_launch"], "model": r["model"]}
+    phases = {k: {"ms": round(v[0], 3), "n": v[1]} for k, v in prof.items() if v[1]}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded spun-up jet state)",
+        "config": {"workload": f"jet {wl[0]}x{wl[1]}x{wl[2]} h={wl[3]} inflow r={wl[4]:g} w={wl[5]}, pool depth "
+                               f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
+                   "solver": {"mgpcg64": "plain FP64 MG-PCG", "mixed": "FP32 MG in FP64 PCG",
+                              "cg64": "FP64 Jacobi-PCG"}[args.solver],
+                   "rtol": 1e-8, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (state > 3 GB)",
+                   "fluid_cells_last": st["fluid_cells"], "particles": st["particles"],
+                   "live_bricks": st["live_bricks"], "cg_iters_per_solve_last": st["iterations"],
+                   "cg_iters_mean": float(np.mean(iters)) if iters else None},
+        "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
+        "phases_ms": phases, "phase_rooflines": {k: {"gbs": round(v["gbs"], 1), "avg_ms": round(v["avg_ms"], 4)}
+                                                 for k, v in rl.items()},
+    }
+    ctx.close()
+    return out
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="jet256")
+    ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mgpcg64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = max(1, min(os.cpu_count() or 1, 8))
+        with tempfile.TemporaryDirectory() as td:
+            # warm-up steps are run too (each replica runs warmup + steps), the
+            # timed value covers all of them
+            v, kind, secs, fcs, wall = cpu_reference_run(args.steps + args.warmup, procs, td)
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": secs * 1e3 / (args.steps + args.warmup),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded jet sub-box)", "impl": "reference",
+                "config": {"workload": "jet sub-box, see cpu_baseline.sample", "rtol": 1e-8},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
+                                 "sample": sample_desc(args.steps + args.warmup, procs)},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td:
+            v, kind, secs, fcs, wall = cpu_reference_run(args.cpu_steps, 1, td)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+                               "sample": sample_desc(args.cpu_steps, 1), "seconds": round(secs, 2)}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

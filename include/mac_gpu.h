@@ -148,6 +148,21 @@ int mac_move_particles(void* ctx);
 int mac_step(void* ctx);
 /* Synchronises the context's stream. */
 int mac_sync(void* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+int mac_stream(void* ctx, void** stream);
+/* Number of kernels the context has launched so far. */
+int mac_launch_count(void* ctx, int64_t* count);
+
+/* Per-phase device timing with CUDA events on the context's stream (the
+ * reference's per-algorithm times() prints, e.g. src/Algorithms_Convection.h:20-36).
+ * mac_get_profile returns and resets the accumulated milliseconds and the
+ * number of timed regions per phase. */
+enum {
+  MAC_PHASE_TOPOLOGY = 0, MAC_PHASE_FORCES, MAC_PHASE_SETUP, MAC_PHASE_DIVERGENCE, MAC_PHASE_SPMV,
+  MAC_PHASE_CGVEC, MAC_PHASE_VCYCLE, MAC_PHASE_GRADIENT, MAC_PHASE_EXTRAPOLATE, MAC_PHASE_MOVE, MAC_NPHASES
+};
+int mac_set_profiling(void* ctx, int on);
+int mac_get_profile(void* ctx, double* ms, int64_t* count, int nphase);
 
 /* ---- drop-in linear solver: the Policy_Solve_Linear_Umfpack member functions
  * (src/Policy_Solve_Linear_Umfpack.h:28-70) over the CSC arrays the reference assembles

@@ -146,19 +146,22 @@ int forces(Ctx* c, int ib) {
   if (c->nlive_host == 0) return MAC_OK;
   size_t cap = (size_t)c->cap_bricks * kCells;
   k_forces<0><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
-                                                    c->f64, cap, ib, c->dp, c->ds);
+                                                    c->f64, cap, ib, c->dp, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
 int rk_stage(Ctx* c, int stage) {
   if (c->nlive_host == 0) return MAC_OK;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  if (stage == 1)
+  prof_begin(c, PH_FORCES);
+  if (stage == 1) {
     k_forces<1><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
-                                                      c->f64, cap, 0, c->dp, c->ds);
-  else
+                                                      c->f64, cap, 0, c->dp, c->ds); MAC_COUNT(c);
+  } else {
     k_forces<2><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
-                                                      c->f64, cap, 1, c->dp, c->ds);
+                                                      c->f64, cap, 1, c->dp, c->ds); MAC_COUNT(c);
+  }
+  prof_end(c, PH_FORCES);
   return check(cudaGetLastError());
 }
 
@@ -245,9 +248,12 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
 int extrapolate(Ctx* c) {
   if (c->nlive_host == 0) return MAC_OK;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  for (int L = 1; L <= c->dp.layer_max + 1; ++L)
+  prof_begin(c, PH_EXTRAPOLATE);
+  for (int L = 1; L <= c->dp.layer_max + 1; ++L) {
     k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, c->f64,
-                                                        cap, L);
+                                                        cap, L); MAC_COUNT(c);
+  }
+  prof_end(c, PH_EXTRAPOLATE);
   return check(cudaGetLastError());
 }
 
@@ -379,8 +385,10 @@ int move_particles(Ctx* c) {
   int g = grid_for(c->np_host, 256);
   if (g > 148 * 16) g = 148 * 16;
   unsigned long long* bad = &c->ds->bad_reads;
+  prof_begin(c, PH_MOVE);
   k_move<<<g, 256, 0, c->stream>>>(c->px, c->py, c->pz, c->np_host, c->nbr, c->hkeys, c->hval, c->hcap, c->lay,
-                                   c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap, c->dp, c->ds, bad);
+                                   c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap, c->dp, c->ds, bad); MAC_COUNT(c);
+  prof_end(c, PH_MOVE);
   return check(cudaGetLastError());
 }
 

@@ -3,6 +3,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <utility>
+#include <vector>
 
 #include "mac_internal.cuh"
 
@@ -89,8 +91,70 @@ __global__ void k_gather_keys(int32_t* out, const int* bkey, const int* blist, i
   if (i < 3 * nlive) out[i] = bkey[blist[i / 3] * 3 + i % 3];
 }
 
+// ------------------------------------------------------------- profiling
+struct Prof {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[kPhases];
+  std::vector<cudaEvent_t> spare;
+  cudaEvent_t open[kPhases] = {};
+  double ms[kPhases] = {};
+  long long n[kPhases] = {};
+};
+
+static cudaEvent_t take_event(Prof* p) {
+  if (!p->spare.empty()) {
+    cudaEvent_t e = p->spare.back();
+    p->spare.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_begin(Ctx* c, int ph) {
+  if (!c->prof) return;
+  cudaEvent_t e = take_event(c->prof);
+  cudaEventRecord(e, c->stream);
+  c->prof->open[ph] = e;
+}
+
+void prof_end(Ctx* c, int ph) {
+  if (!c->prof || !c->prof->open[ph]) return;
+  cudaEvent_t e = take_event(c->prof);
+  cudaEventRecord(e, c->stream);
+  c->prof->pending[ph].push_back({c->prof->open[ph], e});
+  c->prof->open[ph] = nullptr;
+}
+
+static void prof_resolve(Ctx* c) {
+  Prof* p = c->prof;
+  if (!p) return;
+  cudaStreamSynchronize(c->stream);
+  for (int ph = 0; ph < kPhases; ++ph) {
+    for (auto& pr : p->pending[ph]) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pr.first, pr.second);
+      p->ms[ph] += ms;
+      p->n[ph] += 1;
+      p->spare.push_back(pr.first);
+      p->spare.push_back(pr.second);
+    }
+    p->pending[ph].clear();
+  }
+}
+
+static void prof_free(Ctx* c) {
+  Prof* p = c->prof;
+  if (!p) return;
+  prof_resolve(c);
+  for (cudaEvent_t e : p->spare) cudaEventDestroy(e);
+  delete p;
+  c->prof = nullptr;
+}
+
 // ------------------------------------------------------------- lifetime
 static void free_all(Ctx* c) {
+  prof_free(c);
   free_solver(c);
   cudaFree(c->bkey); cudaFree(c->lay); cudaFree(c->type); cudaFree(c->flags); cudaFree(c->f64);
   cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
@@ -193,7 +257,7 @@ static int upload(Ctx* c, const mac_host_state* s) {
     // keys through a staging area (solver vector r), then the fields straight into the pool.
     int32_t* tkeys = (int32_t*)c->r;
     MAC_CUDA(cudaMemcpyAsync(tkeys, s->keys, sizeof(int32_t) * 3 * nb, cudaMemcpyHostToDevice, st));
-    k_set_keys<<<grid_for(3 * nb, 256), 256, 0, st>>>(c->bkey, tkeys, nb);
+    k_set_keys<<<grid_for(3 * nb, 256), 256, 0, st>>>(c->bkey, tkeys, nb); MAC_COUNT(c);
     for (int b = 0; b < 2; ++b)
       for (int i = 0; i < 3; ++i)
         MAC_CUDA(cudaMemcpyAsync(c->f64 + (size_t)(U0X + 3 * b + i) * cap, s->u[b][i], 8 * nc,
@@ -207,17 +271,17 @@ static int upload(Ctx* c, const mac_host_state* s) {
     int32_t* tlay = (int32_t*)c->q;
     MAC_CUDA(cudaMemcpyAsync(tex, s->exists, nc, cudaMemcpyHostToDevice, st));
     MAC_CUDA(cudaMemcpyAsync(tlay, s->layer, 4 * nc, cudaMemcpyHostToDevice, st));
-    k_pack_lay<<<grid_for((int64_t)nc, 256), 256, 0, st>>>(tex, tlay, c->lay, (int64_t)nc);
+    k_pack_lay<<<grid_for((int64_t)nc, 256), 256, 0, st>>>(tex, tlay, c->lay, (int64_t)nc); MAC_COUNT(c);
   }
   if (cap > nc) MAC_CUDA(cudaMemsetAsync(c->lay + nc, 0xFE, cap - nc, st));
-  k_init_lists<<<grid_for(c->cap_bricks, 256), 256, 0, st>>>(c->blist, c->freelist, nb, (int)c->cap_bricks);
+  k_init_lists<<<grid_for(c->cap_bricks, 256), 256, 0, st>>>(c->blist, c->freelist, nb, (int)c->cap_bricks); MAC_COUNT(c);
   // particles, through a bounded staging buffer (solver vector pd)
   int64_t np = s->nparticles;
   int64_t chunk = (int64_t)(cap / 3);
   for (int64_t o = 0; o < np; o += chunk) {
     int64_t n = np - o < chunk ? np - o : chunk;
     MAC_CUDA(cudaMemcpyAsync(c->pd, s->pos + 3 * o, 24 * n, cudaMemcpyHostToDevice, st));
-    k_aos_to_soa<<<grid_for(n, 256), 256, 0, st>>>(c->pd, c->px + o, c->py + o, c->pz + o, n);
+    k_aos_to_soa<<<grid_for(n, 256), 256, 0, st>>>(c->pd, c->px + o, c->py + o, c->pz + o, n); MAC_COUNT(c);
   }
   Scalars h{};
   h.nlive = nb;
@@ -245,23 +309,23 @@ static int download(Ctx* c, mac_host_state* s) {
   int g = grid_for((int64_t)nc, 256);
   if (nb > 0) {
     int32_t* tk = (int32_t*)c->z;
-    k_gather_keys<<<grid_for(3 * nb, 256), 256, 0, st>>>(tk, c->bkey, c->blist, nb);
+    k_gather_keys<<<grid_for(3 * nb, 256), 256, 0, st>>>(tk, c->bkey, c->blist, nb); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->keys, tk, 12 * (size_t)nb, cudaMemcpyDeviceToHost, st));
     for (int f = 0; f < NF64; ++f) {
       double* dst = f < 6 ? s->u[f / 3][f % 3] : (f < 9 ? s->acc[f - 6] : s->p);
-      k_gather_bricks<double><<<g, 256, 0, st>>>(tmp, c->f64 + (size_t)f * cap, c->blist, nb);
+      k_gather_bricks<double><<<g, 256, 0, st>>>(tmp, c->f64 + (size_t)f * cap, c->blist, nb); MAC_COUNT(c);
       MAC_CUDA(cudaMemcpyAsync(dst, tmp, 8 * nc, cudaMemcpyDeviceToHost, st));
       MAC_CUDA(cudaStreamSynchronize(st));
     }
     uint8_t* t8 = (uint8_t*)c->z;
-    k_gather_bricks<uint8_t><<<g, 256, 0, st>>>(t8, c->flags, c->blist, nb);
+    k_gather_bricks<uint8_t><<<g, 256, 0, st>>>(t8, c->flags, c->blist, nb); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->flags, t8, nc, cudaMemcpyDeviceToHost, st));
     MAC_CUDA(cudaStreamSynchronize(st));
-    k_gather_bricks<uint8_t><<<g, 256, 0, st>>>(t8, c->type, c->blist, nb);
+    k_gather_bricks<uint8_t><<<g, 256, 0, st>>>(t8, c->type, c->blist, nb); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->type, t8, nc, cudaMemcpyDeviceToHost, st));
     MAC_CUDA(cudaStreamSynchronize(st));
     int32_t* tl = (int32_t*)c->q;
-    k_unpack_lay<<<g, 256, 0, st>>>(c->lay, c->blist, nb, t8, tl);
+    k_unpack_lay<<<g, 256, 0, st>>>(c->lay, c->blist, nb, t8, tl); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->exists, t8, nc, cudaMemcpyDeviceToHost, st));
     MAC_CUDA(cudaMemcpyAsync(s->layer, tl, 4 * nc, cudaMemcpyDeviceToHost, st));
   }
@@ -269,7 +333,7 @@ static int download(Ctx* c, mac_host_state* s) {
   int64_t chunk = (int64_t)(cap / 3);
   for (int64_t o = 0; o < np; o += chunk) {
     int64_t n = np - o < chunk ? np - o : chunk;
-    k_soa_to_aos<<<grid_for(n, 256), 256, 0, st>>>(c->pd, c->px + o, c->py + o, c->pz + o, n);
+    k_soa_to_aos<<<grid_for(n, 256), 256, 0, st>>>(c->pd, c->px + o, c->py + o, c->pz + o, n); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->pos + 3 * o, c->pd, 24 * n, cudaMemcpyDeviceToHost, st));
     MAC_CUDA(cudaStreamSynchronize(st));
   }
@@ -374,6 +438,45 @@ int mac_sync(void* ctx) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return MAC_ERR_INVALID;
   return mac::check(cudaStreamSynchronize(c->stream));
+}
+
+int mac_stream(void* ctx, void** stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !stream) return MAC_ERR_INVALID;
+  *stream = (void*)c->stream;
+  return MAC_OK;
+}
+
+int mac_launch_count(void* ctx, int64_t* count) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !count) return MAC_ERR_INVALID;
+  *count = c->launches;
+  return MAC_OK;
+}
+
+int mac_set_profiling(void* ctx, int on) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return MAC_ERR_INVALID;
+  if (on && !c->prof) c->prof = new (std::nothrow) mac::Prof();
+  if (!on) mac::prof_free(c);
+  return (on && !c->prof) ? MAC_ERR_OUT_OF_MEMORY : MAC_OK;
+}
+
+int mac_get_profile(void* ctx, double* ms, int64_t* count, int nphase) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !ms || !count || nphase <= 0) return MAC_ERR_INVALID;
+  mac::prof_resolve(c);
+  for (int i = 0; i < nphase; ++i) {
+    bool have = c->prof && i < mac::kPhases;
+    ms[i] = have ? c->prof->ms[i] : 0.0;
+    count[i] = have ? c->prof->n[i] : 0;
+  }
+  if (c->prof)
+    for (int i = 0; i < mac::kPhases; ++i) {
+      c->prof->ms[i] = 0;
+      c->prof->n[i] = 0;
+    }
+  return MAC_OK;
 }
 
 }  // extern "C"

@@ -66,6 +66,22 @@ struct Scalars {
   unsigned long long bad_reads;  // particles whose stencil touched a missing cell
 };
 
+// Phases timed with CUDA events when profiling is on (mac_set_profiling);
+// the order matches MAC_PHASE_* in include/mac_gpu.h.
+enum Phase : int {
+  PH_TOPOLOGY = 0,
+  PH_FORCES,
+  PH_SETUP,
+  PH_DIVERGENCE,
+  PH_SPMV,
+  PH_CGVEC,
+  PH_VCYCLE,
+  PH_GRADIENT,
+  PH_EXTRAPOLATE,
+  PH_MOVE,
+  kPhases
+};
+
 struct Params {
   double h[3], ih[3], ih2[3];
   double cfl, dt_min, dt_max, g;
@@ -131,8 +147,17 @@ struct Ctx {
   int* csc_off = nullptr;
   int* csc_ind = nullptr;
   double* csc_val = nullptr;
-  double* csc_vec = nullptr;   // [6][n]
+  double* csc_vec = nullptr;   // [7][n] + scalars
+  long long launches = 0;      // kernels launched by this context
+  struct Prof* prof = nullptr; // per-phase event timing (null when off)
 };
+
+void prof_begin(Ctx* c, int phase);
+void prof_end(Ctx* c, int phase);
+
+// Every kernel launch is followed by MAC_COUNT(c) so the context can report
+// how many of its kernels ran (mac_launch_count).
+#define MAC_COUNT(ctx) (++(ctx)->launches)
 
 // ---------------------------------------------------------------- helpers
 __host__ __device__ inline unsigned long long pack_key(int x, int y, int z) {

@@ -803,23 +803,25 @@ static void setup_weights(Ctx* c) {
   T* w1 = (T*)c->mg_w[1];
   T* w2 = (T*)c->mg_w[2];
   T* w3 = (T*)c->mg_w[3];
-  k_weights_l1<T><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->fmask, w1, ncap[1], c->dp);
-  k_weights_coarsen<T, 4><<<vec_grid(n), 256, 0, st>>>(c->blist, n, w1, ncap[1], w2, ncap[2]);
-  k_weights_coarsen<T, 2><<<vec_grid(n), 256, 0, st>>>(c->blist, n, w2, ncap[2], w3, ncap[3]);
-  k_weights_diag<T, 4><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1]);
-  k_weights_diag<T, 2><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2]);
-  k_weights_diag<T, 1><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3]);
+  k_weights_l1<T><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->fmask, w1, ncap[1], c->dp); MAC_COUNT(c);
+  k_weights_coarsen<T, 4><<<vec_grid(n), 256, 0, st>>>(c->blist, n, w1, ncap[1], w2, ncap[2]); MAC_COUNT(c);
+  k_weights_coarsen<T, 2><<<vec_grid(n), 256, 0, st>>>(c->blist, n, w2, ncap[2], w3, ncap[3]); MAC_COUNT(c);
+  k_weights_diag<T, 4><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1]); MAC_COUNT(c);
+  k_weights_diag<T, 2><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2]); MAC_COUNT(c);
+  k_weights_diag<T, 1><<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3]); MAC_COUNT(c);
 }
 
 int setup_system(Ctx* c) {
   cudaStream_t st = c->stream;
   int n = c->nlive_host;
-  k_zero_unknown<<<1, 1, 0, st>>>(c->ds);
+  prof_begin(c, PH_SETUP);
+  k_zero_unknown<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   if (n > 0) {
-    k_fmask<<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, c->lay, c->type, c->flags, c->fmask, c->ds);
+    k_fmask<<<vec_grid(n), 256, 0, st>>>(c->blist, n, c->nbr, c->lay, c->type, c->flags, c->fmask, c->ds); MAC_COUNT(c);
     if (c->mg_float) setup_weights<float>(c);
     else setup_weights<double>(c);
   }
+  prof_end(c, PH_SETUP);
   c->system_ready = true;
   return check(cudaGetLastError());
 }
@@ -847,26 +849,26 @@ static void vcycle(Ctx* c) {
   int g0 = vec_grid(n);
   int g1 = grid_for((int64_t)n * 64, 256), g2 = grid_for((int64_t)n * 8, 256), g3 = grid_for(n, 256);
   // down
-  k_pre0<T><<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, c->dp);
-  k_restrict0<T><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, r1, c->dp);
-  k_pre_l<T, 4><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, 2);
-  k_restrict_l<T, 4><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, r2, ncap[2]);
-  k_pre_l<T, 2><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, 2);
-  k_restrict_l<T, 2><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, r3, ncap[3]);
+  k_pre0<T><<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
+  k_restrict0<T><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
+  k_pre_l<T, 4><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, 2); MAC_COUNT(c);
+  k_restrict_l<T, 4><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, r2, ncap[2]); MAC_COUNT(c);
+  k_pre_l<T, 2><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, 2); MAC_COUNT(c);
+  k_restrict_l<T, 2><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, r3, ncap[3]); MAC_COUNT(c);
   // coarsest: Jacobi sweeps from zero
-  k_pre_l<T, 1><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3], r3, e3, 1);
+  k_pre_l<T, 1><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3], r3, e3, 1); MAC_COUNT(c);
   for (int s = 1; s < kCoarseSweeps; ++s) {
-    k_jacobi_l<T, 1, false><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3], r3, e3, nullptr, e3b);
+    k_jacobi_l<T, 1, false><<<g3, 256, 0, st>>>(c->blist, n, c->nbr, w3, ncap[3], r3, e3, nullptr, e3b); MAC_COUNT(c);
     T* t = e3; e3 = e3b; e3b = t;
   }
   // up
-  k_jacobi_l<T, 2, true><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, e3, e2b);
-  k_jacobi_l<T, 2, false><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2b, nullptr, e2);
-  k_jacobi_l<T, 4, true><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, e2, e1b);
-  k_jacobi_l<T, 4, false><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1b, nullptr, e1);
-  k_post0<T, true><<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp);
+  k_jacobi_l<T, 2, true><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2, e3, e2b); MAC_COUNT(c);
+  k_jacobi_l<T, 2, false><<<g2, 256, 0, st>>>(c->blist, n, c->nbr, w2, ncap[2], r2, e2b, nullptr, e2); MAC_COUNT(c);
+  k_jacobi_l<T, 4, true><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1, e2, e1b); MAC_COUNT(c);
+  k_jacobi_l<T, 4, false><<<g1, 256, 0, st>>>(c->blist, n, c->nbr, w1, ncap[1], r1, e1b, nullptr, e1); MAC_COUNT(c);
+  k_post0<T, true><<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp); MAC_COUNT(c);
   k_post0<T, false><<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
-                                        c->dp);
+                                        c->dp); MAC_COUNT(c);
 }
 
 // Jacobi preconditioner (MAC_SOLVER_CG_FP64): z = r / diag, with the r.z partials.
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(256) k_jacobi_prec(const int* __restrict__ bli
 static void precondition(Ctx* c) {
   if (c->prm.solver == MAC_SOLVER_CG_FP64) {
     int n = c->nlive_host;
-    k_jacobi_prec<<<vec_grid(n), 256, 0, c->stream>>>(c->blist, n, c->fmask, c->r, c->z, c->partial, c->dp);
+    k_jacobi_prec<<<vec_grid(n), 256, 0, c->stream>>>(c->blist, n, c->fmask, c->r, c->z, c->partial, c->dp); MAC_COUNT(c);
   } else if (c->mg_float) {
     vcycle<float>(c);
   } else {
@@ -912,35 +914,47 @@ int project(Ctx* c, int ib) {
   int warm = c->prm.warm_start ? 1 : 0;
   double rtol2 = c->prm.rtol * c->prm.rtol;
   // rhs (kept in b) and its norm
+  prof_begin(c, PH_DIVERGENCE);
   k_divergence<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, U[0], U[1], U[2], c->b, c->x, warm, c->partial,
-                                   c->dp);
-  k_fin_bnorm<<<1, 1024, 0, st>>>(c->partial, g0, c->ds);
+                                   c->dp); MAC_COUNT(c);
+  prof_end(c, PH_DIVERGENCE);
+  k_fin_bnorm<<<1, 1024, 0, st>>>(c->partial, g0, c->ds); MAC_COUNT(c);
   if (warm) {
-    k_residual<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->b, c->x, c->r, c->dp);
-    k_dot_rr<<<g0, 256, 0, st>>>(c->blist, n, c->r, c->partial);
-    k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, rtol2);
+    k_residual<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->b, c->x, c->r, c->dp); MAC_COUNT(c);
+    k_dot_rr<<<g0, 256, 0, st>>>(c->blist, n, c->r, c->partial); MAC_COUNT(c);
+    k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, rtol2); MAC_COUNT(c);
   } else {
-    k_copy_vec<<<g0, 256, 0, st>>>(c->blist, n, c->b, c->r);
+    k_copy_vec<<<g0, 256, 0, st>>>(c->blist, n, c->b, c->r); MAC_COUNT(c);
   }
+  prof_begin(c, PH_VCYCLE);
   precondition(c);
-  k_fin_beta<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, 1);
-  k_update_p<<<g0, 256, 0, st>>>(c->blist, n, c->z, c->pd, c->ds, 1);
+  prof_end(c, PH_VCYCLE);
+  k_fin_beta<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, 1); MAC_COUNT(c);
+  k_update_p<<<g0, 256, 0, st>>>(c->blist, n, c->z, c->pd, c->ds, 1); MAC_COUNT(c);
   int rc = check(cudaGetLastError());
   if (rc) return rc;
   int it = 0;
   int status = MAC_OK;
   while (true) {
-    k_spmv_dot<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->pd, c->q, c->partial, c->dp, c->ds);
-    k_fin_alpha<<<1, 1024, 0, st>>>(c->partial, g0, c->ds);
-    k_axpy<<<g0, 256, 0, st>>>(c->blist, n, c->x, c->r, c->pd, c->q, c->partial, c->ds);
-    k_fin_rr<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, rtol2, c->prm.max_iters);
+    prof_begin(c, PH_SPMV);
+    k_spmv_dot<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, c->pd, c->q, c->partial, c->dp, c->ds); MAC_COUNT(c);
+    prof_end(c, PH_SPMV);
+    prof_begin(c, PH_CGVEC);
+    k_fin_alpha<<<1, 1024, 0, st>>>(c->partial, g0, c->ds); MAC_COUNT(c);
+    k_axpy<<<g0, 256, 0, st>>>(c->blist, n, c->x, c->r, c->pd, c->q, c->partial, c->ds); MAC_COUNT(c);
+    k_fin_rr<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, rtol2, c->prm.max_iters); MAC_COUNT(c);
+    prof_end(c, PH_CGVEC);
     ++it;
     rc = read_scalars(c);
     if (rc) return rc;
     if (c->hs->done) break;
+    prof_begin(c, PH_VCYCLE);
     precondition(c);
-    k_fin_beta<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, 0);
-    k_update_p<<<g0, 256, 0, st>>>(c->blist, n, c->z, c->pd, c->ds, 0);
+    prof_end(c, PH_VCYCLE);
+    prof_begin(c, PH_CGVEC);
+    k_fin_beta<<<1, 1024, 0, st>>>(c->partial, g0, c->ds, 0); MAC_COUNT(c);
+    k_update_p<<<g0, 256, 0, st>>>(c->blist, n, c->z, c->pd, c->ds, 0); MAC_COUNT(c);
+    prof_end(c, PH_CGVEC);
   }
   double relres = c->hs->bnorm2 > 0 ? sqrt(c->hs->rr / c->hs->bnorm2) : 0.0;
   c->stats.iterations = c->hs->iters;
@@ -949,11 +963,13 @@ int project(Ctx* c, int ib) {
   c->stats.solves += 1;
   c->stats.unknowns = c->hs->nunknown;
   if (!(relres <= c->prm.rtol)) status = MAC_ERR_NOT_CONVERGED;
+  prof_begin(c, PH_GRADIENT);
   k_gradient<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->lay, c->type, c->flags, c->x, c->f64 + (size_t)PRES * cap,
-                                 U[0], U[1], U[2], c->dp);
+                                 U[0], U[1], U[2], c->dp); MAC_COUNT(c);
+  prof_end(c, PH_GRADIENT);
   if (c->prm.div_check) {
-    k_zero_div<<<1, 1, 0, st>>>(c->ds);
-    k_divmax<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, U[0], U[1], U[2], c->dp, c->ds);
+    k_zero_div<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+    k_divmax<<<g0, 256, 0, st>>>(c->blist, n, c->nbr, c->fmask, U[0], U[1], U[2], c->dp, c->ds); MAC_COUNT(c);
     rc = read_scalars(c);
     if (rc) return rc;
     unsigned long long bits = c->hs->div_bits;

@@ -34,7 +34,7 @@ static int step(Ctx* c) {
   if (ode && ode != MAC_ERR_NOT_CONVERGED) return ode;
   if ((rc = extrapolate(c))) return rc;
   if ((rc = move_particles(c))) return rc;
-  k_advance_time<<<1, 1, 0, c->stream>>>(c->ds);
+  k_advance_time<<<1, 1, 0, c->stream>>>(c->ds); MAC_COUNT(c);
   rc = check(cudaGetLastError());
   return rc ? rc : ode;
 }
@@ -124,9 +124,9 @@ static int csc_solve(Ctx* c, const double* hb, double* hx) {
   if (g > 1184) g = 1184;
   int rc = check(cudaMemcpyAsync(b, hb, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
   if (rc) return rc;
-  k_csc_diag<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, dinv);
+  k_csc_diag<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, dinv); MAC_COUNT(c);
   cudaMemsetAsync(scal, 0, 8 * 8, st);
-  k_csc_vec<<<g, 256, 0, st>>>(n, 0, b, x, r, z, p, q, dinv, scal, 0);
+  k_csc_vec<<<g, 256, 0, st>>>(n, 0, b, x, r, z, p, q, dinv, scal, 0); MAC_COUNT(c);
   double hs[8];
   cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
   if ((rc = check(cudaStreamSynchronize(st)))) return rc;
@@ -136,12 +136,12 @@ static int csc_solve(Ctx* c, const double* hb, double* hx) {
   double rr = bb;
   while (bb > 0 && it < c->prm.max_iters) {
     cudaMemsetAsync(scal, 0, 64, st);
-    k_csc_spmv<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, p, q, scal + 3, p);
+    k_csc_spmv<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, p, q, scal + 3, p); MAC_COUNT(c);
     cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
     if ((rc = check(cudaStreamSynchronize(st)))) return rc;
     double alpha = rz / hs[3];
-    k_csc_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, z, p, q, dinv, scal, alpha);
-    k_csc_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, z, p, q, dinv, scal, 0);
+    k_csc_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, z, p, q, dinv, scal, alpha); MAC_COUNT(c);
+    k_csc_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, z, p, q, dinv, scal, 0); MAC_COUNT(c);
     cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
     if ((rc = check(cudaStreamSynchronize(st)))) return rc;
     ++it;
@@ -149,7 +149,7 @@ static int csc_solve(Ctx* c, const double* hb, double* hx) {
     if (rr <= rtol * rtol * bb) break;
     double beta = hs[0] / rz;
     rz = hs[0];
-    k_csc_vec<<<g, 256, 0, st>>>(n, 3, b, x, r, z, p, q, dinv, scal, beta);
+    k_csc_vec<<<g, 256, 0, st>>>(n, 3, b, x, r, z, p, q, dinv, scal, beta); MAC_COUNT(c);
   }
   if ((rc = check(cudaMemcpyAsync(hx, x, 8 * (size_t)n, cudaMemcpyDeviceToHost, st)))) return rc;
   if ((rc = check(cudaStreamSynchronize(st)))) return rc;

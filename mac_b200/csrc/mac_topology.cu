@@ -422,11 +422,11 @@ __global__ void k_dt_finalize(Params P, Scalars* ds) {
 // ------------------------------------------------------------ drivers
 int rebuild_index(Ctx* c) {
   cudaStream_t st = c->stream;
-  k_hash_clear<<<grid_for(c->hcap, 256), 256, 0, st>>>(c->hkeys, c->hval, c->hcap);
-  k_hash_insert_live<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->ds);
-  k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds);
-  k_bbox_reset<<<1, 1, 0, st>>>(c->ds);
-  k_bbox<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->ds);
+  k_hash_clear<<<grid_for(c->hcap, 256), 256, 0, st>>>(c->hkeys, c->hval, c->hcap); MAC_COUNT(c);
+  k_hash_insert_live<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->ds); MAC_COUNT(c);
+  k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
+  k_bbox_reset<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+  k_bbox<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->ds); MAC_COUNT(c);
   c->system_ready = false;
   return check(cudaGetLastError());
 }
@@ -435,33 +435,33 @@ static void alloc_new(Ctx* c) {
   cudaStream_t st = c->stream;
   k_alloc_bricks<<<kTopoBlocks, 256, 0, st>>>(c->newslots, c->hkeys, c->hval, c->bkey, c->blist, c->freelist,
                                                c->lay, c->type, c->flags, c->f64,
-                                               (size_t)c->cap_bricks * kCells, c->cap_bricks, c->ds);
+                                               (size_t)c->cap_bricks * kCells, c->cap_bricks, c->ds); MAC_COUNT(c);
 }
 
 int topo_initialize(Ctx* c) {
-  k_initialize<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->lay, c->ds);
+  k_initialize<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->lay, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
 int topo_layer_initial(Ctx* c) {
   cudaStream_t st = c->stream;
   int g = kTopoBlocks * 2;
-  k_clear_note<<<1, 1, 0, st>>>(c->ds);
+  k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
-                                      c->cap_bricks, c->lay, c->type, c->ds, 0);
-  k_note_missing<<<1, 1, 0, st>>>(c->ds);
+                                      c->cap_bricks, c->lay, c->type, c->ds, 0); MAC_COUNT(c);
+  k_note_missing<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   alloc_new(c);
-  k_after_alloc<<<1, 1, 0, st>>>(c->ds);
+  k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
-                                      c->cap_bricks, c->lay, c->type, c->ds, 1);
-  k_clear_note<<<1, 1, 0, st>>>(c->ds);
+                                      c->cap_bricks, c->lay, c->type, c->ds, 1); MAC_COUNT(c);
+  k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   c->system_ready = false;
   return check(cudaGetLastError());
 }
 
 int topo_create_fluid(Ctx* c) {
   k_refill<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->bkey, c->lay, c->type, c->px, c->py, c->pz,
-                                                c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds);
+                                                c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -470,22 +470,23 @@ int topo_update_layer(Ctx* c) {
   int R = (c->dp.layer_max + 1 + 7) / 8;
   if (R < 1) R = 1;
   k_dilate<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->lay, c->hkeys, c->hval, c->hcap, c->newslots,
-                                         c->cap_bricks, R, c->ds);
+                                         c->cap_bricks, R, c->ds); MAC_COUNT(c);
   alloc_new(c);
-  k_after_alloc<<<1, 1, 0, st>>>(c->ds);
-  k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds);
-  for (int L = 1; L <= c->dp.layer_max; ++L)
-    k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, L, 0, c->ds);
-  k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, c->dp.layer_max + 1, 1, c->ds);
+  k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+  k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
+  for (int L = 1; L <= c->dp.layer_max; ++L) {
+    k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, L, 0, c->ds); MAC_COUNT(c);
+  }
+  k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, c->dp.layer_max + 1, 1, c->ds); MAC_COUNT(c);
   c->system_ready = false;
   return check(cudaGetLastError());
 }
 
 int topo_delete(Ctx* c) {
   cudaStream_t st = c->stream;
-  k_delete<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->lay, c->flags, c->alive, c->ds);
-  k_compact<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->blist2, c->freelist, c->alive, c->ds);
-  k_compact_done<<<1, 1, 0, st>>>(c->ds);
+  k_delete<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->lay, c->flags, c->alive, c->ds); MAC_COUNT(c);
+  k_compact<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->blist2, c->freelist, c->alive, c->ds); MAC_COUNT(c);
+  k_compact_done<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   int* t = c->blist;
   c->blist = c->blist2;
   c->blist2 = t;
@@ -496,10 +497,10 @@ int topo_delete(Ctx* c) {
 int topo_dt(Ctx* c) {
   cudaStream_t st = c->stream;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  k_cfl_reset<<<1, 1, 0, st>>>(c->ds);
+  k_cfl_reset<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_cfl<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->lay, c->type, c->f64 + U0X * cap, c->f64 + U0Y * cap,
-                                      c->f64 + U0Z * cap, c->dp, c->ds);
-  k_dt_finalize<<<1, 1, 0, st>>>(c->dp, c->ds);
+                                      c->f64 + U0Z * cap, c->dp, c->ds); MAC_COUNT(c);
+  k_dt_finalize<<<1, 1, 0, st>>>(c->dp, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -512,6 +513,7 @@ int topo_finish(Ctx* c) {
 int topology_rebuild(Ctx* c, bool first_init_order) {
   int rc;
   if (!first_init_order) ++c->seed;
+  prof_begin(c, PH_TOPOLOGY);
   if ((rc = topo_initialize(c))) return rc;
   if (first_init_order) {
     if ((rc = topo_create_fluid(c))) return rc;
@@ -524,6 +526,7 @@ int topology_rebuild(Ctx* c, bool first_init_order) {
   if ((rc = topo_delete(c))) return rc;
   if (!first_init_order)
     if ((rc = topo_dt(c))) return rc;
+  prof_end(c, PH_TOPOLOGY);
   return topo_finish(c);
 }
 

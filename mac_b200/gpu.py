@@ -60,7 +60,10 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_layer_initial_with_particle", "mac_create_fluid_particle", "mac_update_celltype_layer",
            "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
            "mac_pressure_project", "mac_rk2tvd", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
+           "mac_stream", "mac_launch_count", "mac_set_profiling", "mac_get_profile",
            "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean"]
+PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
+          "move"]
 
 _lib = None
 
@@ -93,6 +96,10 @@ def load(path: str = LIB_PATH):
     lib.mac_pressure_project.argtypes = [vp, ctypes.c_int]
     lib.mac_csc_factorize.argtypes = [vp, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_double)]
     lib.mac_csc_solve.argtypes = [vp, ctypes.c_int, _P(ctypes.c_double), _P(ctypes.c_double)]
+    lib.mac_stream.argtypes = [vp, _P(vp)]
+    lib.mac_launch_count.argtypes = [vp, _P(ctypes.c_int64)]
+    lib.mac_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.mac_get_profile.argtypes = [vp, _P(ctypes.c_double), _P(ctypes.c_int64), ctypes.c_int]
     _lib = lib
     return lib
 
@@ -165,6 +172,11 @@ class HostState:
         self.t, self.dt, self.step = s.params.t, s.params.dt, s.params.step
         return self
 
+    def nbytes(self) -> int:
+        """Bytes of the current state content (what one transfer moves)."""
+        nc = self.nbricks * BRICK_CELLS
+        return 12 * self.nbricks + nc * (1 + 8 * len(CELL_F64) + 1 + 1 + 4) + 24 * self.nparticles
+
     def c_struct(self) -> mac_host_state:
         h = mac_host_state()
         h.nbricks, h.nparticles = self.nbricks, self.nparticles
@@ -229,7 +241,8 @@ class Context:
             pass
 
     # ---- transfer
-    def upload(self, s: State, host: HostState | None = None):
+    def upload(self, s: State | None, host: HostState | None = None):
+        """Uploads a State, or the content already held in ``host``."""
         host = host or HostState(s.nbricks, s.nparticles).fill(s)
         self._host_in = host
         st = host.c_struct()
@@ -294,6 +307,27 @@ class Context:
 
     def sync(self):
         return self._check(self.lib.mac_sync(self.h), "mac_sync")
+
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.mac_stream(self.h, ctypes.byref(s)), "mac_stream")
+        return s.value or 0
+
+    def launches(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self.lib.mac_launch_count(self.h, ctypes.byref(n)), "mac_launch_count")
+        return n.value
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.mac_set_profiling(self.h, int(on)), "mac_set_profiling")
+
+    def profile(self) -> dict:
+        """Per-phase device milliseconds and region counts since the last call."""
+        n = len(PHASES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        self._check(self.lib.mac_get_profile(self.h, ms, cnt, n), "mac_get_profile")
+        return {PHASES[i]: (ms[i], cnt[i]) for i in range(n)}
 
     # ---- drop-in CSC solver
     def csc_solve(self, offset, indice, value, b):

@@ -219,6 +219,9 @@ static int run(int argc, char** argv) {
   mac_state_file st;
   if (mac_state_read(argv[2], &st) != 0) { fprintf(stderr, "cannot read %s\n", argv[2]); return 1; }
   int nrep = (argc > 4 && cmd != "csc") ? atoi(argv[4]) : 1;
+  // The relative residual of the stand-in solve (1e-14 for parity work; the
+  // throughput metric is quoted at 1e-8).
+  if (const char* rt = getenv("MAC_REF_RTOL")) g_cg_rtol = atof(rt);
 
   const int DIM = 3;
   typedef double type_data_value;
