@@ -184,6 +184,12 @@ static int create(const mac_params* p, Ctx** out) {
     c->dp.ih[i] = 1 / p->h[i];  // Inversible_Value::Inverse (src/Inversible_Value_Vect.h:9-16)
     c->dp.ih2[i] = c->dp.ih[i] * c->dp.ih[i];
   }
+  for (int az = 0; az < 3; ++az)
+    for (int ay = 0; ay < 3; ++ay)
+      for (int ax = 0; ax < 3; ++ax) {
+        double d = ax * c->dp.ih2[0] + ay * c->dp.ih2[1] + az * c->dp.ih2[2];
+        c->dp.dtab[ax + 3 * ay + 9 * az] = d > 0 ? 1.0 / d : 0.0;
+      }
   c->dp.cfl = p->cfl_factor;
   c->dp.dt_min = p->dt_min;
   c->dp.dt_max = p->dt_max;

@@ -62,7 +62,9 @@ struct Scalars {
   double rz, rz_new, pq, rr, bnorm2, alpha, beta;
   int32_t done;
   int32_t iters;
-  int32_t bbox[6];    // brick key bounds of the live set (min xyz, max xyz)
+  int32_t bbox[6];    // brick key bounds of the domain bricks (min xyz, max xyz)
+  int32_t ndom;       // bricks holding an in-domain cell
+  int32_t pad_;
   unsigned long long bad_reads;  // particles whose stencil touched a missing cell
 };
 
@@ -88,6 +90,23 @@ struct Params {
   int gaxis;     // 0..2
   int layer_max;
   int interp_sym;
+  // inverse diagonal of the level-0 operator by active faces per axis
+  // (index ax + 3 ay + 9 az, each 0..2); 0 when no face is active
+  double dtab[27];
+};
+
+// Dense grid over the bounding box of the domain bricks (one cell per brick).
+struct DenseGrid {
+  int x0, y0, z0, nx, ny, nz;
+  __host__ __device__ int64_t index(int bx, int by, int bz) const {
+    return (int64_t)(bx - x0) + (int64_t)nx * ((int64_t)(by - y0) + (int64_t)ny * (bz - z0));
+  }
+};
+
+constexpr int kMaxDense = 12;
+struct DenseDesc {
+  int nx, ny, nz;
+  int64_t n, off;
 };
 
 struct Ctx {
@@ -125,6 +144,7 @@ struct Ctx {
   double* r = nullptr;
   double* z = nullptr;
   double* pd = nullptr;       // search direction
+  double* pd2 = nullptr;      // its previous value (the update reads neighbours' old p)
   double* q = nullptr;
   double* partial = nullptr;  // per-block partial sums
   int64_t npartial = 0;
@@ -135,6 +155,15 @@ struct Ctx {
   void* mg_w[kLevels] = {};   // [4][cells]: left-face weights x,y,z and Dirichlet diagonal
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
+  int* dbl = nullptr;          // bricks holding an in-domain cell
+  int ndom_host = 0;
+  DenseGrid g3{};
+  DenseDesc dense[kMaxDense] = {};
+  int ndense = 0;
+  void* dense_buf = nullptr;   // dense levels: 9 arrays (e, e2, r, 6 weights) per cell
+  size_t dense_bytes = 0;
+  size_t dense_smem = 0;
+  int smem_optin = 0;
   // scalars
   Scalars* ds = nullptr;      // device
   Scalars* hs = nullptr;      // pinned host mirror
@@ -219,6 +248,63 @@ __device__ inline void atomic_max_nonneg(unsigned long long* a, double v) {
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 
+// Level-0 face classes of an in-domain cell: bit f (f = 2*axis + (sign > 0))
+// = interior coupling, bit 8+f = face counts in the diagonal, bit 15 = in domain.
+constexpr uint16_t kDomainBit = 0x8000;
+
+// Inverse-diagonal table index from the face classes: active faces on x + 3*(y) + 9*(z).
+__device__ inline int active_index(uint16_t m) {
+  return __popc((m >> 8) & 3u) + 3 * __popc((m >> 10) & 3u) + 9 * __popc((m >> 12) & 3u);
+}
+
+// Cell-index bases of the six face-neighbour bricks of brick b (x-, x+, y-,
+// y+, z-, z+), -1 when absent; called by the first six threads of a block.
+__device__ inline void load_face_bases(const int* __restrict__ nbr, int b, int64_t* sb) {
+  if (threadIdx.x < 6) {
+    const int idx[6] = {nbr_index(-1, 0, 0), nbr_index(1, 0, 0), nbr_index(0, -1, 0),
+                        nbr_index(0, 1, 0),  nbr_index(0, 0, -1), nbr_index(0, 0, 1)};
+    int nb = nbr[(size_t)b * kNbr + idx[threadIdx.x]];
+    sb[threadIdx.x] = nb < 0 ? -1 : (int64_t)nb * kCells;
+  }
+}
+
+// Index of the face-f neighbour of cell c (slot o of its brick), -1 if its brick is absent.
+__device__ inline int64_t nb0(const int64_t* sb, int64_t c, int o, int f) {
+  int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+  switch (f) {
+    case 0: return x > 0 ? c - 1 : (sb[0] < 0 ? -1 : sb[0] + o + 7);
+    case 1: return x < 7 ? c + 1 : (sb[1] < 0 ? -1 : sb[1] + o - 7);
+    case 2: return y > 0 ? c - 8 : (sb[2] < 0 ? -1 : sb[2] + o + 56);
+    case 3: return y < 7 ? c + 8 : (sb[3] < 0 ? -1 : sb[3] + o - 56);
+    case 4: return z > 0 ? c - 64 : (sb[4] < 0 ? -1 : sb[4] + o + 448);
+    default: return z < 7 ? c + 64 : (sb[5] < 0 ? -1 : sb[5] + o - 448);
+  }
+}
+
+// Sum over a 512-thread block (16 warps) of two values into partial[blockIdx.x]
+// and partial[gridDim.x + blockIdx.x].
+__device__ inline void block_sum512(double a, double b, double* partial) {
+  __shared__ double ra[16], rb[16];
+  for (int s = 16; s > 0; s >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, s);
+    b += __shfl_down_sync(0xffffffffu, b, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    ra[threadIdx.x >> 5] = a;
+    rb[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0, tb = 0;
+    for (int i = 0; i < 16; ++i) {
+      ta += ra[i];
+      tb += rb[i];
+    }
+    partial[blockIdx.x] = ta;
+    partial[gridDim.x + blockIdx.x] = tb;
+  }
+}
+
 inline int grid_for(int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   return (int)(g < 1 ? 1 : g);
@@ -245,5 +331,8 @@ int extrapolate(Ctx* c);
 int move_particles(Ctx* c);
 int alloc_solver(Ctx* c);
 void free_solver(Ctx* c);
+int mg_setup(Ctx* c);
+void mg_vcycle(Ctx* c);
+int mg_configure(Ctx* c);
 
 }  // namespace mac

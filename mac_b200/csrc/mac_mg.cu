@@ -1,0 +1,803 @@
+// Multigrid preconditioner of the pressure solve.
+//
+// Hierarchy (Galerkin products with piecewise-constant transfer, each level's
+// operator scaled by kCoarseScale; stored as three left-face weights, the
+// diagonal, its inverse and the Dirichlet part of the diagonal per cell):
+//   level 0  the fine cells of every brick that holds an in-domain cell
+//            (8^3 per brick; operator from the per-cell face classes),
+//   level 1  4^3 per brick, level 2  2^3 per brick (brick-local, neighbours
+//            through the brick neighbour table),
+//   level 3  one cell per brick on a dense grid over the bounding box of the
+//            domain bricks, levels 4.. dense coarsenings of it.
+// Smoother: weighted Jacobi (two sweeps before and after the coarse
+// correction); the levels from 4 down are solved by one thread block in
+// shared memory. Storage type T is double (plain form) or float (mixed form).
+#include <cstdio>
+#include <cstring>
+
+#include "mac_internal.cuh"
+
+namespace mac {
+
+constexpr double kOmega = 0.8;
+constexpr double kCoarseScale = 0.5;
+constexpr int kCoarsestSweeps = 40;
+
+// Level-1 parent of level-0 cell n (pool index).
+__device__ inline int64_t parent1(int64_t n) {
+  int o = (int)(n & 511);
+  return (n >> 9) * 64 + ((o & 7) >> 1) + 4 * (((o >> 3) & 7) >> 1) + 16 * ((o >> 6) >> 1);
+}
+
+// ---------------------------------------------------------------- level 0
+// Two Jacobi sweeps from zero, fused: e1 = w D^-1 r, e = e1 + w D^-1 (r - M e1)
+// = w D^-1 ((2 - w) r + sum_f ih2_f e1(n_f)).
+template <class T>
+__global__ void __launch_bounds__(512) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
+                                              const uint16_t* __restrict__ fmask, const double* __restrict__ r,
+                                              T* __restrict__ e, Params P) {
+  __shared__ int64_t sb[6];
+  int b = dbl[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  __syncthreads();
+  int o = threadIdx.x;
+  int64_t c = (int64_t)b * kCells + o;
+  uint16_t m = fmask[c];
+  if (!(m & kDomainBit)) {
+    e[c] = (T)0;
+    return;
+  }
+  double s = (2.0 - kOmega) * r[c];
+  for (int f = 0; f < 6; ++f) {
+    if (!(m & (1u << f))) continue;
+    int64_t n = nb0(sb, c, o, f);
+    s += P.ih2[f >> 1] * kOmega * P.dtab[active_index(fmask[n])] * r[n];
+  }
+  e[c] = (T)(kOmega * P.dtab[active_index(m)] * s);
+}
+
+// res = r - M e on the brick, summed over 2x2x2 children into level 1.
+template <class T>
+__global__ void __launch_bounds__(512) k0_restrict(const int* __restrict__ dbl, const int* __restrict__ nbr,
+                                                   const uint16_t* __restrict__ fmask, const double* __restrict__ r,
+                                                   const T* __restrict__ e, T* __restrict__ r1, Params P) {
+  __shared__ int64_t sb[6];
+  __shared__ double res[kCells];
+  int b = dbl[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  __syncthreads();
+  int o = threadIdx.x;
+  int64_t c = (int64_t)b * kCells + o;
+  uint16_t m = fmask[c];
+  double v = 0;
+  if (m & kDomainBit) {
+    double ec = (double)e[c];
+    double me = 0;
+    for (int f = 0; f < 6; ++f) {
+      if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * ec;
+      if (m & (1u << f)) me -= P.ih2[f >> 1] * (double)e[nb0(sb, c, o, f)];
+    }
+    v = r[c] - me;
+  }
+  res[o] = v;
+  __syncthreads();
+  if (o < 64) {
+    int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
+    int base = 2 * X + 16 * Y + 128 * Z;
+    double s = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] + res[base + 65] +
+               res[base + 72] + res[base + 73];
+    r1[(size_t)b * 64 + o] = (T)s;
+  }
+}
+
+// Post-smoothing at level 0. FIRST: ep = e + P e1 (coarse correction added on
+// the fly), out = ep + w D^-1 (r - M ep) into eout. Otherwise a plain sweep
+// writing the FP64 preconditioned residual z and the block's partial r.z.
+template <class T, bool FIRST>
+__global__ void __launch_bounds__(512) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
+                                               const uint16_t* __restrict__ fmask, const double* __restrict__ r,
+                                               const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
+                                               double* __restrict__ z, double* partial, Params P) {
+  __shared__ int64_t sb[6];
+  __shared__ double red[16];
+  int b = dbl[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  __syncthreads();
+  int o = threadIdx.x;
+  int64_t c = (int64_t)b * kCells + o;
+  uint16_t m = fmask[c];
+  double rz = 0;
+  if (!(m & kDomainBit)) {
+    if (FIRST) eout[c] = (T)0;
+    else z[c] = 0.0;
+  } else {
+    double epc = (double)e[c];
+    if (FIRST) epc += (double)e1[parent1(c)];
+    double me = 0;
+    for (int f = 0; f < 6; ++f) {
+      if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * epc;
+      if (m & (1u << f)) {
+        int64_t n = nb0(sb, c, o, f);
+        double en = (double)e[n];
+        if (FIRST) en += (double)e1[parent1(n)];
+        me -= P.ih2[f >> 1] * en;
+      }
+    }
+    double rc = r[c];
+    double out = epc + kOmega * P.dtab[active_index(m)] * (rc - me);
+    if (FIRST) {
+      eout[c] = (T)out;
+    } else {
+      z[c] = out;
+      rz = rc * out;
+    }
+  }
+  if (!FIRST) {
+    for (int s = 16; s > 0; s >>= 1) rz += __shfl_down_sync(0xffffffffu, rz, s);
+    if ((o & 31) == 0) red[o >> 5] = rz;
+    __syncthreads();
+    if (o == 0) {
+      double t = 0;
+      for (int i = 0; i < 16; ++i) t += red[i];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+// ------------------------------------------------------- levels 1, 2 (bricks)
+template <int D>
+__device__ inline int64_t lidx(const int* __restrict__ nbr, int b, int x, int y, int z) {
+  int dx = x < 0 ? -1 : (x >= D ? 1 : 0);
+  int dy = y < 0 ? -1 : (y >= D ? 1 : 0);
+  int dz = z < 0 ? -1 : (z >= D ? 1 : 0);
+  int nb = ((dx | dy | dz) == 0) ? b : nbr[(size_t)b * kNbr + nbr_index(dx, dy, dz)];
+  if (nb < 0) return -1;
+  return (int64_t)nb * (D * D * D) + (x - D * dx) + D * (y - D * dy) + D * D * (z - D * dz);
+}
+
+// Weights w: 6 slots of ncap entries: [0..2] left faces, [3] diagonal, [4] inverse, [5] Dirichlet part.
+template <class T, int D>
+__device__ inline double apply_l(const T* __restrict__ e, const T* __restrict__ w, size_t ncap,
+                                 const int* __restrict__ nbr, int b, int x, int y, int z, size_t i, double ec) {
+  double s = (double)w[3 * ncap + i] * ec;
+  for (int a = 0; a < 3; ++a) {
+    double wl = (double)w[a * ncap + i];
+    int p[3] = {x, y, z};
+    p[a] -= 1;
+    if (wl != 0) s -= wl * (double)e[lidx<D>(nbr, b, p[0], p[1], p[2])];
+    p[a] += 2;
+    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
+    if (n >= 0) {
+      double wr = (double)w[a * ncap + n];
+      if (wr != 0) s -= wr * (double)e[n];
+    }
+  }
+  return s;
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+                                              const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
+                                              T* __restrict__ e) {
+  constexpr int N = D * D * D;
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * N) return;
+  int b = dbl[g / N];
+  int o = (int)(g % N);
+  size_t i = (size_t)b * N + o;
+  double dinv = (double)w[4 * ncap + i];
+  if (dinv == 0) {
+    e[i] = (T)0;
+    return;
+  }
+  int x = o % D, y = (o / D) % D, z = o / (D * D);
+  double s = (2.0 - kOmega) * (double)r[i];
+  for (int a = 0; a < 3; ++a) {
+    double wl = (double)w[a * ncap + i];
+    int p[3] = {x, y, z};
+    p[a] -= 1;
+    if (wl != 0) {
+      int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
+      s += wl * kOmega * (double)w[4 * ncap + n] * (double)r[n];
+    }
+    p[a] += 2;
+    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
+    if (n >= 0) {
+      double wr = (double)w[a * ncap + n];
+      if (wr != 0) s += wr * kOmega * (double)w[4 * ncap + n] * (double)r[n];
+    }
+  }
+  e[i] = (T)(kOmega * dinv * s);
+}
+
+// Residual of a brick level summed over children: D = 4 writes level 2
+// (brick-local), D = 2 writes the dense level 3 at the brick's position.
+template <class T, int D>
+__global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+                                                   const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
+                                                   const T* __restrict__ r, const T* __restrict__ e, T* __restrict__ rc,
+                                                   DenseGrid g3) {
+  constexpr int H = D / 2;
+  constexpr int N = D * D * D;
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * H * H * H) return;
+  int b = dbl[g / (H * H * H)];
+  int o = (int)(g % (H * H * H));
+  int X = o % H, Y = (o / H) % H, Z = o / (H * H);
+  double s = 0;
+  for (int k = 0; k < 8; ++k) {
+    int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+    size_t i = (size_t)b * N + x + D * y + D * D * z;
+    if ((double)w[4 * ncap + i] == 0) continue;
+    s += (double)r[i] - apply_l<T, D>(e, w, ncap, nbr, b, x, y, z, i, (double)e[i]);
+  }
+  if (D == 2) rc[g3.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])] = (T)s;
+  else rc[(size_t)b * H * H * H + o] = (T)s;
+}
+
+// One Jacobi sweep at a brick level, optionally adding the coarse correction
+// first (D = 4: from level 2 bricks; D = 2: from the dense level 3).
+template <class T, int D, bool WITH_COARSE>
+__global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+                                                 const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
+                                                 const T* __restrict__ r, const T* __restrict__ e,
+                                                 const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3) {
+  constexpr int N = D * D * D;
+  constexpr int H = D / 2;
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * N) return;
+  int b = dbl[g / N];
+  int o = (int)(g % N);
+  size_t i = (size_t)b * N + o;
+  double dinv = (double)w[4 * ncap + i];
+  if (dinv == 0) {
+    eout[i] = (T)0;
+    return;
+  }
+  int x = o % D, y = (o / D) % D, z = o / (D * D);
+  auto ev = [&](int64_t n) -> double {
+    double v = (double)e[n];
+    if (WITH_COARSE) {
+      int nb = (int)(n / N);
+      int no = (int)(n % N);
+      if (D == 2) {
+        v += (double)ec[g3.index(bkey[3 * nb], bkey[3 * nb + 1], bkey[3 * nb + 2])];
+      } else {
+        int xx = no % D, yy = (no / D) % D, zz = no / (D * D);
+        v += (double)ec[(size_t)nb * H * H * H + (xx >> 1) + H * (yy >> 1) + H * H * (zz >> 1)];
+      }
+    }
+    return v;
+  };
+  double ecc = ev((int64_t)i);
+  double s = (double)w[3 * ncap + i] * ecc;
+  for (int a = 0; a < 3; ++a) {
+    double wl = (double)w[a * ncap + i];
+    int p[3] = {x, y, z};
+    p[a] -= 1;
+    if (wl != 0) s -= wl * ev(lidx<D>(nbr, b, p[0], p[1], p[2]));
+    p[a] += 2;
+    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
+    if (n >= 0) {
+      double wr = (double)w[a * ncap + n];
+      if (wr != 0) s -= wr * ev(n);
+    }
+  }
+  eout[i] = (T)(ecc + kOmega * dinv * ((double)r[i] - s));
+}
+
+// ------------------------------------------------------------ dense levels
+// Dense level view: arrays of n cells, weights in 6 slots.
+template <class T>
+struct DView {
+  int nx, ny, nz;
+  int64_t n;
+  T* e;
+  T* e2;
+  T* r;
+  T* w;  // [6][n]
+  __device__ int64_t at(int x, int y, int z) const { return x + (int64_t)nx * (y + (int64_t)ny * z); }
+};
+
+template <class T>
+__device__ inline double dense_apply(const DView<T>& L, const T* e, int64_t i, int x, int y, int z, double ec) {
+  int64_t n = L.n;
+  double s = (double)L.w[3 * n + i] * ec;
+  int c[3] = {x, y, z};
+  int dim[3] = {L.nx, L.ny, L.nz};
+  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  for (int a = 0; a < 3; ++a) {
+    double wl = (double)L.w[a * n + i];
+    if (wl != 0 && c[a] > 0) s -= wl * (double)e[i - stride[a]];
+    if (c[a] + 1 < dim[a]) {
+      double wr = (double)L.w[a * n + i + stride[a]];
+      if (wr != 0) s -= wr * (double)e[i + stride[a]];
+    }
+  }
+  return s;
+}
+
+// Device-wide dense kernels for level 3.
+template <class T>
+__global__ void kd_pre(DView<T> L) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  int64_t n = L.n;
+  double dinv = (double)L.w[4 * n + i];
+  if (dinv == 0) {
+    L.e[i] = (T)0;
+    return;
+  }
+  int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+  int c[3] = {x, y, z};
+  int dim[3] = {L.nx, L.ny, L.nz};
+  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  double s = (2.0 - kOmega) * (double)L.r[i];
+  for (int a = 0; a < 3; ++a) {
+    double wl = (double)L.w[a * n + i];
+    if (wl != 0 && c[a] > 0) s += wl * kOmega * (double)L.w[4 * n + i - stride[a]] * (double)L.r[i - stride[a]];
+    if (c[a] + 1 < dim[a]) {
+      double wr = (double)L.w[a * n + i + stride[a]];
+      if (wr != 0) s += wr * kOmega * (double)L.w[4 * n + i + stride[a]] * (double)L.r[i + stride[a]];
+    }
+  }
+  L.e[i] = (T)(kOmega * dinv * s);
+}
+
+template <class T>
+__global__ void kd_restrict(DView<T> F, DView<T> C) {
+  int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= C.n) return;
+  int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
+  double s = 0;
+  for (int k = 0; k < 8; ++k) {
+    int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+    if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
+    int64_t i = F.at(x, y, z);
+    if ((double)F.w[4 * F.n + i] == 0) continue;
+    s += (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+  }
+  C.r[I] = (T)s;
+}
+
+template <class T, bool WITH_COARSE>
+__global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__ eout, DView<T> C) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  int64_t n = L.n;
+  double dinv = (double)L.w[4 * n + i];
+  if (dinv == 0) {
+    eout[i] = (T)0;
+    return;
+  }
+  int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+  auto ev = [&](int64_t j, int xx, int yy, int zz) -> double {
+    double v = (double)ein[j];
+    if (WITH_COARSE) v += (double)C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
+    return v;
+  };
+  int c[3] = {x, y, z};
+  int dim[3] = {L.nx, L.ny, L.nz};
+  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  double ec = ev(i, x, y, z);
+  double s = (double)L.w[3 * n + i] * ec;
+  for (int a = 0; a < 3; ++a) {
+    int p[3] = {x, y, z};
+    double wl = (double)L.w[a * n + i];
+    if (wl != 0 && c[a] > 0) {
+      p[a] = c[a] - 1;
+      s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
+    }
+    if (c[a] + 1 < dim[a]) {
+      double wr = (double)L.w[a * n + i + stride[a]];
+      if (wr != 0) {
+        p[a] = c[a] + 1;
+        s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
+      }
+    }
+  }
+  eout[i] = (T)(ec + kOmega * dinv * ((double)L.r[i] - s));
+}
+
+// ------------------------------------------- coarse V-cycle in one block
+// Levels lo..hi-1 of the dense hierarchy, staged in shared memory when they
+// fit (else worked on in global memory); __syncthreads separates the sweeps.
+template <class T>
+struct DenseSet {
+  DView<T> L[kMaxDense];
+  int lo, hi;
+};
+
+template <class T>
+__device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView<T>* C, bool first) {
+  for (int64_t i = threadIdx.x; i < L.n; i += blockDim.x) {
+    int64_t n = L.n;
+    double dinv = (double)L.w[4 * n + i];
+    if (dinv == 0) {
+      eout[i] = (T)0;
+      continue;
+    }
+    if (first) {
+      eout[i] = (T)(kOmega * dinv * (double)L.r[i]);
+      continue;
+    }
+    int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+    auto ev = [&](int64_t j, int xx, int yy, int zz) -> double {
+      double v = (double)ein[j];
+      if (C) v += (double)C->e[C->at(xx >> 1, yy >> 1, zz >> 1)];
+      return v;
+    };
+    int c[3] = {x, y, z};
+    int dim[3] = {L.nx, L.ny, L.nz};
+    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    double ec = ev(i, x, y, z);
+    double s = (double)L.w[3 * n + i] * ec;
+    for (int a = 0; a < 3; ++a) {
+      int p[3] = {x, y, z};
+      double wl = (double)L.w[a * n + i];
+      if (wl != 0 && c[a] > 0) {
+        p[a] = c[a] - 1;
+        s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
+      }
+      if (c[a] + 1 < dim[a]) {
+        double wr = (double)L.w[a * n + i + stride[a]];
+        if (wr != 0) {
+          p[a] = c[a] + 1;
+          s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
+        }
+      }
+    }
+    eout[i] = (T)(ec + kOmega * dinv * ((double)L.r[i] - s));
+  }
+}
+
+template <class T>
+__device__ void blk_restrict(const DView<T>& F, const DView<T>& C) {
+  for (int64_t I = threadIdx.x; I < C.n; I += blockDim.x) {
+    int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
+    double s = 0;
+    for (int k = 0; k < 8; ++k) {
+      int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+      if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
+      int64_t i = F.at(x, y, z);
+      if ((double)F.w[4 * F.n + i] == 0) continue;
+      s += (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+    }
+    C.r[I] = (T)s;
+  }
+}
+
+template <class T>
+__device__ void blk_copy(T* dst, const T* src, int64_t n) {
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DenseSet<T> S = G;
+  if (use_smem) {
+    T* p = (T*)smem_raw;
+    for (int l = G.lo; l < G.hi; ++l) {
+      DView<T>& d = S.L[l];
+      int64_t n = d.n;
+      d.e = p;
+      d.e2 = p + n;
+      d.r = p + 2 * n;
+      d.w = p + 3 * n;
+      p += 9 * n;
+      blk_copy(d.w, G.L[l].w, 6 * n);
+      if (l == G.lo) blk_copy(d.r, G.L[l].r, n);
+    }
+    __syncthreads();
+  }
+  // down
+  for (int l = S.lo; l < S.hi - 1; ++l) {
+    DView<T>& L = S.L[l];
+    blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
+    __syncthreads();
+    blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+    __syncthreads();
+    T* t = L.e; L.e = L.e2; L.e2 = t;
+    blk_restrict(L, S.L[l + 1]);
+    __syncthreads();
+  }
+  // coarsest: Jacobi sweeps from zero
+  {
+    DView<T>& L = S.L[S.hi - 1];
+    blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
+    __syncthreads();
+    for (int s = 1; s < kCoarsestSweeps; ++s) {
+      blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+      __syncthreads();
+      T* t = L.e; L.e = L.e2; L.e2 = t;
+    }
+  }
+  // up
+  for (int l = S.hi - 2; l >= S.lo; --l) {
+    DView<T>& L = S.L[l];
+    blk_jacobi(L, L.e, L.e2, &S.L[l + 1], false);
+    __syncthreads();
+    blk_jacobi(L, L.e2, L.e, (const DView<T>*)nullptr, false);
+    __syncthreads();
+  }
+  if (use_smem) {
+    blk_copy(G.L[G.lo].e, S.L[G.lo].e, S.L[G.lo].n);
+  } else if (S.L[G.lo].e != G.L[G.lo].e) {
+    __syncthreads();
+    blk_copy(G.L[G.lo].e, S.L[G.lo].e, S.L[G.lo].n);
+  }
+}
+
+// ------------------------------------------------------------ weights setup
+// Level-1 weights from the level-0 face classes (Galerkin, piecewise constant).
+template <class T>
+__global__ void kw_l1(const int* __restrict__ dbl, int nd, const uint16_t* __restrict__ fmask, T* w, size_t ncap1,
+                      Params P) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * 64) return;
+  int b = dbl[g >> 6];
+  int o = (int)(g & 63);
+  int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
+  double wl[3] = {0, 0, 0}, dd = 0;
+  for (int k = 0; k < 8; ++k) {
+    int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+    uint16_t m = fmask[(size_t)b * kCells + x + 8 * y + 64 * z];
+    if (!(m & kDomainBit)) continue;
+    for (int f = 0; f < 6; ++f)
+      if ((m & (1u << (8 + f))) && !(m & (1u << f))) dd += P.ih2[f >> 1];
+    int lc[3] = {k & 1, (k >> 1) & 1, k >> 2};
+    for (int a = 0; a < 3; ++a)
+      if (lc[a] == 0 && (m & (1u << (2 * a)))) wl[a] += P.ih2[a];
+  }
+  size_t i = (size_t)b * 64 + o;
+  for (int a = 0; a < 3; ++a) w[a * ncap1 + i] = (T)(kCoarseScale * wl[a]);
+  w[5 * ncap1 + i] = (T)(kCoarseScale * dd);
+}
+
+// Brick level D -> D/2 (D = 4), or D = 2 -> dense level 3 at the brick position.
+template <class T, int D>
+__global__ void kw_coarsen(const int* __restrict__ dbl, int nd, const int* __restrict__ bkey, const T* __restrict__ wf,
+                           size_t ncapf, T* wc, size_t ncapc, DenseGrid g3) {
+  constexpr int H = D / 2;
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * H * H * H) return;
+  int b = dbl[g / (H * H * H)];
+  int o = (int)(g % (H * H * H));
+  int X = o % H, Y = (o / H) % H, Z = o / (H * H);
+  double wl[3] = {0, 0, 0}, dd = 0;
+  for (int k = 0; k < 8; ++k) {
+    int lc[3] = {k & 1, (k >> 1) & 1, k >> 2};
+    size_t fi = (size_t)b * D * D * D + (2 * X + lc[0]) + D * (2 * Y + lc[1]) + D * D * (2 * Z + lc[2]);
+    dd += (double)wf[5 * ncapf + fi];
+    for (int a = 0; a < 3; ++a)
+      if (lc[a] == 0) wl[a] += (double)wf[a * ncapf + fi];
+  }
+  size_t i = D == 2 ? (size_t)g3.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])
+                    : (size_t)b * H * H * H + o;
+  for (int a = 0; a < 3; ++a) wc[a * ncapc + i] = (T)(kCoarseScale * wl[a]);
+  wc[5 * ncapc + i] = (T)(kCoarseScale * dd);
+}
+
+template <class T, int D>
+__global__ void kw_diag(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr, T* w, size_t ncap) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nd * D * D * D) return;
+  int b = dbl[g / (D * D * D)];
+  int o = (int)(g % (D * D * D));
+  int x = o % D, y = (o / D) % D, z = o / (D * D);
+  size_t i = (size_t)b * D * D * D + o;
+  double d = (double)w[5 * ncap + i];
+  for (int a = 0; a < 3; ++a) {
+    d += (double)w[a * ncap + i];
+    int p[3] = {x, y, z};
+    p[a] += 1;
+    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
+    if (n >= 0) d += (double)w[a * ncap + n];
+  }
+  w[3 * ncap + i] = (T)d;
+  w[4 * ncap + i] = d > 0 ? (T)(1.0 / d) : (T)0;
+}
+
+template <class T>
+__global__ void kwd_coarsen(DView<T> F, DView<T> C) {
+  int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= C.n) return;
+  int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
+  double wl[3] = {0, 0, 0}, dd = 0;
+  for (int k = 0; k < 8; ++k) {
+    int lc[3] = {k & 1, (k >> 1) & 1, k >> 2};
+    int x = 2 * X + lc[0], y = 2 * Y + lc[1], z = 2 * Z + lc[2];
+    if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
+    int64_t i = F.at(x, y, z);
+    dd += (double)F.w[5 * F.n + i];
+    for (int a = 0; a < 3; ++a)
+      if (lc[a] == 0) wl[a] += (double)F.w[a * F.n + i];
+  }
+  for (int a = 0; a < 3; ++a) C.w[a * C.n + I] = (T)(kCoarseScale * wl[a]);
+  C.w[5 * C.n + I] = (T)(kCoarseScale * dd);
+}
+
+template <class T>
+__global__ void kwd_diag(DView<T> L) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.n) return;
+  int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+  int c[3] = {x, y, z};
+  int dim[3] = {L.nx, L.ny, L.nz};
+  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  double d = (double)L.w[5 * L.n + i];
+  for (int a = 0; a < 3; ++a) {
+    d += (double)L.w[a * L.n + i];
+    if (c[a] + 1 < dim[a]) d += (double)L.w[a * L.n + i + stride[a]];
+  }
+  L.w[3 * L.n + i] = (T)d;
+  L.w[4 * L.n + i] = d > 0 ? (T)(1.0 / d) : (T)0;
+}
+
+// ------------------------------------------------------------ host side
+template <class T>
+static DView<T> dview(Ctx* c, int l) {
+  DView<T> v;
+  const DenseDesc& d = c->dense[l];
+  v.nx = d.nx;
+  v.ny = d.ny;
+  v.nz = d.nz;
+  v.n = d.n;
+  T* base = (T*)c->dense_buf;
+  v.e = base + 9 * d.off;
+  v.e2 = v.e + d.n;
+  v.r = v.e + 2 * d.n;
+  v.w = v.e + 3 * d.n;
+  return v;
+}
+
+// Lays out the dense levels for the current bounding box (level 3 = one cell
+// per brick) and grows the buffer when needed.
+static int dense_layout(Ctx* c) {
+  int* bb = c->hs->bbox;
+  int nx = bb[3] - bb[0] + 1, ny = bb[4] - bb[1] + 1, nz = bb[5] - bb[2] + 1;
+  if (nx < 1 || ny < 1 || nz < 1) nx = ny = nz = 1;
+  c->g3.x0 = bb[0];
+  c->g3.y0 = bb[1];
+  c->g3.z0 = bb[2];
+  c->g3.nx = nx;
+  c->g3.ny = ny;
+  c->g3.nz = nz;
+  int nl = 0;
+  int64_t off = 0;
+  while (nl < kMaxDense) {
+    DenseDesc& d = c->dense[nl];
+    d.nx = nx;
+    d.ny = ny;
+    d.nz = nz;
+    d.n = (int64_t)nx * ny * nz;
+    d.off = off;
+    off += d.n;
+    ++nl;
+    if (d.n <= 64 || (nx <= 2 && ny <= 2 && nz <= 2)) break;
+    nx = (nx + 1) / 2;
+    ny = (ny + 1) / 2;
+    nz = (nz + 1) / 2;
+  }
+  c->ndense = nl;
+  size_t ts = c->mg_float ? 4 : 8;
+  size_t need = (size_t)off * 9 * ts;
+  if (need > c->dense_bytes) {
+    cudaFree(c->dense_buf);
+    c->dense_buf = nullptr;
+    c->dense_bytes = 0;
+    int rc = check(cudaMalloc(&c->dense_buf, need + need / 4));
+    if (rc) return rc;
+    c->dense_bytes = need + need / 4;
+  }
+  // smem staging of the block-solved levels (1..): 9 arrays per cell
+  int64_t cells = 0;
+  for (int l = 1; l < nl; ++l) cells += c->dense[l].n;
+  c->dense_smem = (size_t)cells * 9 * ts;
+  return check(cudaMemsetAsync(c->dense_buf, 0, (size_t)off * 9 * ts, c->stream));
+}
+
+template <class T>
+static int mg_setup_t(Ctx* c) {
+  cudaStream_t st = c->stream;
+  int nd = c->ndom_host;
+  int rc = dense_layout(c);
+  if (rc) return rc;
+  size_t ncap1 = (size_t)c->cap_bricks * 64, ncap2 = (size_t)c->cap_bricks * 8;
+  T* w1 = (T*)c->mg_w[1];
+  T* w2 = (T*)c->mg_w[2];
+  DView<T> d3 = dview<T>(c, 0);
+  int g1 = grid_for((int64_t)nd * 64, 256), g2 = grid_for((int64_t)nd * 8, 256), g3 = grid_for(nd, 256);
+  // Bricks without a domain cell keep zero weights, so stencils never couple to them.
+  rc = check(cudaMemsetAsync(w1, 0, ncap1 * 6 * sizeof(T), st));
+  if (!rc) rc = check(cudaMemsetAsync(w2, 0, ncap2 * 6 * sizeof(T), st));
+  if (rc) return rc;
+  kw_l1<T><<<g1, 256, 0, st>>>(c->dbl, nd, c->fmask, w1, ncap1, c->dp); MAC_COUNT(c);
+  kw_coarsen<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->bkey, w1, ncap1, w2, ncap2, c->g3); MAC_COUNT(c);
+  kw_coarsen<T, 2><<<g3, 256, 0, st>>>(c->dbl, nd, c->bkey, w2, ncap2, d3.w, (size_t)d3.n, c->g3); MAC_COUNT(c);
+  for (int l = 0; l + 1 < c->ndense; ++l) {
+    DView<T> F = dview<T>(c, l), C = dview<T>(c, l + 1);
+    kwd_coarsen<T><<<grid_for(C.n, 256), 256, 0, st>>>(F, C); MAC_COUNT(c);
+  }
+  kw_diag<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1); MAC_COUNT(c);
+  kw_diag<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2); MAC_COUNT(c);
+  for (int l = 0; l < c->ndense; ++l) {
+    DView<T> L = dview<T>(c, l);
+    kwd_diag<T><<<grid_for(L.n, 256), 256, 0, st>>>(L); MAC_COUNT(c);
+  }
+  return check(cudaGetLastError());
+}
+
+int mg_setup(Ctx* c) { return c->mg_float ? mg_setup_t<float>(c) : mg_setup_t<double>(c); }
+
+template <class T>
+static void mg_vcycle_t(Ctx* c) {
+  cudaStream_t st = c->stream;
+  int nd = c->ndom_host;
+  size_t ncap1 = (size_t)c->cap_bricks * 64, ncap2 = (size_t)c->cap_bricks * 8;
+  T* e0 = (T*)c->mg_e[0];
+  T* e0b = (T*)c->mg_e2[0];
+  T* e1 = (T*)c->mg_e[1];
+  T* e1b = (T*)c->mg_e2[1];
+  T* e2 = (T*)c->mg_e[2];
+  T* e2b = (T*)c->mg_e2[2];
+  T* r1 = (T*)c->mg_r[1];
+  T* r2 = (T*)c->mg_r[2];
+  T* w1 = (T*)c->mg_w[1];
+  T* w2 = (T*)c->mg_w[2];
+  DView<T> d3 = dview<T>(c, 0);
+  int g1 = grid_for((int64_t)nd * 64, 256), g2 = grid_for((int64_t)nd * 8, 256);
+  DenseGrid G = c->g3;
+  // down
+  k0_pre<T><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
+  k0_restrict<T><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
+  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1); MAC_COUNT(c);
+  kl_restrict<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G); MAC_COUNT(c);
+  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2); MAC_COUNT(c);
+  kl_restrict<T, 2><<<grid_for(nd, 256), 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G); MAC_COUNT(c);
+  // dense level 3 on the device, levels 4.. in one block
+  if (c->ndense > 1) {
+    DView<T> d4 = dview<T>(c, 1);
+    kd_pre<T><<<grid_for(d3.n, 256), 256, 0, st>>>(d3); MAC_COUNT(c);
+    kd_restrict<T><<<grid_for(d4.n, 256), 256, 0, st>>>(d3, d4); MAC_COUNT(c);
+    DenseSet<T> S;
+    for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
+    S.lo = 1;
+    S.hi = c->ndense;
+    int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
+    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem); MAC_COUNT(c);
+    kd_jacobi<T, true><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e, d3.e2, d4); MAC_COUNT(c);
+    kd_jacobi<T, false><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e2, d3.e, d4); MAC_COUNT(c);
+  } else {
+    DenseSet<T> S;
+    S.L[0] = d3;
+    S.lo = 0;
+    S.hi = 1;
+    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0); MAC_COUNT(c);
+  }
+  // up
+  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G); MAC_COUNT(c);
+  kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G); MAC_COUNT(c);
+  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G); MAC_COUNT(c);
+  kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G); MAC_COUNT(c);
+  k0_post<T, true><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp); MAC_COUNT(c);
+  k0_post<T, false><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
+                                         c->dp); MAC_COUNT(c);
+}
+
+void mg_vcycle(Ctx* c) {
+  if (c->mg_float) mg_vcycle_t<float>(c);
+  else mg_vcycle_t<double>(c);
+}
+
+int mg_configure(Ctx* c) {
+  int dev = c->prm.device, optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  c->smem_optin = optin;
+  int rc = check(cudaFuncSetAttribute(kd_coarse_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  if (!rc) rc = check(cudaFuncSetAttribute(kd_coarse_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  return rc;
+}
+
+}  // namespace mac

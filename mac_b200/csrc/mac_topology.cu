@@ -425,8 +425,6 @@ int rebuild_index(Ctx* c) {
   k_hash_clear<<<grid_for(c->hcap, 256), 256, 0, st>>>(c->hkeys, c->hval, c->hcap); MAC_COUNT(c);
   k_hash_insert_live<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->ds); MAC_COUNT(c);
   k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
-  k_bbox_reset<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
-  k_bbox<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->ds); MAC_COUNT(c);
   c->system_ready = false;
   return check(cudaGetLastError());
 }
