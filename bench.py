@@ -162,6 +162,22 @@ def sample_desc(steps, procs):
             f"solver stand-in FP64 Jacobi-CG at rel-resid 1e-8")
 
 
+# ------------------------------------------------------------- ranks
+def reduce_over_ranks(seconds: float, count: float, device) -> tuple:
+    """Replicas only: every rank runs its own world; the job's time is the
+    slowest rank's, its work the sum over ranks. Returns (max seconds, summed
+    count); a no-op without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return seconds, count
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([float(count)], dtype=torch.float64, device=device)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(n.item())
+
+
 # ------------------------------------------------------------- our arm
 def roofline_models(ctx_stats, prof, np_count, n_exist):
     """Achieved GB/s per phase from algorithmic bytes (every array element a
@@ -235,17 +251,7 @@ def run_ours(args, rank, world, local_rank):
     prof = ctx.profile()
     ctx.set_profiling(False)
     st = ctx.stats()
-    sec = ms / 1e3
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([sec], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
-        n = torch.tensor([float(fluid_steps)], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        total_fluid_steps = float(n.item())
-    else:
-        total_fluid_steps = float(fluid_steps)
+    sec, total_fluid_steps = reduce_over_ranks(ms / 1e3, fluid_steps, f"cuda:{dev}")
     value = total_fluid_steps / sec
 
     # e2e through the C-ABI with pinned host buffers: upload, step, download per step
@@ -270,15 +276,7 @@ def run_ours(args, rank, world, local_rank):
         bo += host.nbytes()
     a1.record(stream)
     a1.synchronize()
-    e2e_sec = a0.elapsed_time(a1) / 1e3
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_sec], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_sec = float(t.item())
-        n = torch.tensor([float(f2)], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        f2 = float(n.item())
+    e2e_sec, f2 = reduce_over_ranks(a0.elapsed_time(a1) / 1e3, f2, f"cuda:{dev}")
     e2e = {"value": f2 / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": bi // e2e_steps,
            "d2h_bytes_per_step": bo // e2e_steps, "steps": e2e_steps}
 

@@ -5,6 +5,8 @@
 // The library is compiled with -fmad=false and every expression keeps the
 // reference's operation order, so these kernels reproduce the reference's
 // FP64 results bit for bit from the same input state.
+#include <utility>
+
 #include "mac_internal.cuh"
 
 namespace mac {
@@ -281,20 +283,59 @@ __device__ inline int64_t pcell(const PBase& pb, const int* __restrict__ nbr, co
   return (int64_t)b * kCells + (kx & 7) + 8 * (ky & 7) + 64 * (kz & 7);
 }
 
-__device__ inline void get_speed(const double* pos, double* out, const PBase& pb, const int* nbr,
-                                 const unsigned long long* hk, const int* hv, int64_t hcap, const int8_t* lay,
-                                 const double* const* U, const Params& P, int sym, int* bad) {
+// Field read through the brick table (any cell; used for particles whose
+// stencil leaves the staged region and for unbinned particles).
+struct GlobalField {
+  PBase pb;
+  const int* nbr;
+  const unsigned long long* hk;
+  const int* hv;
+  int64_t hcap;
+  const int8_t* lay;
+  const double* const* U;
+  __device__ double u(int k, int kx, int ky, int kz, int* bad) const {
+    int64_t ci = pcell(pb, nbr, hk, hv, hcap, kx, ky, kz);
+    if (ci < 0 || lay[ci] == kMissing) *bad = 1;
+    return ci < 0 ? 0.0 : U[k][ci];
+  }
+};
+
+// Field read from a shared-memory copy of the 12^3 region around a brick
+// (its cells with a two-cell halo), falling back to the brick table outside it.
+constexpr int kStage = 12;
+constexpr int kStageCells = kStage * kStage * kStage;
+struct StagedField {
+  const double* s;        // [3][kStageCells]
+  const uint8_t* miss;    // [kStageCells] 1 = cell missing
+  int ox, oy, oz;         // cell key of stage slot (0,0,0)
+  GlobalField g;
+  __device__ double u(int k, int kx, int ky, int kz, int* bad) const {
+    unsigned x = (unsigned)(kx - ox), y = (unsigned)(ky - oy), z = (unsigned)(kz - oz);
+    if (x < (unsigned)kStage && y < (unsigned)kStage && z < (unsigned)kStage) {
+      int i = (int)(x + kStage * (y + kStage * z));
+      if (miss[i]) *bad = 1;
+      return s[k * kStageCells + i];
+    }
+    return g.u(k, kx, ky, kz, bad);
+  }
+};
+
+template <class F>
+__device__ inline void get_speed(const double* pos, double* out, const F& field, const Params& P, int sym, int* bad) {
   double pd[3];
   int k0[3];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
     pd[i] = pos[i] * P.ih[i];
     k0[i] = (int)lround(pd[i]);
     pd[i] -= k0[i];
   }
+#pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (!sym) pd[k] += 0.5;
     int key[3];
     double d[3];
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
       if (j != k && pd[j] < 0) {
         key[j] = k0[j] - 1;
@@ -305,6 +346,7 @@ __device__ inline void get_speed(const double* pos, double* out, const PBase& pb
       }
     }
     double w0[3], w1[3];
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
       if (sym && i == k) {
         w0[i] = 0.5 - d[i];
@@ -315,11 +357,8 @@ __device__ inline void get_speed(const double* pos, double* out, const PBase& pb
       }
     }
     double u[8];
-    for (int n = 0; n < 8; ++n) {
-      int64_t ci = pcell(pb, nbr, hk, hv, hcap, key[0] + (n >> 2), key[1] + ((n >> 1) & 1), key[2] + (n & 1));
-      if (ci < 0 || lay[ci] == kMissing) *bad = 1;
-      u[n] = ci < 0 ? 0.0 : U[k][ci];
-    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) u[n] = field.u(k, key[0] + (n >> 2), key[1] + ((n >> 1) & 1), key[2] + (n & 1), bad);
     // u[(X<<2)|(Y<<1)|Z]
     double l00 = w0[2] * u[0] + w1[2] * u[1];
     double l01 = w0[2] * u[2] + w1[2] * u[3];
@@ -332,62 +371,221 @@ __device__ inline void get_speed(const double* pos, double* out, const PBase& pb
   }
 }
 
-// Algorithms_Move_Particles::Do + Policy_Advance_Ode_RungeKutta::AdvanceSolveODE
-// (src/Algorithms_Move_Particles.h:29-32, src/Policy_Advance_ODE_RungeKutta.h:15-27).
-__global__ void __launch_bounds__(256) k_move(double* px, double* py, double* pz, int64_t np, const int* __restrict__ nbr,
-                                              const unsigned long long* __restrict__ hk, const int* __restrict__ hv,
-                                              int64_t hcap, const int8_t* __restrict__ lay, const double* __restrict__ ux,
-                                              const double* __restrict__ uy, const double* __restrict__ uz, Params P,
-                                              const Scalars* __restrict__ ds, unsigned long long* bad_count) {
+// Policy_Advance_Ode_RungeKutta::AdvanceSolveODE (src/Policy_Advance_ODE_RungeKutta.h:15-27):
+// classic RK4 in this accumulation order.
+template <class F>
+__device__ inline void rk4(double* pos, const F& field, const Params& P, double dt, int* bad) {
+  double res[3], k[3], a[3], v[3];
+  for (int i = 0; i < 3; ++i) res[i] = pos[i];
+  get_speed(pos, v, field, P, P.interp_sym, bad);
+  for (int i = 0; i < 3; ++i) {
+    k[i] = dt * v[i];
+    res[i] += (1. / 6.) * k[i];
+  }
+  for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
+  get_speed(a, v, field, P, P.interp_sym, bad);
+  for (int i = 0; i < 3; ++i) {
+    k[i] = dt * v[i];
+    res[i] += (1. / 3.) * k[i];
+  }
+  for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
+  get_speed(a, v, field, P, P.interp_sym, bad);
+  for (int i = 0; i < 3; ++i) {
+    k[i] = dt * v[i];
+    res[i] += (1. / 3.) * k[i];
+  }
+  for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i];
+  get_speed(a, v, field, P, P.interp_sym, bad);
+  for (int i = 0; i < 3; ++i) {
+    k[i] = dt * v[i];
+    res[i] += (1. / 6.) * k[i];
+  }
+  for (int i = 0; i < 3; ++i) pos[i] = res[i];
+}
+
+// Particles are binned by the brick of their cell each step (counting sort,
+// order inside a brick unspecified; every particle moves independently, so
+// the order changes no result).
+__global__ void k_bin_count(const double* __restrict__ px, const double* __restrict__ py,
+                            const double* __restrict__ pz, int64_t np, Params P,
+                            const unsigned long long* __restrict__ hk, const int* __restrict__ hv, int64_t hcap,
+                            int* pbrick, int* bcount, int stray) {
+  // Whole warps iterate together so the lanes that share a brick can add
+  // their count with one atomic (the array is mostly sorted by brick already).
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < np; q0 += stride) {
+    int64_t q = q0 + (threadIdx.x & 31);
+    int b = -2;
+    if (q < np) {
+      int bx = fdiv8((int)lround(px[q] * P.ih[0]));
+      int by = fdiv8((int)lround(py[q] * P.ih[1]));
+      int bz = fdiv8((int)lround(pz[q] * P.ih[2]));
+      b = hash_find(hk, hv, hcap, pack_key(bx, by, bz));
+      if (b < 0) b = stray;
+      pbrick[q] = b;
+    }
+    unsigned peers = __match_any_sync(0xffffffffu, b);
+    int leader = __ffs(peers) - 1;
+    if (b >= 0 && (int)(threadIdx.x & 31) == leader) atomicAdd(&bcount[b], __popc(peers));
+  }
+}
+
+// Exclusive scan of n counts (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) k_bin_scan(const int* __restrict__ cnt, int64_t* __restrict__ off, int n) {
+  __shared__ int64_t part[1024];
+  int per = (n + 1023) / 1024;
+  int lo = threadIdx.x * per, hi = lo + per < n ? lo + per : n;
+  int64_t s = 0;
+  for (int i = lo; i < hi; ++i) s += cnt[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    int64_t v = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int64_t base = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = lo; i < hi; ++i) {
+    off[i] = base;
+    base += cnt[i];
+  }
+  if (threadIdx.x == 1023) off[n] = part[1023];
+}
+
+__global__ void k_bin_scatter(const double* __restrict__ px, const double* __restrict__ py,
+                              const double* __restrict__ pz, int64_t np, const int* __restrict__ pbrick,
+                              const int64_t* __restrict__ off, int* cursor, double* qx, double* qy, double* qz) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int lane = threadIdx.x & 31;
+  for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < np; q0 += stride) {
+    int64_t q = q0 + lane;
+    int b = q < np ? pbrick[q] : -2;
+    unsigned peers = __match_any_sync(0xffffffffu, b);
+    int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(&cursor[b], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (b >= 0) {
+      int64_t pos = off[b] + base + __popc(peers & ((1u << lane) - 1));
+      qx[pos] = px[q];
+      qy[pos] = py[q];
+      qz[pos] = pz[q];
+    }
+  }
+}
+
+// Algorithms_Move_Particles::Do (src/Algorithms_Move_Particles.h:29-32) for
+// the particles binned to one brick: the brick's speed field with a two-cell
+// halo (12^3 cells from up to 27 bricks) is staged in shared memory and the
+// 96 stencil reads of each particle's RK4 come from there.
+__global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, double* pz,
+                                                     const int* __restrict__ blist, const int* __restrict__ bkey,
+                                                     const int* __restrict__ nbr, const int64_t* __restrict__ off,
+                                                     const unsigned long long* __restrict__ hk, const int* __restrict__ hv,
+                                                     int64_t hcap, const int8_t* __restrict__ lay,
+                                                     const double* __restrict__ ux, const double* __restrict__ uy,
+                                                     const double* __restrict__ uz, Params P,
+                                                     const Scalars* __restrict__ ds, unsigned long long* bad_count) {
+  __shared__ double s[3 * kStageCells];
+  __shared__ uint8_t miss[kStageCells];
+  __shared__ int sn[kNbr];
+  int b = blist[blockIdx.x];
+  int64_t p0 = off[b], p1 = off[b + 1];
+  if (p0 == p1) return;
+  if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
+  __syncthreads();
+  const double* U[3] = {ux, uy, uz};
+  int ox = bkey[3 * b] * 8 - 2, oy = bkey[3 * b + 1] * 8 - 2, oz = bkey[3 * b + 2] * 8 - 2;
+  for (int i = threadIdx.x; i < kStageCells; i += blockDim.x) {
+    int x = i % kStage, y = (i / kStage) % kStage, z = i / (kStage * kStage);
+    int lx = x - 2, ly = y - 2, lz = z - 2;  // local coordinates in brick b, -2..9
+    int dx = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), dy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0), dz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
+    int nb = sn[nbr_index(dx, dy, dz)];
+    if (nb < 0) {
+      s[i] = s[kStageCells + i] = s[2 * kStageCells + i] = 0.0;
+      miss[i] = 1;
+    } else {
+      int64_t gi = (int64_t)nb * kCells + (lx - 8 * dx) + 8 * (ly - 8 * dy) + 64 * (lz - 8 * dz);
+      s[i] = U[0][gi];
+      s[kStageCells + i] = U[1][gi];
+      s[2 * kStageCells + i] = U[2][gi];
+      miss[i] = lay[gi] == kMissing;
+    }
+  }
+  __syncthreads();
+  const double dt = ds->dt;
+  PBase pb;
+  pb.key[0] = bkey[3 * b];
+  pb.key[1] = bkey[3 * b + 1];
+  pb.key[2] = bkey[3 * b + 2];
+  pb.b = b;
+  StagedField f{s, miss, ox, oy, oz, GlobalField{pb, nbr, hk, hv, hcap, lay, U}};
+  int bad = 0;
+  for (int64_t q = p0 + threadIdx.x; q < p1; q += blockDim.x) {
+    double pos[3] = {px[q], py[q], pz[q]};
+    rk4(pos, f, P, dt, &bad);
+    px[q] = pos[0];
+    py[q] = pos[1];
+    pz[q] = pos[2];
+  }
+  if (bad) atomicAdd(bad_count, 1ull);
+}
+
+// Particles whose cell has no brick (never the case in a valid state; the
+// reference would create the cell) move through the brick table.
+__global__ void __launch_bounds__(256) k_move_stray(double* px, double* py, double* pz, const int64_t* __restrict__ off,
+                                                    int stray, const int* __restrict__ nbr,
+                                                    const unsigned long long* __restrict__ hk, const int* __restrict__ hv,
+                                                    int64_t hcap, const int8_t* __restrict__ lay,
+                                                    const double* __restrict__ ux, const double* __restrict__ uy,
+                                                    const double* __restrict__ uz, Params P,
+                                                    const Scalars* __restrict__ ds, unsigned long long* bad_count) {
   const double dt = ds->dt;
   const double* U[3] = {ux, uy, uz};
   int bad = 0;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < np; q += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t q = off[stray] + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < off[stray + 1];
+       q += (int64_t)gridDim.x * blockDim.x) {
     double pos[3] = {px[q], py[q], pz[q]};
     PBase pb;
     for (int i = 0; i < 3; ++i) pb.key[i] = fdiv8((int)lround(pos[i] * P.ih[i]));
     pb.b = hash_find(hk, hv, hcap, pack_key(pb.key[0], pb.key[1], pb.key[2]));
-    double res[3], k[3], a[3], v[3];
-    for (int i = 0; i < 3; ++i) res[i] = pos[i];
-    get_speed(pos, v, pb, nbr, hk, hv, hcap, lay, U, P, P.interp_sym, &bad);
-    for (int i = 0; i < 3; ++i) {
-      k[i] = dt * v[i];
-      res[i] += (1. / 6.) * k[i];
-    }
-    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
-    get_speed(a, v, pb, nbr, hk, hv, hcap, lay, U, P, P.interp_sym, &bad);
-    for (int i = 0; i < 3; ++i) {
-      k[i] = dt * v[i];
-      res[i] += (1. / 3.) * k[i];
-    }
-    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i] * 0.5;
-    get_speed(a, v, pb, nbr, hk, hv, hcap, lay, U, P, P.interp_sym, &bad);
-    for (int i = 0; i < 3; ++i) {
-      k[i] = dt * v[i];
-      res[i] += (1. / 3.) * k[i];
-    }
-    for (int i = 0; i < 3; ++i) a[i] = pos[i] + k[i];
-    get_speed(a, v, pb, nbr, hk, hv, hcap, lay, U, P, P.interp_sym, &bad);
-    for (int i = 0; i < 3; ++i) {
-      k[i] = dt * v[i];
-      res[i] += (1. / 6.) * k[i];
-    }
-    px[q] = res[0];
-    py[q] = res[1];
-    pz[q] = res[2];
+    GlobalField f{pb, nbr, hk, hv, hcap, lay, U};
+    rk4(pos, f, P, dt, &bad);
+    px[q] = pos[0];
+    py[q] = pos[1];
+    pz[q] = pos[2];
   }
   if (bad) atomicAdd(bad_count, 1ull);
 }
 
 int move_particles(Ctx* c) {
-  if (c->np_host == 0) return MAC_OK;
+  if (c->np_host == 0 || c->nlive_host == 0) return MAC_OK;
+  cudaStream_t st = c->stream;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  int g = grid_for(c->np_host, 256);
+  int64_t np = c->np_host;
+  int stray = (int)c->cap_bricks;
+  int g = grid_for(np, 256);
   if (g > 148 * 16) g = 148 * 16;
   unsigned long long* bad = &c->ds->bad_reads;
   prof_begin(c, PH_MOVE);
-  k_move<<<g, 256, 0, c->stream>>>(c->px, c->py, c->pz, c->np_host, c->nbr, c->hkeys, c->hval, c->hcap, c->lay,
-                                   c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap, c->dp, c->ds, bad); MAC_COUNT(c);
+  int rc = check(cudaMemsetAsync(c->bcount, 0, sizeof(int) * (c->cap_bricks + 1), st));
+  if (!rc) rc = check(cudaMemsetAsync(c->bcursor, 0, sizeof(int) * (c->cap_bricks + 1), st));
+  if (rc) return rc;
+  k_bin_count<<<g, 256, 0, st>>>(c->px, c->py, c->pz, np, c->dp, c->hkeys, c->hval, c->hcap, c->pbrick, c->bcount,
+                                 stray); MAC_COUNT(c);
+  k_bin_scan<<<1, 1024, 0, st>>>(c->bcount, c->boff, stray + 1); MAC_COUNT(c);
+  k_bin_scatter<<<g, 256, 0, st>>>(c->px, c->py, c->pz, np, c->pbrick, c->boff, c->bcursor, c->px2, c->py2,
+                                   c->pz2); MAC_COUNT(c);
+  std::swap(c->px, c->px2);
+  std::swap(c->py, c->py2);
+  std::swap(c->pz, c->pz2);
+  k_move_binned<<<c->nlive_host, 256, 0, st>>>(c->px, c->py, c->pz, c->blist, c->bkey, c->nbr, c->boff, c->hkeys,
+                                               c->hval, c->hcap, c->lay, c->f64 + U0X * cap, c->f64 + U0Y * cap,
+                                               c->f64 + U0Z * cap, c->dp, c->ds, bad); MAC_COUNT(c);
+  k_move_stray<<<4, 256, 0, st>>>(c->px, c->py, c->pz, c->boff, stray, c->nbr, c->hkeys, c->hval, c->hcap, c->lay,
+                                  c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap, c->dp, c->ds,
+                                  bad); MAC_COUNT(c);
   prof_end(c, PH_MOVE);
   return check(cudaGetLastError());
 }

@@ -160,6 +160,8 @@ static void free_all(Ctx* c) {
   cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
+  cudaFree(c->px2); cudaFree(c->py2); cudaFree(c->pz2); cudaFree(c->pbrick);
+  cudaFree(c->bcount); cudaFree(c->bcursor); cudaFree(c->boff);
   cudaFree(c->ds);
   if (c->hs) cudaFreeHost(c->hs);
   cudaFree(c->csc_off); cudaFree(c->csc_ind); cudaFree(c->csc_val); cudaFree(c->csc_vec);
@@ -223,6 +225,13 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->py, c->cap_particles));
   A(dalloc(&c->pz, c->cap_particles));
   A(dalloc(&c->pending, c->cap_pending));
+  A(dalloc(&c->px2, c->cap_particles));
+  A(dalloc(&c->py2, c->cap_particles));
+  A(dalloc(&c->pz2, c->cap_particles));
+  A(dalloc(&c->pbrick, c->cap_particles));
+  A(dalloc(&c->bcount, c->cap_bricks + 1));
+  A(dalloc(&c->bcursor, c->cap_bricks + 1));
+  A(dalloc(&c->boff, c->cap_bricks + 2));
   A(dalloc(&c->ds, 1));
   if (rc == MAC_OK) A(check(cudaMallocHost((void**)&c->hs, sizeof(Scalars))));
   if (rc == MAC_OK) A(alloc_solver(c));

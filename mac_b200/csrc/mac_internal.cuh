@@ -137,6 +137,13 @@ struct Ctx {
   double* py = nullptr;
   double* pz = nullptr;
   int64_t* pending = nullptr; // particle indices waiting for a brick
+  double* px2 = nullptr;      // binned copy (swapped with px each move)
+  double* py2 = nullptr;
+  double* pz2 = nullptr;
+  int* pbrick = nullptr;      // brick of each particle's cell
+  int* bcount = nullptr;      // [cap+1] particles per brick (last: no brick)
+  int* bcursor = nullptr;     // [cap+1]
+  int64_t* boff = nullptr;    // [cap+2] bin offsets
   // pressure system and solver
   uint16_t* fmask = nullptr;  // [cap*512] face classes of the level-0 operator
   double* x = nullptr;        // solution (pressure in domain)
@@ -281,10 +288,17 @@ __device__ inline int64_t nb0(const int64_t* sb, int64_t c, int o, int f) {
   }
 }
 
-// Sum over a 512-thread block (16 warps) of two values into partial[blockIdx.x]
-// and partial[gridDim.x + blockIdx.x].
-__device__ inline void block_sum512(double a, double b, double* partial) {
-  __shared__ double ra[16], rb[16];
+// Level-0 brick kernels: one block of kBT threads per brick, kCPT cells per
+// thread (slots threadIdx.x + kBT*k), so every thread keeps several
+// independent load chains in flight.
+constexpr int kBT = 128;
+constexpr int kCPT = kCells / kBT;
+
+// Sum over an NT-thread block of two values into partial[blockIdx.x] and
+// partial[gridDim.x + blockIdx.x] (fixed order).
+template <int NT>
+__device__ inline void block_sum(double a, double b, double* partial) {
+  __shared__ double ra[NT / 32], rb[NT / 32];
   for (int s = 16; s > 0; s >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, s);
     b += __shfl_down_sync(0xffffffffu, b, s);
@@ -296,7 +310,7 @@ __device__ inline void block_sum512(double a, double b, double* partial) {
   __syncthreads();
   if (threadIdx.x == 0) {
     double ta = 0, tb = 0;
-    for (int i = 0; i < 16; ++i) {
+    for (int i = 0; i < NT / 32; ++i) {
       ta += ra[i];
       tb += rb[i];
     }

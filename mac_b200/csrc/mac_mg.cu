@@ -33,32 +33,36 @@ __device__ inline int64_t parent1(int64_t n) {
 // Two Jacobi sweeps from zero, fused: e1 = w D^-1 r, e = e1 + w D^-1 (r - M e1)
 // = w D^-1 ((2 - w) r + sum_f ih2_f e1(n_f)).
 template <class T>
-__global__ void __launch_bounds__(512) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                               const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                               T* __restrict__ e, Params P) {
   __shared__ int64_t sb[6];
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
-  uint16_t m = fmask[c];
-  if (!(m & kDomainBit)) {
-    e[c] = (T)0;
-    return;
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    uint16_t m = fmask[c];
+    double out = 0;
+    if (m & kDomainBit) {
+      double s = (2.0 - kOmega) * r[c];
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (!(m & (1u << f))) continue;
+        int64_t n = nb0(sb, c, o, f);
+        s += P.ih2[f >> 1] * kOmega * P.dtab[active_index(fmask[n])] * r[n];
+      }
+      out = kOmega * P.dtab[active_index(m)] * s;
+    }
+    e[c] = (T)out;
   }
-  double s = (2.0 - kOmega) * r[c];
-  for (int f = 0; f < 6; ++f) {
-    if (!(m & (1u << f))) continue;
-    int64_t n = nb0(sb, c, o, f);
-    s += P.ih2[f >> 1] * kOmega * P.dtab[active_index(fmask[n])] * r[n];
-  }
-  e[c] = (T)(kOmega * P.dtab[active_index(m)] * s);
 }
 
 // res = r - M e on the brick, summed over 2x2x2 children into level 1.
 template <class T>
-__global__ void __launch_bounds__(512) k0_restrict(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P) {
   __shared__ int64_t sb[6];
@@ -66,21 +70,26 @@ __global__ void __launch_bounds__(512) k0_restrict(const int* __restrict__ dbl, 
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
-  uint16_t m = fmask[c];
-  double v = 0;
-  if (m & kDomainBit) {
-    double ec = (double)e[c];
-    double me = 0;
-    for (int f = 0; f < 6; ++f) {
-      if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * ec;
-      if (m & (1u << f)) me -= P.ih2[f >> 1] * (double)e[nb0(sb, c, o, f)];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    uint16_t m = fmask[c];
+    double v = 0;
+    if (m & kDomainBit) {
+      double ec = (double)e[c];
+      double me = 0;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * ec;
+        if (m & (1u << f)) me -= P.ih2[f >> 1] * (double)e[nb0(sb, c, o, f)];
+      }
+      v = r[c] - me;
     }
-    v = r[c] - me;
+    res[o] = v;
   }
-  res[o] = v;
   __syncthreads();
+  int o = threadIdx.x;
   if (o < 64) {
     int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
     int base = 2 * X + 16 * Y + 128 * Z;
@@ -94,26 +103,29 @@ __global__ void __launch_bounds__(512) k0_restrict(const int* __restrict__ dbl, 
 // the fly), out = ep + w D^-1 (r - M ep) into eout. Otherwise a plain sweep
 // writing the FP64 preconditioned residual z and the block's partial r.z.
 template <class T, bool FIRST>
-__global__ void __launch_bounds__(512) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P) {
   __shared__ int64_t sb[6];
-  __shared__ double red[16];
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
-  uint16_t m = fmask[c];
   double rz = 0;
-  if (!(m & kDomainBit)) {
-    if (FIRST) eout[c] = (T)0;
-    else z[c] = 0.0;
-  } else {
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    uint16_t m = fmask[c];
+    if (!(m & kDomainBit)) {
+      if (FIRST) eout[c] = (T)0;
+      else z[c] = 0.0;
+      continue;
+    }
     double epc = (double)e[c];
     if (FIRST) epc += (double)e1[parent1(c)];
     double me = 0;
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * epc;
       if (m & (1u << f)) {
@@ -129,19 +141,10 @@ __global__ void __launch_bounds__(512) k0_post(const int* __restrict__ dbl, cons
       eout[c] = (T)out;
     } else {
       z[c] = out;
-      rz = rc * out;
+      rz += rc * out;
     }
   }
-  if (!FIRST) {
-    for (int s = 16; s > 0; s >>= 1) rz += __shfl_down_sync(0xffffffffu, rz, s);
-    if ((o & 31) == 0) red[o >> 5] = rz;
-    __syncthreads();
-    if (o == 0) {
-      double t = 0;
-      for (int i = 0; i < 16; ++i) t += red[i];
-      partial[blockIdx.x] = t;
-    }
-  }
+  if (!FIRST) block_sum<kBT>(rz, 0.0, partial);
 }
 
 // ------------------------------------------------------- levels 1, 2 (bricks)
@@ -750,8 +753,8 @@ static void mg_vcycle_t(Ctx* c) {
   int g1 = grid_for((int64_t)nd * 64, 256), g2 = grid_for((int64_t)nd * 8, 256);
   DenseGrid G = c->g3;
   // down
-  k0_pre<T><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
-  k0_restrict<T><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
+  k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
+  k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
   kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1); MAC_COUNT(c);
   kl_restrict<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G); MAC_COUNT(c);
   kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2); MAC_COUNT(c);
@@ -781,8 +784,8 @@ static void mg_vcycle_t(Ctx* c) {
   kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G); MAC_COUNT(c);
   kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G); MAC_COUNT(c);
   kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G); MAC_COUNT(c);
-  k0_post<T, true><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp); MAC_COUNT(c);
-  k0_post<T, false><<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
+  k0_post<T, true><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp); MAC_COUNT(c);
+  k0_post<T, false><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
                                          c->dp); MAC_COUNT(c);
 }
 

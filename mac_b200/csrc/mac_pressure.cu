@@ -164,7 +164,7 @@ __global__ void k_setup_reset(Scalars* ds) {
 // Divergence (Policy_Divergence::Get_Divergence, src/Policy_Divergence.h:20-29)
 // of speed buffer ib into rhs = -div (the right-hand side of M x = -div) and
 // the block's partial |div|^2; x starts at 0 or, warm, at the cell pressure.
-__global__ void __launch_bounds__(512) k_divergence(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                     const uint16_t* __restrict__ fmask, const double* __restrict__ ux,
                                                     const double* __restrict__ uy, const double* __restrict__ uz,
                                                     const double* __restrict__ pres, double* __restrict__ rhs,
@@ -174,16 +174,20 @@ __global__ void __launch_bounds__(512) k_divergence(const int* __restrict__ dbl,
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
   double bb = 0;
-  if (!(fmask[c] & kDomainBit)) {
-    rhs[c] = 0.0;
-    x[c] = 0.0;
-    r[c] = 0.0;
-  } else {
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    if (!(fmask[c] & kDomainBit)) {
+      rhs[c] = 0.0;
+      x[c] = 0.0;
+      r[c] = 0.0;
+      continue;
+    }
     const double* U[3] = {ux, uy, uz};
     double d = 0;
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
       d -= U[i][c] * P.ih[i];
       int64_t n = nb0(sb, c, o, 2 * i + 1);
@@ -192,9 +196,9 @@ __global__ void __launch_bounds__(512) k_divergence(const int* __restrict__ dbl,
     rhs[c] = -d;
     r[c] = -d;
     x[c] = warm ? pres[c] : 0.0;
-    bb = d * d;
+    bb += d * d;
   }
-  block_sum512(bb, 0.0, partial);
+  block_sum<kBT>(bb, 0.0, partial);
 }
 
 __device__ inline double apply0(const double* __restrict__ v, const uint16_t* __restrict__ fmask, const int64_t* sb,
@@ -209,7 +213,7 @@ __device__ inline double apply0(const double* __restrict__ v, const uint16_t* __
 }
 
 // r = rhs - M x for a warm start, with the block's partial r.r
-__global__ void __launch_bounds__(512) k_residual(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_residual(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                   const uint16_t* __restrict__ fmask, const double* __restrict__ rhs,
                                                   const double* __restrict__ x, double* __restrict__ r,
                                                   double* partial, Params P) {
@@ -217,21 +221,24 @@ __global__ void __launch_bounds__(512) k_residual(const int* __restrict__ dbl, c
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
-  uint16_t m = fmask[c];
   double rr = 0;
-  if (m & kDomainBit) {
-    double v = rhs[c] - apply0(x, fmask, sb, c, o, m, P);
-    r[c] = v;
-    rr = v * v;
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    uint16_t m = fmask[c];
+    if (m & kDomainBit) {
+      double v = rhs[c] - apply0(x, fmask, sb, c, o, m, P);
+      r[c] = v;
+      rr += v * v;
+    }
   }
-  block_sum512(rr, 0.0, partial);
+  block_sum<kBT>(rr, 0.0, partial);
 }
 
 // p = z + beta p (first: p = z), then q = M p and the partial p.q; the
 // neighbours' new p is formed on the fly so p is read once and written once.
-__global__ void __launch_bounds__(512) k_update_spmv(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                      const uint16_t* __restrict__ fmask, const double* __restrict__ z,
                                                      const double* __restrict__ pold, double* __restrict__ pnew,
                                                      double* __restrict__ q, double* partial, Params P,
@@ -242,26 +249,30 @@ __global__ void __launch_bounds__(512) k_update_spmv(const int* __restrict__ dbl
   load_face_bases(nbr, b, sb);
   __syncthreads();
   double be = first ? 0.0 : ds->beta;
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
-  uint16_t m = fmask[c];
+  auto pv = [&](int64_t i) -> double { return first ? z[i] : z[i] + be * pold[i]; };
   double pq = 0;
-  if (!(m & kDomainBit)) {
-    pnew[c] = 0.0;
-    q[c] = 0.0;
-  } else {
-    auto pv = [&](int64_t i) -> double { return first ? z[i] : z[i] + be * pold[i]; };
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    uint16_t m = fmask[c];
+    if (!(m & kDomainBit)) {
+      pnew[c] = 0.0;
+      q[c] = 0.0;
+      continue;
+    }
     double pc = pv(c);
     double s = 0;
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) s += P.ih2[f >> 1] * pc;
       if (m & (1u << f)) s -= P.ih2[f >> 1] * pv(nb0(sb, c, o, f));
     }
     pnew[c] = pc;
     q[c] = s;
-    pq = pc * s;
+    pq += pc * s;
   }
-  block_sum512(pq, 0.0, partial);
+  block_sum<kBT>(pq, 0.0, partial);
 }
 
 __global__ void k_fin_alpha(const double* partial, int nblk, Scalars* ds) {
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(512) k_axpy(const int* __restrict__ dbl, doubl
   x[c] += a * p[c];
   double rv = r[c] - a * q[c];
   r[c] = rv;
-  block_sum512(rv * rv, 0.0, partial);
+  block_sum<512>(rv * rv, 0.0, partial);
 }
 
 __global__ void k_fin_rr(const double* partial, int nblk, Scalars* ds, double rtol2, int max_iters) {
@@ -337,7 +348,7 @@ __global__ void __launch_bounds__(512) k_jacobi_prec(const int* __restrict__ dbl
   uint16_t m = fmask[c];
   double v = (m & kDomainBit) ? r[c] * P.dtab[active_index(m)] : 0.0;
   z[c] = v;
-  block_sum512(r[c] * v, 0.0, partial);
+  block_sum<512>(r[c] * v, 0.0, partial);
 }
 
 // Pressure write-back and velocity correction, fused
@@ -377,7 +388,7 @@ __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist,
 }
 
 // max |div| over domain cells (the check of src/Algorithms_Solve_Pressure.h:208-219)
-__global__ void __launch_bounds__(512) k_divmax(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_divmax(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                 const uint16_t* __restrict__ fmask, const double* __restrict__ ux,
                                                 const double* __restrict__ uy, const double* __restrict__ uz, Params P,
                                                 Scalars* ds) {
@@ -385,18 +396,21 @@ __global__ void __launch_bounds__(512) k_divmax(const int* __restrict__ dbl, con
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  int o = threadIdx.x;
-  int64_t c = (int64_t)b * kCells + o;
   double mx = 0;
-  if (fmask[c] & kDomainBit) {
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    int64_t c = (int64_t)b * kCells + o;
+    if (!(fmask[c] & kDomainBit)) continue;
     const double* U[3] = {ux, uy, uz};
     double d = 0;
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
       d -= U[i][c] * P.ih[i];
       int64_t n = nb0(sb, c, o, 2 * i + 1);
       d += (n < 0 ? 0.0 : U[i][n]) * P.ih[i];
     }
-    mx = fabs(d);
+    mx = fmax(mx, fabs(d));
   }
   for (int s = 16; s > 0; s >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, s));
   if ((threadIdx.x & 31) == 0) atomicMax(&ds->div_bits, (unsigned long long)__double_as_longlong(mx));
@@ -450,12 +464,12 @@ int project(Ctx* c, int ib) {
     int warm = c->prm.warm_start ? 1 : 0;
     double rtol2 = c->prm.rtol * c->prm.rtol;
     prof_begin(c, PH_DIVERGENCE);
-    k_divergence<<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,
+    k_divergence<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,
                                      c->x, c->r, warm, c->partial, c->dp); MAC_COUNT(c);
     prof_end(c, PH_DIVERGENCE);
     k_fin_bnorm<<<1, 1024, 0, st>>>(c->partial, nd, c->ds); MAC_COUNT(c);
     if (warm) {
-      k_residual<<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
+      k_residual<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
       k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
     }
     int first = 1;
@@ -468,7 +482,7 @@ int project(Ctx* c, int ib) {
       prof_end(c, PH_CGVEC);
       prof_begin(c, PH_SPMV);
       std::swap(c->pd, c->pd2);  // pd2: previous direction, pd: new one
-      k_update_spmv<<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
+      k_update_spmv<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
                                         first); MAC_COUNT(c);
       prof_end(c, PH_SPMV);
       first = 0;
@@ -501,7 +515,7 @@ int project(Ctx* c, int ib) {
   }
   if (c->prm.div_check && nd > 0) {
     k_zero_div<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
-    k_divmax<<<nd, 512, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->dp, c->ds); MAC_COUNT(c);
+    k_divmax<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->dp, c->ds); MAC_COUNT(c);
     rc = read_scalars(c);
     if (rc) return rc;
     unsigned long long bits = c->hs->div_bits;

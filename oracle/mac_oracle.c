@@ -1044,6 +1044,37 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
   return rc;
 }
 
+/* Single-policy probes on a state (for the reference's known-answer tests):
+ * what = 0: Get_Speed(pos) of the symmetric (sym != 0) or plain interpolation,
+ *           out[0..2];
+ * what = 1: Get_Convection_Speed(cell key, axis i) of the upwind policy, out[0];
+ * what = 2: Get_Divergence(cell key), out[0];
+ * what = 3: Get_Gradiant(cell key, axis i) from the stored pressures, out[0]. */
+int mac_oracle_probe(const char* in_path, int what, const double* pos, const int* key, int i, int sym,
+                     double* out) {
+  mac_state_file st;
+  if (mac_state_read(in_path, &st) != 0) return -1;
+  world_t* w = world_from_file(&st);
+  mac_state_free(&st);
+  if (what == 0) {
+    get_speed(w, pos, out, sym);
+  } else if (what == 1) {
+    out[0] = convection_speed(w, 0, key, i);
+  } else if (what == 2) {
+    out[0] = divergence(w, 0, key);
+  } else if (what == 3) {
+    cell_t c = cell_at(w, key[0], key[1], key[2]);
+    double g = (c.b >= 0 ? B(c)->p[c.o] : 0.0) * w->ih[i];
+    g -= rd_p(w, key, -(i == 0), -(i == 1), -(i == 2)) * w->ih[i];
+    out[0] = g;
+  } else {
+    world_free(w);
+    return -2;
+  }
+  world_free(w);
+  return 0;
+}
+
 /* The jitter function, exported so the tests can compare it with the device's. */
 void mac_oracle_jitter8(uint64_t seed, int kx, int ky, int kz, int s, double hx, double hy,
                         double hz, double* out) {

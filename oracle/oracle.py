@@ -40,6 +40,10 @@ def lib():
         _lib.mac_oracle_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                         ctypes.c_int, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_double)]
+        _lib.mac_oracle_probe.restype = ctypes.c_int
+        _lib.mac_oracle_probe.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_double)]
         _lib.mac_oracle_jitter8.restype = None
         _lib.mac_oracle_jitter8.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -57,6 +61,18 @@ def run_oracle(cmd: str, in_path: str, out_path: str, n: int = 1, rtol: float = 
         raise RuntimeError(f"oracle {cmd} failed ({rc})")
     return {"invalid_reads": stats[0], "created_cells": stats[1], "cg_iters": stats[2],
             "relres": stats[3], "max_div": stats[4], "fluid_cell_steps": stats[5]}
+
+
+def probe(in_path: str, what: str, pos=(0.0, 0.0, 0.0), key=(0, 0, 0), i=0, sym=1):
+    """One policy evaluation on a state: speed | convection | divergence | gradient."""
+    code = {"speed": 0, "convection": 1, "divergence": 2, "gradient": 3}[what]
+    p = (ctypes.c_double * 3)(*pos)
+    k = (ctypes.c_int * 3)(*key)
+    out = (ctypes.c_double * 3)()
+    rc = lib().mac_oracle_probe(in_path.encode(), code, p, k, i, sym, out)
+    if rc != 0:
+        raise RuntimeError(f"probe {what} failed ({rc})")
+    return [out[0], out[1], out[2]] if code == 0 else out[0]
 
 
 def jitter8(seed, k, s, h):

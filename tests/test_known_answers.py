@@ -1,0 +1,117 @@
+"""Known-answer cases of the reference's own tests, rebuilt on small 3D worlds
+and checked on the oracle (and, where the reference runner was built here, on
+the reference itself):
+
+* particle -> key: test/TestAlgorithm_Layer_Initial_With_Particle.h:106-123
+* air layers around one fluid cell: test/TestAlgorithms_Update_CellType_Layer.h:103-149
+* upwind convection -1.0 / 0.11: test/old/TestPolicy_Upwind_1_Order.h:99-104
+* staggered interpolation 1, 1.5, 1.4: test/old/TestPolicy_Speed_Interpolation_Linear.h:100-120
+* divergence and gradient of simple fields: test/old/TestPolicy_Divergence.h,
+  test/old/TestPolicy_Gradiant.h (values -1, -10, 1)
+"""
+import numpy as np
+import pytest
+
+from mac_b200.state import FLUID, Params, from_cells
+
+EPS = 1e-12
+
+
+def _block(x0, x1, y0, y1, z0, z1):
+    z, y, x = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1), indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=-1)
+
+
+def _field_world(h=1.0, ux=None):
+    """Fluid cells x in [-2,3], y,z in [-1,1]; u_x set per x column."""
+    keys = _block(-2, 3, -1, 1, -1, 1)
+    u = np.zeros((len(keys), 3))
+    for x, v in (ux or {}).items():
+        u[keys[:, 0] == x, 0] = v
+    pr = Params(h=(h, h, h), gravity=0.0)
+    return from_cells(pr, keys, np.full(len(keys), FLUID, np.uint8), np.zeros(len(keys), np.uint8), u)
+
+
+def _write(s, tmp_path, name="k.state"):
+    p = str(tmp_path / name)
+    s.write(p)
+    return p
+
+
+def test_particle_to_key(run_oracle):
+    pr = Params(h=(1.0, 1.0, 1.0), layer_max=4)
+    s = from_cells(pr, np.zeros((0, 3)), np.zeros(0), np.zeros(0), np.zeros((0, 3)),
+                   pos=np.array([[2.2, 4.3, 5.4]]))
+    got, _ = run_oracle("topology", s)
+    keys = got.cell_keys()
+    hit = (keys[..., 0] == 2) & (keys[..., 1] == 4) & (keys[..., 2] == 5)
+    assert got.exists[hit].item() == 1
+    assert got.layer[hit].item() == 0
+    assert got.type[hit].item() == FLUID
+
+
+def _layer_of(s, k):
+    keys = s.cell_keys()
+    hit = (keys[..., 0] == k[0]) & (keys[..., 1] == k[1]) & (keys[..., 2] == k[2])
+    if not hit.any() or not s.exists[hit].item():
+        return None
+    return s.layer[hit].item()
+
+
+def test_layers_around_one_fluid_cell(run_oracle):
+    pr = Params(h=(1.0, 1.0, 1.0), layer_max=1)
+    s = from_cells(pr, np.zeros((0, 3)), np.zeros(0), np.zeros(0), np.zeros((0, 3)), pos=np.array([[0.0, 0, 0]]))
+    got, _ = run_oracle("topology", s)
+    assert _layer_of(got, (0, 0, 0)) == 0
+    for k in [(1, 0, 0), (0, 1, 0), (-1, 0, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]:
+        assert _layer_of(got, k) == 1, k
+    # the reference's 2D expectations (slice z = 0) of the LayerMax+1 ring
+    for k in [(2, 0, 0), (1, 1, 0), (1, -1, 0), (0, 2, 0), (-1, 1, 0)]:
+        assert _layer_of(got, k) == 2, k
+    # ring = +e_i faces of the layer-1 cells only
+    assert _layer_of(got, (-2, 0, 0)) is None
+    assert _layer_of(got, (-1, -1, 0)) is None
+
+
+def test_upwind_known_answers(oracle_lib, tmp_path):
+    s = _field_world(ux={0: 0.0, 1: 1.0})
+    p = _write(s, tmp_path)
+    assert abs(oracle_lib.probe(p, "convection", key=(1, 0, 0), i=0) - (-1.0)) < EPS
+    s = _field_world(ux={0: -0.1, 1: 1.0})
+    p = _write(s, tmp_path, "k2.state")
+    assert abs(oracle_lib.probe(p, "convection", key=(0, 0, 0), i=0) - 0.11) < EPS
+
+
+@pytest.mark.parametrize("sym", [0, 1])
+def test_interpolation_known_answers(oracle_lib, tmp_path, sym):
+    p = _write(_field_world(ux={0: 1.0, 1: 1.0}), tmp_path)
+    assert abs(oracle_lib.probe(p, "speed", pos=(0.0, 0, 0), sym=sym)[0] - 1.0) < EPS
+    assert abs(oracle_lib.probe(p, "speed", pos=(0.1, 0, 0), sym=sym)[0] - 1.0) < EPS
+    p = _write(_field_world(ux={0: 2.0, 1: 1.0}), tmp_path, "k2.state")
+    assert abs(oracle_lib.probe(p, "speed", pos=(0.0, 0, 0), sym=sym)[0] - 1.5) < EPS
+    assert abs(oracle_lib.probe(p, "speed", pos=(0.1, 0, 0), sym=sym)[0] - 1.4) < EPS
+
+
+def test_divergence_and_gradient(oracle_lib, tmp_path):
+    p = _write(_field_world(h=1.0, ux={0: 1.0}), tmp_path)
+    assert abs(oracle_lib.probe(p, "divergence", key=(0, 0, 0)) - (-1.0)) < EPS
+    p = _write(_field_world(h=0.1, ux={0: 1.0}), tmp_path, "k2.state")
+    assert abs(oracle_lib.probe(p, "divergence", key=(0, 0, 0)) - (-10.0)) < 1e-9
+    s = _field_world()
+    keys = s.cell_keys()
+    s.f64["p"][(keys[..., 0] == 0) & s.exists.astype(bool)] = 1.0
+    p = _write(s, tmp_path, "k3.state")
+    assert abs(oracle_lib.probe(p, "gradient", key=(0, 0, 0), i=0) - 1.0) < EPS
+    assert abs(oracle_lib.probe(p, "gradient", key=(0, 0, 0), i=1)) < EPS
+
+
+def test_brick_layout_and_floor_division():
+    """Chunk key = floor(key / 8), slot x + 8y + 64z (src/ChunkHashTable.tpp:180-196,
+    src/Offset.h:14-24)."""
+    pr = Params()
+    keys = np.array([[-1, 0, 0], [-8, 0, 0], [-9, 0, 0], [7, 7, 7], [8, 0, 0]])
+    s = from_cells(pr, keys, np.zeros(5), np.zeros(5), np.zeros((5, 3)))
+    bk = {tuple(k) for k in s.keys.tolist()}
+    assert bk == {(-1, 0, 0), (-2, 0, 0), (0, 0, 0), (1, 0, 0)}
+    ck = s.cell_keys()[s.exists.astype(bool)]
+    assert sorted(map(tuple, ck.tolist())) == sorted(map(tuple, keys.tolist()))
