@@ -306,19 +306,43 @@ constexpr int kStage = 12;
 constexpr int kStageCells = kStage * kStage * kStage;
 struct StagedField {
   const double* s;        // [3][kStageCells]
-  const uint8_t* miss;    // [kStageCells] 1 = cell missing
   int ox, oy, oz;         // cell key of stage slot (0,0,0)
   GlobalField g;
   __device__ double u(int k, int kx, int ky, int kz, int* bad) const {
     unsigned x = (unsigned)(kx - ox), y = (unsigned)(ky - oy), z = (unsigned)(kz - oz);
-    if (x < (unsigned)kStage && y < (unsigned)kStage && z < (unsigned)kStage) {
-      int i = (int)(x + kStage * (y + kStage * z));
-      if (miss[i]) *bad = 1;
-      return s[k * kStageCells + i];
-    }
+    if (x < (unsigned)kStage && y < (unsigned)kStage && z < (unsigned)kStage)
+      return s[k * kStageCells + (int)(x + kStage * (y + kStage * z))];
     return g.u(k, kx, ky, kz, bad);
   }
+  // The 2x2x2 stencil of component k at corner key (index n = 4X + 2Y + Z);
+  // one bounds test for the whole stencil.
+  __device__ void u8(int k, const int* key, double* out, int* bad) const {
+    unsigned x = (unsigned)(key[0] - ox), y = (unsigned)(key[1] - oy), z = (unsigned)(key[2] - oz);
+    if (x + 1 < (unsigned)kStage && y + 1 < (unsigned)kStage && z + 1 < (unsigned)kStage) {
+      const double* p = s + k * kStageCells + (int)(x + kStage * (y + kStage * z));
+      out[0] = p[0];
+      out[1] = p[kStage * kStage];
+      out[2] = p[kStage];
+      out[3] = p[kStage + kStage * kStage];
+      out[4] = p[1];
+      out[5] = p[1 + kStage * kStage];
+      out[6] = p[1 + kStage];
+      out[7] = p[1 + kStage + kStage * kStage];
+      return;
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) out[n] = g.u(k, key[0] + (n >> 2), key[1] + ((n >> 1) & 1), key[2] + (n & 1), bad);
+  }
 };
+
+template <class F>
+__device__ inline void stencil8(const F& field, int k, const int* key, double* u, int* bad) {
+#pragma unroll
+  for (int n = 0; n < 8; ++n) u[n] = field.u(k, key[0] + (n >> 2), key[1] + ((n >> 1) & 1), key[2] + (n & 1), bad);
+}
+__device__ inline void stencil8(const StagedField& field, int k, const int* key, double* u, int* bad) {
+  field.u8(k, key, u, bad);
+}
 
 template <class F>
 __device__ inline void get_speed(const double* pos, double* out, const F& field, const Params& P, int sym, int* bad) {
@@ -357,8 +381,7 @@ __device__ inline void get_speed(const double* pos, double* out, const F& field,
       }
     }
     double u[8];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) u[n] = field.u(k, key[0] + (n >> 2), key[1] + ((n >> 1) & 1), key[2] + (n & 1), bad);
+    stencil8(field, k, key, u, bad);
     // u[(X<<2)|(Y<<1)|Z]
     double l00 = w0[2] * u[0] + w1[2] * u[1];
     double l01 = w0[2] * u[2] + w1[2] * u[3];
@@ -488,7 +511,6 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
                                                      const double* __restrict__ uz, Params P,
                                                      const Scalars* __restrict__ ds, unsigned long long* bad_count) {
   __shared__ double s[3 * kStageCells];
-  __shared__ uint8_t miss[kStageCells];
   __shared__ int sn[kNbr];
   int b = blist[blockIdx.x];
   int64_t p0 = off[b], p1 = off[b + 1];
@@ -504,13 +526,11 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
     int nb = sn[nbr_index(dx, dy, dz)];
     if (nb < 0) {
       s[i] = s[kStageCells + i] = s[2 * kStageCells + i] = 0.0;
-      miss[i] = 1;
     } else {
       int64_t gi = (int64_t)nb * kCells + (lx - 8 * dx) + 8 * (ly - 8 * dy) + 64 * (lz - 8 * dz);
       s[i] = U[0][gi];
       s[kStageCells + i] = U[1][gi];
       s[2 * kStageCells + i] = U[2][gi];
-      miss[i] = lay[gi] == kMissing;
     }
   }
   __syncthreads();
@@ -520,7 +540,7 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
   pb.key[1] = bkey[3 * b + 1];
   pb.key[2] = bkey[3 * b + 2];
   pb.b = b;
-  StagedField f{s, miss, ox, oy, oz, GlobalField{pb, nbr, hk, hv, hcap, lay, U}};
+  StagedField f{s, ox, oy, oz, GlobalField{pb, nbr, hk, hv, hcap, lay, U}};
   int bad = 0;
   for (int64_t q = p0 + threadIdx.x; q < p1; q += blockDim.x) {
     double pos[3] = {px[q], py[q], pz[q]};

@@ -294,6 +294,42 @@ __device__ inline int64_t nb0(const int64_t* sb, int64_t c, int o, int f) {
 constexpr int kBT = 128;
 constexpr int kCPT = kCells / kBT;
 
+// Shared-memory staging of one brick with its six face halos: a 10^3 array,
+// interior (x,y,z) at (x+1) + 10(y+1) + 100(z+1); edge and corner entries are
+// not used by 7-point stencils. val(global index) produces the staged value;
+// cells of an absent neighbour brick stage `zero`. All loads are independent,
+// so a block has its whole brick in flight at once.
+constexpr int kS1 = 1000;
+__device__ inline int s1(int x, int y, int z) { return (x + 1) + 10 * (y + 1) + 100 * (z + 1); }
+__device__ inline int s1_of(int o) { return s1(o & 7, (o >> 3) & 7, o >> 6); }
+__device__ inline int s1_off(int f) {
+  const int mag = (f >> 1) == 0 ? 1 : ((f >> 1) == 1 ? 10 : 100);
+  return (f & 1) ? mag : -mag;
+}
+
+template <class V, class F>
+__device__ inline void stage_h1(V* s, int b, const int64_t* sb, V zero, F val) {
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    int o = threadIdx.x + kBT * k;
+    s[s1_of(o)] = val((int64_t)b * kCells + o);
+  }
+  for (int j = threadIdx.x; j < 384; j += kBT) {
+    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
+    int x, y, z;
+    int64_t gi;
+    switch (f) {
+      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
+      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
+      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
+      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
+      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
+      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
+    }
+    s[s1(x, y, z)] = gi < 0 ? zero : val(gi);
+  }
+}
+
 // Sum over an NT-thread block of two values into partial[blockIdx.x] and
 // partial[gridDim.x + blockIdx.x] (fixed order).
 template <int NT>

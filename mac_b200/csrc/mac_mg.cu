@@ -37,24 +37,29 @@ __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const
                                               const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                               T* __restrict__ e, Params P) {
   __shared__ int64_t sb[6];
+  __shared__ double sr[kS1];  // w D^-1 r of the brick and its face halo
+  __shared__ uint16_t sm[kCells];
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  __syncthreads();
+  stage_h1(sr, b, sb, 0.0, [&](int64_t i) { return kOmega * P.dtab[active_index(fmask[i])] * r[i]; });
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) sm[threadIdx.x + kBT * k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = fmask[c];
+    uint16_t m = sm[o];
     double out = 0;
     if (m & kDomainBit) {
+      int si = s1_of(o);
+      double dinv = P.dtab[active_index(m)];
       double s = (2.0 - kOmega) * r[c];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        if (!(m & (1u << f))) continue;
-        int64_t n = nb0(sb, c, o, f);
-        s += P.ih2[f >> 1] * kOmega * P.dtab[active_index(fmask[n])] * r[n];
-      }
-      out = kOmega * P.dtab[active_index(m)] * s;
+      for (int f = 0; f < 6; ++f)
+        if (m & (1u << f)) s += P.ih2[f >> 1] * sr[si + s1_off(f)];
+      out = kOmega * dinv * s;
     }
     e[c] = (T)out;
   }
@@ -67,8 +72,11 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P) {
   __shared__ int64_t sb[6];
   __shared__ double res[kCells];
+  __shared__ double se[kS1];
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  __syncthreads();
+  stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i]; });
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
@@ -77,12 +85,13 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
     uint16_t m = fmask[c];
     double v = 0;
     if (m & kDomainBit) {
-      double ec = (double)e[c];
+      int si = s1_of(o);
+      double ec = se[si];
       double me = 0;
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
         if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * ec;
-        if (m & (1u << f)) me -= P.ih2[f >> 1] * (double)e[nb0(sb, c, o, f)];
+        if (m & (1u << f)) me -= P.ih2[f >> 1] * se[si + s1_off(f)];
       }
       v = r[c] - me;
     }
@@ -108,8 +117,12 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P) {
   __shared__ int64_t sb[6];
+  __shared__ double se[kS1];  // e (plus the coarse correction when FIRST) with face halo
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  __syncthreads();
+  if (FIRST) stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i] + (double)e1[parent1(i)]; });
+  else stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i]; });
   __syncthreads();
   double rz = 0;
 #pragma unroll
@@ -122,18 +135,13 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
       else z[c] = 0.0;
       continue;
     }
-    double epc = (double)e[c];
-    if (FIRST) epc += (double)e1[parent1(c)];
+    int si = s1_of(o);
+    double epc = se[si];
     double me = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * epc;
-      if (m & (1u << f)) {
-        int64_t n = nb0(sb, c, o, f);
-        double en = (double)e[n];
-        if (FIRST) en += (double)e1[parent1(n)];
-        me -= P.ih2[f >> 1] * en;
-      }
+      if (m & (1u << f)) me -= P.ih2[f >> 1] * se[si + s1_off(f)];
     }
     double rc = r[c];
     double out = epc + kOmega * P.dtab[active_index(m)] * (rc - me);

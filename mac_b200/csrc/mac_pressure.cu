@@ -245,11 +245,14 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
                                                      const Scalars* ds, int first) {
   if (ds->done) return;
   __shared__ int64_t sb[6];
+  __shared__ double sp[kS1];  // the new direction on the brick and its face halo
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
   double be = first ? 0.0 : ds->beta;
-  auto pv = [&](int64_t i) -> double { return first ? z[i] : z[i] + be * pold[i]; };
+  if (first) stage_h1(sp, b, sb, 0.0, [&](int64_t i) { return z[i]; });
+  else stage_h1(sp, b, sb, 0.0, [&](int64_t i) { return z[i] + be * pold[i]; });
+  __syncthreads();
   double pq = 0;
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
@@ -261,12 +264,13 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
       q[c] = 0.0;
       continue;
     }
-    double pc = pv(c);
+    int si = s1_of(o);
+    double pc = sp[si];
     double s = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) s += P.ih2[f >> 1] * pc;
-      if (m & (1u << f)) s -= P.ih2[f >> 1] * pv(nb0(sb, c, o, f));
+      if (m & (1u << f)) s -= P.ih2[f >> 1] * sp[si + s1_off(f)];
     }
     pnew[c] = pc;
     q[c] = s;

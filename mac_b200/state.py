@@ -244,4 +244,5 @@ def pool_particles(nx, ny, depth, h, ppc=8, seed=1):
         o = np.array([0.25 if (s >> i) & 1 else -0.25 for i in range(3)])
         j = (rng.random(base.shape) - 0.5) * 0.499
         out.append((base + o + j) * h)
-    return np.concatenate(out, axis=0)
+    # cell-major: the particles of one cell are consecutive, cells in (z, y, x) order
+    return np.stack(out, axis=1).reshape(-1, 3)
