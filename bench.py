@@ -212,7 +212,7 @@ def run_ours(args, rank, world, local_rank):
     s = make_world(args.workload)
     log(f"[rank {rank}] world built in {time.perf_counter() - t0:.1f}s: {s.nbricks} bricks, {s.nparticles} particles")
     ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
-                  device=dev, div_check=True)
+                  device=dev, div_check=True, warm_start=args.warm_start)
     t0 = time.perf_counter()
     first_init(ctx, s)
     ctx.sync()
@@ -312,7 +312,8 @@ def run_ours(args, rank, world, local_rank):
                                f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
                    "solver": {"mgpcg64": "plain FP64 MG-PCG", "mixed": "FP32 MG in FP64 PCG",
                               "cg64": "FP64 Jacobi-PCG"}[args.solver],
-                   "rtol": 1e-8, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
                    "fluid_cells_last": st["fluid_cells"], "particles": st["particles"],
                    "live_bricks": st["live_bricks"], "cg_iters_per_solve_last": st["iterations"],
@@ -335,6 +336,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="jet256")
     ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mgpcg64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warm-start", action="store_true",
+                    help="start each pressure solve from the previous pressure (the reference starts from zero)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

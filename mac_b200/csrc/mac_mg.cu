@@ -19,8 +19,11 @@
 
 namespace mac {
 
-constexpr double kOmega = 0.8;
-constexpr double kCoarseScale = 0.5;
+// Jacobi weight (the V-cycle stays positive definite for omega < 1) and the
+// per-level scale of the Galerkin operator (piecewise-constant transfer
+// over-weights the coarse operator; 0.6 was the best of 0.4-0.7 on pool masks).
+constexpr double kOmega = 0.9;
+constexpr double kCoarseScale = 0.6;
 constexpr int kCoarsestSweeps = 40;
 
 // Level-1 parent of level-0 cell n (pool index).
