@@ -172,6 +172,35 @@ int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, co
 int mac_csc_solve(void* ctx, int n, const double* b, double* x);
 int mac_csc_clean(void* ctx);
 
+/* ---- allocation-free CSC solve (no counterpart in the reference) ----
+ * The same FP64 Jacobi-PCG as mac_csc_factorize + mac_csc_solve, for callers
+ * that must not allocate device memory: a host program whose device memory is
+ * already handed out by its own allocator (a caching allocator that keeps HBM
+ * reserved), or a per-step loop that cannot pay for the device-wide
+ * synchronisation a cudaMalloc/cudaFree pair can cause. No context is needed.
+ *
+ * - offset/indice/value (CSC, as mac_csc_factorize), b and x are DEVICE
+ *   pointers owned by the caller; x is overwritten (the solve starts from 0).
+ * - Work vectors live in one fixed device array of MAC_NOALLOC_MAX_N rows per
+ *   device; n > MAC_NOALLOC_MAX_N returns MAC_ERR_CAPACITY and touches nothing.
+ *   Its reduction slots must be zero before each reduction, and the call clears
+ *   them itself, so the caller prepares nothing.
+ * - Runs on `stream` (a cudaStream_t, 0 for the legacy stream) on the current
+ *   device and returns after the solve has finished (it reads the CG scalars
+ *   on the host every iteration).
+ * - The first call on a device looks up the array's address with
+ *   cudaGetSymbolAddress; make that first call before any stream capture
+ *   begins on that device.
+ * - All calls on one device share the array: two calls in flight at the same
+ *   time on one device (other streams or host threads) race and corrupt each
+ *   other's result. Serialise them.
+ * Stops when ||b - A x|| <= rtol ||b|| (MAC_OK) or after max_iters iterations
+ * (MAC_ERR_NOT_CONVERGED); iterations and relres may be NULL. */
+#define MAC_NOALLOC_MAX_N 65536
+int mac_csc_solve_noalloc(void* stream, int n, const int* offset, const int* indice, const double* value,
+                          const double* b, double* x, double rtol, int max_iters, int* iterations,
+                          double* relres);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,7 +61,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
            "mac_pressure_project", "mac_rk2tvd", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
            "mac_stream", "mac_launch_count", "mac_set_profiling", "mac_get_profile",
-           "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean"]
+           "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -100,6 +100,9 @@ def load(path: str = LIB_PATH):
     lib.mac_launch_count.argtypes = [vp, _P(ctypes.c_int64)]
     lib.mac_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.mac_get_profile.argtypes = [vp, _P(ctypes.c_double), _P(ctypes.c_int64), ctypes.c_int]
+    # Device pointers are passed as integers (c_void_p).
+    lib.mac_csc_solve_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
+                                          _P(ctypes.c_int), _P(ctypes.c_double)]
     _lib = lib
     return lib
 
