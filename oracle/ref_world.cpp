@@ -106,6 +106,11 @@
 #include "Algorithms_Move_Particles.h"
 #include "Algorithms_RungeKutta_RK2_TVD.h"
 
+#ifdef MAC_WITH_GPU
+// The C++ drop-in layer of the device path; compiled in only for _ref/mac_ref_gpu.
+#include "mac_gpu/Mac_GPU.h"
+#endif
+
 #include "state_format.h"
 
 using namespace std;
@@ -466,6 +471,38 @@ static int run(int argc, char** argv) {
   typedef Algorithms_Move_Particles<type_data_ref, type_pol_move_lin> type_alg_move_lin;
   type_alg_move_lin m_alg_move_lin(m_data_ref, m_pol_move_lin);
 
+#ifdef MAC_WITH_GPU
+  // The same world driven through the drop-in layer: the unmodified
+  // Algorithms_Solve_Pressure with Policy_Solve_Linear_GPU as its solver policy,
+  // and the pipeline-A step as device algorithms.
+  typedef Policies<Policy_Solve_Linear_GPU, type_pol_divergence, type_pol_gradiant, type_pol_vn, type_pol_pres_if> type_pol_pres_gpu;
+  Policy_Solve_Linear_GPU m_pol_solve_gpu(g_cg_rtol);
+  type_pol_pres_gpu m_pol_pres_gpu(m_pol_solve_gpu, m_pol_divergence, m_pol_gradiant, m_pol_vn, m_pol_pres_if);
+  typedef Algorithms_Solve_Pressure<type_data_ref, type_pol_pres_gpu> type_alg_solve_pressure_gpu;
+  type_alg_solve_pressure_gpu m_alg_solve_pressure_gpu(m_data_ref, m_pol_pres_gpu);
+  typedef Algorithms_Do_Pressure<type_data_ref, type_alg_solve_pressure_gpu> type_alg_do_pressure_gpu;
+  type_alg_do_pressure_gpu m_alg_do_pressure_gpu(m_data_ref, m_alg_solve_pressure_gpu);
+
+  mac_params gprm;
+  mac_default_params(&gprm);
+  for (int i = 0; i < 3; ++i) gprm.h[i] = st.hdr.h[i];
+  gprm.cfl_factor = st.hdr.cfl_factor;
+  gprm.dt_min = st.hdr.dt_min;
+  gprm.dt_max = st.hdr.dt_max;
+  gprm.gravity = st.hdr.gravity;
+  gprm.gravity_axis = st.hdr.gravity_axis;
+  gprm.layer_max = st.hdr.layer_max;
+  gprm.interp_symmetric = st.hdr.interp_symmetric;
+  gprm.rtol = g_cg_rtol;
+  gprm.max_iters = 5000;
+  gprm.max_bricks = 8192;
+  gprm.max_particles = 1 << 22;
+  typedef Policy_Mac_GPU<type_data_ref> type_pol_gpu;
+  type_pol_gpu m_pol_gpu(m_data_ref, gprm, g_refill_seed);
+  Algorithms_Step_GPU<type_data_ref, type_pol_gpu> m_alg_step_gpu(m_data_ref, m_pol_gpu);
+  Algorithms_To_Host_GPU<type_data_ref, type_pol_gpu> m_alg_to_host_gpu(m_data_ref, m_pol_gpu);
+#endif
+
   // The reference algorithms print timing lines on std::cout; keep them out of the way.
   std::ofstream devnull("/dev/null");
   std::streambuf* saved = std::cout.rdbuf(devnull.rdbuf());
@@ -511,6 +548,22 @@ static int run(int argc, char** argv) {
       m_alg_move.Do();
     } else if (cmd == "movelin") {
       m_alg_move_lin.Do();
+#ifdef MAC_WITH_GPU
+    } else if (cmd == "gpuproject") {
+      type_chunk_speed::ispeed = 0;
+      m_alg_do_pressure_gpu.Do();
+    } else if (cmd == "gpustep") {
+      m_alg_step_gpu.Do();
+      if (r + 1 == nrep) {
+        m_alg_to_host_gpu.Do();
+        g_refill_seed = m_pol_gpu.Session().Step();
+        if (m_pol_gpu.Session().Status() != MAC_OK) {
+          std::cout.rdbuf(saved);
+          fprintf(stderr, "device step failed: %s\n", mac_error_string(m_pol_gpu.Session().Status()));
+          return 1;
+        }
+      }
+#endif
     } else if (cmd == "csc") {
       // Projection of speed 0 with the assembled system written to argv[4].
       g_csc_dump = fopen(argv[4], "wb");
