@@ -200,6 +200,60 @@ def roofline_models(ctx_stats, prof, np_count, n_exist):
     return out
 
 
+POISSON_N = 128
+POISSON_RTOL = 1e-10
+
+
+def poisson_solves(dev, reps=3):
+    """Standalone pressure solve of the 128^3 pool + 12 spheres world (solid box,
+    face speeds uniform in [-1, 1]) to a relative residual of 1e-10: device time
+    of one projection and of its solve (system set-up + CG iterations), per
+    solver form, with the pressure error against an FP64 MG-PCG solve to 1e-13."""
+    import torch
+    from mac_b200.gpu import Context
+    from mac_b200.state import FLUID, pool_spheres_world
+    from mac_b200.world import setup_passes
+
+    s = setup_passes(pool_spheres_world(POISSON_N))
+    dom = s.exists.astype(bool) & (s.type == FLUID)
+    res = {"workload": f"pool z<0.4n + 12 spheres r~U[6,20], {POISSON_N}^3, solid box, u~U[-1,1] (seeds 2, 3)",
+           "rtol": POISSON_RTOL}
+    p_ref = None
+    for name, solver, rtol in (("reference", "mgpcg64", 1e-13), ("plain", "mgpcg64", POISSON_RTOL),
+                               ("mixed", "mixed", POISSON_RTOL)):
+        with Context(s.params, max_bricks=8192, max_particles=1024, solver=solver, rtol=rtol, max_iters=1000,
+                     device=dev) as ctx:
+            stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+            times, solve = [], []
+            for r in range(reps + 1):
+                ctx.upload(s)
+                ctx.sync()
+                ctx.set_profiling(True)
+                ctx.profile()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.project(0)
+                e1.record(stream)
+                e1.synchronize()
+                prof = ctx.profile()
+                if r:
+                    times.append(e0.elapsed_time(e1))
+                    solve.append(sum(prof[k][0] for k in ("setup", "spmv", "cg_vector", "vcycle")))
+            st = ctx.stats()
+            p = ctx.download().sorted().f64["p"]
+        p = p[dom] if p.shape == dom.shape else None
+        if name == "reference":
+            p_ref = p
+            res["unknowns"] = int(st["unknowns"])
+            continue
+        err = None
+        if p is not None and p_ref is not None:
+            err = float(np.linalg.norm(p - p_ref) / np.linalg.norm(p_ref))
+        res[name] = {"project_ms": round(float(np.median(times)), 3), "solve_ms": round(float(np.median(solve)), 3),
+                     "iterations": int(st["iterations"]), "relres": st["relres"], "p_rel_err_vs_fp64": err}
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from mac_b200.gpu import Context, HostState
@@ -323,6 +377,8 @@ def run_ours(args, rank, world, local_rank):
                                                  for k, v in rl.items()},
     }
     ctx.close()
+    if rank == 0 and not args.no_poisson:
+        out["poisson"] = poisson_solves(dev)
     return out
 
 
@@ -336,6 +392,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="jet256")
     ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mgpcg64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",
                     help="start each pressure solve from the previous pressure (the reference starts from zero)")
     ap.add_argument("--cpu-steps", type=int, default=2)

@@ -233,6 +233,34 @@ def jet_world(nx=32, ny=32, nz=64, h=0.05, r_inflow=4.0, w_inflow=1.0, pool_dept
     return from_cells(pr, keys, typ, flags, u, pos)
 
 
+def pool_spheres_world(n=128, nspheres=12, r_range=(6.0, 20.0), pool_frac=0.4, seed=2, vel_seed=3) -> State:
+    """Standalone pressure-solve world: cells 0..n-1 on each axis with h = 1/n,
+    fluid where z < pool_frac*n or inside one of ``nspheres`` balls (radius
+    uniform in ``r_range`` cells, centre uniform in [r, n-r]^3, seeded), air
+    elsewhere, and a solid shell on all six box faces. Every face speed of the
+    open cells is uniform in [-1, 1] (seeded). Run ``world.setup_passes`` on it
+    before use (const faces of the shell, as Algorithms_Solid_To_Const)."""
+    h = 1.0 / n
+    pr = Params(h=(h, h, h), cfl_factor=0.5, dt_max=0.01, layer_max=4)
+    rng = np.random.default_rng(seed)
+    cells = _box(0, n - 1, 0, n - 1, 0, n - 1)
+    fluid = cells[:, 2] < pool_frac * n
+    for _ in range(nspheres):
+        r = rng.uniform(r_range[0], r_range[1])
+        c = rng.uniform(r, n - r, size=3)
+        fluid |= ((cells - c) ** 2).sum(axis=1) <= r * r
+    shell = _box(-1, n, -1, n, -1, n)
+    shell = shell[(shell.min(axis=1) < 0) | (shell.max(axis=1) >= n)]
+    keys = np.concatenate([shell, cells], axis=0)
+    typ = np.concatenate([np.full(len(shell), SOLID, np.uint8), np.where(fluid, FLUID, AIR).astype(np.uint8)])
+    u = np.zeros((len(keys), 3))
+    u[len(shell):] = np.random.default_rng(vel_seed).uniform(-1.0, 1.0, size=(len(cells), 3))
+    s = from_cells(pr, keys, typ, np.zeros(len(keys), np.uint8), u)
+    # fluid cells are layer 0 and the air cells layer 1, as after a topology pass
+    s.layer[:] = np.where(s.exists.astype(bool), np.where(s.type == FLUID, 0, 1), -1)
+    return s
+
+
 def pool_particles(nx, ny, depth, h, ppc=8, seed=1):
     """Jittered 2x2x2 lattice (offsets +-h/4 plus uniform jitter in (-h/4, h/4))
     in every cell of the slab 0..nx-1 x 0..ny-1 x 0..depth-1."""
