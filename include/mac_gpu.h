@@ -172,6 +172,37 @@ int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, co
 int mac_csc_solve(void* ctx, int n, const double* b, double* x);
 int mac_csc_clean(void* ctx);
 
+/* ---- learned preconditioner (no counterpart in the reference) ----
+ * A 3-level 3D U-Net (16/32/64 channels, 3x3x3 convolutions, ReLU; BF16
+ * weights and activations, FP32 accumulation) mapping a residual and a cell
+ * mask (1 fluid, 0 air, -1 solid) on a dense grid to a correction, for the
+ * unit-spacing operator; trained on (residual, error) pairs from plain FP64
+ * CG iterates. Grids are [n][d][h][w] with x fastest, d, h, w multiples of 4.
+ * Parameters are FP32 [layer][tap][cout][cin] + bias, the layout of
+ * mac_unet_get_params; tscale is the fixed output scale of the network. */
+int mac_unet_create(int device, void** net);
+int mac_unet_destroy(void* net);
+int mac_unet_nparams(void* net, int64_t* n);
+int mac_unet_init(void* net, uint64_t seed);
+int mac_unet_get_params(void* net, float* params, float* tscale);
+int mac_unet_set_params(void* net, const float* params, float tscale);
+/* out = net(r / rms(r), mask) * rms(r) * tscale on fluid cells, 0 elsewhere (host arrays). */
+int mac_unet_forward(void* net, int n, int d, int h, int w, const float* r, const int8_t* mask, float* out);
+/* loss = mean over fluid cells of (net(r / rms(r), mask) - e / (rms(r) tscale))^2 and its
+ * gradient with respect to every parameter (host arrays). */
+int mac_unet_loss_grad(void* net, int n, int d, int h, int w, const float* r, const int8_t* mask, const float* e,
+                       double* loss, float* grad);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) with the given gradient. */
+int mac_unet_adam_step(void* net, const float* grad, float lr);
+/* Training set on the device: nmasks random pool + 12 sphere masks on a size^3 grid,
+ * each solved by plain FP64 CG for niter iterations from 0; pairs at iterations
+ * 1, 2, 4, ... (nsnap). stats[0]: worst final relative residual, stats[1]: tscale. */
+int mac_unet_make_dataset(void* net, int nmasks, int size, int nsnap, int niter, uint64_t seed, double* stats);
+int mac_unet_get_sample(void* net, int index, float* r, float* e, int8_t* mask);
+/* steps Adam steps on random batches of the training set; losses[steps] (may be NULL). */
+int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, float* losses);
+int mac_unet_launch_count(void* net, int64_t* count);
+
 /* ---- allocation-free CSC solve (no counterpart in the reference) ----
  * The same FP64 Jacobi-PCG as mac_csc_factorize + mac_csc_solve, for callers
  * that must not allocate device memory: a host program whose device memory is

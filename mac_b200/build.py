@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmac_gpu.so")
-SOURCES = ["mac_ctx.cu", "mac_topology.cu", "mac_advect.cu", "mac_pressure.cu", "mac_mg.cu", "mac_step.cu", "mac_noalloc.cu"]
+SOURCES = ["mac_ctx.cu", "mac_topology.cu", "mac_advect.cu", "mac_pressure.cu", "mac_mg.cu", "mac_step.cu", "mac_noalloc.cu", "mac_unet.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
          "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]

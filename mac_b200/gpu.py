@@ -61,7 +61,10 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
            "mac_pressure_project", "mac_rk2tvd", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
            "mac_stream", "mac_launch_count", "mac_set_profiling", "mac_get_profile",
-           "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc"]
+           "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc",
+           "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
+           "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
+           "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -103,6 +106,21 @@ def load(path: str = LIB_PATH):
     # Device pointers are passed as integers (c_void_p).
     lib.mac_csc_solve_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                           _P(ctypes.c_int), _P(ctypes.c_double)]
+    i32, i64, f32, f64 = ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+    lib.mac_unet_create.argtypes = [i32, _P(vp)]
+    lib.mac_unet_destroy.argtypes = [vp]
+    lib.mac_unet_nparams.argtypes = [vp, _P(i64)]
+    lib.mac_unet_init.argtypes = [vp, ctypes.c_uint64]
+    lib.mac_unet_get_params.argtypes = [vp, _P(f32), _P(f32)]
+    lib.mac_unet_set_params.argtypes = [vp, _P(f32), f32]
+    lib.mac_unet_forward.argtypes = [vp, i32, i32, i32, i32, _P(f32), _P(ctypes.c_int8), _P(f32)]
+    lib.mac_unet_loss_grad.argtypes = [vp, i32, i32, i32, i32, _P(f32), _P(ctypes.c_int8), _P(f32), _P(f64),
+                                       _P(f32)]
+    lib.mac_unet_adam_step.argtypes = [vp, _P(f32), f32]
+    lib.mac_unet_make_dataset.argtypes = [vp, i32, i32, i32, i32, ctypes.c_uint64, _P(f64)]
+    lib.mac_unet_get_sample.argtypes = [vp, i32, _P(f32), _P(f32), _P(ctypes.c_int8)]
+    lib.mac_unet_train.argtypes = [vp, i32, i32, f32, ctypes.c_uint64, _P(f32)]
+    lib.mac_unet_launch_count.argtypes = [vp, _P(i64)]
     _lib = lib
     return lib
 
