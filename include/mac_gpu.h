@@ -34,7 +34,10 @@ enum {
 enum {
   MAC_SOLVER_MGPCG_FP64 = 0,  /* plain form: FP64 multigrid-preconditioned CG */
   MAC_SOLVER_MGPCG_MIXED = 1, /* FP32 multigrid inside FP64 CG */
-  MAC_SOLVER_CG_FP64 = 2      /* Jacobi-preconditioned CG (reference for the others) */
+  MAC_SOLVER_CG_FP64 = 2,     /* Jacobi-preconditioned CG (reference for the others) */
+  MAC_SOLVER_LEARNED = 3,     /* flexible CG with the learned preconditioner (mac_set_preconditioner_net);
+                                 FP64 MG-PCG takes over when it stalls */
+  MAC_SOLVER_LEARNED_MIXED = 4 /* the same, with the FP32 multigrid as the fall-back */
 };
 
 /* Cell materials, as Data_CellType_Fluid_Air_Solid_Inflow::MaterialToInt
@@ -94,6 +97,8 @@ typedef struct {
   int64_t live_bricks;
   int64_t particles;
   int64_t total_iterations; /* accumulated over the context's life */
+  int32_t learned_iterations; /* iterations of the last solve with the learned preconditioner */
+  int32_t fallbacks;          /* solves (over the context's life) where MG-PCG took over */
 } mac_stats;
 
 /* ---- context ---- */
@@ -201,7 +206,17 @@ int mac_unet_make_dataset(void* net, int nmasks, int size, int nsnap, int niter,
 int mac_unet_get_sample(void* net, int index, float* r, float* e, int8_t* mask);
 /* steps Adam steps on random batches of the training set; losses[steps] (may be NULL). */
 int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, float* losses);
+/* Training loss: 0 = mean squared error of the correction (default), 1 = its
+ * energy norm sum d (M d) / count, d = correction - target, M the unit operator. */
+int mac_unet_set_loss(void* net, int kind);
 int mac_unet_launch_count(void* net, int64_t* count);
+
+/* Attaches a network (mac_unet_create) as the preconditioner of the
+ * MAC_SOLVER_LEARNED* solvers; NULL detaches it. The context does not own it. */
+int mac_set_preconditioner_net(void* ctx, void* net);
+/* Weight of the Jacobi step applied after the network (z += omega D^-1 (r - M z));
+ * 0 turns it off. Default 0.8. */
+int mac_set_learned_smoothing(void* ctx, double omega);
 
 /* ---- allocation-free CSC solve (no counterpart in the reference) ----
  * The same FP64 Jacobi-PCG as mac_csc_factorize + mac_csc_solve, for callers

@@ -162,6 +162,10 @@ struct Ctx {
   void* mg_w[kLevels] = {};   // [4][cells]: left-face weights x,y,z and Dirichlet diagonal
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
+  // learned preconditioner (flexible CG): the network and the previous z
+  void* unet = nullptr;
+  double* zold = nullptr;
+  double learned_omega = 0.8;
   int* dbl = nullptr;          // bricks holding an in-domain cell
   int ndom_host = 0;
   DenseGrid g3{};
@@ -363,6 +367,9 @@ inline int grid_for(int64_t n, int threads) {
 // ------------------------------------------------------------- launchers
 // Implemented in the .cu files; all enqueue on ctx->stream.
 int check(cudaError_t e);
+bool learned_solver(const Ctx* c);
+int learned_begin(Ctx* c);
+int learned_precondition(Ctx* c, int first);
 int topology_rebuild(Ctx* c, bool first_init_order);
 int topo_initialize(Ctx* c);
 int topo_layer_initial(Ctx* c);

@@ -19,7 +19,10 @@
 #include <cstring>
 #include <utility>
 
+#include <vector>
+
 #include "mac_internal.cuh"
+#include "mac_unet.cuh"
 
 namespace mac {
 
@@ -44,7 +47,7 @@ int alloc_solver(Ctx* c) {
   A(dalloc(&c->dbl, c->cap_bricks));
   c->npartial = 2 * c->cap_bricks + 64;
   A(dalloc(&c->partial, c->npartial));
-  c->mg_float = c->prm.solver == MAC_SOLVER_MGPCG_MIXED;
+  c->mg_float = c->prm.solver == MAC_SOLVER_MGPCG_MIXED || c->prm.solver == MAC_SOLVER_LEARNED_MIXED;
   size_t ts = c->mg_float ? 4 : 8;
   for (int l = 0; l < 3; ++l) {
     size_t n = (size_t)c->cap_bricks * (size_t)((8 >> l) * (8 >> l) * (8 >> l));
@@ -66,6 +69,7 @@ int alloc_solver(Ctx* c) {
 void free_solver(Ctx* c) {
   cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
+  cudaFree(c->zold);
   for (int l = 0; l < kLevels; ++l) {
     cudaFree(c->mg_e[l]); cudaFree(c->mg_e2[l]); cudaFree(c->mg_r[l]); cudaFree(c->mg_w[l]);
   }
@@ -423,6 +427,122 @@ __global__ void __launch_bounds__(kBT) k_divmax(const int* __restrict__ dbl, con
 __global__ void k_zero_div(Scalars* ds) { ds->div_bits = 0; }
 
 // ------------------------------------------------------------ drivers
+// ------------------------------------------- learned preconditioner glue
+// The domain's bounding box of bricks as a dense grid (x fastest): residual
+// (FP32) and the network's cell mask (1 in the domain, -1 solid, 0 otherwise:
+// air and missing cells are Dirichlet), one block per brick of the box.
+__global__ void __launch_bounds__(512) k_to_dense(const unsigned long long* __restrict__ hk,
+                                                  const int* __restrict__ hv, int64_t hcap,
+                                                  const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
+                                                  const uint16_t* __restrict__ fmask, const double* __restrict__ r,
+                                                  int bx, int by, int bz, int nbx, int nby, float* rd, int8_t* md) {
+  const int i = blockIdx.x;
+  const int kx = i % nbx, ky = (i / nbx) % nby, kz = i / (nbx * nby);
+  __shared__ int b;
+  if (threadIdx.x == 0) b = hash_find(hk, hv, hcap, pack_key(bx + kx, by + ky, bz + kz));
+  __syncthreads();
+  const int o = threadIdx.x;
+  const int x = kx * 8 + (o & 7), y = ky * 8 + ((o >> 3) & 7), z = kz * 8 + (o >> 6);
+  const size_t di = ((size_t)z * (nby * 8) + y) * (size_t)(nbx * 8) + x;
+  float rv = 0.0f;
+  int8_t mv = 0;
+  if (b >= 0) {
+    const int64_t c = (int64_t)b * kCells + o;
+    if (fmask[c] & kDomainBit) {
+      rv = (float)r[c];
+      mv = 1;
+    } else if (lay[c] != kMissing && type[c] == MAC_CELL_SOLID) {
+      mv = -1;
+    }
+  }
+  rd[di] = rv;
+  md[di] = mv;
+}
+
+// z = scale * (network correction) on domain cells, 0 elsewhere, then one
+// weighted Jacobi step z += omega D^-1 (r - M z) (omega = 0: none; the
+// neighbours' corrections are read from the dense grid); partials of r.z (new)
+// and r.zold for the flexible (Polak-Ribiere) beta.
+__global__ void __launch_bounds__(512) k_from_dense(const int* __restrict__ dbl, const int* __restrict__ bkey,
+                                                    const uint16_t* __restrict__ fmask, const float* __restrict__ zd,
+                                                    int bx, int by, int bz, int nbx, int nby, double scale,
+                                                    double omega, const double* __restrict__ r,
+                                                    const double* __restrict__ zold, double* __restrict__ z,
+                                                    double* partial, Params P) {
+  const int b = dbl[blockIdx.x];
+  const int o = threadIdx.x;
+  const int64_t c = (int64_t)b * kCells + o;
+  const int x = (bkey[3 * b] - bx) * 8 + (o & 7), y = (bkey[3 * b + 1] - by) * 8 + ((o >> 3) & 7),
+            zz = (bkey[3 * b + 2] - bz) * 8 + (o >> 6);
+  const uint16_t m = fmask[c];
+  double v = 0.0, rz = 0.0, rzo = 0.0;
+  if (m & kDomainBit) {
+    const int64_t sx = 1, sy = (int64_t)nbx * 8, sz = sy * (int64_t)(nby * 8);
+    const int64_t di = zz * sz + y * sy + x;
+    v = scale * (double)zd[di];
+    if (omega > 0.0) {
+      const int64_t off[6] = {-sx, sx, -sy, sy, -sz, sz};
+      double mz = 0.0;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (m & (1u << (8 + f))) mz += P.ih2[f >> 1] * v;
+        if (m & (1u << f)) mz -= P.ih2[f >> 1] * scale * (double)zd[di + off[f]];
+      }
+      v += omega * P.dtab[active_index(m)] * (r[c] - mz);
+    }
+    rz = r[c] * v;
+    rzo = r[c] * zold[c];
+  }
+  z[c] = v;
+  block_sum<512>(rz, rzo, partial);
+}
+
+// beta = (r.z - r.zold) / rz_prev (Polak-Ribiere; 0 on a restart), rz = r.z
+__global__ void k_fin_beta_flex(const double* partial, int nblk, Scalars* ds, int first) {
+  if (ds->done) return;
+  double rz, rzo;
+  sum_partials(partial, nblk, &rz, &rzo);
+  if (threadIdx.x == 0) {
+    ds->beta = first ? 0.0 : (ds->rz != 0 ? (rz - rzo) / ds->rz : 0.0);
+    ds->rz = rz;
+  }
+}
+
+bool learned_solver(const Ctx* c) {
+  return (c->prm.solver == MAC_SOLVER_LEARNED || c->prm.solver == MAC_SOLVER_LEARNED_MIXED) && c->unet;
+}
+
+// Allocates (once) and clears the previous-z vector of the flexible CG.
+int learned_begin(Ctx* c) {
+  if (!c->zold) {
+    int rc = check(cudaMalloc((void**)&c->zold, 8 * (size_t)c->cap_bricks * kCells));
+    if (rc) return rc;
+  }
+  return check(cudaMemsetAsync(c->zold, 0, 8 * (size_t)c->cap_bricks * kCells, c->stream));
+}
+
+// z = network(r) on the domain's brick box (+ the Jacobi step), then beta.
+int learned_precondition(Ctx* c, int first) {
+  const int* bb = c->hs->bbox;
+  const int nbx = bb[3] - bb[0] + 1, nby = bb[4] - bb[1] + 1, nbz = bb[5] - bb[2] + 1;
+  float *rd = nullptr, *zd = nullptr;
+  int8_t* md = nullptr;
+  int rc = unet::stage((unet::Net*)c->unet, 1, nbz * 8, nby * 8, nbx * 8, &rd, &md, &zd);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  std::swap(c->z, c->zold);
+  k_to_dense<<<nbx * nby * nbz, 512, 0, st>>>(c->hkeys, c->hval, c->hcap, c->lay, c->type, c->fmask, c->r, bb[0],
+                                              bb[1], bb[2], nbx, nby, rd, md); MAC_COUNT(c);
+  rc = unet::apply((unet::Net*)c->unet, st);
+  if (rc) return rc;
+  // the network inverts the unit-spacing operator; M = (unit operator) / h^2
+  const double scale = 1.0 / c->dp.ih2[0];
+  k_from_dense<<<c->ndom_host, 512, 0, st>>>(c->dbl, c->bkey, c->fmask, zd, bb[0], bb[1], bb[2], nbx, nby, scale,
+                                             c->learned_omega, c->r, c->zold, c->z, c->partial, c->dp); MAC_COUNT(c);
+  k_fin_beta_flex<<<1, 1024, 0, st>>>(c->partial, c->ndom_host, c->ds, first); MAC_COUNT(c);
+  return check(cudaGetLastError());
+}
+
 int setup_system(Ctx* c) {
   cudaStream_t st = c->stream;
   int n = c->nlive_host;
@@ -477,12 +597,26 @@ int project(Ctx* c, int ib) {
       k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
     }
     int first = 1;
+    // Learned preconditioner: flexible CG until it stalls (the residual norm
+    // falls by less than 2x over kStallWindow iterations, or kLearnedMax
+    // iterations pass), then MG-PCG restarts from the current iterate.
+    bool learned = learned_solver(c);
+    if (learned && (rc = learned_begin(c))) return rc;
+    constexpr int kStallWindow = 8, kLearnedMax = 200;
+    std::vector<double> hist;
+    c->stats.learned_iterations = 0;
     while (true) {
       prof_begin(c, PH_VCYCLE);
-      precondition(c);
+      if (learned) {
+        if ((rc = learned_precondition(c, first))) return rc;
+      } else {
+        precondition(c);
+      }
       prof_end(c, PH_VCYCLE);
       prof_begin(c, PH_CGVEC);
-      k_fin_beta<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, first); MAC_COUNT(c);
+      if (!learned) {
+        k_fin_beta<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, first); MAC_COUNT(c);
+      }
       prof_end(c, PH_CGVEC);
       prof_begin(c, PH_SPMV);
       std::swap(c->pd, c->pd2);  // pd2: previous direction, pd: new one
@@ -498,6 +632,20 @@ int project(Ctx* c, int ib) {
       rc = read_scalars(c);
       if (rc) return rc;
       if (c->hs->done) break;
+      if (learned) {
+        hist.push_back(c->hs->rr);
+        const int k = (int)hist.size();
+        c->stats.learned_iterations = k;
+        const bool stalled = k >= kStallWindow && hist[k - 1] > 0.25 * hist[k - kStallWindow];
+        if (stalled || k >= kLearnedMax) {
+          // MG-PCG from the current x: true residual, fresh directions
+          learned = false;
+          c->stats.fallbacks += 1;
+          k_residual<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
+          k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
+          first = 1;
+        }
+      }
     }
     double relres = c->hs->bnorm2 > 0 ? sqrt(c->hs->rr / c->hs->bnorm2) : 0.0;
     c->stats.iterations = c->hs->iters;

@@ -236,6 +236,19 @@ int mac_step(void* ctx) {
   return mac::step(c);
 }
 
+int mac_set_preconditioner_net(void* ctx, void* net) {
+  CTX_OR_FAIL();
+  c->unet = net;
+  return MAC_OK;
+}
+
+int mac_set_learned_smoothing(void* ctx, double omega) {
+  CTX_OR_FAIL();
+  if (!(omega >= 0.0 && omega < 2.0)) return MAC_ERR_INVALID;
+  c->learned_omega = omega;
+  return MAC_OK;
+}
+
 int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value) {
   CTX_OR_FAIL();
   if (n < 0 || (n > 0 && (!offset || !indice || !value))) return MAC_ERR_INVALID;

@@ -535,6 +535,55 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
   if (threadIdx.x == 0) atomicAdd(loss, acc * inv_count);
 }
 
+// Energy-norm loss, first pass: d = out - e / (rms(r) tscale) on fluid voxels, 0 elsewhere.
+__global__ void k_loss_diff(const float* __restrict__ out, const float* __restrict__ e, const int8_t* __restrict__ m,
+                            const double* sums, int V1, float tscale, float* dbuf) {
+  const size_t base = (size_t)blockIdx.y * V1;
+  const double tinv = 1.0 / (sample_scale(sums, blockIdx.y) * tscale);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < V1; i += gridDim.x * blockDim.x)
+    dbuf[base + i] = m[base + i] == 1 ? (float)((double)out[base + i] - (double)e[base + i] * tinv) : 0.0f;
+}
+
+// Second pass: loss = sum over fluid voxels of d (M d) / count with M the
+// unit-spacing operator of the mask (the one the training pairs solve), and
+// the output gradient 2 (M d) / count (M is symmetric).
+__global__ void k_loss_energy(const float* __restrict__ dbuf, const int8_t* __restrict__ m, const double* sums,
+                              int nsamples, int d, int h, int w, bf16* gout, double* loss) {
+  double total = 0;
+  for (int k = 0; k < nsamples; ++k) total += sums[2 * k + 1];
+  const double inv_count = total > 0 ? 1.0 / total : 0.0;
+  const int V1 = d * h * w;
+  const size_t base = (size_t)blockIdx.y * V1;
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < V1; i += gridDim.x * blockDim.x) {
+    float gv = 0.0f;
+    if (m[base + i] == 1) {
+      const int x = i % w, y = (i / w) % h, z = i / (w * h);
+      const int c[3] = {x, y, z}, n[3] = {w, h, d}, stride[3] = {1, w, w * h};
+      const double dc = dbuf[base + i];
+      double q = 0;
+      for (int a = 0; a < 3; ++a)
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+          const int cc = c[a] + sgn;
+          if (cc < 0 || cc >= n[a]) continue;
+          const size_t j = base + i + sgn * stride[a];
+          if (m[j] == -1) continue;
+          q += dc - (m[j] == 1 ? (double)dbuf[j] : 0.0);
+        }
+      acc += dc * q;
+      gv = (float)(2.0 * q * inv_count);
+    }
+    uint4 qv = make_uint4(0, 0, 0, 0);
+    __nv_bfloat162 b2 = __floats2bfloat162_rn(gv, 0.0f);
+    qv.x = *reinterpret_cast<uint32_t*>(&b2);
+    uint4* dst = reinterpret_cast<uint4*>(gout + (base + i) * 16);
+    dst[0] = qv;
+    dst[1] = make_uint4(0, 0, 0, 0);
+  }
+  acc = bsum(acc);
+  if (threadIdx.x == 0) atomicAdd(loss, acc * inv_count);
+}
+
 // Correction in the units of r: z = out * rms(r) * tscale on fluid voxels, 0 elsewhere.
 __global__ void k_out_scale(const float* __restrict__ out, const int8_t* __restrict__ m, const double* sums, int V1,
                             float tscale, float* z) {
@@ -803,11 +852,12 @@ struct Net {
   bf16* wb = nullptr;
   long adam_t = 0;
   float tscale = 1.0f;
+  int loss_kind = 0;  // 0: mean squared error, 1: energy norm of the error
   int n = 0, d = 0, h = 0, w = 0;
   size_t cap = 0;  // level-0 voxels the shape buffers hold
   bf16* act[kNumAct] = {};
   bf16* grad[kNumAct] = {};
-  float *out = nullptr, *r = nullptr, *e = nullptr;
+  float *out = nullptr, *r = nullptr, *e = nullptr, *dbuf = nullptr;
   int8_t* m = nullptr;
   double *sums = nullptr, *loss = nullptr;
   int* err = nullptr;
@@ -833,7 +883,8 @@ static void free_shape(Net& t) {
   cudaFree(t.r);
   cudaFree(t.e);
   cudaFree(t.m);
-  t.out = t.r = t.e = nullptr;
+  cudaFree(t.dbuf);
+  t.out = t.r = t.e = t.dbuf = nullptr;
   t.m = nullptr;
   t.cap = 0;
 }
@@ -859,6 +910,7 @@ static int ensure_shape(Net& t, int n, int d, int h, int w) {
     if (!rc) rc = cuda_ok(cudaMalloc((void**)&t.r, v0 * 4));
     if (!rc) rc = cuda_ok(cudaMalloc((void**)&t.e, v0 * 4));
     if (!rc) rc = cuda_ok(cudaMalloc((void**)&t.m, v0));
+    if (!rc) rc = cuda_ok(cudaMalloc((void**)&t.dbuf, v0 * 4));
     if (rc) {
       free_shape(t);
       return rc;
@@ -1144,8 +1196,14 @@ static int loss_grad(Net& t, double* loss_dst, cudaStream_t st) {
   const int V1 = t.d * t.h * t.w;
   cudaMemsetAsync(loss_dst, 0, sizeof(double), st);
   const dim3 g((V1 + 255) / 256 < 148 ? (V1 + 255) / 256 : 148, t.n);
-  k_loss<<<g, 256, 0, st>>>(t.out, t.e, t.m, t.sums, t.n, V1, t.tscale, t.grad[GOUT], loss_dst);
-  ++t.launches;
+  if (t.loss_kind == 1) {
+    k_loss_diff<<<g, 256, 0, st>>>(t.out, t.e, t.m, t.sums, V1, t.tscale, t.dbuf);
+    k_loss_energy<<<g, 256, 0, st>>>(t.dbuf, t.m, t.sums, t.n, t.d, t.h, t.w, t.grad[GOUT], loss_dst);
+    t.launches += 2;
+  } else {
+    k_loss<<<g, 256, 0, st>>>(t.out, t.e, t.m, t.sums, t.n, V1, t.tscale, t.grad[GOUT], loss_dst);
+    ++t.launches;
+  }
   if (!rc) rc = backward(t, st);
   return rc;
 }
@@ -1428,6 +1486,12 @@ int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, flo
   if (!t) return MAC_ERR_INVALID;
   cudaSetDevice(t->device);
   return mac::unet::train(*t, steps, batch, lr, seed, losses, 0);
+}
+
+int mac_unet_set_loss(void* net, int kind) {
+  if (!net || kind < 0 || kind > 1) return MAC_ERR_INVALID;
+  ((Net*)net)->loss_kind = kind;
+  return MAC_OK;
 }
 
 int mac_unet_launch_count(void* net, int64_t* count) {

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "libmac_gpu.so")
 MAC_OK = 0
 ERRORS = {-1: "invalid", -2: "cuda", -3: "capacity", -4: "not converged", -5: "no device",
           -6: "out of memory", -7: "timeout"}
-SOLVERS = {"mgpcg64": 0, "mixed": 1, "cg64": 2}
+SOLVERS = {"mgpcg64": 0, "mixed": 1, "cg64": 2, "learned": 3, "learned_mixed": 4}
 
 
 class MacError(RuntimeError):
@@ -52,7 +52,8 @@ class mac_stats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("solves", ctypes.c_int32), ("relres", ctypes.c_double),
                 ("max_div", ctypes.c_double), ("fluid_cells", ctypes.c_int64), ("unknowns", ctypes.c_int64),
                 ("live_bricks", ctypes.c_int64), ("particles", ctypes.c_int64),
-                ("total_iterations", ctypes.c_int64)]
+                ("total_iterations", ctypes.c_int64), ("learned_iterations", ctypes.c_int32),
+                ("fallbacks", ctypes.c_int32)]
 
 
 EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_stats", "mac_error_string",
@@ -64,7 +65,8 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc",
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
-           "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count"]
+           "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_unet_set_loss"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -121,6 +123,9 @@ def load(path: str = LIB_PATH):
     lib.mac_unet_get_sample.argtypes = [vp, i32, _P(f32), _P(f32), _P(ctypes.c_int8)]
     lib.mac_unet_train.argtypes = [vp, i32, i32, f32, ctypes.c_uint64, _P(f32)]
     lib.mac_unet_launch_count.argtypes = [vp, _P(i64)]
+    lib.mac_set_preconditioner_net.argtypes = [vp, vp]
+    lib.mac_set_learned_smoothing.argtypes = [vp, f64]
+    lib.mac_unet_set_loss.argtypes = [vp, i32]
     _lib = lib
     return lib
 
@@ -349,6 +354,15 @@ class Context:
         cnt = (ctypes.c_int64 * n)()
         self._check(self.lib.mac_get_profile(self.h, ms, cnt, n), "mac_get_profile")
         return {PHASES[i]: (ms[i], cnt[i]) for i in range(n)}
+
+    def set_preconditioner(self, net):
+        """Attaches a mac_b200.unet.UNet (or None) for the "learned" solvers."""
+        self._check(self.lib.mac_set_preconditioner_net(self.h, net.h if net is not None else None),
+                    "mac_set_preconditioner_net")
+        self._net = net
+
+    def set_learned_smoothing(self, omega):
+        self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
 
     # ---- drop-in CSC solver
     def csc_solve(self, offset, indice, value, b):

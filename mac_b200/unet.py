@@ -105,6 +105,19 @@ class UNet:
                                             losses.ctypes.data_as(_P(ctypes.c_float))), "mac_unet_train")
         return losses
 
+    def set_loss(self, kind):
+        """Training loss: "mse" (mean squared error) or "energy" (energy norm of the error)."""
+        self._check(self.lib.mac_unet_set_loss(self.h, {"mse": 0, "energy": 1}[kind]), "mac_unet_set_loss")
+
+    def save(self, path):
+        p, t = self.params()
+        np.savez_compressed(path, params=p, tscale=np.float32(t))
+
+    def load(self, path):
+        """Weights saved by save() or by mac_b200.train_preconditioner."""
+        d = np.load(path)
+        self.set_params(d["params"], float(d["tscale"]))
+
     def launches(self):
         n = ctypes.c_int64()
         self._check(self.lib.mac_unet_launch_count(self.h, ctypes.byref(n)), "mac_unet_launch_count")

@@ -121,6 +121,7 @@ class Net:
         self.W, self.b = unpack(params)
         self.tscale = float(tscale)
         self.q = to_bf16 if bf16 else (lambda a: np.asarray(a, np.float64))
+        self.f32 = (lambda a: np.asarray(a, np.float32).astype(np.float64)) if bf16 else self.q
         if bf16:
             self.W = [to_bf16(w) for w in self.W]
 
@@ -176,18 +177,27 @@ class Net:
         out, c = self.forward(r, m)
         return np.where(m == 1, out * (c["s"][:, None, None, None] * self.tscale), 0.0)
 
-    def loss_grad(self, r, m, e):
-        """Loss and the flattened parameter gradient (device layout)."""
+    def loss_grad(self, r, m, e, kind="mse"):
+        """Loss and the flattened parameter gradient (device layout). kind
+        "mse": mean squared error of the output against e / (rms(r) tscale);
+        "energy": sum d (M d) / count with d that difference and M the
+        unit-spacing operator of the mask."""
         q, W = self.q, self.W
         out, c = self.forward(r, m)
         s = c["s"]
         fluid = m == 1
         count = fluid.sum()
         t = e / (s[:, None, None, None] * self.tscale)
-        diff = np.where(fluid, out - t, 0.0)
-        loss = float(np.sum(diff ** 2) / count)
         g = np.zeros(out.shape + (16,))
-        g[..., 0] = q(2.0 * diff / count)
+        if kind == "energy":
+            d = np.where(fluid, self.f32(out - t), 0.0)
+            Md = np.stack([dense_operator_apply(d[k], m[k]) for k in range(d.shape[0])])
+            loss = float(np.sum(d * Md) / count)
+            g[..., 0] = q(np.where(fluid, 2.0 * Md / count, 0.0))
+        else:
+            diff = np.where(fluid, out - t, 0.0)
+            loss = float(np.sum(diff ** 2) / count)
+            g[..., 0] = q(2.0 * diff / count)
         dW = [None] * 13
         dB = [None] * 13
 

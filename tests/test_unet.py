@@ -6,7 +6,7 @@ Device tolerances: the device stores activations and activation gradients in
 BF16 exactly where the oracle rounds them, but accumulates in FP32 (the oracle
 in FP64), so a rounding can land on the other side of a BF16 step: relative L2
 error <= 2e-2 for the network output and the loss, <= 5e-2 for each layer's
-weight gradient, 1e-5 for the FP32 Adam update.
+weight gradient (1e-1 under the energy loss), 1e-5 for the FP32 Adam update.
 """
 import numpy as np
 import pytest
@@ -64,6 +64,24 @@ def test_oracle_gradient_matches_finite_differences():
             assert abs(fd - g[i]) <= 1e-5 * max(1e-3, abs(fd), abs(g[i])), (i, fd, g[i])
             checked += 1
     assert checked == 3 * len(U.LAYERS)
+
+
+def test_oracle_energy_gradient_matches_finite_differences():
+    p = _random_params(7)
+    r, m, e = _problem(1, 8, 8)
+    _, g = U.Net(p, 0.7, bf16=False).loss_grad(r, m, e, kind="energy")
+    rng = np.random.default_rng(9)
+    offs, _ = U.offsets()
+    for (wo, bo), (cin, cout, taps, relu, rcin, rcout) in list(zip(offs, U.LAYERS))[::3]:
+        i = wo + (int(rng.integers(taps)) * cout + int(rng.integers(rcout))) * cin + int(rng.integers(rcin))
+        h = 1e-6 * max(1.0, abs(p[i]))
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        lp = U.Net(pp, 0.7, bf16=False).loss_grad(r, m, e, kind="energy")[0]
+        lm = U.Net(pm, 0.7, bf16=False).loss_grad(r, m, e, kind="energy")[0]
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-5 * max(1e-3, abs(fd), abs(g[i])), (i, fd, g[i])
 
 
 def test_oracle_padding_gradients_vanish():
@@ -125,6 +143,24 @@ def test_device_gradients_match_oracle(unet):
     offs, _ = U.offsets()
     for (wo, bo), (cin, cout, *_r) in zip(offs, U.LAYERS):
         assert _rel(g[bo:bo + cout], wg[bo:bo + cout]) <= 5e-2
+
+
+@pytest.mark.gpu
+def test_device_energy_loss_gradients_match_oracle(unet):
+    p = _random_params(25).astype(np.float32)
+    unet.set_params(p, 0.5)
+    unet.set_loss("energy")
+    try:
+        r, m, e = _problem(2, 16, 26)
+        loss, g = unet.loss_grad(r, m, e)
+    finally:
+        unet.set_loss("mse")
+    wl, wg = U.Net(p, 0.5).loss_grad(r, m, e, kind="energy")
+    assert abs(loss - wl) <= 2e-2 * wl, (loss, wl)
+    # the energy gradient 2 M d / count differences neighbouring output errors,
+    # so the BF16 rounding flips weigh about twice as much as in the MSE case
+    errs = [_rel(g[a:b], wg[a:b]) for a, b in _layer_slices()]
+    assert max(errs) <= 1e-1, errs
 
 
 @pytest.mark.gpu
