@@ -179,14 +179,22 @@ def reduce_over_ranks(seconds: float, count: float, device) -> tuple:
 
 
 # ------------------------------------------------------------- our arm
-def roofline_models(ctx_stats, prof, np_count, n_exist):
+def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8):
     """Achieved GB/s per phase from algorithmic bytes (every array element a
-    kernel must touch, read or written once) over the measured event times."""
+    kernel must touch, read or written once) over the measured event times.
+    A "launch" is one timed region of the phase (one V-cycle, one CG update)."""
     unk = ctx_stats["unknowns"]
+    # V-cycle: per cell of a level, 2 pre + 2 post sweeps of 17 B, residual 25 B,
+    # restriction 8 B and prolongation 16 B at FP64 (117 B), the levels adding
+    # up to 8/7 of the finest; FP32 storage halves it.
+    vc = 117.0 * 8.0 / 7.0 * (mg_bytes / 8.0)
     models = {
         # phase: (bytes per launch, description)
         "move": (48.0 * np_count, "48 B per particle (read + write 3 FP64 positions)"),
-        "spmv": (18.0 * unk, "18 B per unknown (read p 8, face mask 2, write q 8)"),
+        "vcycle": (vc * unk, f"{vc:.1f} B per unknown per V-cycle (levels 0.. at {mg_bytes} B per value)"),
+        "spmv": (34.0 * unk, "34 B per unknown (read z, p_old 16, face mask 2, write p, q 16)"),
+        "cg_vector": (24.0 * unk, "24 B per unknown per region (x, p, r, q read, x, r written: 48 B "
+                                   "per iteration over its 2 regions)"),
         "forces": (75.0 * n_exist, "75 B per existing cell (mean of stage 1: 51, stage 2: 99)"),
         "gradient": (67.0 * n_exist, "67 B per existing cell (x 8, flags 3, p 8, u read+write 48)"),
         "divergence": (42.0 * unk, "42 B per unknown (u 24, mask 2, rhs 8, x 8)"),
@@ -202,27 +210,48 @@ def roofline_models(ctx_stats, prof, np_count, n_exist):
 
 POISSON_N = 128
 POISSON_RTOL = 1e-10
+WEIGHTS = os.path.join(ROOT, "mac_b200", "weights", "unet_pool64.npz")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def poisson_solves(dev, reps=3):
     """Standalone pressure solve of the 128^3 pool + 12 spheres world (solid box,
     face speeds uniform in [-1, 1]) to a relative residual of 1e-10: device time
     of one projection and of its solve (system set-up + CG iterations), per
-    solver form, with the pressure error against an FP64 MG-PCG solve to 1e-13."""
+    solver form, with the pressure error against an FP64 MG-PCG solve to 1e-13.
+    The learned forms use the weights trained by mac_b200.train_preconditioner
+    (skipped when the weights file is absent); the network's forward pass on the
+    solve's dense grid is timed alone for its tensor-pipe roofline."""
     import torch
     from mac_b200.gpu import Context
     from mac_b200.state import FLUID, pool_spheres_world
     from mac_b200.world import setup_passes
+    net = None
+    if os.path.exists(WEIGHTS):
+        from mac_b200.unet import UNet
+        net = UNet(dev)
+        net.load(WEIGHTS)
 
     s = setup_passes(pool_spheres_world(POISSON_N))
     dom = s.exists.astype(bool) & (s.type == FLUID)
     res = {"workload": f"pool z<0.4n + 12 spheres r~U[6,20], {POISSON_N}^3, solid box, u~U[-1,1] (seeds 2, 3)",
            "rtol": POISSON_RTOL}
     p_ref = None
-    for name, solver, rtol in (("reference", "mgpcg64", 1e-13), ("plain", "mgpcg64", POISSON_RTOL),
-                               ("mixed", "mixed", POISSON_RTOL)):
+    forms = [("reference", "mgpcg64", 1e-13), ("plain", "mgpcg64", POISSON_RTOL), ("mixed", "mixed", POISSON_RTOL)]
+    if net is not None:
+        forms += [("learned", "learned", POISSON_RTOL), ("learned_mixed", "learned_mixed", POISSON_RTOL)]
+    for name, solver, rtol in forms:
         with Context(s.params, max_bricks=8192, max_particles=1024, solver=solver, rtol=rtol, max_iters=1000,
                      device=dev) as ctx:
+            if net is not None:
+                ctx.set_preconditioner(net)
             stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
             times, solve = [], []
             for r in range(reps + 1):
@@ -251,6 +280,19 @@ def poisson_solves(dev, reps=3):
             err = float(np.linalg.norm(p - p_ref) / np.linalg.norm(p_ref))
         res[name] = {"project_ms": round(float(np.median(times)), 3), "solve_ms": round(float(np.median(solve)), 3),
                      "iterations": int(st["iterations"]), "relres": st["relres"], "p_rel_err_vs_fp64": err}
+        if solver.startswith("learned"):
+            res[name].update({"learned_iterations": int(st["learned_iterations"]),
+                              "fallback_to_mgpcg": bool(st["fallbacks"])})
+    if net is not None:
+        ms, flops = net.time_forward(1, POISSON_N, POISSON_N, POISSON_N, reps=5)
+        pk = _peaks()
+        peak = pk.get("bf16_tflops", 1590.0)
+        tf = flops / (ms * 1e-3) / 1e12
+        res["network_roofline"] = {"bound": "tensor", "grid": f"{POISSON_N}^3", "ms_per_forward": round(ms, 3),
+                                   "flops_per_forward": flops, "achieved": round(tf, 1), "peak": peak,
+                                   "unit": "TFLOP/s", "frac": round(tf / peak, 4),
+                                   "peak_source": "measured" if "bf16_tflops" in pk else "fallback"}
+        net.close()
     return res
 
 
@@ -335,7 +377,7 @@ def run_ours(args, rank, world, local_rank):
            "d2h_bytes_per_step": bo // e2e_steps, "steps": e2e_steps}
 
     n_exist = int(st["live_bricks"] * 512)  # upper bound of existing cells (slots of live bricks)
-    rl = roofline_models(st, prof, st["particles"], n_exist)
+    rl = roofline_models(st, prof, st["particles"], n_exist, 4 if args.solver == "mixed" else 8)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

@@ -210,6 +210,9 @@ int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, flo
  * energy norm sum d (M d) / count, d = correction - target, M the unit operator. */
 int mac_unet_set_loss(void* net, int kind);
 int mac_unet_launch_count(void* net, int64_t* count);
+/* Device time of one forward pass (mean over reps, CUDA events) on an n x d x h x w
+ * grid and its algorithmic FLOPs (2 taps cin cout per output cell, unpadded channels). */
+int mac_unet_time_forward(void* net, int n, int d, int h, int w, int reps, double* ms, double* flops);
 
 /* Attaches a network (mac_unet_create) as the preconditioner of the
  * MAC_SOLVER_LEARNED* solvers; NULL detaches it. The context does not own it. */

@@ -174,6 +174,8 @@ struct Ctx {
   void* dense_buf = nullptr;   // dense levels: 9 arrays (e, e2, r, 6 weights) per cell
   size_t dense_bytes = 0;
   size_t dense_smem = 0;
+  double* coarse_inv = nullptr;  // [64][64] inverse of the coarsest dense level
+  int* coarse_ok = nullptr;      // 1 when coarse_inv is valid
   int smem_optin = 0;
   // scalars
   Scalars* ds = nullptr;      // device

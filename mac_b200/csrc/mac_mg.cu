@@ -11,7 +11,8 @@
 //            domain bricks, levels 4.. dense coarsenings of it.
 // Smoother: weighted Jacobi (two sweeps before and after the coarse
 // correction); the levels from 4 down are solved by one thread block in
-// shared memory. Storage type T is double (plain form) or float (mixed form).
+// shared memory, the coarsest (at most 64 cells) exactly with an inverse built
+// at set-up. Storage type T is double (plain form) or float (mixed form).
 #include <cstdio>
 #include <cstring>
 
@@ -424,8 +425,8 @@ struct DenseSet {
 
 template <class T>
 __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView<T>* C, bool first) {
-  for (int64_t i = threadIdx.x; i < L.n; i += blockDim.x) {
-    int64_t n = L.n;
+  const int n = (int)L.n;  // block-solved levels hold a few thousand cells: 32-bit index math
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double dinv = (double)L.w[4 * n + i];
     if (dinv == 0) {
       eout[i] = (T)0;
@@ -435,15 +436,16 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView
       eout[i] = (T)(kOmega * dinv * (double)L.r[i]);
       continue;
     }
-    int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
-    auto ev = [&](int64_t j, int xx, int yy, int zz) -> double {
+    const int xy = i / L.nx;
+    int x = i - xy * L.nx, y = xy % L.ny, z = xy / L.ny;
+    auto ev = [&](int j, int xx, int yy, int zz) -> double {
       double v = (double)ein[j];
-      if (C) v += (double)C->e[C->at(xx >> 1, yy >> 1, zz >> 1)];
+      if (C) v += (double)C->e[(xx >> 1) + C->nx * ((yy >> 1) + C->ny * (zz >> 1))];
       return v;
     };
     int c[3] = {x, y, z};
     int dim[3] = {L.nx, L.ny, L.nz};
-    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    int stride[3] = {1, L.nx, L.nx * L.ny};
     double ec = ev(i, x, y, z);
     double s = (double)L.w[3 * n + i] * ec;
     for (int a = 0; a < 3; ++a) {
@@ -467,18 +469,81 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView
 
 template <class T>
 __device__ void blk_restrict(const DView<T>& F, const DView<T>& C) {
-  for (int64_t I = threadIdx.x; I < C.n; I += blockDim.x) {
-    int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
+  for (int I = threadIdx.x; I < (int)C.n; I += blockDim.x) {
+    const int XY = I / C.nx;
+    int X = I - XY * C.nx, Y = XY % C.ny, Z = XY / C.ny;
     double s = 0;
     for (int k = 0; k < 8; ++k) {
       int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
       if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
-      int64_t i = F.at(x, y, z);
+      const int i = x + F.nx * (y + F.ny * z);
       if ((double)F.w[4 * F.n + i] == 0) continue;
       s += (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
     }
     C.r[I] = (T)s;
   }
+}
+
+// Inverse of the coarsest level's operator (n <= 64 cells), by Gauss-Jordan
+// elimination without pivoting (the operator is symmetric positive definite
+// once a cell without a stencil is given a unit row). ok = 0 when a pivot is
+// not positive (no Dirichlet cell anywhere: the V-cycle then keeps Jacobi sweeps).
+template <class T>
+__global__ void __launch_bounds__(1024) kd_coarsest_inverse(DView<T> L, double* inv, int* ok) {
+  __shared__ double A[64 * 64];
+  __shared__ double colk[64];
+  const int n = (int)L.n;
+  if (n > 64) {
+    if (threadIdx.x == 0) *ok = 0;
+    return;
+  }
+  for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) A[t] = 0.0;
+  __syncthreads();
+  if ((int)threadIdx.x < n) {
+    const int i = threadIdx.x;
+    const int xy = i / L.nx;
+    const int c[3] = {i - xy * L.nx, xy % L.ny, xy / L.ny};
+    const int dim[3] = {L.nx, L.ny, L.nz};
+    const int stride[3] = {1, L.nx, L.nx * L.ny};
+    if ((double)L.w[4 * L.n + i] == 0) {
+      A[i * 64 + i] = 1.0;
+    } else {
+      A[i * 64 + i] = (double)L.w[3 * L.n + i];
+      for (int a = 0; a < 3; ++a) {
+        if (c[a] > 0) {
+          const int j = i - stride[a];
+          if ((double)L.w[4 * L.n + j] != 0) A[i * 64 + j] = -(double)L.w[a * L.n + i];
+        }
+        if (c[a] + 1 < dim[a]) {
+          const int j = i + stride[a];
+          if ((double)L.w[4 * L.n + j] != 0) A[i * 64 + j] = -(double)L.w[a * L.n + j];
+        }
+      }
+    }
+  }
+  for (int k = 0; k < n; ++k) {
+    __syncthreads();
+    const double p = A[k * 64 + k];
+    if (!(p > 1e-300)) {
+      if (threadIdx.x == 0) *ok = 0;
+      return;
+    }
+    if ((int)threadIdx.x < n) colk[threadIdx.x] = A[threadIdx.x * 64 + k];
+    __syncthreads();
+    if ((int)threadIdx.x < n) {
+      const int j = threadIdx.x;
+      A[k * 64 + j] = (j == k ? 1.0 : A[k * 64 + j]) / p;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int i = t / n, j = t - i * n;
+      if (i == k) continue;
+      A[i * 64 + j] = (j == k ? 0.0 : A[i * 64 + j]) - colk[i] * A[k * 64 + j];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) inv[t] = A[t];
+  if (threadIdx.x == 0) *ok = 1;
 }
 
 template <class T>
@@ -487,7 +552,8 @@ __device__ void blk_copy(T* dst, const T* src, int64_t n) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem) {
+__global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem, const double* __restrict__ inv,
+                                                        const int* __restrict__ inv_ok) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   DenseSet<T> S = G;
   if (use_smem) {
@@ -516,15 +582,26 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
     blk_restrict(L, S.L[l + 1]);
     __syncthreads();
   }
-  // coarsest: Jacobi sweeps from zero
+  // coarsest: exact solve with the set-up's inverse, else Jacobi sweeps from zero
   {
     DView<T>& L = S.L[S.hi - 1];
-    blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
-    __syncthreads();
-    for (int s = 1; s < kCoarsestSweeps; ++s) {
-      blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+    if (*inv_ok && L.n <= 64) {
+      const int n = (int)L.n;
+      if ((int)threadIdx.x < n) {
+        const int i = threadIdx.x;
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += inv[i * 64 + j] * (double)L.r[j];
+        L.e[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
+      }
       __syncthreads();
-      T* t = L.e; L.e = L.e2; L.e2 = t;
+    } else {
+      blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
+      __syncthreads();
+      for (int s = 1; s < kCoarsestSweeps; ++s) {
+        blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+        __syncthreads();
+        T* t = L.e; L.e = L.e2; L.e2 = t;
+      }
     }
   }
   // up
@@ -740,6 +817,7 @@ static int mg_setup_t(Ctx* c) {
     DView<T> L = dview<T>(c, l);
     kwd_diag<T><<<grid_for(L.n, 256), 256, 0, st>>>(L); MAC_COUNT(c);
   }
+  kd_coarsest_inverse<T><<<1, 1024, 0, st>>>(dview<T>(c, c->ndense - 1), c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -780,7 +858,7 @@ static void mg_vcycle_t(Ctx* c) {
     S.lo = 1;
     S.hi = c->ndense;
     int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
-    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem); MAC_COUNT(c);
+    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem, c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
     kd_jacobi<T, true><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e, d3.e2, d4); MAC_COUNT(c);
     kd_jacobi<T, false><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e2, d3.e, d4); MAC_COUNT(c);
   } else {
@@ -788,7 +866,7 @@ static void mg_vcycle_t(Ctx* c) {
     S.L[0] = d3;
     S.lo = 0;
     S.hi = 1;
-    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0); MAC_COUNT(c);
+    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0, c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
   }
   // up
   kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G); MAC_COUNT(c);

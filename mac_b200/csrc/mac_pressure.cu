@@ -45,6 +45,9 @@ int alloc_solver(Ctx* c) {
   A(dalloc(&c->pd2, nc));
   A(dalloc(&c->q, nc));
   A(dalloc(&c->dbl, c->cap_bricks));
+  A(dalloc(&c->coarse_inv, 64 * 64));
+  A(dalloc(&c->coarse_ok, 1));
+  if (rc == MAC_OK) A(check(cudaMemset(c->coarse_ok, 0, sizeof(int))));
   c->npartial = 2 * c->cap_bricks + 64;
   A(dalloc(&c->partial, c->npartial));
   c->mg_float = c->prm.solver == MAC_SOLVER_MGPCG_MIXED || c->prm.solver == MAC_SOLVER_LEARNED_MIXED;
@@ -70,6 +73,8 @@ void free_solver(Ctx* c) {
   cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
   cudaFree(c->zold);
+  cudaFree(c->coarse_inv);
+  cudaFree(c->coarse_ok);
   for (int l = 0; l < kLevels; ++l) {
     cudaFree(c->mg_e[l]); cudaFree(c->mg_e2[l]); cudaFree(c->mg_r[l]); cudaFree(c->mg_w[l]);
   }
@@ -631,11 +636,11 @@ int project(Ctx* c, int ib) {
       prof_end(c, PH_CGVEC);
       rc = read_scalars(c);
       if (rc) return rc;
+      if (learned) c->stats.learned_iterations = c->hs->iters;
       if (c->hs->done) break;
       if (learned) {
         hist.push_back(c->hs->rr);
         const int k = (int)hist.size();
-        c->stats.learned_iterations = k;
         const bool stalled = k >= kStallWindow && hist[k - 1] > 0.25 * hist[k - kStallWindow];
         if (stalled || k >= kLearnedMax) {
           // MG-PCG from the current x: true residual, fresh directions

@@ -1488,6 +1488,41 @@ int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, flo
   return mac::unet::train(*t, steps, batch, lr, seed, losses, 0);
 }
 
+int mac_unet_time_forward(void* net, int n, int d, int h, int w, int reps, double* ms, double* flops) {
+  Net* t = (Net*)net;
+  if (!t || reps < 1 || !ms || !flops) return MAC_ERR_INVALID;
+  cudaSetDevice(t->device);
+  int rc = mac::unet::ensure_shape(*t, n, d, h, w);
+  if (rc) return rc;
+  const size_t v0 = (size_t)n * d * h * w;
+  // a smooth-ish residual on an all-fluid grid: the timing does not depend on the values
+  cudaMemset(t->r, 0, v0 * 4);
+  cudaMemset(t->m, 1, v0);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  rc = mac::unet::apply(t, 0);
+  cudaEventRecord(e0, 0);
+  for (int k = 0; k < reps && !rc; ++k) rc = mac::unet::apply(t, 0);
+  cudaEventRecord(e1, 0);
+  cudaEventSynchronize(e1);
+  float f = 0;
+  cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc) rc = mac::unet::check_err(*t, 0);
+  *ms = f / reps;
+  // algorithmic FLOPs: 2 * taps * cin * cout per output voxel over the real (unpadded) channels
+  double fl = 0;
+  for (int l = 0; l < mac::unet::kNumLayers; ++l) {
+    const auto& L = mac::unet::kLayers[l];
+    const int lvl = (l <= 1 || l >= 10) ? 0 : ((l <= 3 || l == 7 || l == 8 || l == 9) ? 1 : 2);
+    fl += 2.0 * L.taps * L.real_cin * L.real_cout * (double)v0 / (double)(1 << (3 * lvl));
+  }
+  *flops = fl;
+  return rc;
+}
+
 int mac_unet_set_loss(void* net, int kind) {
   if (!net || kind < 0 || kind > 1) return MAC_ERR_INVALID;
   ((Net*)net)->loss_kind = kind;

@@ -66,7 +66,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
            "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
-           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_unet_set_loss"]
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_unet_set_loss", "mac_unet_time_forward"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -126,6 +126,7 @@ def load(path: str = LIB_PATH):
     lib.mac_set_preconditioner_net.argtypes = [vp, vp]
     lib.mac_set_learned_smoothing.argtypes = [vp, f64]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
+    lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
     _lib = lib
     return lib
 

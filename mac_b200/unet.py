@@ -118,6 +118,13 @@ class UNet:
         d = np.load(path)
         self.set_params(d["params"], float(d["tscale"]))
 
+    def time_forward(self, n, d, h, w, reps=5):
+        """(ms per forward pass, algorithmic FLOPs per pass) on an n x d x h x w grid."""
+        ms, fl = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mac_unet_time_forward(self.h, n, d, h, w, reps, ctypes.byref(ms), ctypes.byref(fl)),
+                    "mac_unet_time_forward")
+        return ms.value, fl.value
+
     def launches(self):
         n = ctypes.c_int64()
         self._check(self.lib.mac_unet_launch_count(self.h, ctypes.byref(n)), "mac_unet_launch_count")

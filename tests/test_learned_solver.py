@@ -1,10 +1,13 @@
 """The learned preconditioner inside the projection (flexible CG, solver
-"learned"): a network trained on the device for a few hundred steps on CG
-pairs from random 32^3 masks is used on a held-out 64^3 pool + spheres world.
+"learned") with the committed trained network, on a 64^3 pool + spheres world
+that was not in its training set.
 
 Checks: the solve reaches the requested relative residual and the pressure
-matches the oracle's FP64 projection (relative L2 <= 1e-9 at rtol 1e-12); a
-network that makes no progress stalls and the MG-PCG fall-back still converges.
+matches the oracle's FP64 projection (relative L2 <= 1e-9 at rtol 1e-12); to
+1e-8 the network needs at most 40 iterations without falling back, under a
+quarter of Jacobi-PCG's, while the same loop with the network switched off
+stalls; a network that makes no progress at all falls back to MG-PCG, which
+still converges.
 """
 import numpy as np
 import pytest
@@ -33,12 +36,15 @@ def oracle_p(world, tmp_path_factory):
 
 @pytest.fixture(scope="module")
 def trained():
+    """The committed network (mac_b200/weights/unet_pool64.npz, trained by
+    mac_b200.train_preconditioner on 2000 random masks at 64^3, none of them
+    the test world)."""
+    import os
+
     from mac_b200.unet import UNet
-    net = UNet(0, seed=3)
-    net.set_loss("energy")
-    net.make_dataset(nmasks=64, size=32, nsnap=8, niter=800, seed=11)
-    losses = net.train(300, batch=8, lr=1e-3, seed=5)
-    assert losses[-20:].mean() < 0.5 * losses[:20].mean(), (losses[:20].mean(), losses[-20:].mean())
+    path = os.path.join(os.path.dirname(__file__), "..", "mac_b200", "weights", "unet_pool64.npz")
+    net = UNet(0)
+    net.load(path)
     yield net
     net.close()
 
@@ -61,6 +67,34 @@ def test_learned_solve_converges_to_the_oracle(world, oracle_p, trained):
           st["fallbacks"], "fall-backs; errors", e)
     assert st["relres"] <= 1e-12
     assert e["p"] <= 1e-9 and max(e["u0x"], e["u0y"], e["u0z"]) <= 1e-10, e
+
+
+def test_network_cuts_iterations(world, trained):
+    """What the trained network gains over the same flexible CG without it
+    (network output zero: its Jacobi step alone) and over Jacobi-PCG."""
+    from mac_b200.gpu import Context
+    from mac_b200.unet import UNet
+
+    def run(net, omega, solver="learned"):
+        with Context(world.params, max_bricks=2048, max_particles=1024, solver=solver, rtol=1e-8,
+                     max_iters=2000) as ctx:
+            ctx.set_preconditioner(net)
+            ctx.set_learned_smoothing(omega)
+            ctx.upload(world)
+            ctx.project(0)
+            return ctx.stats()
+
+    st_l = run(trained, 0.8)
+    with UNet(0) as zero:
+        zero.set_params(np.zeros(zero.nparams, np.float32), 1.0)
+        st_0 = run(zero, 0.8)
+    st_j = run(None, 0.8, "cg64")
+    print("to 1e-8: learned", st_l["iterations"], "network off", st_0["iterations"],
+          "(fall-back", st_0["fallbacks"], ") Jacobi-PCG", st_j["iterations"])
+    assert st_l["fallbacks"] == 0 and st_l["learned_iterations"] == st_l["iterations"]
+    assert st_l["iterations"] <= 40
+    assert st_l["iterations"] < 0.25 * st_j["iterations"]
+    assert st_0["fallbacks"] >= 1  # without the network the same loop stalls
 
 
 def test_stalled_network_falls_back(world, oracle_p):
