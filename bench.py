@@ -6,7 +6,8 @@ CFL 0.5) in a synthetic spun-up state: a pool of depth 122 cells (~8.0M fluid
 cells) with 8 jittered particles per fluid cell (~64M particles). Each step is
 the reference's whole step (test/TestJetDEau_Basic.cpp:434-441): topology
 rebuild, CFL time step, RK2-TVD with gravity + upwind convection and two
-pressure projections (plain FP64 MG-PCG at relative residual 1e-8), air-layer
+pressure projections (FP64 CG with the FP32 multigrid preconditioner, to an
+FP64 relative residual of 1e-8; --solver mgpcg64 for the all-FP64 form), air-layer
 extrapolation, RK4 particle move.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -432,7 +433,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="jet256")
-    ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mgpcg64")
+    ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mixed",
+                    help="projection solver: mixed = FP64 CG with the FP32 multigrid (default), "
+                         "mgpcg64 = plain FP64 MG-PCG, cg64 = FP64 Jacobi-PCG")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

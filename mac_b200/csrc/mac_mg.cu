@@ -225,8 +225,17 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
   e[i] = (T)(kOmega * dinv * s);
 }
 
+// Sum over aligned groups of 8 lanes; the result is valid in the group's first lane.
+__device__ inline double sum8(double v) {
+  v += __shfl_down_sync(0xffffffffu, v, 4, 8);
+  v += __shfl_down_sync(0xffffffffu, v, 2, 8);
+  v += __shfl_down_sync(0xffffffffu, v, 1, 8);
+  return v;
+}
+
 // Residual of a brick level summed over children: D = 4 writes level 2
-// (brick-local), D = 2 writes the dense level 3 at the brick's position.
+// (brick-local), D = 2 writes the dense level 3 at the brick's position. One
+// thread per fine cell, the 8 children of a coarse cell on 8 adjacent lanes.
 template <class T, int D>
 __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                                    const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
@@ -234,20 +243,26 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
                                                    DenseGrid g3) {
   constexpr int H = D / 2;
   constexpr int N = D * D * D;
-  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (int64_t)nd * H * H * H) return;
-  int b = dbl[g / (H * H * H)];
-  int o = (int)(g % (H * H * H));
-  int X = o % H, Y = (o / H) % H, Z = o / (H * H);
-  double s = 0;
-  for (int k = 0; k < 8; ++k) {
-    int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-    size_t i = (size_t)b * N + x + D * y + D * D * z;
-    if ((double)w[4 * ncap + i] == 0) continue;
-    s += (double)r[i] - apply_l<T, D>(e, w, ncap, nbr, b, x, y, z, i, (double)e[i]);
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = g < (int64_t)nd * N;  // nd * N is a multiple of 8: groups are whole
+  double v = 0;
+  int b = 0, p = 0;
+  if (live) {
+    b = dbl[g / N];
+    const int o = (int)(g % N);
+    p = o >> 3;
+    const int k = o & 7;
+    const int X = p % H, Y = (p / H) % H, Z = p / (H * H);
+    const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+    const size_t i = (size_t)b * N + x + D * y + D * D * z;
+    if ((double)w[4 * ncap + i] != 0)
+      v = (double)r[i] - apply_l<T, D>(e, w, ncap, nbr, b, x, y, z, i, (double)e[i]);
   }
-  if (D == 2) rc[g3.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])] = (T)s;
-  else rc[(size_t)b * H * H * H + o] = (T)s;
+  v = sum8(v);
+  if (live && (threadIdx.x & 7) == 0) {
+    if (D == 2) rc[g3.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])] = (T)v;
+    else rc[(size_t)b * H * H * H + p] = (T)v;
+  }
 }
 
 // One Jacobi sweep at a brick level, optionally adding the coarse correction
@@ -359,20 +374,24 @@ __global__ void kd_pre(DView<T> L) {
   L.e[i] = (T)(kOmega * dinv * s);
 }
 
+// One thread per (coarse cell, child), the 8 children on adjacent lanes.
 template <class T>
 __global__ void kd_restrict(DView<T> F, DView<T> C) {
-  int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= C.n) return;
-  int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t I = g >> 3;
+  const int k = (int)(g & 7);
   double s = 0;
-  for (int k = 0; k < 8; ++k) {
-    int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-    if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
-    int64_t i = F.at(x, y, z);
-    if ((double)F.w[4 * F.n + i] == 0) continue;
-    s += (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+  if (I < C.n) {
+    const int XY = (int)(I / C.nx);
+    const int X = (int)(I - (int64_t)XY * C.nx), Y = XY % C.ny, Z = XY / C.ny;
+    const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+    if (x < F.nx && y < F.ny && z < F.nz) {
+      const int64_t i = F.at(x, y, z);
+      if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+    }
   }
-  C.r[I] = (T)s;
+  s = sum8(s);
+  if (I < C.n && k == 0) C.r[I] = (T)s;
 }
 
 template <class T, bool WITH_COARSE>
@@ -469,18 +488,23 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView
 
 template <class T>
 __device__ void blk_restrict(const DView<T>& F, const DView<T>& C) {
-  for (int I = threadIdx.x; I < (int)C.n; I += blockDim.x) {
-    const int XY = I / C.nx;
-    int X = I - XY * C.nx, Y = XY % C.ny, Z = XY / C.ny;
+  // one thread per (coarse cell, child), the 8 children on adjacent lanes; the
+  // loop runs a whole number of warps so every lane reaches the shuffles
+  const int total = ((int)C.n * 8 + 31) & ~31;
+  for (int g = threadIdx.x; g < total; g += blockDim.x) {
+    const int I = g >> 3, k = g & 7;
     double s = 0;
-    for (int k = 0; k < 8; ++k) {
-      int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-      if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
-      const int i = x + F.nx * (y + F.ny * z);
-      if ((double)F.w[4 * F.n + i] == 0) continue;
-      s += (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+    if (I < (int)C.n) {
+      const int XY = I / C.nx;
+      const int X = I - XY * C.nx, Y = XY % C.ny, Z = XY / C.ny;
+      const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
+      if (x < F.nx && y < F.ny && z < F.nz) {
+        const int i = x + F.nx * (y + F.ny * z);
+        if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+      }
     }
-    C.r[I] = (T)s;
+    s = sum8(s);
+    if (I < (int)C.n && k == 0) C.r[I] = (T)s;
   }
 }
 
@@ -845,14 +869,14 @@ static void mg_vcycle_t(Ctx* c) {
   k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
   k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
   kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1); MAC_COUNT(c);
-  kl_restrict<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G); MAC_COUNT(c);
+  kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G); MAC_COUNT(c);
   kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2); MAC_COUNT(c);
-  kl_restrict<T, 2><<<grid_for(nd, 256), 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G); MAC_COUNT(c);
+  kl_restrict<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
     DView<T> d4 = dview<T>(c, 1);
     kd_pre<T><<<grid_for(d3.n, 256), 256, 0, st>>>(d3); MAC_COUNT(c);
-    kd_restrict<T><<<grid_for(d4.n, 256), 256, 0, st>>>(d3, d4); MAC_COUNT(c);
+    kd_restrict<T><<<grid_for(8 * d4.n, 256), 256, 0, st>>>(d3, d4); MAC_COUNT(c);
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
     S.lo = 1;
