@@ -442,52 +442,60 @@ struct DenseSet {
   int lo, hi;
 };
 
+// One Jacobi sweep of a block-solved level (first: from zero). ce (the next
+// coarser level's correction, on a cnx x cny grid) is added to every e first
+// when given.
 template <class T>
-__device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const DView<T>* C, bool first) {
+__device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce, int cnx, int cny, bool first) {
   const int n = (int)L.n;  // block-solved levels hold a few thousand cells: 32-bit index math
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const T* __restrict__ w = L.w;
+  const T* __restrict__ r = L.r;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double dinv = (double)L.w[4 * n + i];
+    const double dinv = (double)w[4 * n + i];
     if (dinv == 0) {
       eout[i] = (T)0;
       continue;
     }
     if (first) {
-      eout[i] = (T)(kOmega * dinv * (double)L.r[i]);
+      eout[i] = (T)(kOmega * dinv * (double)r[i]);
       continue;
     }
-    const int xy = i / L.nx;
-    int x = i - xy * L.nx, y = xy % L.ny, z = xy / L.ny;
+    const int xy = i / nx;
+    const int x = i - xy * nx, y = xy % ny, z = xy / ny;
     auto ev = [&](int j, int xx, int yy, int zz) -> double {
       double v = (double)ein[j];
-      if (C) v += (double)C->e[(xx >> 1) + C->nx * ((yy >> 1) + C->ny * (zz >> 1))];
+      if (ce) v += (double)ce[(xx >> 1) + cnx * ((yy >> 1) + cny * (zz >> 1))];
       return v;
     };
-    int c[3] = {x, y, z};
-    int dim[3] = {L.nx, L.ny, L.nz};
-    int stride[3] = {1, L.nx, L.nx * L.ny};
-    double ec = ev(i, x, y, z);
-    double s = (double)L.w[3 * n + i] * ec;
+    const int c[3] = {x, y, z};
+    const int dim[3] = {nx, ny, nz};
+    const int stride[3] = {1, nx, nx * ny};
+    const double ec = ev(i, x, y, z);
+    double s = (double)w[3 * n + i] * ec;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
       int p[3] = {x, y, z};
-      double wl = (double)L.w[a * n + i];
+      const double wl = (double)w[a * n + i];
       if (wl != 0 && c[a] > 0) {
         p[a] = c[a] - 1;
         s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
       }
       if (c[a] + 1 < dim[a]) {
-        double wr = (double)L.w[a * n + i + stride[a]];
+        const double wr = (double)w[a * n + i + stride[a]];
         if (wr != 0) {
           p[a] = c[a] + 1;
           s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
         }
       }
     }
-    eout[i] = (T)(ec + kOmega * dinv * ((double)L.r[i] - s));
+    eout[i] = (T)(ec + kOmega * dinv * ((double)r[i] - s));
   }
 }
 
+// Residual of F (correction fe) restricted into C.r.
 template <class T>
-__device__ void blk_restrict(const DView<T>& F, const DView<T>& C) {
+__device__ void blk_restrict(const DView<T>& F, const T* fe, const DView<T>& C) {
   // one thread per (coarse cell, child), the 8 children on adjacent lanes; the
   // loop runs a whole number of warps so every lane reaches the shuffles
   const int total = ((int)C.n * 8 + 31) & ~31;
@@ -500,7 +508,7 @@ __device__ void blk_restrict(const DView<T>& F, const DView<T>& C) {
       const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
       if (x < F.nx && y < F.ny && z < F.nz) {
         const int i = x + F.nx * (y + F.ny * z);
-        if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+        if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, fe, i, x, y, z, (double)fe[i]);
       }
     }
     s = sum8(s);
@@ -579,69 +587,78 @@ template <class T>
 __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem, const double* __restrict__ inv,
                                                         const int* __restrict__ inv_ok) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  DenseSet<T> S = G;
-  if (use_smem) {
+  // Level descriptors live in shared memory (one copy per block); which of a
+  // level's two correction buffers is current is a bit in a register.
+  __shared__ DView<T> SL[kMaxDense];
+  const int lo = G.lo, hi = G.hi;
+  if (threadIdx.x == 0) {
     T* p = (T*)smem_raw;
-    for (int l = G.lo; l < G.hi; ++l) {
-      DView<T>& d = S.L[l];
-      int64_t n = d.n;
-      d.e = p;
-      d.e2 = p + n;
-      d.r = p + 2 * n;
-      d.w = p + 3 * n;
-      p += 9 * n;
-      blk_copy(d.w, G.L[l].w, 6 * n);
-      if (l == G.lo) blk_copy(d.r, G.L[l].r, n);
+    for (int l = lo; l < hi; ++l) {
+      SL[l] = G.L[l];
+      if (use_smem) {
+        const int64_t n = G.L[l].n;
+        SL[l].e = p;
+        SL[l].e2 = p + n;
+        SL[l].r = p + 2 * n;
+        SL[l].w = p + 3 * n;
+        p += 9 * n;
+      }
+    }
+  }
+  __syncthreads();
+  if (use_smem) {
+    for (int l = lo; l < hi; ++l) {
+      blk_copy(SL[l].w, G.L[l].w, 6 * SL[l].n);
+      if (l == lo) blk_copy(SL[l].r, G.L[l].r, SL[l].n);
     }
     __syncthreads();
   }
+  unsigned swapped = 0;
+  auto cur = [&](int l) -> T* { return ((swapped >> l) & 1) ? SL[l].e2 : SL[l].e; };
+  auto oth = [&](int l) -> T* { return ((swapped >> l) & 1) ? SL[l].e : SL[l].e2; };
   // down
-  for (int l = S.lo; l < S.hi - 1; ++l) {
-    DView<T>& L = S.L[l];
-    blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
+  for (int l = lo; l < hi - 1; ++l) {
+    const DView<T>& L = SL[l];
+    blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true);
     __syncthreads();
-    blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+    blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false);
     __syncthreads();
-    T* t = L.e; L.e = L.e2; L.e2 = t;
-    blk_restrict(L, S.L[l + 1]);
+    swapped ^= 1u << l;
+    blk_restrict(L, cur(l), SL[l + 1]);
     __syncthreads();
   }
   // coarsest: exact solve with the set-up's inverse, else Jacobi sweeps from zero
   {
-    DView<T>& L = S.L[S.hi - 1];
+    const int l = hi - 1;
+    const DView<T>& L = SL[l];
     if (*inv_ok && L.n <= 64) {
       const int n = (int)L.n;
       if ((int)threadIdx.x < n) {
         const int i = threadIdx.x;
         double s = 0.0;
         for (int j = 0; j < n; ++j) s += inv[i * 64 + j] * (double)L.r[j];
-        L.e[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
+        cur(l)[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
       }
       __syncthreads();
     } else {
-      blk_jacobi(L, L.e, L.e, (const DView<T>*)nullptr, true);
+      blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true);
       __syncthreads();
       for (int s = 1; s < kCoarsestSweeps; ++s) {
-        blk_jacobi(L, L.e, L.e2, (const DView<T>*)nullptr, false);
+        blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false);
         __syncthreads();
-        T* t = L.e; L.e = L.e2; L.e2 = t;
+        swapped ^= 1u << l;
       }
     }
   }
   // up
-  for (int l = S.hi - 2; l >= S.lo; --l) {
-    DView<T>& L = S.L[l];
-    blk_jacobi(L, L.e, L.e2, &S.L[l + 1], false);
+  for (int l = hi - 2; l >= lo; --l) {
+    const DView<T>& L = SL[l];
+    blk_jacobi(L, cur(l), oth(l), cur(l + 1), SL[l + 1].nx, SL[l + 1].ny, false);
     __syncthreads();
-    blk_jacobi(L, L.e2, L.e, (const DView<T>*)nullptr, false);
+    blk_jacobi(L, oth(l), cur(l), (const T*)nullptr, 0, 0, false);
     __syncthreads();
   }
-  if (use_smem) {
-    blk_copy(G.L[G.lo].e, S.L[G.lo].e, S.L[G.lo].n);
-  } else if (S.L[G.lo].e != G.L[G.lo].e) {
-    __syncthreads();
-    blk_copy(G.L[G.lo].e, S.L[G.lo].e, S.L[G.lo].n);
-  }
+  if (use_smem || cur(lo) != G.L[lo].e) blk_copy(G.L[lo].e, cur(lo), SL[lo].n);
 }
 
 // ------------------------------------------------------------ weights setup
@@ -910,9 +927,15 @@ void mg_vcycle(Ctx* c) {
 int mg_configure(Ctx* c) {
   int dev = c->prm.device, optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  c->smem_optin = optin;
-  int rc = check(cudaFuncSetAttribute(kd_coarse_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  if (!rc) rc = check(cudaFuncSetAttribute(kd_coarse_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  // the dynamic part may use what the kernel's static shared memory leaves
+  cudaFuncAttributes fa64, fa32;
+  int rc = check(cudaFuncGetAttributes(&fa64, kd_coarse_block<double>));
+  if (!rc) rc = check(cudaFuncGetAttributes(&fa32, kd_coarse_block<float>));
+  if (rc) return rc;
+  const int dyn64 = optin - (int)fa64.sharedSizeBytes, dyn32 = optin - (int)fa32.sharedSizeBytes;
+  c->smem_optin = dyn64 < dyn32 ? dyn64 : dyn32;
+  rc = check(cudaFuncSetAttribute(kd_coarse_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn64));
+  if (!rc) rc = check(cudaFuncSetAttribute(kd_coarse_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn32));
   return rc;
 }
 
