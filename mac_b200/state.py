@@ -233,6 +233,35 @@ def jet_world(nx=32, ny=32, nz=64, h=0.05, r_inflow=4.0, w_inflow=1.0, pool_dept
     return from_cells(pr, keys, typ, flags, u, pos)
 
 
+def lateral_jet_world(nx=384, ny=192, nz=192, h=0.01, r_inflow=16.0, speed=3.0, angle_deg=15.0, z_centre=None,
+                      layer_max=4, cfl=0.5, dt_max=0.01) -> State:
+    """Lateral jet: cells 0..nx-1 x 0..ny-1 x 0..nz-1 open, solid walls at
+    x = -1 / nx, y = -1 / ny and the floor z = -1. A disc of radius
+    ``r_inflow`` cells on the x = 0 plane (centred at y = (ny-1)/2, z =
+    ``z_centre``, default nz/4) is Inflow with face speed ``speed`` aimed
+    ``angle_deg`` above horizontal and all three faces const, as the reference's
+    lateral jet sets its inflow cells (``test/Lateral_jet_3.cpp:416-440``)."""
+    pr = Params(h=(h, h, h), cfl_factor=cfl, dt_max=dt_max, layer_max=layer_max)
+    walls = [
+        _box(-1, -1, -1, ny, -1, nz - 1), _box(nx, nx, -1, ny, -1, nz - 1),
+        _box(0, nx - 1, -1, -1, -1, nz - 1), _box(0, nx - 1, ny, ny, -1, nz - 1),
+        _box(0, nx - 1, 0, ny - 1, -1, -1),
+    ]
+    wk = np.concatenate(walls, axis=0)
+    plane = _box(0, 0, 0, ny - 1, 0, nz - 1)
+    cy = (ny - 1) / 2.0
+    cz = nz / 4.0 if z_centre is None else float(z_centre)
+    disc = plane[(plane[:, 1] - cy) ** 2 + (plane[:, 2] - cz) ** 2 <= r_inflow ** 2]
+    keys = np.concatenate([wk, disc], axis=0)
+    typ = np.concatenate([np.full(len(wk), SOLID, np.uint8), np.full(len(disc), INFLOW, np.uint8)])
+    flags = np.concatenate([np.zeros(len(wk), np.uint8), np.full(len(disc), 7, np.uint8)])
+    u = np.zeros((len(keys), 3))
+    a = np.deg2rad(angle_deg)
+    u[len(wk):, 0] = speed * np.cos(a)
+    u[len(wk):, 2] = speed * np.sin(a)
+    return from_cells(pr, keys, typ, flags, u)
+
+
 def pool_spheres_world(n=128, nspheres=12, r_range=(6.0, 20.0), pool_frac=0.4, seed=2, vel_seed=3) -> State:
     """Standalone pressure-solve world: cells 0..n-1 on each axis with h = 1/n,
     fluid where z < pool_frac*n or inside one of ``nspheres`` balls (radius
