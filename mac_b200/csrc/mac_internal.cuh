@@ -336,6 +336,65 @@ __device__ inline void stage_h1(V* s, int b, const int64_t* sb, V zero, F val) {
   }
 }
 
+// The same staging of a plain array: the brick's own 512 cells with 16-byte
+// vector loads (thread t takes cells 4t..4t+3, half a row), the face halos
+// with scalar loads; the values land in s as doubles.
+__device__ inline void load4(const double* p, double* v) {
+  const double2 a = *reinterpret_cast<const double2*>(p);
+  const double2 c = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+}
+__device__ inline void load4(const float* p, double* v) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+
+// Only the face halos of stage_h1 (value 0 where the neighbour brick is absent).
+template <class F>
+__device__ inline void stage_h1_halo(double* s, const int64_t* sb, F val) {
+  for (int j = threadIdx.x; j < 384; j += kBT) {
+    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
+    int x, y, z;
+    int64_t gi;
+    switch (f) {
+      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
+      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
+      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
+      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
+      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
+      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
+    }
+    s[s1(x, y, z)] = gi < 0 ? 0.0 : val(gi);
+  }
+}
+
+template <class T>
+__device__ inline void stage_arr(double* s, const T* __restrict__ a, int b, const int64_t* sb) {
+  static_assert(kBT * 4 == kCells, "one 4-cell vector per thread");
+  {
+    const int o = 4 * threadIdx.x;
+    double v[4];
+    load4(a + (int64_t)b * kCells + o, v);
+    const int si = s1_of(o);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s[si + q] = v[q];
+  }
+  for (int j = threadIdx.x; j < 384; j += kBT) {
+    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
+    int x, y, z;
+    int64_t gi;
+    switch (f) {
+      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
+      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
+      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
+      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
+      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
+      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
+    }
+    s[s1(x, y, z)] = gi < 0 ? 0.0 : (double)a[gi];
+  }
+}
+
 // Sum over an NT-thread block of two values into partial[blockIdx.x] and
 // partial[gridDim.x + blockIdx.x] (fixed order).
 template <int NT>

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i]; });
+  stage_arr(se, e, b, sb);
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
@@ -122,11 +122,55 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
                                                double* __restrict__ z, double* partial, Params P) {
   __shared__ int64_t sb[6];
   __shared__ double se[kS1];  // e (plus the coarse correction when FIRST) with face halo
+  __shared__ double s1p[64 + 96];  // FIRST: level-1 parents of the brick (64) and of its face halos (6 x 16)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  if (FIRST) stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i] + (double)e1[parent1(i)]; });
-  else stage_h1(se, b, sb, 0.0, [&](int64_t i) { return (double)e[i]; });
+  stage_arr(se, e, b, sb);
+  if (FIRST) {
+    // parents staged once: own level-1 cells, then for face f the 4x4 level-1
+    // cells of the neighbour brick next to it
+    for (int j = threadIdx.x; j < 160; j += kBT) {
+      double v;
+      if (j < 64) {
+        v = (double)e1[(size_t)b * 64 + j];
+      } else {
+        const int f = (j - 64) >> 4, p = (j - 64) & 3, q = ((j - 64) >> 2) & 3;
+        const int64_t base = sb[f];
+        int l;
+        switch (f) {
+          case 0: l = 3 + 4 * p + 16 * q; break;
+          case 1: l = 4 * p + 16 * q; break;
+          case 2: l = p + 12 + 16 * q; break;
+          case 3: l = p + 16 * q; break;
+          case 4: l = p + 4 * q + 48; break;
+          default: l = p + 4 * q; break;
+        }
+        v = base < 0 ? 0.0 : (double)e1[(base >> 9) * 64 + l];
+      }
+      s1p[j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kCPT; ++k) {
+      const int o = threadIdx.x + kBT * k;
+      const int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+      se[s1_of(o)] += s1p[(x >> 1) + 4 * (y >> 1) + 16 * (z >> 1)];
+    }
+    for (int j = threadIdx.x; j < 384; j += kBT) {
+      const int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
+      int x, y, z;
+      switch (f) {
+        case 0: x = -1; y = u; z = v; break;
+        case 1: x = 8; y = u; z = v; break;
+        case 2: y = -1; x = u; z = v; break;
+        case 3: y = 8; x = u; z = v; break;
+        case 4: z = -1; x = u; y = v; break;
+        default: z = 8; x = u; y = v; break;
+      }
+      se[s1(x, y, z)] += s1p[64 + 16 * f + (u >> 1) + 4 * (v >> 1)];
+    }
+  }
   __syncthreads();
   double rz = 0;
 #pragma unroll

@@ -259,8 +259,19 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   load_face_bases(nbr, b, sb);
   __syncthreads();
   double be = first ? 0.0 : ds->beta;
-  if (first) stage_h1(sp, b, sb, 0.0, [&](int64_t i) { return z[i]; });
-  else stage_h1(sp, b, sb, 0.0, [&](int64_t i) { return z[i] + be * pold[i]; });
+  if (first) {
+    stage_arr(sp, z, b, sb);
+  } else {
+    // p = z + beta p_old: the brick with vector loads of both, the halo with scalars
+    const int o4 = 4 * threadIdx.x;
+    double vz[4], vp[4];
+    load4(z + (int64_t)b * kCells + o4, vz);
+    load4(pold + (int64_t)b * kCells + o4, vp);
+    const int si = s1_of(o4);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sp[si + q] = vz[q] + be * vp[q];
+    stage_h1_halo(sp, sb, [&](int64_t i) { return z[i] + be * pold[i]; });
+  }
   __syncthreads();
   double pq = 0;
 #pragma unroll
