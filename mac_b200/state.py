@@ -28,7 +28,7 @@ AIR, FLUID, SOLID, INFLOW = 0, 1, 2, 3
 FLAG_CONST = (1, 2, 4)
 FLAG_NODELETE = 8
 
-_HDR = struct.Struct("<8sqq3d6dii Q ii136x")
+_HDR = struct.Struct("<8sqq3d6dii Q ii d128x")
 assert _HDR.size == 256
 
 CELL_F64 = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
@@ -48,6 +48,7 @@ class Params:
     layer_max: int = 4
     step: int = 0
     interp_symmetric: int = 1
+    viscosity: float = 0.0
 
 
 @dataclasses.dataclass
@@ -75,7 +76,7 @@ class State:
         pr = self.params
         hdr = _HDR.pack(b"MACST001", self.nbricks, self.nparticles, *pr.h, pr.t, pr.dt,
                         pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
-                        pr.layer_max, pr.step, pr.interp_symmetric, 0)
+                        pr.layer_max, pr.step, pr.interp_symmetric, 0, pr.viscosity)
         with open(path, "wb") as f:
             f.write(hdr)
             f.write(np.ascontiguousarray(self.keys, dtype="<i4").tobytes())
@@ -93,7 +94,7 @@ class State:
         with open(path, "rb") as f:
             buf = f.read()
         (magic, nb, npart, h0, h1, h2, t, dt, cfl, dtmin, dtmax, g, gax, lmax, step, isym,
-         _r) = _HDR.unpack_from(buf, 0)
+         _r, visc) = _HDR.unpack_from(buf, 0)
         if magic != b"MACST001":
             raise ValueError(f"{path}: not a state file")
         off = _HDR.size
@@ -115,14 +116,14 @@ class State:
         pos = take("<f8", npart * 3, (npart, 3))
         params = Params(h=(h0, h1, h2), t=t, dt=dt, cfl_factor=cfl, dt_min=dtmin, dt_max=dtmax,
                         gravity=g, gravity_axis=gax, layer_max=lmax, step=step,
-                        interp_symmetric=isym)
+                        interp_symmetric=isym, viscosity=visc)
         return State(params, keys, exists, f64, flags, typ, layer, ids, pos)
 
     def save_npz(self, path: str) -> None:
         """Compressed copy (used for the committed fixtures)."""
         pr = self.params
         hdr = np.array([*pr.h, pr.t, pr.dt, pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
-                        pr.layer_max, pr.step, pr.interp_symmetric], dtype=np.float64)
+                        pr.layer_max, pr.step, pr.interp_symmetric, pr.viscosity], dtype=np.float64)
         np.savez_compressed(path, hdr=hdr, keys=self.keys, exists=self.exists, flags=self.flags, type=self.type,
                             layer=self.layer, id=self.id, pos=self.pos, **self.f64)
 
@@ -132,7 +133,7 @@ class State:
         h = z["hdr"]
         pr = Params(h=(h[0], h[1], h[2]), t=h[3], dt=h[4], cfl_factor=h[5], dt_min=h[6], dt_max=h[7],
                     gravity=h[8], gravity_axis=int(h[9]), layer_max=int(h[10]), step=int(h[11]),
-                    interp_symmetric=int(h[12]))
+                    interp_symmetric=int(h[12]), viscosity=float(h[13]) if h.size > 13 else 0.0)
         return State(pr, z["keys"], z["exists"], {n: z[n] for n in CELL_F64}, z["flags"], z["type"], z["layer"],
                      z["id"], z["pos"])
 

@@ -47,6 +47,7 @@ typedef struct {
   double* pos;
   int64_t np, capp;
   uint64_t seed;
+  int viscous; /* 1: Algorithms_Viscosity and the Dirichlet pressure are composed */
   /* statistics */
   int64_t invalid_reads, created_cells, cg_iters;
   double max_div, last_relres;
@@ -416,6 +417,58 @@ static void alg_convection(world_t* w, int ib) {
   }
 }
 
+/* Policy_Viscosity_Apply_If::Get_If_Apply_Viscosity (src/Policy_Viscosity_Apply_If.h:17-38). */
+static int visc_apply(world_t* w, int64_t bi, int o) {
+  brick_t* b = w->b[bi];
+  if (is_fluid(b->type[o])) return 1;
+  if (b->layer[o] == -1) return 0;
+  int k[3];
+  key_of(w, bi, o, k);
+  for (int i = 0; i < 3; ++i) {
+    int m[3] = {k[0], k[1], k[2]};
+    m[i] -= 1;
+    cell_t n = cell_at(w, m[0], m[1], m[2]);
+    if (!cell_valid(w, n)) continue;
+    if (is_fluid(B(n)->type[n.o])) return 1;
+  }
+  return 0;
+}
+
+/* Algorithms_Viscosity::Do (src/Algorithms_Viscosity.h:24-30) with
+ * Policy_Laplacian_Speed::Get_Laplacian_Speed (src/Policy_Laplacian_Speed.h:22-36):
+ * acc += viscosity * (sum_j u_i(c+e_j) + u_i(c-e_j) - 2 u_i(c)) / h_j^2, through
+ * the non-forced Set, in the reference's summation order. */
+static void alg_viscosity(world_t* w, int ib) {
+  const double nu = w->hdr.viscosity;
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o] || !visc_apply(w, bi, o)) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      double lap[3];
+      for (int i = 0; i < 3; ++i) {
+        double temp = 0;
+        for (int j = 0; j < 3; ++j) {
+          const double ih2 = pow(w->ih[j], 2);
+          temp -= 2 * rd_u(w, ib, i, k, 0, 0, 0) * ih2;
+          temp += rd_u(w, ib, i, k, j == 0, j == 1, j == 2) * ih2;
+          temp += rd_u(w, ib, i, k, -(j == 0), -(j == 1), -(j == 2)) * ih2;
+        }
+        lap[i] = temp;
+      }
+      for (int i = 0; i < 3; ++i) set_u(b, b->acc[i], o, i, b->acc[i][o] + lap[i] * nu, 0);
+    }
+  }
+}
+
+/* Gravity, convection and, in the viscous composition, viscosity. */
+static void grid_forces(world_t* w, int ib) {
+  alg_gravity(w, ib);
+  alg_convection(w, ib);
+  if (w->viscous) alg_viscosity(w, ib);
+}
+
 static void acc_zero(world_t* w) {
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o)
@@ -557,8 +610,59 @@ static int correction_applies(world_t* w, int64_t bi, int o, int i) {
   return in_domain(B(n)->type[n.o]);
 }
 
+/* Policy_Dirichlet_Boundary (src/Policy_Dirichlet_Boundary.h:27-109).
+ * GetIsAir compares Material_To_Type_Fluid with Air, and that map sends
+ * Solid to Air as well (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:21-35):
+ * "air" here means air or solid. */
+static int is_air(uint8_t t) { return t == MAC_AIR || t == MAC_SOLID; }
+
+/* GetIsDirichletBoundary: an air cell with a non-air face neighbour. */
+static int dir_boundary(world_t* w, const int k[3]) {
+  cell_t c = cell_at(w, k[0], k[1], k[2]);
+  if (!cell_valid(w, c) || !is_air(B(c)->type[c.o])) return 0;
+  for (int i = 0; i < 3; ++i)
+    for (int s = -1; s <= 1; s += 2) {
+      cell_t n = cell_at(w, k[0] + s * (i == 0), k[1] + s * (i == 1), k[2] + s * (i == 2));
+      if (cell_valid(w, n) && !is_air(B(n)->type[n.o])) return 1;
+    }
+  return 0;
+}
+
+/* GetDirichletBoundaryPressure: -sum over non-air face neighbours (i, s) of
+ * 2 viscosity (u_i(c+e_i) - u_i(c)) / h_i * s, in the reference's order. */
+static double dir_pressure(world_t* w, int ib, const int k[3]) {
+  cell_t c = cell_at(w, k[0], k[1], k[2]);
+  if (!cell_valid(w, c) || !is_air(B(c)->type[c.o])) return 0;
+  const double nu = w->hdr.viscosity;
+  double ret = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int s = -1; s <= 1; s += 2) {
+      cell_t n = cell_at(w, k[0] + s * (i == 0), k[1] + s * (i == 1), k[2] + s * (i == 2));
+      if (cell_valid(w, n) && !is_air(B(n)->type[n.o])) {
+        const double v1 = rd_u(w, ib, i, k, 0, 0, 0);
+        const double v2 = rd_u(w, ib, i, k, i == 0, i == 1, i == 2);
+        ret -= 2 * nu * (v2 - v1) * w->ih[i] * s;
+      }
+    }
+  return ret;
+}
+
+/* GetDirichletSumBoundaryPressure: sum over Dirichlet face neighbours of p_D / h_i^2. */
+static double dir_sum(world_t* w, int ib, const int k[3]) {
+  double ret = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int s = -1; s <= 1; s += 2) {
+      int m[3] = {k[0] + s * (i == 0), k[1] + s * (i == 1), k[2] + s * (i == 2)};
+      if (dir_boundary(w, m)) ret += dir_pressure(w, ib, m) * w->ih[i] * w->ih[i];
+    }
+  return ret;
+}
+
 /* Algorithms_Solve_Pressure::Divergence_Projection (src/Algorithms_Solve_Pressure.h:168-222)
- * on speed buffer ib with an already assembled system. */
+ * on speed buffer ib with an already assembled system; in the viscous
+ * composition Algorithms_Solve_Pressure_Dirichlet::Divergence_Projection
+ * (src/Algorithms_Solve_Pressure_Dirichlet.h:171-233): b -= the Dirichlet sum,
+ * and Dirichlet air cells take their boundary pressure. */
 static void project_with(world_t* w, const csr_t* A, int ib) {
   int64_t n = A->n;
   double* b = (double*)malloc(8 * (n + 1));
@@ -567,13 +671,22 @@ static void project_with(world_t* w, const csr_t* A, int ib) {
     int k[3];
     key_of(w, A->bi[r], A->o[r], k);
     b[r] = divergence(w, ib, k);
+    if (w->viscous) b[r] -= dir_sum(w, ib, k);
   }
   solve(w, A, b, x);
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
       brick_t* br = w->b[bi];
       if (!br->exists[o]) continue;
-      br->p[o] = in_domain(br->type[o]) ? x[br->id[o]] : 0.0;
+      if (in_domain(br->type[o])) {
+        br->p[o] = x[br->id[o]];
+      } else if (w->viscous) {
+        int k[3];
+        key_of(w, bi, o, k);
+        br->p[o] = dir_boundary(w, k) ? dir_pressure(w, ib, k) : 0.0;
+      } else {
+        br->p[o] = 0.0;
+      }
     }
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
@@ -606,8 +719,7 @@ static void alg_rk2(world_t* w) {
   assemble(w, &A);
   double dt = w->hdr.dt;
   acc_zero(w);
-  alg_gravity(w, 0);
-  alg_convection(w, 0);
+  grid_forces(w, 0);
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
       brick_t* b = w->b[bi];
@@ -616,8 +728,7 @@ static void alg_rk2(world_t* w) {
     }
   acc_zero(w);
   project_with(w, &A, 1);
-  alg_gravity(w, 1);
-  alg_convection(w, 1);
+  grid_forces(w, 1);
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
       brick_t* b = w->b[bi];
@@ -1004,6 +1115,25 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
       alg_move(w, sym);
       w->hdr.t += w->hdr.dt;
       fcs += fluid_count(w);
+    } else if (!strcmp(cmd, "vstep")) {
+      w->viscous = 1;
+      ++w->seed;
+      topology(w);
+      alg_rk2(w);
+      alg_extrapolate(w);
+      alg_move(w, sym);
+      w->hdr.t += w->hdr.dt;
+      fcs += fluid_count(w);
+    } else if (!strcmp(cmd, "vforces")) {
+      w->viscous = 1;
+      acc_zero(w);
+      grid_forces(w, 0);
+    } else if (!strcmp(cmd, "vode")) {
+      w->viscous = 1;
+      alg_rk2(w);
+    } else if (!strcmp(cmd, "vproject")) {
+      w->viscous = 1;
+      alg_project(w);
     } else if (!strcmp(cmd, "topology")) {
       ++w->seed;
       topology(w);

@@ -14,7 +14,10 @@
 //    functions, because libumfpack is not installed: FP64 Jacobi-CG to a relative
 //    residual of 1e-14 (a direct-solve stand-in; tests pin it against a sparse
 //    LU on the same CSC arrays),
-//  * Viscosity and Wind are not composed (the configs run inviscid, no wind),
+//  * Wind is not composed; viscosity (Algorithms_Viscosity and the Dirichlet
+//    pressure of Algorithms_Solve_Pressure_Dirichlet, as test/Lateral_jet_3.cpp
+//    composes them under VISCOSITY) only in the v* commands, with the
+//    viscosity of the state header,
 //  * prototype speed/pressure/layer/id are initialised explicitly (the reference
 //    leaves them uninitialised: src/Physvector.tpp:8-10),
 //  * inflow refill uses Policy_Add_Particle_Jitter8 (8 jittered particles per
@@ -105,6 +108,11 @@
 #include "Algorithms_Convection.h"
 #include "Algorithms_Move_Particles.h"
 #include "Algorithms_RungeKutta_RK2_TVD.h"
+#include "Policy_Laplacian_Speed.h"
+#include "Policy_Viscosity_Apply_If.h"
+#include "Policy_Dirichlet_Boundary.h"
+#include "Algorithms_Viscosity.h"
+#include "Algorithms_Solve_Pressure_Dirichlet.h"
 
 #ifdef MAC_WITH_GPU
 // The C++ drop-in layer of the device path; compiled in only for _ref/mac_ref_gpu.
@@ -304,7 +312,7 @@ static int run(int argc, char** argv) {
 
   typedef Data_Viscosity<type_chunk_table> type_data_viscosity;
   type_data_viscosity m_data_viscosity(m_chunk_table);
-  m_data_viscosity.m_viscosity = 0.0;
+  m_data_viscosity.m_viscosity = st.hdr.viscosity;
   typedef Data_Grid_Base_Spacing<type_data_viscosity, Physvector<DIM, type_data_value>> type_data_grid;
   type_data_grid m_data_grid(m_data_viscosity);
   Physvector<DIM, type_data_value> h;
@@ -458,6 +466,30 @@ static int run(int argc, char** argv) {
   typedef Algorithms_RungeKutta_RK2_TVD<type_data_ref, type_pol_ODE> type_alg_ODE;
   type_alg_ODE m_alg_ODE(m_data_ref, m_pol_ODE);
 
+  // viscous composition (test/Lateral_jet_3.cpp:533-605 with VISCOSITY)
+  typedef Policy_Laplacian_Speed<type_data_ref> type_pol_lap_speed;
+  type_pol_lap_speed m_pol_lap_speed(m_data_ref);
+  typedef Policy_Viscosity_Apply_If<type_data_ref> type_pol_visc_if;
+  type_pol_visc_if m_pol_visc_if;
+  typedef Policies<type_pol_gravity, type_pol_conv_if, type_pol_conv, type_pol_lap_speed, type_pol_visc_if> type_pol_grid_v;
+  type_pol_grid_v m_pol_grid_v(m_pol_gravity, m_pol_conv_if, m_pol_conv, m_pol_lap_speed, m_pol_visc_if);
+  typedef Algorithms_Viscosity<type_data_ref, type_pol_grid_v> type_alg_viscosity;
+  type_alg_viscosity m_alg_viscosity(m_data_ref, m_pol_grid_v);
+  typedef Algorithms<type_alg_gravity, type_alg_convection, type_alg_viscosity> type_alg_solve_grid_v;
+  type_alg_solve_grid_v m_alg_solve_grid_v(m_alg_gravity, m_alg_convection, m_alg_viscosity);
+  typedef Policy_Dirichlet_Boundary<type_data_ref> type_pol_dirichlet;
+  type_pol_dirichlet m_pol_dirichlet(m_data_ref);
+  typedef Policies<type_pol_solve_linear, type_pol_divergence, type_pol_gradiant, type_pol_vn, type_pol_pres_if, type_pol_dirichlet> type_pol_pres_v;
+  type_pol_pres_v m_pol_pres_v(m_pol_solve_linear, m_pol_divergence, m_pol_gradiant, m_pol_vn, m_pol_pres_if, m_pol_dirichlet);
+  typedef Algorithms_Solve_Pressure_Dirichlet<type_data_ref, type_pol_pres_v> type_alg_solve_pressure_v;
+  type_alg_solve_pressure_v m_alg_solve_pressure_v(m_data_ref, m_pol_pres_v);
+  typedef Algorithms_Do_Pressure<type_data_ref, type_alg_solve_pressure_v> type_alg_do_pressure_v;
+  type_alg_do_pressure_v m_alg_do_pressure_v(m_data_ref, m_alg_solve_pressure_v);
+  typedef Policies<type_alg_solve_grid_v, type_alg_solve_pressure_v> type_pol_ODE_v;
+  type_pol_ODE_v m_pol_ODE_v(m_alg_solve_grid_v, m_alg_solve_pressure_v);
+  typedef Algorithms_RungeKutta_RK2_TVD<type_data_ref, type_pol_ODE_v> type_alg_ODE_v;
+  type_alg_ODE_v m_alg_ODE_v(m_data_ref, m_pol_ODE_v);
+
   typedef Policy_Advance_Ode_RungeKutta<type_data_ref> type_pol_advance;
   type_pol_advance m_pol_advance;
   typedef Policies<type_pol_advance, type_pol_interp_sym> type_pol_move;
@@ -564,6 +596,22 @@ static int run(int argc, char** argv) {
         }
       }
 #endif
+    } else if (cmd == "vforces") {
+      type_chunk_speed::ispeed = 0;
+      for (auto it = grid.begin(); it != grid.end(); ++it) it.data().Acceleration_GetRef().SetZero(true);
+      m_alg_solve_grid_v.Do();
+    } else if (cmd == "vproject") {
+      type_chunk_speed::ispeed = 0;
+      m_alg_do_pressure_v.Do();
+    } else if (cmd == "vode") {
+      m_alg_ODE_v.Do();
+    } else if (cmd == "vstep") {
+      ++g_refill_seed;
+      m_alg_init.Do();
+      m_alg_ODE_v.Do();
+      m_alg_extrapolate.Do();
+      m_alg_move.Do();
+      timing.m_t += timing.m_dt;
     } else if (cmd == "csc") {
       // Projection of speed 0 with the assembled system written to argv[4].
       g_csc_dump = fopen(argv[4], "wb");

@@ -48,7 +48,8 @@ typedef struct {
   uint64_t step;           /* refill seed counter */
   int32_t interp_symmetric;
   int32_t reserved_i;
-  uint8_t reserved[256 - 8 - 16 - 24 - 48 - 8 - 8 - 8];
+  double viscosity;        /* Data_Viscosity::m_viscosity (0: inviscid) */
+  uint8_t reserved[256 - 8 - 16 - 24 - 48 - 8 - 8 - 8 - 8];
 } mac_state_header;
 
 typedef struct {

@@ -17,7 +17,15 @@ CFL 0.5) produced by the unmodified reference algorithms:
   c1_ref_t30_csc.bin   the CSC system the reference assembled for the projection
                        of c1_ref_t30 (n, nnz, offset, indice, value, b, x)
 
-Usage: python tests/golden/make_golden.py
+Viscous fixtures (viscosity 1e-3 in the state header; the reference's
+Algorithms_Viscosity and Algorithms_Solve_Pressure_Dirichlet with
+Policy_Dirichlet_Boundary, composed as test/Lateral_jet_3.cpp does):
+
+  c1_ref_t30v_<stage>.npz  c1_ref_t30 with viscosity after vforces, vproject, vode
+  c1_ref_s31v.npz      one viscous step from c1_ref_s30 (with viscosity)
+  c1_ref_s40v.npz      ten viscous steps from c1_ref_s30
+
+Usage: python tests/golden/make_golden.py [--viscous-only]
 """
 from __future__ import annotations
 
@@ -34,6 +42,22 @@ from mac_b200.state import State, jet_world  # noqa: E402
 import oracle  # noqa: E402
 
 STAGES = ["forces", "ode", "project", "extrapolate", "move", "movelin"]
+VSTAGES = ["vforces", "vproject", "vode"]
+VISCOSITY = 1e-3
+
+
+def viscous(t, out):
+    for name in ("t30", "s30"):
+        s = State.load_npz(out("c1_ref_" + name))
+        s.params.viscosity = VISCOSITY
+        s.write(t(name + "v"))
+    for st in VSTAGES:
+        oracle.run_ref(st, t("t30v"), t("t30v_" + st))
+        State.read(t("t30v_" + st)).save_npz(out("c1_ref_t30v_" + st))
+    oracle.run_ref("vstep", t("s30v"), t("s31v"), 1)
+    State.read(t("s31v")).save_npz(out("c1_ref_s31v"))
+    oracle.run_ref("vstep", t("s30v"), t("s40v"), 10)
+    State.read(t("s40v")).save_npz(out("c1_ref_s40v"))
 
 
 def main():
@@ -43,6 +67,10 @@ def main():
     tmp = tempfile.mkdtemp()
     t = lambda n: os.path.join(tmp, n + ".state")
     out = lambda n: os.path.join(HERE, n + ".npz")
+    if "--viscous-only" in sys.argv:
+        viscous(t, out)
+        print("viscous fixtures written to", HERE)
+        return
     s = jet_world()
     s.write(t("setup"))
     s.save_npz(out("c1_setup"))
@@ -62,6 +90,7 @@ def main():
         oracle.run_ref(st, t("t30"), t("t30_" + st))
         State.read(t("t30_" + st)).save_npz(out("c1_ref_t30_" + st))
     oracle.run_ref("csc", t("t30"), t("junk"), os.path.join(HERE, "c1_ref_t30_csc.bin"))
+    viscous(t, out)
     print("fixtures written to", HERE)
 
 

@@ -122,3 +122,47 @@ def test_cg_stand_in_matches_direct_solve():
         assert err <= 1e-10, err
         checked += 1
     assert checked >= 1
+
+
+# ------------------------------------------------- viscosity (Dirichlet pressure)
+def _viscous(golden, name, nu=1e-3):
+    s = golden(name)
+    s.params.viscosity = nu
+    return s
+
+
+def test_viscous_forces_bit_exact(golden, run_oracle):
+    """Algorithms<Gravity, Convection, Viscosity> (src/Algorithms_Viscosity.h:24-30)."""
+    got, st = run_oracle("vforces", _viscous(golden, "c1_ref_t30"))
+    ref = golden("c1_ref_t30v_vforces")
+    compare_topology(got, ref)
+    _exact(got, ref)
+    assert st["invalid_reads"] == 0
+    plain = golden("c1_ref_t30_forces")
+    assert max_abs_diff(got, plain, ("ax", "ay", "az"))["az"] > 1e-3  # the viscous term is there
+
+
+@pytest.mark.parametrize("stage", ["vproject", "vode"])
+def test_viscous_solver_stages_within_rounding(golden, run_oracle, stage):
+    """Algorithms_Solve_Pressure_Dirichlet with Policy_Dirichlet_Boundary
+    (src/Algorithms_Solve_Pressure_Dirichlet.h:171-233, src/Policy_Dirichlet_Boundary.h:27-109)."""
+    got, st = run_oracle(stage, _viscous(golden, "c1_ref_t30"))
+    ref = golden("c1_ref_t30v_" + stage)
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ALL)
+    assert max(e.values()) <= 1e-12, e
+    assert st["relres"] <= 1e-14
+
+
+def test_viscous_steps_track_reference(golden, run_oracle):
+    got, _ = run_oracle("vstep", _viscous(golden, "c1_ref_s30"))
+    ref = golden("c1_ref_s31v")
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("u0x", "u0y", "u0z", "p"))
+    assert max(e.values()) <= 1e-12, e
+    compare_particles(got, ref, atol=1e-14)
+    got, _ = run_oracle("vstep", _viscous(golden, "c1_ref_s30"), n=10)
+    ref = golden("c1_ref_s40v")
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("u0x", "u0y", "u0z", "p"))
+    assert max(e.values()) <= 1e-10, e
