@@ -66,6 +66,13 @@ typedef struct {
   int64_t max_particles;
   int32_t device;
   int32_t div_check;    /* 1: compute max |div| after each projection */
+  /* Kinematic viscosity (Data_Grid_Base::m_viscosity). 0 runs the inviscid
+   * composition (Algorithms_Gravity + Algorithms_Convection, Algorithms_Solve_Pressure);
+   * > 0 adds Algorithms_Viscosity with Policy_Laplacian_Speed and
+   * Policy_Viscosity_Apply_If to the forces and projects with
+   * Algorithms_Solve_Pressure_Dirichlet + Policy_Dirichlet_Boundary
+   * (src/Algorithms_Viscosity.h:24-30, src/Algorithms_Solve_Pressure_Dirichlet.h:171-233). */
+  double viscosity;
 } mac_params;
 
 /* Host view of a world, arrays owned by the caller. Brick b holds cells

@@ -70,11 +70,42 @@ __device__ inline double convection(const double* const* U, const int* sn, int x
   return ret;
 }
 
+// Policy_Viscosity_Apply_If::Get_Viscosity_Apply_If (src/Policy_Viscosity_Apply_If.h:15-42):
+// a fluid cell, or a cell with a layer one of whose -e_j neighbours (any axis)
+// exists and is fluid. One answer for the three faces of the cell.
+__device__ inline bool viscosity_applies(const int* sn, const int8_t* __restrict__ lay,
+                                         const uint8_t* __restrict__ type, int64_t c, bool fluid, int x, int y,
+                                         int z) {
+  if (fluid) return true;
+  if (lay[c] == kEmpty) return false;
+  for (int j = 0; j < 3; ++j) {
+    int64_t n = cidx(sn, x - (j == 0), y - (j == 1), z - (j == 2));
+    if (n >= 0 && lay[n] != kMissing && is_fluid(type[n])) return true;
+  }
+  return false;
+}
+
+// Policy_Laplacian_Speed::Get_Laplacian_Speed(neigh, i) (src/Policy_Laplacian_Speed.h:22-36):
+// per axis j, -2 u(c)/h_j^2 + u(c+e_j)/h_j^2 + u(c-e_j)/h_j^2 with h_j^-2 = pow(1/h_j, 2),
+// accumulated in that order.
+__device__ inline double laplacian(const double* __restrict__ Ui, const int* sn, int x, int y, int z,
+                                   const Params& P) {
+  double t = 0;
+  const double uc = rdv(Ui, cidx(sn, x, y, z));
+  for (int j = 0; j < 3; ++j) {
+    t -= 2 * uc * P.lih2[j];
+    t += rdv(Ui, cidx(sn, x + (j == 0), y + (j == 1), z + (j == 2))) * P.lih2[j];
+    t += rdv(Ui, cidx(sn, x - (j == 0), y - (j == 1), z - (j == 2))) * P.lih2[j];
+  }
+  return t;
+}
+
 // Acceleration of face i of cell (x,y,z): forced zero, then Policy_Gravity and
 // Policy_Upwind_1_Order applied through the non-forced Set (const faces keep 0).
 // Gravity applies if the cell is fluid, or has a layer and its -e_g neighbour
 // is fluid (src/Policy_Gravity.h:14-34); convection uses the same rule on axis
-// i (src/Policy_Convection_Apply_If.h:41-61).
+// i (src/Policy_Convection_Apply_If.h:41-61). With a viscosity, Algorithms_Viscosity
+// (src/Algorithms_Viscosity.h:24-30) then adds viscosity * Laplacian.
 __device__ inline double face_accel(const double* const* U, const int* sn, const int8_t* __restrict__ lay,
                                     const uint8_t* __restrict__ type, int64_t c, uint8_t fl, int x, int y, int z,
                                     int i, const Params& P) {
@@ -99,6 +130,8 @@ __device__ inline double face_accel(const double* const* U, const int* sn, const
     if (g) a = a + P.g;
   }
   if (apply) a = a + convection(U, sn, x, y, z, i, P);
+  if (P.nu != 0.0 && viscosity_applies(sn, lay, type, c, fluid, x, y, z))
+    a = a + laplacian(U[i], sn, x, y, z, P) * P.nu;
   return a;
 }
 

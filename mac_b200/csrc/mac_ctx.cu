@@ -1,4 +1,5 @@
 // Context lifetime, host <-> device state transfer and the C-ABI entry points.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -157,6 +158,7 @@ static void free_all(Ctx* c) {
   prof_free(c);
   free_solver(c);
   cudaFree(c->bkey); cudaFree(c->lay); cudaFree(c->type); cudaFree(c->flags); cudaFree(c->f64);
+  cudaFree(c->pdir);
   cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
@@ -176,6 +178,7 @@ static int create(const mac_params* p, Ctx** out) {
     return MAC_ERR_INVALID;
   for (int i = 0; i < 3; ++i)
     if (!(p->h[i] > 0)) return MAC_ERR_INVALID;
+  if (!(p->viscosity >= 0) || !std::isfinite(p->viscosity)) return MAC_ERR_INVALID;
   if (p->device < 0 || p->device >= ndev) return MAC_ERR_INVALID;
   MAC_CUDA(cudaSetDevice(p->device));
   Ctx* c = new (std::nothrow) Ctx();
@@ -199,6 +202,8 @@ static int create(const mac_params* p, Ctx** out) {
   c->dp.gaxis = p->gravity_axis - 1;
   c->dp.layer_max = p->layer_max;
   c->dp.interp_sym = p->interp_symmetric;
+  c->dp.nu = p->viscosity;
+  for (int i = 0; i < 3; ++i) c->dp.lih2[i] = std::pow(c->dp.ih[i], 2);
   c->cap_bricks = p->max_bricks;
   c->cap_particles = p->max_particles;
   c->hcap = 64;
@@ -213,6 +218,7 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->type, nc));
   A(dalloc(&c->flags, nc));
   A(dalloc(&c->f64, NF64 * nc));
+  if (p->viscosity > 0) A(dalloc(&c->pdir, nc));
   A(dalloc(&c->nbr, kNbr * c->cap_bricks));
   A(dalloc(&c->blist, c->cap_bricks));
   A(dalloc(&c->blist2, c->cap_bricks));

@@ -90,6 +90,9 @@ struct Params {
   int gaxis;     // 0..2
   int layer_max;
   int interp_sym;
+  // viscosity (0: inviscid composition) and pow(1/h, 2) as the Laplacian of
+  // src/Policy_Laplacian_Speed.h:22-36 computes it
+  double nu, lih2[3];
   // inverse diagonal of the level-0 operator by active faces per axis
   // (index ax + 3 ay + 9 az, each 0..2); 0 when no face is active
   double dtab[27];
@@ -123,6 +126,7 @@ struct Ctx {
   uint8_t* type = nullptr;    // [cap*512]
   uint8_t* flags = nullptr;   // [cap*512]
   double* f64 = nullptr;      // [NF64][cap*512]
+  double* pdir = nullptr;     // [cap*512] Dirichlet air pressure, NaN off the boundary (viscous only)
   int* nbr = nullptr;         // [cap][27]
   int* blist = nullptr;       // live bricks (current)
   int* blist2 = nullptr;      // scratch for compaction

@@ -169,16 +169,62 @@ __global__ void k_setup_reset(Scalars* ds) {
   }
 }
 
+// ------------------------------------------------------------ Dirichlet air
+// Policy_Dirichlet_Boundary (src/Policy_Dirichlet_Boundary.h:27-109) over the
+// live bricks, for the viscous projection. "Air" there is GetIsAir, which the
+// cell-type map answers true for air and for solid cells
+// (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:21-35), i.e. !is_fluid. A
+// Dirichlet cell is an existing air cell with an existing non-air face
+// neighbour; its pressure is
+//   p_D = - sum over such neighbours (i, s) of 2 nu (u_i(c+e_i) - u_i(c)) / h_i * s
+// on speed buffer U, in the reference's (i, s) order. pdir gets p_D there and
+// NaN everywhere else (every slot of every live brick is written).
+__global__ void __launch_bounds__(512) k_dirichlet(const int* __restrict__ blist, const int* __restrict__ nbr,
+                                                   const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
+                                                   const double* __restrict__ ux, const double* __restrict__ uy,
+                                                   const double* __restrict__ uz, double* __restrict__ pdir,
+                                                   Params P) {
+  __shared__ int64_t sb[6];
+  int b = blist[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  __syncthreads();
+  int o = threadIdx.x;
+  int64_t c = (int64_t)b * kCells + o;
+  double out = __longlong_as_double(0x7ff8000000000000ll);
+  if (lay[c] != kMissing && !is_fluid(type[c])) {
+    const double* U[3] = {ux, uy, uz};
+    double ret = 0;
+    bool db = false;
+    for (int i = 0; i < 3; ++i) {
+      for (int s = -1; s <= 1; s += 2) {
+        int64_t n = nb0(sb, c, o, 2 * i + (s > 0));
+        if (n >= 0 && lay[n] != kMissing && is_fluid(type[n])) {
+          db = true;
+          const double v1 = U[i][c];
+          const int64_t n2 = nb0(sb, c, o, 2 * i + 1);
+          const double v2 = n2 < 0 ? 0.0 : U[i][n2];
+          ret -= 2 * P.nu * (v2 - v1) * P.ih[i] * s;
+        }
+      }
+    }
+    if (db) out = ret;
+  }
+  pdir[c] = out;
+}
+
 // ------------------------------------------------------------ CG kernels
 // Divergence (Policy_Divergence::Get_Divergence, src/Policy_Divergence.h:20-29)
 // of speed buffer ib into rhs = -div (the right-hand side of M x = -div) and
 // the block's partial |div|^2; x starts at 0 or, warm, at the cell pressure.
+// With Dirichlet air pressures (pdir non-null, the viscous projection of
+// src/Algorithms_Solve_Pressure_Dirichlet.h:178-188), a cell next to a
+// Dirichlet cell first takes div -= sum over those neighbours of p_D / h_i^2.
 __global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                     const uint16_t* __restrict__ fmask, const double* __restrict__ ux,
                                                     const double* __restrict__ uy, const double* __restrict__ uz,
                                                     const double* __restrict__ pres, double* __restrict__ rhs,
                                                     double* __restrict__ x, double* __restrict__ r, int warm,
-                                                    double* partial, Params P) {
+                                                    double* partial, Params P, const double* __restrict__ pdir) {
   __shared__ int64_t sb[6];
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
@@ -201,6 +247,20 @@ __global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ dbl,
       d -= U[i][c] * P.ih[i];
       int64_t n = nb0(sb, c, o, 2 * i + 1);
       d += (n < 0 ? 0.0 : U[i][n]) * P.ih[i];
+    }
+    if (pdir) {
+      double sum = 0;
+      bool any = false;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        int64_t n = nb0(sb, c, o, f);
+        double q = n < 0 ? 0.0 : pdir[n];
+        if (n >= 0 && q == q) {
+          any = true;
+          sum += q * P.ih[f >> 1] * P.ih[f >> 1];
+        }
+      }
+      if (any) d -= sum;
     }
     rhs[c] = -d;
     r[c] = -d;
@@ -377,15 +437,18 @@ __global__ void __launch_bounds__(512) k_jacobi_prec(const int* __restrict__ dbl
 
 // Pressure write-back and velocity correction, fused
 // (src/Algorithms_Solve_Pressure.h:185-207): existing cells get p = x in the
-// domain and 0 elsewhere; face i of a cell in the domain, or whose -e_i
+// domain, p_D on Dirichlet air cells of the viscous projection
+// (src/Algorithms_Solve_Pressure_Dirichlet.h:196-208) and 0 elsewhere; face i of a cell in the domain, or whose -e_i
 // neighbour is, gets u_i -= p(c)/h_i - p(c-e_i)/h_i
 // (Policy_Gradiant::Get_Gradiant, src/Policy_Gradiant.h:32-37) through the
 // non-forced Set (const faces keep their value).
+__device__ inline double dir_or_zero(double q) { return q == q ? q : 0.0; }
+
 __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist, const int* __restrict__ nbr,
                                                   const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
                                                   const uint8_t* __restrict__ flags, const double* __restrict__ x,
                                                   double* __restrict__ pres, double* ux, double* uy, double* uz,
-                                                  Params P) {
+                                                  Params P, const double* __restrict__ pdir) {
   __shared__ int64_t sb[6];
   int b = blist[blockIdx.x];
   load_face_bases(nbr, b, sb);
@@ -394,7 +457,7 @@ __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist,
   int64_t c = (int64_t)b * kCells + o;
   if (lay[c] == kMissing) return;
   bool dc = is_fluid(type[c]);
-  double pc = dc ? x[c] : 0.0;
+  double pc = dc ? x[c] : (pdir ? dir_or_zero(pdir[c]) : 0.0);
   pres[c] = pc;
   uint8_t fl = flags[c];
   double* U[3] = {ux, uy, uz};
@@ -404,7 +467,7 @@ __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist,
     bool dn = nexists && is_fluid(type[n]);
     if (!(dc || dn)) continue;
     if (fl & (1u << i)) continue;
-    double pn = nexists ? (dn ? x[n] : 0.0) : (n >= 0 ? pres[n] : 0.0);
+    double pn = nexists ? (dn ? x[n] : (pdir ? dir_or_zero(pdir[n]) : 0.0)) : (n >= 0 ? pres[n] : 0.0);
     double gr = pc * P.ih[i];
     gr -= pn * P.ih[i];
     U[i][c] = U[i][c] - gr;
@@ -600,12 +663,22 @@ int project(Ctx* c, int ib) {
                   c->f64 + (size_t)(3 * ib + 2) * cap};
   int status = MAC_OK;
   int rc;
+  // the viscous composition projects with Dirichlet air pressures
+  double* pdir = c->dp.nu > 0 ? c->pdir : nullptr;
+  if (pdir && nd == 0 && c->nlive_host > 0) {
+    k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, U[0], U[1], U[2], pdir,
+                                               c->dp); MAC_COUNT(c);
+  }
   if (nd > 0) {
     int warm = c->prm.warm_start ? 1 : 0;
     double rtol2 = c->prm.rtol * c->prm.rtol;
     prof_begin(c, PH_DIVERGENCE);
+    if (pdir) {
+      k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, U[0], U[1], U[2], pdir,
+                                                 c->dp); MAC_COUNT(c);
+    }
     k_divergence<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,
-                                     c->x, c->r, warm, c->partial, c->dp); MAC_COUNT(c);
+                                     c->x, c->r, warm, c->partial, c->dp, pdir); MAC_COUNT(c);
     prof_end(c, PH_DIVERGENCE);
     k_fin_bnorm<<<1, 1024, 0, st>>>(c->partial, nd, c->ds); MAC_COUNT(c);
     if (warm) {
@@ -678,7 +751,7 @@ int project(Ctx* c, int ib) {
   if (n > 0) {
     prof_begin(c, PH_GRADIENT);
     k_gradient<<<n, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, c->flags, c->x, c->f64 + (size_t)PRES * cap,
-                                  U[0], U[1], U[2], c->dp); MAC_COUNT(c);
+                                  U[0], U[1], U[2], c->dp, pdir); MAC_COUNT(c);
     prof_end(c, PH_GRADIENT);
   }
   if (c->prm.div_check && nd > 0) {

@@ -34,7 +34,7 @@ class mac_params(ctypes.Structure):
                 ("layer_max", ctypes.c_int32), ("interp_symmetric", ctypes.c_int32), ("solver", ctypes.c_int32),
                 ("rtol", ctypes.c_double), ("max_iters", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("max_bricks", ctypes.c_int64), ("max_particles", ctypes.c_int64), ("device", ctypes.c_int32),
-                ("div_check", ctypes.c_int32)]
+                ("div_check", ctypes.c_int32), ("viscosity", ctypes.c_double)]
 
 
 _P = ctypes.POINTER
@@ -156,6 +156,7 @@ def make_params(pr: Params, max_bricks: int, max_particles: int, solver="mgpcg64
     p.max_particles = int(max_particles)
     p.device = device
     p.div_check = int(div_check)
+    p.viscosity = float(getattr(pr, "viscosity", 0.0))
     return p
 
 

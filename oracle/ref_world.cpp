@@ -525,6 +525,7 @@ static int run(int argc, char** argv) {
   gprm.gravity_axis = st.hdr.gravity_axis;
   gprm.layer_max = st.hdr.layer_max;
   gprm.interp_symmetric = st.hdr.interp_symmetric;
+  gprm.viscosity = st.hdr.viscosity;
   gprm.rtol = g_cg_rtol;
   gprm.max_iters = 5000;
   gprm.max_bricks = 8192;
