@@ -25,10 +25,15 @@ import numpy as np
 BRICK = 8
 BRICK_CELLS = 512
 AIR, FLUID, SOLID, INFLOW = 0, 1, 2, 3
+# The Interior material of Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres
+# (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:3-22): a fluid cell
+# deep enough below the surface to carry no particles (depth composition only).
+INTERIOR = 4
+FLUID_TYPES = (FLUID, INFLOW, INTERIOR)
 FLAG_CONST = (1, 2, 4)
 FLAG_NODELETE = 8
 
-_HDR = struct.Struct("<8sqq3d6dii Q ii d128x")
+_HDR = struct.Struct("<8sqq3d6dii Q ii d 6i 104x")
 assert _HDR.size == 256
 
 CELL_F64 = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
@@ -49,6 +54,14 @@ class Params:
     step: int = 0
     interp_symmetric: int = 1
     viscosity: float = 0.0
+    # depth composition of the topology (test/Jet3.cpp:519-549): Policy_Depth(max,
+    # interior, remove); 0 = the pipeline-A topology without depth
+    depth_mode: int = 0
+    depth_max: int = 0
+    depth_interior: int = 0
+    depth_remove: int = 0
+    # inflow refill: 0 = 8 jittered particles, n >= 1 = Policy_Add_Particle_Cube(n)
+    refill_cube: int = 0
 
 
 @dataclasses.dataclass
@@ -62,6 +75,11 @@ class State:
     layer: np.ndarray         # (nb, 512) int32
     id: np.ndarray            # (nb, 512) int32
     pos: np.ndarray           # (np, 3) float64
+    depth: np.ndarray = None  # (nb, 512) int32, -1 = empty (src/Data_Grid_Depth_Empty.h:6-14)
+
+    def __post_init__(self):
+        if self.depth is None:
+            self.depth = np.full(self.layer.shape, -1, dtype=np.int32)
 
     @property
     def nbricks(self) -> int:
@@ -74,9 +92,10 @@ class State:
     # ------------------------------------------------------------------ io
     def write(self, path: str) -> None:
         pr = self.params
-        hdr = _HDR.pack(b"MACST001", self.nbricks, self.nparticles, *pr.h, pr.t, pr.dt,
+        hdr = _HDR.pack(b"MACST002", self.nbricks, self.nparticles, *pr.h, pr.t, pr.dt,
                         pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
-                        pr.layer_max, pr.step, pr.interp_symmetric, 0, pr.viscosity)
+                        pr.layer_max, pr.step, pr.interp_symmetric, 0, pr.viscosity, pr.depth_mode,
+                        pr.depth_max, pr.depth_interior, pr.depth_remove, pr.refill_cube, 0)
         with open(path, "wb") as f:
             f.write(hdr)
             f.write(np.ascontiguousarray(self.keys, dtype="<i4").tobytes())
@@ -87,6 +106,7 @@ class State:
             f.write(np.ascontiguousarray(self.type, dtype="u1").tobytes())
             f.write(np.ascontiguousarray(self.layer, dtype="<i4").tobytes())
             f.write(np.ascontiguousarray(self.id, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(self.depth, dtype="<i4").tobytes())
             f.write(np.ascontiguousarray(self.pos, dtype="<f8").tobytes())
 
     @staticmethod
@@ -94,8 +114,8 @@ class State:
         with open(path, "rb") as f:
             buf = f.read()
         (magic, nb, npart, h0, h1, h2, t, dt, cfl, dtmin, dtmax, g, gax, lmax, step, isym,
-         _r, visc) = _HDR.unpack_from(buf, 0)
-        if magic != b"MACST001":
+         _r, visc, dmode, dmax, dint, drem, cube, _r2) = _HDR.unpack_from(buf, 0)
+        if magic != b"MACST002":
             raise ValueError(f"{path}: not a state file")
         off = _HDR.size
         nc = nb * BRICK_CELLS
@@ -113,19 +133,22 @@ class State:
         typ = take("u1", nc, (nb, BRICK_CELLS))
         layer = take("<i4", nc, (nb, BRICK_CELLS))
         ids = take("<i4", nc, (nb, BRICK_CELLS))
+        depth = take("<i4", nc, (nb, BRICK_CELLS))
         pos = take("<f8", npart * 3, (npart, 3))
         params = Params(h=(h0, h1, h2), t=t, dt=dt, cfl_factor=cfl, dt_min=dtmin, dt_max=dtmax,
                         gravity=g, gravity_axis=gax, layer_max=lmax, step=step,
-                        interp_symmetric=isym, viscosity=visc)
-        return State(params, keys, exists, f64, flags, typ, layer, ids, pos)
+                        interp_symmetric=isym, viscosity=visc, depth_mode=dmode, depth_max=dmax,
+                        depth_interior=dint, depth_remove=drem, refill_cube=cube)
+        return State(params, keys, exists, f64, flags, typ, layer, ids, pos, depth)
 
     def save_npz(self, path: str) -> None:
         """Compressed copy (used for the committed fixtures)."""
         pr = self.params
         hdr = np.array([*pr.h, pr.t, pr.dt, pr.cfl_factor, pr.dt_min, pr.dt_max, pr.gravity, pr.gravity_axis,
-                        pr.layer_max, pr.step, pr.interp_symmetric, pr.viscosity], dtype=np.float64)
+                        pr.layer_max, pr.step, pr.interp_symmetric, pr.viscosity, pr.depth_mode, pr.depth_max,
+                        pr.depth_interior, pr.depth_remove, pr.refill_cube], dtype=np.float64)
         np.savez_compressed(path, hdr=hdr, keys=self.keys, exists=self.exists, flags=self.flags, type=self.type,
-                            layer=self.layer, id=self.id, pos=self.pos, **self.f64)
+                            layer=self.layer, id=self.id, pos=self.pos, depth=self.depth, **self.f64)
 
     @staticmethod
     def load_npz(path: str) -> "State":
@@ -134,8 +157,10 @@ class State:
         pr = Params(h=(h[0], h[1], h[2]), t=h[3], dt=h[4], cfl_factor=h[5], dt_min=h[6], dt_max=h[7],
                     gravity=h[8], gravity_axis=int(h[9]), layer_max=int(h[10]), step=int(h[11]),
                     interp_symmetric=int(h[12]), viscosity=float(h[13]) if h.size > 13 else 0.0)
+        if h.size > 18:
+            pr.depth_mode, pr.depth_max, pr.depth_interior, pr.depth_remove, pr.refill_cube = (int(v) for v in h[14:19])
         return State(pr, z["keys"], z["exists"], {n: z[n] for n in CELL_F64}, z["flags"], z["type"], z["layer"],
-                     z["id"], z["pos"])
+                     z["id"], z["pos"], z["depth"] if "depth" in z.files else None)
 
     @staticmethod
     def load(path: str) -> "State":
@@ -150,14 +175,14 @@ class State:
 
     def fluid_cells(self) -> int:
         ex = self.exists.astype(bool)
-        return int(np.count_nonzero(ex & ((self.type == FLUID) | (self.type == INFLOW))))
+        return int(np.count_nonzero(ex & np.isin(self.type, FLUID_TYPES)))
 
     def sorted(self) -> "State":
         """Bricks in (z, y, x) key order (the canonical order of state files)."""
         order = np.lexsort((self.keys[:, 0], self.keys[:, 1], self.keys[:, 2]))
         return State(self.params, self.keys[order], self.exists[order],
                      {n: v[order] for n, v in self.f64.items()}, self.flags[order],
-                     self.type[order], self.layer[order], self.id[order], self.pos)
+                     self.type[order], self.layer[order], self.id[order], self.pos, self.depth[order])
 
 
 def from_cells(params: Params, keys, typ, flags, u, pos=None) -> State:

@@ -33,6 +33,7 @@ typedef struct {
   uint8_t type[512];
   int32_t layer[512];
   int32_t id[512];
+  int32_t depth[512]; /* Data_Grid_Depth_Empty: -1 = empty */
   int32_t mark[512]; /* scratch */
 } brick_t;
 
@@ -102,7 +103,7 @@ static int offs(int x, int y, int z) { return (x & 7) + 8 * (y & 7) + 64 * (z & 
 static void brick_prototype(brick_t* b, int bx, int by, int bz) {
   memset(b, 0, sizeof(*b));
   b->key[0] = bx; b->key[1] = by; b->key[2] = bz;
-  for (int o = 0; o < 512; ++o) { b->layer[o] = -1; b->id[o] = -1; }
+  for (int o = 0; o < 512; ++o) { b->layer[o] = -1; b->id[o] = -1; b->depth[o] = -1; }
 }
 
 static int64_t brick_create(world_t* w, int bx, int by, int bz) {
@@ -169,12 +170,20 @@ static double rd_p(world_t* w, const int k[3], int dx, int dy, int dz) {
   return c.b >= 0 ? B(c)->p[c.o] : 0.0;
 }
 
-static int is_fluid(uint8_t t) { return t == MAC_FLUID || t == MAC_INFLOW; }
-/* Data_CellType_Domain_Fluid: in domain <=> GetIsFluid (src/Data_CellType_Domain_Fluid.h:59-62). */
+/* GetIsFluid: Material_To_Type_Fluid(m) == Fluid, true for fluid, inflow and, in
+ * the depth composition's cell type, interior
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:24-44; the
+ * 0-pressure material is never set by any algorithm). */
+static int is_fluid(uint8_t t) { return t == MAC_FLUID || t == MAC_INFLOW || t == MAC_INTERIOR; }
+/* Data_CellType_Domain_Fluid: in domain <=> GetIsFluid (src/Data_CellType_Domain_Fluid.h:59-62);
+ * Data_CellType_Domain_Fluid_Without_0_Pres adds "and not 0-pressure"
+ * (src/Data_CellType_Domain_Fluid_Without_0_Pres.h:59-62), the same here. */
 static int in_domain(uint8_t t) { return is_fluid(t); }
-/* Sticky setters (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:141-157). */
-static uint8_t set_air(uint8_t t) { return t == MAC_FLUID ? MAC_AIR : t; }
-static uint8_t set_fluid(uint8_t t) { return t == MAC_AIR ? MAC_FLUID : t; }
+/* Sticky setters (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:141-157; with the
+ * interior material, src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:217-249:
+ * SetAir from fluid or interior, SetFluid from air or interior, SetInterior always). */
+static uint8_t set_air(uint8_t t) { return (t == MAC_FLUID || t == MAC_INTERIOR) ? MAC_AIR : t; }
+static uint8_t set_fluid(uint8_t t) { return (t == MAC_AIR || t == MAC_INTERIOR) ? MAC_FLUID : t; }
 
 /* Data_Grid_Speed::Set(i, v, force) (src/Data_Grid_Speed.tpp:19-26): the three
  * buffers of a cell share its const bits (src/Data_Chunk_Speed.h:99-123). */
@@ -215,6 +224,32 @@ static void add_particle(world_t* w, const double p[3]) {
   ++w->np;
 }
 
+/* The refill policy's AddParticle(key): 8 jittered particles, or
+ * Policy_Add_Particle_Cube(n) (src/Policy_Add_Particle_Cube.h:29-59): (2n+1)^3
+ * particles at (k_i + t_i/(2n+1)) h_i, t_i = -n..n, x fastest. */
+static void add_refill(world_t* w, const int k[3]) {
+  const int n = w->hdr.refill_cube;
+  if (n <= 0) {
+    for (int s = 0; s < 8; ++s) {
+      double p[3];
+      mac_jitter8_position(w->seed, k[0], k[1], k[2], s, w->h[0], w->h[1], w->h[2], p);
+      add_particle(w, p);
+    }
+    return;
+  }
+  const double dh = 1. / (2 * n + 1);
+  int t[3] = {-n, -n, -n};
+  while (1) {
+    double p[3];
+    for (int i = 0; i < 3; ++i) p[i] = (k[i] + t[i] * dh) * w->h[i];
+    add_particle(w, p);
+    int j = 0;
+    while (j < 3 && t[j] >= n) { t[j] = -n; ++j; }
+    if (j < 3) ++t[j];
+    else break;
+  }
+}
+
 /* src/Algorithms_Create_Fluid_Particle.h:25-33 with
  * Policy_Is_Inbound_Filling_Layer_CellType (src/Policy_Is_Inbound_Filling_Layer_CellType.h:16-19)
  * and the 8-jittered-particles refill. */
@@ -225,13 +260,76 @@ static void alg_create_fluid(world_t* w) {
       if (!b->exists[o] || b->type[o] != MAC_INFLOW || b->layer[o] != -1) continue;
       int k[3];
       key_of(w, bi, o, k);
-      for (int s = 0; s < 8; ++s) {
-        double p[3];
-        mac_jitter8_position(w->seed, k[0], k[1], k[2], s, w->h[0], w->h[1], w->h[2], p);
-        add_particle(w, p);
-      }
+      add_refill(w, k);
       b->layer[o] = 0;
       b->type[o] = set_fluid(b->type[o]);
+    }
+  }
+}
+
+/* ------------------------------------------------ depth composition
+ * The topology passes of test/Jet3.cpp:519-549 (Policy_Depth(max, interior,
+ * remove), src/Policy_Depth.h:12-26). */
+
+/* src/Algorithms_Initialize_Layer_And_Depth.h:16-33: every cell's layer empty;
+ * fluid cells that are not interior lose their depth. */
+static void alg_initialize_depth(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o]) continue;
+      b->layer[o] = -1;
+      if (is_fluid(b->type[o]) && b->type[o] != MAC_INTERIOR) b->depth[o] = -1;
+    }
+  }
+}
+
+/* src/Algorithms_Layer_Initial_With_Particle_Depth.h:26-47: a particle in an
+ * interior cell gives it layer 0 and is erased when the cell is deeper than the
+ * removal depth; elsewhere layer 0 and SetFluid. The list keeps its order. */
+static void alg_layer_initial_depth(world_t* w) {
+  int64_t keep = 0;
+  for (int64_t q = 0; q < w->np; ++q) {
+    int k[3];
+    particle_key(w, w->pos + 3 * q, k);
+    cell_t c = cell_get(w, k[0], k[1], k[2]);
+    brick_t* b = B(c);
+    int erase = 0;
+    if (b->type[c.o] == MAC_INTERIOR) {
+      b->layer[c.o] = 0;
+      erase = b->depth[c.o] > w->hdr.depth_remove;
+    } else {
+      b->layer[c.o] = 0;
+      b->type[c.o] = set_fluid(b->type[c.o]);
+    }
+    if (!erase) {
+      if (keep != q) memmove(w->pos + 3 * keep, w->pos + 3 * q, 24);
+      ++keep;
+    }
+  }
+  w->np = keep;
+}
+
+/* src/Algorithms_Create_Fluid_Particle_Depth.h:21-43: inflow cells still empty
+ * are refilled (layer 0, SetFluid); empty interior cells no deeper than the
+ * removal depth are refilled (layer 0); every other interior cell gets layer 0. */
+static void alg_create_fluid_depth(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o]) continue;
+      int k[3];
+      key_of(w, bi, o, k);
+      if (b->type[o] == MAC_INFLOW && b->layer[o] == -1) {
+        add_refill(w, k);
+        b->layer[o] = 0;
+        b->type[o] = set_fluid(b->type[o]);
+      } else if (b->type[o] == MAC_INTERIOR && b->layer[o] == -1 && b->depth[o] <= w->hdr.depth_remove) {
+        add_refill(w, k);
+        b->layer[o] = 0;
+      } else if (b->type[o] == MAC_INTERIOR) {
+        b->layer[o] = 0;
+      }
     }
   }
 }
@@ -250,18 +348,29 @@ static int empty_or_invalid(world_t* w, int x, int y, int z) {
   return !cell_valid(w, c) || B(c)->layer[c.o] == -1;
 }
 
-/* src/Algorithms_Update_CellType_Layer.h:22-89 */
-static void alg_update_layer(world_t* w) {
-  keylist s = {0}, s2 = {0};
+/* src/Algorithms_Update_CellType_Layer.h:22-89; with_depth: the depth form
+ * src/Algorithms_Update_CellType_Layer_Depth.h:24-138, which first empties
+ * every cell's depth and gives the seeds depth 0, then after the air layers
+ * runs a BFS inward over layer-0 cells: depth d < DepthInterior -> SetFluid,
+ * else SetInterior (seeds keep their material). */
+static void alg_update_layer_depth_bfs(world_t* w, keylist* sback);
+static void alg_update_layer_impl(world_t* w, int with_depth) {
+  keylist s = {0}, s2 = {0}, sback = {0};
   int lmax = w->hdr.layer_max;
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
-      if (!w->b[bi]->exists[o] || w->b[bi]->layer[o] != 0) continue;
+      if (!w->b[bi]->exists[o]) continue;
+      if (with_depth) w->b[bi]->depth[o] = -1;
+      if (w->b[bi]->layer[o] != 0) continue;
       int k[3];
       key_of(w, bi, o, k);
       for (int d = 0; d < 6; ++d)
         if (empty_or_invalid(w, k[0] + DIRS[d][0], k[1] + DIRS[d][1], k[2] + DIRS[d][2])) {
           kl_push(&s, k);
+          if (with_depth) {
+            w->b[bi]->depth[o] = 0;
+            kl_push(&sback, k);
+          }
           break;
         }
     }
@@ -292,8 +401,35 @@ static void alg_update_layer(world_t* w) {
       }
     }
   }
-  free(s.k); free(s2.k);
+  if (with_depth) alg_update_layer_depth_bfs(w, &sback);
+  free(s.k); free(s2.k); free(sback.k);
 }
+
+static void alg_update_layer_depth_bfs(world_t* w, keylist* sback) {
+  keylist s2 = {0};
+  for (int depth = 1;; ++depth) {
+    for (int64_t q = 0; q < sback->n; ++q) {
+      int* k = sback->k + 3 * q;
+      for (int d = 0; d < 6; ++d) {
+        int x = k[0] + DIRS[d][0], y = k[1] + DIRS[d][1], z = k[2] + DIRS[d][2];
+        cell_t c = cell_at(w, x, y, z);
+        if (c.b < 0) continue; /* every neighbour of a layer-0 cell exists by now */
+        brick_t* b = B(c);
+        if (b->layer[c.o] != 0 || b->depth[c.o] != -1) continue;
+        b->depth[c.o] = depth;
+        b->type[c.o] = depth < w->hdr.depth_interior ? set_fluid(b->type[c.o]) : MAC_INTERIOR;
+        int kk[3] = {x, y, z};
+        kl_push(&s2, kk);
+      }
+    }
+    keylist t = *sback; *sback = s2; s2 = t; s2.n = 0;
+    if (sback->n == 0) break;
+  }
+  free(s2.k);
+}
+
+static void alg_update_layer(world_t* w) { alg_update_layer_impl(w, 0); }
+static void alg_update_layer_depth(world_t* w) { alg_update_layer_impl(w, 1); }
 
 /* src/Algorithms_Delete_MacCell.h:22-44 and chunk freeing in erase
  * (src/ChunkHashTable.tpp:132-147). */
@@ -1022,6 +1158,7 @@ static world_t* world_from_file(const mac_state_file* st) {
     memcpy(b->type, st->type + base, 512);
     memcpy(b->layer, st->layer + base, 512 * 4);
     memcpy(b->id, st->id + base, 512 * 4);
+    memcpy(b->depth, st->depth + base, 512 * 4);
   }
   for (int64_t q = 0; q < st->hdr.nparticles; ++q) add_particle(w, st->pos + 3 * q);
   return w;
@@ -1056,6 +1193,7 @@ static void world_to_file(world_t* w, mac_state_file* st) {
     memcpy(st->type + base, b->type, 512);
     memcpy(st->layer + base, b->layer, 512 * 4);
     memcpy(st->id + base, b->id, 512 * 4);
+    memcpy(st->depth + base, b->depth, 512 * 4);
   }
   memcpy(st->pos, w->pos, (size_t)w->np * 24);
 }
@@ -1073,10 +1211,21 @@ static int64_t fluid_count(world_t* w) {
 }
 
 static void topology(world_t* w) {
-  alg_initialize(w);
-  alg_layer_initial(w);
-  alg_create_fluid(w);
-  alg_update_layer(w);
+  if (w->hdr.depth_mode) {
+    /* Algorithms<Initialize_Layer_And_Depth, Layer_Initial_With_Particle_Depth,
+     * Create_Fluid_Particle_Depth, Update_CellType_Layer_Depth, Delete_MacCell,
+     * Calculate_Time_Step> (test/Jet3.cpp:546, without the jet's own particle
+     * filter and the extrapolations, which the step runs after the ODE) */
+    alg_initialize_depth(w);
+    alg_layer_initial_depth(w);
+    alg_create_fluid_depth(w);
+    alg_update_layer_depth(w);
+  } else {
+    alg_initialize(w);
+    alg_layer_initial(w);
+    alg_create_fluid(w);
+    alg_update_layer(w);
+  }
   alg_delete(w);
   alg_dt(w);
 }
@@ -1098,10 +1247,17 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
     if (!strcmp(cmd, "firstinit")) {
       alg_solid_to_const(w);
       alg_mirror(w);
-      alg_initialize(w);
-      alg_create_fluid(w);
-      alg_layer_initial(w);
-      alg_update_layer(w);
+      if (w->hdr.depth_mode) {
+        alg_initialize_depth(w);
+        alg_create_fluid_depth(w);
+        alg_layer_initial_depth(w);
+        alg_update_layer_depth(w);
+      } else {
+        alg_initialize(w);
+        alg_create_fluid(w);
+        alg_layer_initial(w);
+        alg_update_layer(w);
+      }
       alg_delete(w);
       alg_extrapolate(w);
     } else if (!strcmp(cmd, "setup")) {

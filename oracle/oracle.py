@@ -16,6 +16,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libmac_oracle.so")
 REF = os.path.join(HERE, "_ref", "mac_ref")
+REF_DEPTH = os.path.join(HERE, "_ref", "mac_ref_depth")
 
 _lib = None
 
@@ -85,9 +86,17 @@ def have_ref() -> bool:
     return os.path.exists(REF)
 
 
+def _depth_mode(path: str) -> int:
+    """depth_mode of a state file's header (byte offset 128, ``state_format.h``)."""
+    with open(path, "rb") as f:
+        head = f.read(132)
+    return int.from_bytes(head[128:132], "little", signed=True) if len(head) == 132 else 0
+
+
 def run_ref(cmd: str, in_path: str, out_path: str, arg=None, timeout: float = 600.0) -> str:
-    """Runs the reference's own code on a state (``cmd`` as in ``ref_world.cpp``)."""
-    args = [REF, cmd, in_path, out_path]
+    """Runs the reference's own code on a state (``cmd`` as in ``ref_world.cpp``);
+    a state in the depth composition goes to the depth build of the runner."""
+    args = [REF_DEPTH if _depth_mode(in_path) else REF, cmd, in_path, out_path]
     if arg is not None:
         args.append(str(arg))
     out = subprocess.run(args, capture_output=True, text=True, timeout=timeout)

@@ -21,7 +21,19 @@
 //  * prototype speed/pressure/layer/id are initialised explicitly (the reference
 //    leaves them uninitialised: src/Physvector.tpp:8-10),
 //  * inflow refill uses Policy_Add_Particle_Jitter8 (8 jittered particles per
-//    cell, seeded by a counter-based hash shared with the oracle and the GPU).
+//    cell, seeded by a counter-based hash shared with the oracle and the GPU)
+//    or, when the state header asks for it, the reference's own
+//    Policy_Add_Particle_Cube(n) (test/Jet3.cpp:509-510 uses n = 1).
+//
+// Built with -DMAC_DEPTH (oracle/_ref/mac_ref_depth) the world takes the cell
+// type and topology of the depth composition of test/Jet3.cpp:326-386,503-549:
+// Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres with
+// Data_CellType_Domain_Fluid_Without_0_Pres, a depth per cell, Policy_Depth
+// from the state header, and Initialize_Layer_And_Depth,
+// Layer_Initial_With_Particle_Depth, Create_Fluid_Particle_Depth and
+// Update_CellType_Layer_Depth in place of the four pipeline-A topology passes
+// (the jet's own particle filter, Algorithm_DelParticle of test/Jet3.cpp:259-288,
+// is not part of it).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -113,6 +125,20 @@
 #include "Policy_Dirichlet_Boundary.h"
 #include "Algorithms_Viscosity.h"
 #include "Algorithms_Solve_Pressure_Dirichlet.h"
+#include "Policy_Add_Particle_Cube.h"
+#ifdef MAC_DEPTH
+#include "Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.h"
+#include "Data_CellType_Domain_Fluid_Without_0_Pres.h"
+#include "Data_Grid_Depth.h"
+#include "Data_Grid_Depth_Empty.h"
+#include "Data_Chunk_Depth.h"
+#include "Offset_Base_Depth.h"
+#include "Policy_Depth.h"
+#include "Algorithms_Initialize_Layer_And_Depth.h"
+#include "Algorithms_Layer_Initial_With_Particle_Depth.h"
+#include "Algorithms_Create_Fluid_Particle_Depth.h"
+#include "Algorithms_Update_CellType_Layer_Depth.h"
+#endif
 
 #ifdef MAC_WITH_GPU
 // The C++ drop-in layer of the device path; compiled in only for _ref/mac_ref_gpu.
@@ -218,6 +244,23 @@ class Policy_Add_Particle_Jitter8 {
   }
 };
 
+// The refill policy named by the state header: Jitter8, or the reference's
+// Policy_Add_Particle_Cube(n) for n >= 1.
+template <typename Data>
+class Policy_Add_Particle_Select {
+  Policy_Add_Particle_Jitter8<Data> m_jitter;
+  Policy_Add_Particle_Cube<Data> m_cube;
+  int m_n;
+
+ public:
+  Policy_Add_Particle_Select(const Data& data, int n) : m_jitter(data), m_cube(data, n > 0 ? n : 1), m_n(n) {}
+  template <typename Key>
+  void AddParticle(const Key& k) {
+    if (m_n > 0) m_cube.AddParticle(k);
+    else m_jitter.AddParticle(k);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // The world.
 // ---------------------------------------------------------------------------
@@ -247,14 +290,22 @@ static int run(int argc, char** argv) {
   typedef Data_Staggered_Left<type_Data_Type> type_Data_Base;
   type_Data_Base data_base(m_data_type);
 
+#ifdef MAC_DEPTH
+  typedef Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres<type_Data_Base> type_cell_type2;
+#else
   typedef Data_CellType_Fluid_Air_Solid_Inflow<type_Data_Base> type_cell_type2;
+#endif
   typedef Inversible_Value<type_data_value> type_inversible_value;
   type_inversible_value rho_air(1);
   type_inversible_value rho_fluid(1000);
   type_cell_type2 m_celltype2(data_base);
   m_celltype2.SetRhoAir(rho_air);
   m_celltype2.SetRhoFluid(rho_fluid);
+#ifdef MAC_DEPTH
+  typedef Data_CellType_Domain_Fluid_Without_0_Pres<type_cell_type2> type_cell_type;
+#else
   typedef Data_CellType_Domain_Fluid<type_cell_type2> type_cell_type;
+#endif
   type_cell_type m_celltype(m_celltype2);
   typedef Data_Grid_CellType_To_Grid_CellType<type_cell_type> type_cell_cell;
   type_cell_cell m_cell_cell(m_celltype);
@@ -291,15 +342,31 @@ static int run(int argc, char** argv) {
   type_chunk_speed m_chunk_speed(m_grid_speed);
   typedef Data_Chunk_Pressure<type_grid_pressure, NStock> type_chunk_pressure;
   type_chunk_pressure m_chunk_pressure(m_grid_pressure);
+#ifdef MAC_DEPTH
+  typedef Data_Grid_Depth<int> type_depth2;
+  type_depth2 m_depth2(-1);
+  typedef Data_Grid_Depth_Empty<type_depth2> type_depth;
+  type_depth m_depth(m_depth2);
+  typedef Data_Chunk_Depth<type_depth, NStock> type_chunk_depth;
+  type_chunk_depth m_chunk_depth(m_depth);
+  typedef Data_Chunk<type_bool_array, type_chunk_layer, type_chunk_depth, type_chunk_id, type_chunk_celltype, type_chunk_speed, type_chunk_pressure> type_chunk;
+  type_chunk m_chunk(m_bool_array, m_chunk_layer, m_chunk_depth, m_chunk_id, m_chunk_celltype, m_chunk_speed, m_chunk_pressure);
+#else
   typedef Data_Chunk<type_bool_array, type_chunk_layer, type_chunk_id, type_chunk_celltype, type_chunk_speed, type_chunk_pressure> type_chunk;
   type_chunk m_chunk(m_bool_array, m_chunk_layer, m_chunk_id, m_chunk_celltype, m_chunk_speed, m_chunk_pressure);
+#endif
   typedef Neighbour_List_Empty<DIM, type_chunk> type_neigh;
   type_neigh m_neigh(m_chunk);
 
   typedef Offset<int, DIM, N> type_off;
   typedef Offset_Base<type_off, type_neigh> type_off_base;
   typedef Offset_Base_Layer<type_layer, type_off_base> type_off_base_layer;
+#ifdef MAC_DEPTH
+  typedef Offset_Base_Depth<type_depth, type_off_base_layer> type_off_base_depth;
+  typedef Offset_Base_Id_Cell<type_id, type_off_base_depth> type_off_base_id;
+#else
   typedef Offset_Base_Id_Cell<type_id, type_off_base_layer> type_off_base_id;
+#endif
   typedef Offset_Base_CellType<type_cell_cell, type_off_base_id> type_off_base_celltype;
   typedef Offset_Base_Speed<type_grid_speed, type_off_base_celltype> type_off_base_speed;
   typedef Offset_Base_Pressure<type_grid_pressure, type_off_base_speed> type_off_base_pressure;
@@ -373,8 +440,14 @@ static int run(int argc, char** argv) {
         case MAC_AIR: ct.m_mat = Mat::Air; break;
         case MAC_FLUID: ct.m_mat = Mat::Fluid; break;
         case MAC_SOLID: ct.m_mat = Mat::Solid; break;
+#ifdef MAC_DEPTH
+        case MAC_INTERIOR: ct.m_mat = Mat::Interior; break;
+#endif
         default: ct.m_mat = Mat::Inflow; break;
       }
+#ifdef MAC_DEPTH
+      ch.Depth_GetPointer()[o].SetDepth(st.depth[idx]);
+#endif
       ct.SetIsNoDelete((st.flags[idx] & MAC_FLAG_NODELETE) != 0);
       ch.Layer_GetPointer()[o].SetLayer(st.layer[idx]);
       ch.Id_Cell_GetPointer()[o].SetLayer(st.id[idx]);
@@ -402,20 +475,43 @@ static int run(int argc, char** argv) {
   type_pol_part_to_key m_pol_part_to_key(m_data_ref);
   typedef Policy_CheckDT<type_data_ref> type_pol_check_dt;
   type_pol_check_dt m_pol_check_dt(st.hdr.dt_min, st.hdr.dt_max);
-  typedef Policy_Add_Particle_Jitter8<type_data_ref> type_pol_add_particle;
-  type_pol_add_particle m_add_particle(m_data_ref);
+  typedef Policy_Add_Particle_Select<type_data_ref> type_pol_add_particle;
+  type_pol_add_particle m_add_particle(m_data_ref, st.hdr.refill_cube);
   typedef Policy_Is_Inbound_Filling_Layer_CellType<type_data_ref> type_pol_fill;
   type_pol_fill m_pol_fill;
+#ifdef MAC_DEPTH
+  typedef Policy_Depth<type_data_ref> type_pol_depth;
+  type_pol_depth m_pol_depth(st.hdr.depth_max, st.hdr.depth_interior, st.hdr.depth_remove);
+  typedef Policies<type_pol_layer, type_pol_part_to_key, type_pol_check_dt, type_pol_add_particle, type_pol_fill, type_pol_depth> type_pol_init;
+  type_pol_init m_pol_init(m_pol_layer, m_pol_part_to_key, m_pol_check_dt, m_add_particle, m_pol_fill, m_pol_depth);
+#else
   typedef Policies<type_pol_layer, type_pol_part_to_key, type_pol_check_dt, type_pol_add_particle, type_pol_fill> type_pol_init;
   type_pol_init m_pol_init(m_pol_layer, m_pol_part_to_key, m_pol_check_dt, m_add_particle, m_pol_fill);
+#endif
 
+#ifdef MAC_DEPTH
+  typedef Algorithms_Initialize_Layer_And_Depth<type_data_ref, type_pol_init> type_alg_initialize_mac;
+#else
   typedef Algorithms_Initialize_MacCell<type_data_ref, type_pol_init> type_alg_initialize_mac;
+#endif
   type_alg_initialize_mac m_alg_initialize_mac(m_data_ref, m_pol_init);
+#ifdef MAC_DEPTH
+  typedef Algorithms_Create_Fluid_Particle_Depth<type_data_ref, type_pol_init> type_alg_create;
+#else
   typedef Algorithms_Create_Fluid_Particle<type_data_ref, type_pol_init> type_alg_create;
+#endif
   type_alg_create m_alg_create(m_data_ref, m_pol_init);
+#ifdef MAC_DEPTH
+  typedef Algorithms_Layer_Initial_With_Particle_Depth<type_data_ref, type_pol_init> type_alg_layer_initial;
+#else
   typedef Algorithms_Layer_Initial_With_Particle<type_data_ref, type_pol_init> type_alg_layer_initial;
+#endif
   type_alg_layer_initial m_alg_layer_initial(m_data_ref, m_pol_init);
+#ifdef MAC_DEPTH
+  typedef Algorithms_Update_CellType_Layer_Depth<type_data_ref, type_pol_init> type_alg_update_celltype;
+#else
   typedef Algorithms_Update_CellType_Layer<type_data_ref, type_pol_init> type_alg_update_celltype;
+#endif
   type_alg_update_celltype m_alg_update_celltype(m_data_ref, m_pol_init);
   typedef Algorithms_Delete_MacCell<type_data_ref, type_pol_init> type_alg_delete;
   type_alg_delete m_alg_delete(m_data_ref, m_pol_init);
@@ -675,6 +771,11 @@ static int run(int argc, char** argv) {
       out.type[idx] = (uint8_t)m_celltype2.MaterialToInt(ct.m_mat);
       out.layer[idx] = ch.Layer_GetPointer()[o].GetLayer();
       out.id[idx] = ch.Id_Cell_GetPointer()[o].GetLayer();
+#ifdef MAC_DEPTH
+      out.depth[idx] = ch.Depth_GetPointer()[o].GetDepth();
+#else
+      out.depth[idx] = -1;
+#endif
     }
     ++c;
   }

@@ -15,9 +15,11 @@
  *   double ax,ay,az                    [nchunks*512] each (acceleration)
  *   double p                           [nchunks*512]
  *   uint8  flags[nchunks*512]          bit0..2 const face x,y,z; bit3 no-delete
- *   uint8  type[nchunks*512]           0 air, 1 fluid, 2 solid, 3 inflow
+ *   uint8  type[nchunks*512]           0 air, 1 fluid, 2 solid, 3 inflow, 4 interior
  *   int32  layer[nchunks*512]          -1 = empty
  *   int32  id[nchunks*512]             solver numbering (-1 = none)
+ *   int32  depth[nchunks*512]          distance to the surface (-1 = empty),
+ *                                      src/Data_Grid_Depth_Empty.h:6-14
  *   double pos[nparticles][3]
  * Cell offset inside a chunk is x + 8y + 64z (src/Offset.h:14-24).
  */
@@ -35,10 +37,11 @@
 #define MAC_FLUID 1
 #define MAC_SOLID 2
 #define MAC_INFLOW 3
+#define MAC_INTERIOR 4
 #define MAC_FLAG_NODELETE 8
 
 typedef struct {
-  char magic[8];           /* "MACST001" */
+  char magic[8];           /* "MACST002" */
   int64_t nchunks;
   int64_t nparticles;
   double h[3];
@@ -49,7 +52,11 @@ typedef struct {
   int32_t interp_symmetric;
   int32_t reserved_i;
   double viscosity;        /* Data_Viscosity::m_viscosity (0: inviscid) */
-  uint8_t reserved[256 - 8 - 16 - 24 - 48 - 8 - 8 - 8 - 8];
+  int32_t depth_mode;      /* 1: the depth composition of the topology (Interior cells) */
+  int32_t depth_max, depth_interior, depth_remove; /* Policy_Depth(max, interior, remove) */
+  int32_t refill_cube;     /* 0: Jitter8 refill; n >= 1: Policy_Add_Particle_Cube(n) */
+  int32_t reserved_j;
+  uint8_t reserved[256 - 8 - 16 - 24 - 48 - 8 - 8 - 8 - 8 - 24];
 } mac_state_header;
 
 typedef struct {
@@ -63,6 +70,7 @@ typedef struct {
   uint8_t* type;
   int32_t* layer;
   int32_t* id;
+  int32_t* depth;
   double* pos;
 } mac_state_file;
 
@@ -78,6 +86,7 @@ static inline void mac_state_alloc(mac_state_file* s, int64_t nchunks, int64_t n
   s->type = (uint8_t*)calloc(nc + 1, 1);
   s->layer = (int32_t*)calloc(nc + 1, 4);
   s->id = (int32_t*)calloc(nc + 1, 4);
+  s->depth = (int32_t*)calloc(nc + 1, 4);
   s->pos = (double*)calloc((size_t)np * 3 + 1, 8);
 }
 
@@ -86,7 +95,7 @@ static inline void mac_state_free(mac_state_file* s) {
   for (int b = 0; b < 2; ++b)
     for (int i = 0; i < 3; ++i) free(s->u[b][i]);
   for (int i = 0; i < 3; ++i) free(s->acc[i]);
-  free(s->p); free(s->flags); free(s->type); free(s->layer); free(s->id); free(s->pos);
+  free(s->p); free(s->flags); free(s->type); free(s->layer); free(s->id); free(s->depth); free(s->pos);
   memset(s, 0, sizeof(*s));
 }
 
@@ -109,6 +118,7 @@ static inline int mac_state_rw_(FILE* f, mac_state_file* s, int wr) {
   e |= mac_state_io_(f, s->type, 1, nc, wr);
   e |= mac_state_io_(f, s->layer, 4, nc, wr);
   e |= mac_state_io_(f, s->id, 4, nc, wr);
+  e |= mac_state_io_(f, s->depth, 4, nc, wr);
   e |= mac_state_io_(f, s->pos, 8, (size_t)s->hdr.nparticles * 3, wr);
   return e;
 }
@@ -117,7 +127,7 @@ static inline int mac_state_read(const char* path, mac_state_file* s) {
   FILE* f = fopen(path, "rb");
   if (!f) return -1;
   mac_state_header h;
-  if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "MACST001", 8) != 0) { fclose(f); return -1; }
+  if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "MACST002", 8) != 0) { fclose(f); return -1; }
   mac_state_alloc(s, h.nchunks, h.nparticles);
   s->hdr = h;
   int e = mac_state_rw_(f, s, 0);
@@ -128,7 +138,7 @@ static inline int mac_state_read(const char* path, mac_state_file* s) {
 static inline int mac_state_write(const char* path, mac_state_file* s) {
   FILE* f = fopen(path, "wb");
   if (!f) return -1;
-  memcpy(s->hdr.magic, "MACST001", 8);
+  memcpy(s->hdr.magic, "MACST002", 8);
   int e = fwrite(&s->hdr, sizeof(s->hdr), 1, f) == 1 ? 0 : -1;
   e |= mac_state_rw_(f, s, 1);
   fclose(f);

@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from mac_b200.state import CELL_F64, FLUID, INFLOW, State
+from mac_b200.state import CELL_F64, FLUID_TYPES, State
 
 SPEEDS = ("u0x", "u0y", "u0z")
 
@@ -18,18 +18,18 @@ def _align(a: State, b: State):
 
 
 def compare_topology(a: State, b: State, check_stale=True) -> None:
-    """Bit-exact: live bricks, existence, material, layer, const/no-delete bits."""
+    """Bit-exact: live bricks, existence, material, layer, depth, const/no-delete bits."""
     a, b = _align(a, b)
     ex = a.exists.astype(bool)
     if not np.array_equal(a.exists, b.exists):
         idx = np.argwhere(a.exists != b.exists)[:5]
         raise AssertionError(f"existence differs at {idx.tolist()} keys {a.cell_keys()[tuple(idx.T)].tolist()}")
     mask = np.ones_like(ex) if check_stale else ex
-    for name in ("type", "layer", "flags"):
+    for name in ("type", "layer", "depth", "flags"):
         x, y = getattr(a, name), getattr(b, name)
-        # the layer of an erased cell is never read before it is rewritten; only
-        # existing cells' layers are compared
-        bad = (x != y) & (ex if name == "layer" else mask)
+        # the layer and depth of an erased cell are never read before they are
+        # rewritten; only existing cells' layers and depths are compared
+        bad = (x != y) & (ex if name in ("layer", "depth") else mask)
         if bad.any():
             idx = np.argwhere(bad)[:5]
             raise AssertionError(f"{name} differs ({int(bad.sum())} cells) e.g. at keys "
@@ -87,4 +87,4 @@ def compare_particles(a: State, b: State, rtol=0.0, atol=0.0) -> float:
 
 
 def fluid_mask(s: State):
-    return s.exists.astype(bool) & ((s.type == FLUID) | (s.type == INFLOW))
+    return s.exists.astype(bool) & np.isin(s.type, FLUID_TYPES)

@@ -25,7 +25,18 @@ Policy_Dirichlet_Boundary, composed as test/Lateral_jet_3.cpp does):
   c1_ref_s31v.npz      one viscous step from c1_ref_s30 (with viscosity)
   c1_ref_s40v.npz      ten viscous steps from c1_ref_s30
 
-Usage: python tests/golden/make_golden.py [--viscous-only]
+Depth-composition fixtures (oracle/_ref/mac_ref_depth: the Interior cell type,
+Policy_Depth(4, 3, 3) as test/Lateral_jet_3.cpp:494 and the reference's
+Policy_Add_Particle_Cube(1) refill) of a 24x24x32 jet over a 12-cell pool
+(``depth_world()``):
+
+  d_ref_s0.npz         after the first init
+  d_ref_s10.npz        after 10 steps
+  d_ref_t10.npz        d_ref_s10 after the per-step init (depth topology + dt)
+  d_ref_s11.npz        one step from d_ref_s10
+  d_ref_s20.npz        ten steps from d_ref_s10
+
+Usage: python tests/golden/make_golden.py [--viscous-only | --depth-only]
 """
 from __future__ import annotations
 
@@ -60,6 +71,25 @@ def viscous(t, out):
     State.read(t("s40v")).save_npz(out("c1_ref_s40v"))
 
 
+def depth_world() -> State:
+    """The depth fixtures' input: jet_world(24, 24, 32) over a 12-cell pool."""
+    s = jet_world(nx=24, ny=24, nz=32, pool_depth=12)
+    pr = s.params
+    pr.depth_mode, pr.depth_max, pr.depth_interior, pr.depth_remove, pr.refill_cube = 1, 4, 3, 3, 1
+    return s
+
+
+def depth(t, out):
+    depth_world().write(t("dsetup"))
+    oracle.run_ref("firstinit", t("dsetup"), t("ds0"))
+    oracle.run_ref("step", t("ds0"), t("ds10"), 10)
+    oracle.run_ref("topology", t("ds10"), t("dt10"))
+    oracle.run_ref("step", t("ds10"), t("ds11"), 1)
+    oracle.run_ref("step", t("ds10"), t("ds20"), 10)
+    for name in ("s0", "s10", "t10", "s11", "s20"):
+        State.read(t("d" + name)).save_npz(out("d_ref_" + name))
+
+
 def main():
     oracle.build()
     if not oracle.have_ref():
@@ -70,6 +100,10 @@ def main():
     if "--viscous-only" in sys.argv:
         viscous(t, out)
         print("viscous fixtures written to", HERE)
+        return
+    if "--depth-only" in sys.argv:
+        depth(t, out)
+        print("depth fixtures written to", HERE)
         return
     s = jet_world()
     s.write(t("setup"))
@@ -91,6 +125,7 @@ def main():
         State.read(t("t30_" + st)).save_npz(out("c1_ref_t30_" + st))
     oracle.run_ref("csc", t("t30"), t("junk"), os.path.join(HERE, "c1_ref_t30_csc.bin"))
     viscous(t, out)
+    depth(t, out)
     print("fixtures written to", HERE)
 
 
