@@ -64,6 +64,7 @@ class _Grid:
         s.type = np.concatenate([s.type, add.type])
         s.layer = np.concatenate([s.layer, add.layer])
         s.id = np.concatenate([s.id, add.id])
+        s.depth = np.concatenate([s.depth, add.depth])
         self._index()
 
 
