@@ -41,8 +41,11 @@ enum {
 };
 
 /* Cell materials, as Data_CellType_Fluid_Air_Solid_Inflow::MaterialToInt
- * (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:3-18). */
-enum { MAC_CELL_AIR = 0, MAC_CELL_FLUID = 1, MAC_CELL_SOLID = 2, MAC_CELL_INFLOW = 3 };
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:3-18); interior is the fifth
+ * material of Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:3-22), used
+ * by the depth composition only. */
+enum { MAC_CELL_AIR = 0, MAC_CELL_FLUID = 1, MAC_CELL_SOLID = 2, MAC_CELL_INFLOW = 3, MAC_CELL_INTERIOR = 4 };
 /* Per-cell flag bits: const faces x/y/z (src/Data_Grid_Speed.h:54-59) and the
  * no-delete mark (src/Data_CellType_Fluid_Air_Solid_Inflow.h:331-338). */
 enum { MAC_FLAG_CONST_X = 1, MAC_FLAG_CONST_Y = 2, MAC_FLAG_CONST_Z = 4, MAC_FLAG_NODELETE = 8 };
@@ -73,6 +76,17 @@ typedef struct {
    * Algorithms_Solve_Pressure_Dirichlet + Policy_Dirichlet_Boundary
    * (src/Algorithms_Viscosity.h:24-30, src/Algorithms_Solve_Pressure_Dirichlet.h:171-233). */
   double viscosity;
+  /* 1: the depth composition of the topology (test/Jet3.cpp:519-549):
+   * Algorithms_Initialize_Layer_And_Depth, _Layer_Initial_With_Particle_Depth,
+   * _Create_Fluid_Particle_Depth and _Update_CellType_Layer_Depth with
+   * Policy_Depth(depth_max, depth_interior, depth_remove) in place of the four
+   * pipeline-A topology passes; cells get a depth and the interior material. */
+  int32_t depth_mode;
+  int32_t depth_max, depth_interior, depth_remove;
+  /* inflow (and interior) refill: 0 = 8 jittered particles per cell,
+   * n >= 1 = Policy_Add_Particle_Cube(n), (2n+1)^3 particles per cell */
+  int32_t refill_cube;
+  int32_t reserved0;
 } mac_params;
 
 /* Host view of a world, arrays owned by the caller. Brick b holds cells
@@ -92,6 +106,8 @@ typedef struct {
   double* pos;          /* [nparticles][3] */
   double t, dt;
   uint64_t step;        /* refill seed counter */
+  int32_t* depth;       /* [nbricks*512] distance to the surface, -1 empty
+                           (src/Data_Grid_Depth_Empty.h:6-14); NULL: not carried */
 } mac_host_state;
 
 typedef struct {
@@ -99,7 +115,7 @@ typedef struct {
   int32_t solves;
   double relres;        /* final relative residual of the last solve */
   double max_div;       /* max |div u| over domain cells after the last projection */
-  int64_t fluid_cells;  /* fluid + inflow cells after the last topology rebuild */
+  int64_t fluid_cells;  /* fluid + inflow (+ interior) cells after the last topology rebuild */
   int64_t unknowns;     /* in-domain cells of the last system */
   int64_t live_bricks;
   int64_t particles;
@@ -123,13 +139,16 @@ int mac_download_state(void* ctx, mac_host_state* s);
 /* ---- topology rebuild: Algorithms<Initialize_MacCell, Layer_Initial_With_Particle,
  *      Create_Fluid_Particle, Update_CellType_Layer, Delete_MacCell, Calculate_Time_Step>
  *      (test/TestJetDEau_Basic.cpp:325-326) ---- */
-/* src/Algorithms_Initialize_MacCell.h:15-21 */
+/* src/Algorithms_Initialize_MacCell.h:15-21; depth_mode: src/Algorithms_Initialize_Layer_And_Depth.h:16-33 */
 int mac_initialize_maccell(void* ctx);
-/* src/Algorithms_Layer_Initial_With_Particle.h:20-34 + Policy_Particle_To_Key (src/Policy_Particle_To_Key.h:24-35) */
+/* src/Algorithms_Layer_Initial_With_Particle.h:20-34 + Policy_Particle_To_Key (src/Policy_Particle_To_Key.h:24-35);
+ * depth_mode: src/Algorithms_Layer_Initial_With_Particle_Depth.h:26-47 (removes particles of deep interior cells) */
 int mac_layer_initial_with_particle(void* ctx);
-/* src/Algorithms_Create_Fluid_Particle.h:19-33 (8 jittered particles per refilled inflow cell) */
+/* src/Algorithms_Create_Fluid_Particle.h:19-33 (refill: 8 jittered particles, or
+ * Policy_Add_Particle_Cube(refill_cube)); depth_mode: src/Algorithms_Create_Fluid_Particle_Depth.h:21-43 */
 int mac_create_fluid_particle(void* ctx);
-/* src/Algorithms_Update_CellType_Layer.h:22-89 */
+/* src/Algorithms_Update_CellType_Layer.h:22-89; depth_mode: src/Algorithms_Update_CellType_Layer_Depth.h:24-138
+ * with Policy_Depth (src/Policy_Depth.h:12-26) */
 int mac_update_celltype_layer(void* ctx);
 /* src/Algorithms_Delete_MacCell.h:22-44 */
 int mac_delete_maccell(void* ctx);

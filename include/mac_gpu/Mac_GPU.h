@@ -125,7 +125,7 @@ class Mac_GPU_Session {
     std::vector<int32_t> keys, layer;
     std::vector<uint8_t> exists, flags, type;
     std::vector<double> f[10], pos;  // u0x..u1z, ax..az, p
-    mac_host_state view;
+    mac_host_state view{};
     void size(int64_t nb, int64_t np) {
       size_t nc = (size_t)nb * MAC_BRICK_CELLS;
       keys.assign(3 * (size_t)nb, 0);
@@ -147,6 +147,7 @@ class Mac_GPU_Session {
       view.type = type.data();
       view.layer = layer.data();
       view.pos = pos.data();
+      view.depth = nullptr;  // the reference world of this layer carries no depth
     }
   };
 

@@ -43,6 +43,23 @@ __global__ void k_pack_lay(const uint8_t* __restrict__ ex, const int32_t* __rest
   if (i < n) lay[i] = ex[i] ? (int8_t)layer[i] : kMissing;
 }
 
+// depth: int32 on the host, int16 in the pool (-1 empty; depths stay far below
+// 2^15 in any world the pool holds)
+__global__ void k_pack_depth(const int32_t* __restrict__ in, int16_t* __restrict__ out, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    int32_t v = in[i];
+    out[i] = (int16_t)(v < -1 ? -1 : (v > 32766 ? 32766 : v));
+  }
+}
+
+__global__ void k_unpack_depth(const int16_t* __restrict__ d, const int* __restrict__ blist, int nlive,
+                               int32_t* __restrict__ out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nlive * kCells) return;
+  out[i] = d[(size_t)blist[i >> 9] * kCells + (i & 511)];
+}
+
 __global__ void k_set_keys(int* bkey, const int32_t* __restrict__ keys, int nb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * nb) bkey[i] = keys[i];
@@ -159,6 +176,7 @@ static void free_all(Ctx* c) {
   free_solver(c);
   cudaFree(c->bkey); cudaFree(c->lay); cudaFree(c->type); cudaFree(c->flags); cudaFree(c->f64);
   cudaFree(c->pdir);
+  cudaFree(c->depth); cudaFree(c->pkeep);
   cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
@@ -179,6 +197,8 @@ static int create(const mac_params* p, Ctx** out) {
   for (int i = 0; i < 3; ++i)
     if (!(p->h[i] > 0)) return MAC_ERR_INVALID;
   if (!(p->viscosity >= 0) || !std::isfinite(p->viscosity)) return MAC_ERR_INVALID;
+  if (p->refill_cube < 0 || p->refill_cube > 4) return MAC_ERR_INVALID;
+  if (p->depth_mode && (p->depth_interior < 0 || p->depth_remove < 0)) return MAC_ERR_INVALID;
   if (p->device < 0 || p->device >= ndev) return MAC_ERR_INVALID;
   MAC_CUDA(cudaSetDevice(p->device));
   Ctx* c = new (std::nothrow) Ctx();
@@ -203,6 +223,10 @@ static int create(const mac_params* p, Ctx** out) {
   c->dp.layer_max = p->layer_max;
   c->dp.interp_sym = p->interp_symmetric;
   c->dp.nu = p->viscosity;
+  c->dp.depth_mode = p->depth_mode ? 1 : 0;
+  c->dp.depth_interior = p->depth_interior;
+  c->dp.depth_remove = p->depth_remove;
+  c->dp.refill_cube = p->refill_cube;
   for (int i = 0; i < 3; ++i) c->dp.lih2[i] = std::pow(c->dp.ih[i], 2);
   c->cap_bricks = p->max_bricks;
   c->cap_particles = p->max_particles;
@@ -219,6 +243,10 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->flags, nc));
   A(dalloc(&c->f64, NF64 * nc));
   if (p->viscosity > 0) A(dalloc(&c->pdir, nc));
+  if (p->depth_mode) {
+    A(dalloc(&c->depth, nc));
+    A(dalloc(&c->pkeep, (size_t)c->cap_particles));
+  }
   A(dalloc(&c->nbr, kNbr * c->cap_bricks));
   A(dalloc(&c->blist, c->cap_bricks));
   A(dalloc(&c->blist2, c->cap_bricks));
@@ -293,8 +321,15 @@ static int upload(Ctx* c, const mac_host_state* s) {
     MAC_CUDA(cudaMemcpyAsync(tex, s->exists, nc, cudaMemcpyHostToDevice, st));
     MAC_CUDA(cudaMemcpyAsync(tlay, s->layer, 4 * nc, cudaMemcpyHostToDevice, st));
     k_pack_lay<<<grid_for((int64_t)nc, 256), 256, 0, st>>>(tex, tlay, c->lay, (int64_t)nc); MAC_COUNT(c);
+    if (c->depth && s->depth) {
+      MAC_CUDA(cudaMemcpyAsync(tlay, s->depth, 4 * nc, cudaMemcpyHostToDevice, st));
+      k_pack_depth<<<grid_for((int64_t)nc, 256), 256, 0, st>>>(tlay, c->depth, (int64_t)nc); MAC_COUNT(c);
+    } else if (c->depth) {
+      MAC_CUDA(cudaMemsetAsync(c->depth, 0xFF, 2 * nc, st));
+    }
   }
   if (cap > nc) MAC_CUDA(cudaMemsetAsync(c->lay + nc, 0xFE, cap - nc, st));
+  if (cap > nc && c->depth) MAC_CUDA(cudaMemsetAsync(c->depth + nc, 0xFF, 2 * (cap - nc), st));
   k_init_lists<<<grid_for(c->cap_bricks, 256), 256, 0, st>>>(c->blist, c->freelist, nb, (int)c->cap_bricks); MAC_COUNT(c);
   // particles, through a bounded staging buffer (solver vector pd)
   int64_t np = s->nparticles;
@@ -349,6 +384,12 @@ static int download(Ctx* c, mac_host_state* s) {
     k_unpack_lay<<<g, 256, 0, st>>>(c->lay, c->blist, nb, t8, tl); MAC_COUNT(c);
     MAC_CUDA(cudaMemcpyAsync(s->exists, t8, nc, cudaMemcpyDeviceToHost, st));
     MAC_CUDA(cudaMemcpyAsync(s->layer, tl, 4 * nc, cudaMemcpyDeviceToHost, st));
+    if (s->depth && c->depth) {
+      k_unpack_depth<<<g, 256, 0, st>>>(c->depth, c->blist, nb, tl); MAC_COUNT(c);
+      MAC_CUDA(cudaMemcpyAsync(s->depth, tl, 4 * nc, cudaMemcpyDeviceToHost, st));
+    } else if (s->depth) {
+      for (size_t i = 0; i < nc; ++i) s->depth[i] = -1;
+    }
   }
   int64_t np = c->np_host;
   int64_t chunk = (int64_t)(cap / 3);

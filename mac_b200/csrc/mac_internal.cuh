@@ -66,6 +66,9 @@ struct Scalars {
   int32_t ndom;       // bricks holding an in-domain cell
   int32_t pad_;
   unsigned long long bad_reads;  // particles whose stencil touched a missing cell
+  unsigned long long np_new;     // particle count after the removal pass (depth composition)
+  int32_t dchanged;              // a depth relaxation launch lowered some depth
+  int32_t pad2_;
 };
 
 // Phases timed with CUDA events when profiling is on (mac_set_profiling);
@@ -93,6 +96,8 @@ struct Params {
   // viscosity (0: inviscid composition) and pow(1/h, 2) as the Laplacian of
   // src/Policy_Laplacian_Speed.h:22-36 computes it
   double nu, lih2[3];
+  // depth composition (Policy_Depth) and the refill policy (0: jitter8, n: cube(n))
+  int depth_mode, depth_interior, depth_remove, refill_cube;
   // inverse diagonal of the level-0 operator by active faces per axis
   // (index ax + 3 ay + 9 az, each 0..2); 0 when no face is active
   double dtab[27];
@@ -127,6 +132,8 @@ struct Ctx {
   uint8_t* flags = nullptr;   // [cap*512]
   double* f64 = nullptr;      // [NF64][cap*512]
   double* pdir = nullptr;     // [cap*512] Dirichlet air pressure, NaN off the boundary (viscous only)
+  int16_t* depth = nullptr;   // [cap*512] distance to the surface, -1 empty (depth composition only)
+  uint8_t* pkeep = nullptr;   // [max_particles] removal marks of the particle pass (depth composition only)
   int* nbr = nullptr;         // [cap][27]
   int* blist = nullptr;       // live bricks (current)
   int* blist2 = nullptr;      // scratch for compaction
@@ -258,7 +265,11 @@ __device__ inline int wrap(int v) { return v < 0 ? v + D : (v >= D ? v - D : v);
 template <int D>
 __device__ inline int slot(int x, int y, int z) { return x + D * y + D * D * z; }
 
-__device__ inline bool is_fluid(uint8_t t) { return t == MAC_CELL_FLUID || t == MAC_CELL_INFLOW; }
+// GetIsFluid: fluid, inflow and (depth composition) interior cells
+// (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:24-44).
+__device__ inline bool is_fluid(uint8_t t) {
+  return t == MAC_CELL_FLUID || t == MAC_CELL_INFLOW || t == MAC_CELL_INTERIOR;
+}
 
 // Ordered-bits max for non-negative doubles.
 __device__ inline void atomic_max_nonneg(unsigned long long* a, double v) {

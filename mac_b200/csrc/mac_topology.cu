@@ -2,7 +2,11 @@
 // sequence Algorithms<Initialize_MacCell, Layer_Initial_With_Particle,
 // Create_Fluid_Particle, Update_CellType_Layer, Delete_MacCell,
 // Calculate_Time_Step> (test/TestJetDEau_Basic.cpp:325-326), bit-exact with
-// the reference, plus the index maintenance of the brick pool.
+// the reference, plus the index maintenance of the brick pool. With
+// depth_mode the same kernels run the depth composition of test/Jet3.cpp:519-549
+// (Initialize_Layer_And_Depth, Layer_Initial_With_Particle_Depth,
+// Create_Fluid_Particle_Depth, Update_CellType_Layer_Depth): cells carry a
+// depth and deep fluid becomes the interior material.
 //
 // Cell creation (the reference's auto-creating operator[],
 // src/ChunkHashTable.tpp:62-87) is split in two so that no thread ever waits
@@ -10,6 +14,8 @@
 // second kernel gives each new key a pool brick initialised to the prototype
 // (speed 0, pressure 0, air, no flags, no existing cell), and the pass that
 // needed the cells runs again.
+#include <utility>
+
 #include "mac_internal.cuh"
 
 namespace mac {
@@ -105,8 +111,8 @@ __global__ void k_bbox_reset(Scalars* ds) {
 // src/Data_Chunk_Base.h:20-29, src/Data_Chunk_Speed.h:99-123).
 __global__ void k_alloc_bricks(const int* __restrict__ newslots, const unsigned long long* __restrict__ hk,
                                int* hv, int* bkey, int* blist, const int* __restrict__ freelist,
-                               int8_t* lay, uint8_t* type, uint8_t* flags, double* f64, size_t cap_cells,
-                               int64_t cap_bricks, Scalars* ds) {
+                               int8_t* lay, uint8_t* type, uint8_t* flags, double* f64, int16_t* depth,
+                               size_t cap_cells, int64_t cap_bricks, Scalars* ds) {
   __shared__ int sb;
   int n = ds->nnew;
   if (n > cap_bricks) n = (int)cap_bricks;
@@ -138,6 +144,7 @@ __global__ void k_alloc_bricks(const int* __restrict__ newslots, const unsigned 
         lay[c] = kMissing;
         type[c] = MAC_CELL_AIR;
         flags[c] = 0;
+        if (depth) depth[c] = -1;
         for (int f = 0; f < NF64; ++f) f64[(size_t)f * cap_cells + c] = 0.0;
       }
     }
@@ -152,12 +159,21 @@ __global__ void k_after_alloc(Scalars* ds) {
 
 // ------------------------------------------------- Initialize_MacCell
 // src/Algorithms_Initialize_MacCell.h:15-21: every existing cell -> empty layer.
-__global__ void k_initialize(const int* __restrict__ blist, int8_t* lay, Scalars* ds) {
+// Depth composition (src/Algorithms_Initialize_Layer_And_Depth.h:16-33): also
+// fluid cells that are not interior lose their depth.
+__global__ void k_initialize(const int* __restrict__ blist, int8_t* lay, const uint8_t* __restrict__ type,
+                             int16_t* depth, Scalars* ds) {
   int n = ds->nlive;
   for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
     size_t base = (size_t)blist[bi] * kCells;
-    for (int o = threadIdx.x; o < kCells; o += blockDim.x)
-      if (lay[base + o] != kMissing) lay[base + o] = kEmpty;
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      if (lay[base + o] == kMissing) continue;
+      lay[base + o] = kEmpty;
+      if (depth) {
+        uint8_t t = type[base + o];
+        if (is_fluid(t) && t != MAC_CELL_INTERIOR) depth[base + o] = -1;
+      }
+    }
   }
 }
 
@@ -165,11 +181,16 @@ __global__ void k_initialize(const int* __restrict__ blist, int8_t* lay, Scalars
 // src/Algorithms_Layer_Initial_With_Particle.h:26-30 with
 // Policy_Particle_To_Key::GetKeyFromParticle (src/Policy_Particle_To_Key.h:24-35):
 // key_i = lround(pos_i * (1/h_i)); grid[key] -> layer 0, SetFluid (air -> fluid only,
-// src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:150-157).
+// src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:150-157). Depth composition
+// (src/Algorithms_Layer_Initial_With_Particle_Depth.h:26-47): a particle in an
+// interior cell gives it layer 0 and keeps the material; it is marked for
+// removal (pkeep = 0) when the cell is deeper than the removal depth. The
+// marks depend only on state no thread of this pass changes (air -> fluid
+// never makes an interior cell), so the passes are order-free.
 __global__ void k_mark_particles(const double* __restrict__ px, const double* __restrict__ py,
                                  const double* __restrict__ pz, Params P, unsigned long long* hk, int* hv,
                                  int64_t hcap, int* newslots, int64_t cap_new, int8_t* lay, uint8_t* type,
-                                 Scalars* ds, int pass) {
+                                 const int16_t* __restrict__ depth, uint8_t* pkeep, Scalars* ds, int pass) {
   if (pass == 1 && ds->done == 0) return;  // no brick was missing in pass 0
   int64_t n = ds->np;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
@@ -181,13 +202,50 @@ __global__ void k_mark_particles(const double* __restrict__ px, const double* __
     if (b < 0) {
       if (pass == 0) hash_insert(hk, hcap, key, newslots, ds, cap_new);
       else atomicOr(&ds->err, kErrBricks);
+      if (pkeep) pkeep[q] = 1;  // a new cell is air, never interior
       continue;
     }
     size_t c = (size_t)b * kCells + (kx & 7) + 8 * (ky & 7) + 64 * (kz & 7);
     lay[c] = 0;
     uint8_t t = type[c];
-    if (t == MAC_CELL_AIR) type[c] = MAC_CELL_FLUID;
+    if (pkeep && t == MAC_CELL_INTERIOR) {
+      pkeep[q] = depth[c] > P.depth_remove ? 0 : 1;
+    } else {
+      if (t == MAC_CELL_AIR) type[c] = MAC_CELL_FLUID;
+      if (pkeep) pkeep[q] = 1;
+    }
   }
+}
+
+// Removal of the marked particles (the list erase of
+// src/Algorithms_Layer_Initial_With_Particle_Depth.h:33-36): kept particles are
+// packed into the second position arrays with one atomic per warp. The order
+// changes; nothing depends on the particle order.
+__global__ void k_compact_particles(const double* __restrict__ px, const double* __restrict__ py,
+                                    const double* __restrict__ pz, const uint8_t* __restrict__ pkeep,
+                                    double* __restrict__ qx, double* __restrict__ qy, double* __restrict__ qz,
+                                    Scalars* ds) {
+  const int64_t n = ds->np;
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = base + threadIdx.x;
+    const bool keep = q < n && pkeep[q];
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    unsigned long long w = 0;
+    if (lane == 0 && m) w = atomicAdd(&ds->np_new, (unsigned long long)__popc(m));
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (keep) {
+      const unsigned long long i = w + __popc(m & ((1u << lane) - 1u));
+      qx[i] = px[q];
+      qy[i] = py[q];
+      qz[i] = pz[q];
+    }
+  }
+}
+
+__global__ void k_compact_particles_done(Scalars* ds) {
+  ds->np = (int64_t)ds->np_new;
+  ds->np_new = 0;
 }
 
 // Remembers across the alloc kernel whether pass 1 of the particle marking must run.
@@ -220,30 +278,63 @@ __device__ inline void jitter8(unsigned long long seed, int kx, int ky, int kz, 
 
 // src/Algorithms_Create_Fluid_Particle.h:25-33 with
 // Policy_Is_Inbound_Filling_Layer_CellType (src/Policy_Is_Inbound_Filling_Layer_CellType.h:16-19):
-// inflow cells whose layer is still empty get 8 jittered particles and layer 0.
+// inflow cells whose layer is still empty are refilled and get layer 0 (SetFluid
+// leaves an inflow cell inflow). The refill is 8 jittered particles, or
+// Policy_Add_Particle_Cube(n) (src/Policy_Add_Particle_Cube.h:29-59): (2n+1)^3
+// particles at (k_i + t_i/(2n+1)) h_i, t_i = -n..n. Depth composition
+// (src/Algorithms_Create_Fluid_Particle_Depth.h:21-43): an interior cell with
+// an empty layer no deeper than the removal depth is refilled too, and every
+// interior cell gets layer 0.
 __global__ void k_refill(const int* __restrict__ blist, const int* __restrict__ bkey, int8_t* lay,
-                         const uint8_t* __restrict__ type, double* px, double* py, double* pz,
-                         int64_t cap_particles, unsigned long long seed, Params P, Scalars* ds) {
+                         const uint8_t* __restrict__ type, const int16_t* __restrict__ depth, double* px,
+                         double* py, double* pz, int64_t cap_particles, unsigned long long seed, Params P,
+                         Scalars* ds) {
   int n = ds->nlive;
+  const int side = 2 * P.refill_cube + 1;
+  const int per = P.refill_cube > 0 ? side * side * side : 8;
+  const double dh = 1. / side;
   for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
     int b = blist[bi];
     size_t base = (size_t)b * kCells;
     for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
-      if (type[base + o] != MAC_CELL_INFLOW || lay[base + o] != kEmpty) continue;
+      const uint8_t t = type[base + o];
+      const bool empty = lay[base + o] == kEmpty;
+      bool refill = t == MAC_CELL_INFLOW && empty;
+      if (P.depth_mode && t == MAC_CELL_INTERIOR) {
+        refill = empty && depth[base + o] <= P.depth_remove;
+        if (!refill) {
+          lay[base + o] = 0;
+          continue;
+        }
+      }
+      if (!refill) continue;
       int kx = bkey[3 * b] * 8 + (o & 7), ky = bkey[3 * b + 1] * 8 + ((o >> 3) & 7),
           kz = bkey[3 * b + 2] * 8 + (o >> 6);
-      unsigned long long pos = atomicAdd((unsigned long long*)&ds->np, 8ull);
-      if ((int64_t)pos + 8 > cap_particles) {
+      unsigned long long pos = atomicAdd((unsigned long long*)&ds->np, (unsigned long long)per);
+      if ((int64_t)pos + per > cap_particles) {
         atomicOr(&ds->err, kErrParticles);
-        atomicAdd((unsigned long long*)&ds->np, (unsigned long long)(-8ll));
+        atomicAdd((unsigned long long*)&ds->np, (unsigned long long)(-(long long)per));
         continue;
       }
-      for (int s = 0; s < 8; ++s) {
-        double p[3];
-        jitter8(seed, kx, ky, kz, s, P, p);
-        px[pos + s] = p[0];
-        py[pos + s] = p[1];
-        pz[pos + s] = p[2];
+      if (P.refill_cube > 0) {
+        const int k[3] = {kx, ky, kz};
+        for (int s = 0; s < per; ++s) {
+          const int tt[3] = {s % side - P.refill_cube, (s / side) % side - P.refill_cube,
+                             s / (side * side) - P.refill_cube};
+          double p[3];
+          for (int i = 0; i < 3; ++i) p[i] = (k[i] + tt[i] * dh) * P.h[i];
+          px[pos + s] = p[0];
+          py[pos + s] = p[1];
+          pz[pos + s] = p[2];
+        }
+      } else {
+        for (int s = 0; s < 8; ++s) {
+          double p[3];
+          jitter8(seed, kx, ky, kz, s, P, p);
+          px[pos + s] = p[0];
+          py[pos + s] = p[1];
+          pz[pos + s] = p[2];
+        }
       }
       lay[base + o] = 0;
     }
@@ -294,7 +385,9 @@ __device__ inline int8_t lay_at(const int8_t* __restrict__ lay, const int* __res
 // written in this launch change from {-2,-1} to L, never to L-1, so the reads
 // of neighbour layers are race-free. ring != 0 runs the final +1-face ring
 // (:73-88): only the -e_i neighbours (i.e. the cell is the +e_i face of a
-// layer-LayerMax cell) count.
+// layer-LayerMax cell) count. SetAir turns fluid and (depth composition)
+// interior cells into air
+// (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.tpp:217-223).
 __global__ void k_bfs_level(const int* __restrict__ blist, const int* __restrict__ nbr, int8_t* lay,
                             uint8_t* type, int L, int ring, Scalars* ds) {
   int n = ds->nlive;
@@ -313,7 +406,124 @@ __global__ void k_bfs_level(const int* __restrict__ blist, const int* __restrict
               lay_at(lay, nbr, b, x, y, z + 1) == want;
       if (hit) {
         lay[c] = (int8_t)L;
-        if (type[c] == MAC_CELL_FLUID) type[c] = MAC_CELL_AIR;
+        const uint8_t t = type[c];
+        if (t == MAC_CELL_FLUID || t == MAC_CELL_INTERIOR) type[c] = MAC_CELL_AIR;
+      }
+    }
+  }
+}
+
+// ------------------------------------- Update_CellType_Layer_Depth: depth
+// src/Algorithms_Update_CellType_Layer_Depth.h:33-55: every existing cell's
+// depth is emptied, and a layer-0 cell with a missing or empty-layer face
+// neighbour (read before the air layers are added) gets depth 0 and seeds the
+// inward BFS of :104-134.
+__global__ void k_depth_seed(const int* __restrict__ blist, const int* __restrict__ nbr,
+                             const int8_t* __restrict__ lay, int16_t* depth, Scalars* ds) {
+  int n = ds->nlive;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    int b = blist[bi];
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      size_t c = (size_t)b * kCells + o;
+      int8_t l = lay[c];
+      if (l == kMissing) continue;
+      int16_t d = -1;
+      if (l == 0) {
+        int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+        const int8_t nl[6] = {lay_at(lay, nbr, b, x - 1, y, z), lay_at(lay, nbr, b, x + 1, y, z),
+                              lay_at(lay, nbr, b, x, y - 1, z), lay_at(lay, nbr, b, x, y + 1, z),
+                              lay_at(lay, nbr, b, x, y, z - 1), lay_at(lay, nbr, b, x, y, z + 1)};
+        for (int f = 0; f < 6; ++f)
+          if (nl[f] == kMissing || nl[f] == kEmpty) d = 0;
+      }
+      depth[c] = d;
+    }
+  }
+}
+
+// The inward BFS of src/Algorithms_Update_CellType_Layer_Depth.h:104-134 as a
+// min-plus relaxation, which reaches the same fixed point (the BFS distance
+// through face-adjacent layer-0 cells from the depth-0 seeds) in any order:
+// each block takes one brick with a one-cell halo into shared memory and
+// relaxes d(c) = min(d(c), d(n) + 1) over its layer-0 cells until nothing
+// changes, then writes the lowered depths back. Halo values read while a
+// neighbouring brick is being relaxed are older upper bounds, so the host
+// repeats the launch until no depth changes (about max depth / 8 launches).
+// Unreached layer-0 cells keep -1, as in the reference.
+constexpr int16_t kDepthInf = 0x7fff;
+constexpr int16_t kDepthNone = -2;
+
+__global__ void __launch_bounds__(512) k_depth_relax(const int* __restrict__ blist, const int* __restrict__ nbr,
+                                                     const int8_t* __restrict__ lay, int16_t* depth, Scalars* ds) {
+  __shared__ int16_t sd[1000];  // 10^3 with halo: kDepthNone off the layer-0 set, kDepthInf unreached
+  int n = ds->nlive;
+  const int t = threadIdx.x;
+  const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
+  const int me = (x + 1) + 10 * ((y + 1) + 10 * (z + 1));
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = blist[bi];
+    for (int i = t; i < 1000; i += blockDim.x) {
+      const int hx = i % 10 - 1, hy = (i / 10) % 10 - 1, hz = i / 100 - 1;
+      const int nb = nb_brick<8>(nbr, b, hx, hy, hz);
+      int16_t v = kDepthNone;
+      if (nb >= 0) {
+        const size_t c = (size_t)nb * kCells + slot<8>(wrap<8>(hx), wrap<8>(hy), wrap<8>(hz));
+        if (lay[c] == 0) {
+          const int16_t d = depth[c];
+          v = d < 0 ? kDepthInf : d;
+        }
+      }
+      sd[i] = v;
+    }
+    __syncthreads();
+    const int16_t start = sd[me];
+    const bool part = start != kDepthNone && start != 0;  // relaxed: layer-0 non-seed cells
+    int16_t cur = start;
+    while (true) {
+      bool ch = false;
+      if (part) {
+        int16_t m = kDepthInf;
+        const int nn[6] = {me - 1, me + 1, me - 10, me + 10, me - 100, me + 100};
+        for (int f = 0; f < 6; ++f) {
+          const int16_t v = sd[nn[f]];
+          if (v >= 0 && v < m) m = v;
+        }
+        if (m < kDepthInf - 1 && m + 1 < cur) {
+          cur = (int16_t)(m + 1);
+          sd[me] = cur;
+          ch = true;
+        }
+      }
+      if (!__syncthreads_or(ch)) break;
+    }
+    if (part && cur < start) {
+      depth[(size_t)b * kCells + t] = cur;
+      ds->dchanged = 1;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_depth_flag_clear(Scalars* ds) { ds->dchanged = 0; }
+
+// Materials of :117-124: a layer-0 cell reached at depth d >= 1 becomes fluid
+// (SetFluid: from air or interior) when d < DepthInterior and interior
+// (SetInterior: always) otherwise; the seeds keep their material.
+__global__ void k_depth_types(const int* __restrict__ blist, const int8_t* __restrict__ lay,
+                              const int16_t* __restrict__ depth, uint8_t* type, Params P, Scalars* ds) {
+  int n = ds->nlive;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    size_t base = (size_t)blist[bi] * kCells;
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      size_t c = base + o;
+      if (lay[c] != 0) continue;
+      int16_t d = depth[c];
+      if (d < 1) continue;
+      uint8_t t = type[c];
+      if (d < P.depth_interior) {
+        if (t == MAC_CELL_AIR || t == MAC_CELL_INTERIOR) type[c] = MAC_CELL_FLUID;
+      } else {
+        type[c] = MAC_CELL_INTERIOR;
       }
     }
   }
@@ -432,12 +642,13 @@ int rebuild_index(Ctx* c) {
 static void alloc_new(Ctx* c) {
   cudaStream_t st = c->stream;
   k_alloc_bricks<<<kTopoBlocks, 256, 0, st>>>(c->newslots, c->hkeys, c->hval, c->bkey, c->blist, c->freelist,
-                                               c->lay, c->type, c->flags, c->f64,
+                                               c->lay, c->type, c->flags, c->f64, c->depth,
                                                (size_t)c->cap_bricks * kCells, c->cap_bricks, c->ds); MAC_COUNT(c);
 }
 
 int topo_initialize(Ctx* c) {
-  k_initialize<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->lay, c->ds); MAC_COUNT(c);
+  k_initialize<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->lay, c->type, c->dp.depth_mode ? c->depth : nullptr,
+                                                   c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -445,21 +656,47 @@ int topo_layer_initial(Ctx* c) {
   cudaStream_t st = c->stream;
   int g = kTopoBlocks * 2;
   k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+  uint8_t* keep = c->dp.depth_mode ? c->pkeep : nullptr;
   k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
-                                      c->cap_bricks, c->lay, c->type, c->ds, 0); MAC_COUNT(c);
+                                      c->cap_bricks, c->lay, c->type, c->depth, keep, c->ds, 0); MAC_COUNT(c);
   k_note_missing<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   alloc_new(c);
   k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
-                                      c->cap_bricks, c->lay, c->type, c->ds, 1); MAC_COUNT(c);
+                                      c->cap_bricks, c->lay, c->type, c->depth, keep, c->ds, 1); MAC_COUNT(c);
   k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+  if (keep) {
+    k_compact_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, keep, c->px2, c->py2, c->pz2, c->ds); MAC_COUNT(c);
+    k_compact_particles_done<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+    std::swap(c->px, c->px2);
+    std::swap(c->py, c->py2);
+    std::swap(c->pz, c->pz2);
+  }
   c->system_ready = false;
   return check(cudaGetLastError());
 }
 
 int topo_create_fluid(Ctx* c) {
-  k_refill<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->bkey, c->lay, c->type, c->px, c->py, c->pz,
+  k_refill<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->bkey, c->lay, c->type, c->depth, c->px, c->py, c->pz,
                                                 c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds); MAC_COUNT(c);
+  return check(cudaGetLastError());
+}
+
+// Relaxation launches until no depth changes; each launch carries the front at
+// least one brick further, so the bound below (the pool's brick count) is
+// never reached by a valid world.
+static int depth_bfs(Ctx* c) {
+  cudaStream_t st = c->stream;
+  const int limit = (int)(c->cap_bricks < 1000000 ? c->cap_bricks : 1000000) + 2;
+  for (int it = 0;; ++it) {
+    if (it >= limit) return MAC_ERR_TIMEOUT;
+    k_depth_flag_clear<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+    k_depth_relax<<<kTopoBlocks, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->depth, c->ds); MAC_COUNT(c);
+    int rc = read_scalars(c);
+    if (rc) return rc;
+    if (!c->hs->dchanged) break;
+  }
+  k_depth_types<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->lay, c->depth, c->type, c->dp, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -472,11 +709,18 @@ int topo_update_layer(Ctx* c) {
   alloc_new(c);
   k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
+  if (c->dp.depth_mode) {
+    k_depth_seed<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->depth, c->ds); MAC_COUNT(c);
+  }
   for (int L = 1; L <= c->dp.layer_max; ++L) {
     k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, L, 0, c->ds); MAC_COUNT(c);
   }
   k_bfs_level<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->type, c->dp.layer_max + 1, 1, c->ds); MAC_COUNT(c);
   c->system_ready = false;
+  if (c->dp.depth_mode) {
+    int rc = depth_bfs(c);
+    if (rc) return rc;
+  }
   return check(cudaGetLastError());
 }
 

@@ -34,7 +34,9 @@ class mac_params(ctypes.Structure):
                 ("layer_max", ctypes.c_int32), ("interp_symmetric", ctypes.c_int32), ("solver", ctypes.c_int32),
                 ("rtol", ctypes.c_double), ("max_iters", ctypes.c_int32), ("warm_start", ctypes.c_int32),
                 ("max_bricks", ctypes.c_int64), ("max_particles", ctypes.c_int64), ("device", ctypes.c_int32),
-                ("div_check", ctypes.c_int32), ("viscosity", ctypes.c_double)]
+                ("div_check", ctypes.c_int32), ("viscosity", ctypes.c_double), ("depth_mode", ctypes.c_int32),
+                ("depth_max", ctypes.c_int32), ("depth_interior", ctypes.c_int32), ("depth_remove", ctypes.c_int32),
+                ("refill_cube", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
 
 
 _P = ctypes.POINTER
@@ -45,7 +47,7 @@ class mac_host_state(ctypes.Structure):
                 ("exists", _P(ctypes.c_uint8)), ("u", (_P(ctypes.c_double) * 3) * 2), ("acc", _P(ctypes.c_double) * 3),
                 ("p", _P(ctypes.c_double)), ("flags", _P(ctypes.c_uint8)), ("type", _P(ctypes.c_uint8)),
                 ("layer", _P(ctypes.c_int32)), ("pos", _P(ctypes.c_double)), ("t", ctypes.c_double),
-                ("dt", ctypes.c_double), ("step", ctypes.c_uint64)]
+                ("dt", ctypes.c_double), ("step", ctypes.c_uint64), ("depth", _P(ctypes.c_int32))]
 
 
 class mac_stats(ctypes.Structure):
@@ -157,13 +159,16 @@ def make_params(pr: Params, max_bricks: int, max_particles: int, solver="mgpcg64
     p.device = device
     p.div_check = int(div_check)
     p.viscosity = float(getattr(pr, "viscosity", 0.0))
+    for k in ("depth_mode", "depth_max", "depth_interior", "depth_remove", "refill_cube"):
+        setattr(p, k, int(getattr(pr, k, 0)))
     return p
 
 
 class HostState:
-    """Host arrays laid out as mac_host_state expects (optionally in pinned memory)."""
+    """Host arrays laid out as mac_host_state expects (optionally in pinned
+    memory); ``depth`` carries the per-cell depth of the depth composition."""
 
-    def __init__(self, nbricks: int, nparticles: int, pinned: bool = False):
+    def __init__(self, nbricks: int, nparticles: int, pinned: bool = False, depth: bool = False):
         nc = nbricks * BRICK_CELLS
         if pinned:
             import torch
@@ -182,6 +187,7 @@ class HostState:
         self.flags = u8(max(nc, 1))
         self.type = u8(max(nc, 1))
         self.layer = i32(max(nc, 1))
+        self.depth = i32(max(nc, 1)) if depth else None
         self.pos = f64(3 * max(nparticles, 1))
         self.t = self.dt = 0.0
         self.step = 0
@@ -195,6 +201,8 @@ class HostState:
         self.flags[:nc] = s.flags.reshape(-1)
         self.type[:nc] = s.type.reshape(-1)
         self.layer[:nc] = s.layer.reshape(-1)
+        if self.depth is not None:
+            self.depth[:nc] = s.depth.reshape(-1)
         self.pos[:3 * s.nparticles] = s.pos.reshape(-1)
         self.nbricks, self.nparticles = nb, s.nparticles
         self.t, self.dt, self.step = s.params.t, s.params.dt, s.params.step
@@ -203,7 +211,8 @@ class HostState:
     def nbytes(self) -> int:
         """Bytes of the current state content (what one transfer moves)."""
         nc = self.nbricks * BRICK_CELLS
-        return 12 * self.nbricks + nc * (1 + 8 * len(CELL_F64) + 1 + 1 + 4) + 24 * self.nparticles
+        per_cell = 1 + 8 * len(CELL_F64) + 1 + 1 + 4 + (4 if self.depth is not None else 0)
+        return 12 * self.nbricks + nc * per_cell + 24 * self.nparticles
 
     def c_struct(self) -> mac_host_state:
         h = mac_host_state()
@@ -219,6 +228,7 @@ class HostState:
         h.flags = _ptr(self.flags, ctypes.c_uint8)
         h.type = _ptr(self.type, ctypes.c_uint8)
         h.layer = _ptr(self.layer, ctypes.c_int32)
+        h.depth = _ptr(self.depth, ctypes.c_int32) if self.depth is not None else None
         h.pos = _ptr(self.pos, ctypes.c_double)
         h.t, h.dt, h.step = self.t, self.dt, self.step
         return h
@@ -232,7 +242,8 @@ class HostState:
                      {n: self.f64[n][:nc].reshape(shp).copy() for n in CELL_F64},
                      self.flags[:nc].reshape(shp).copy(), self.type[:nc].reshape(shp).copy(),
                      self.layer[:nc].reshape(shp).copy(), np.full(shp, -1, np.int32),
-                     self.pos[:3 * npart].reshape(npart, 3).copy()).sorted()
+                     self.pos[:3 * npart].reshape(npart, 3).copy(),
+                     self.depth[:nc].reshape(shp).copy() if self.depth is not None else None).sorted()
 
 
 class Context:
@@ -271,7 +282,7 @@ class Context:
     # ---- transfer
     def upload(self, s: State | None, host: HostState | None = None):
         """Uploads a State, or the content already held in ``host``."""
-        host = host or HostState(s.nbricks, s.nparticles).fill(s)
+        host = host or HostState(s.nbricks, s.nparticles, depth=bool(s.params.depth_mode)).fill(s)
         self._host_in = host
         st = host.c_struct()
         self._check(self.lib.mac_upload_state(self.h, ctypes.byref(st)), "mac_upload_state")
@@ -284,7 +295,7 @@ class Context:
     def download(self, host: HostState | None = None) -> State:
         nb, npart = self.sizes()
         if host is None or host.nbricks < nb or len(host.pos) < 3 * npart:
-            host = HostState(nb, npart)
+            host = HostState(nb, npart, depth=bool(self.params.depth_mode))
         host.nbricks, host.nparticles = nb, npart
         st = host.c_struct()
         self._check(self.lib.mac_download_state(self.h, ctypes.byref(st)), "mac_download_state")
