@@ -23,11 +23,12 @@
 
 #include "state_format.h"
 
+#define ACC 3 /* index of the acceleration among the brick's vector fields */
+
 typedef struct {
   int32_t key[3];
   uint8_t exists[512];
-  double u[2][3][512];
-  double acc[3][512];
+  double u[4][3][512]; /* speed buffers 0..2 and, at index ACC, the acceleration */
   double p[512];
   uint8_t flags[512];
   uint8_t type[512];
@@ -49,6 +50,12 @@ typedef struct {
   int64_t np, capp;
   uint64_t seed;
   int viscous; /* 1: Algorithms_Viscosity and the Dirichlet pressure are composed */
+  /* Data_Chunk_Speed::ispeed (the speed buffer the stencils read) and
+   * Data_Particle::imove_particle (the particle position the topology and the
+   * interpolation use), src/Data_Chunk_Speed.h:17-19, src/Data_Particle.h:11-60;
+   * pos1 / pos2 are the extra particle positions of pipeline B */
+  int ispeed, imove;
+  double *pos1, *pos2;
   /* statistics */
   int64_t invalid_reads, created_cells, cg_iters;
   double max_div, last_relres;
@@ -199,6 +206,11 @@ static void alg_initialize(world_t* w) {
       if (w->b[bi]->exists[o]) w->b[bi]->layer[o] = -1;
 }
 
+/* Position buffer b of particle q. */
+static double* pbuf(world_t* w, int b, int64_t q) { return (b == 0 ? w->pos : (b == 1 ? w->pos1 : w->pos2)) + 3 * q; }
+/* The current position (Data_Particle::GetParticlePos with imove_particle). */
+static double* ppos(world_t* w, int64_t q) { return pbuf(w, w->imove, q); }
+
 /* Policy_Particle_To_Key::GetKeyFromParticle (src/Policy_Particle_To_Key.h:24-35). */
 static void particle_key(const world_t* w, const double* pos, int k[3]) {
   for (int i = 0; i < 3; ++i) k[i] = (int)lround(pos[i] * w->ih[i]);
@@ -208,20 +220,31 @@ static void particle_key(const world_t* w, const double* pos, int k[3]) {
 static void alg_layer_initial(world_t* w) {
   for (int64_t q = 0; q < w->np; ++q) {
     int k[3];
-    particle_key(w, w->pos + 3 * q, k);
+    particle_key(w, ppos(w, q), k);
     cell_t c = cell_get(w, k[0], k[1], k[2]);
     B(c)->layer[c.o] = 0;
     B(c)->type[c.o] = set_fluid(B(c)->type[c.o]);
   }
 }
 
+/* A new particle sets its current position only (src/Data_Particle.h:17-24);
+ * the other buffers are written before they are read. */
 static void add_particle(world_t* w, const double p[3]) {
   if (w->np == w->capp) {
     w->capp = w->capp ? 2 * w->capp : 1024;
     w->pos = (double*)realloc(w->pos, sizeof(double) * 3 * w->capp);
+    w->pos1 = (double*)realloc(w->pos1, sizeof(double) * 3 * w->capp);
+    w->pos2 = (double*)realloc(w->pos2, sizeof(double) * 3 * w->capp);
   }
-  memcpy(w->pos + 3 * w->np, p, sizeof(double) * 3);
+  for (int b = 0; b < 3; ++b) memset(pbuf(w, b, w->np), 0, 24);
+  memcpy(ppos(w, w->np), p, sizeof(double) * 3);
   ++w->np;
+}
+
+/* Erasing a particle keeps the order of the others in every buffer. */
+static void particle_move(world_t* w, int64_t to, int64_t from) {
+  if (to == from) return;
+  for (int b = 0; b < 3; ++b) memmove(pbuf(w, b, to), pbuf(w, b, from), 24);
 }
 
 /* The refill policy's AddParticle(key): 8 jittered particles, or
@@ -291,7 +314,7 @@ static void alg_layer_initial_depth(world_t* w) {
   int64_t keep = 0;
   for (int64_t q = 0; q < w->np; ++q) {
     int k[3];
-    particle_key(w, w->pos + 3 * q, k);
+    particle_key(w, ppos(w, q), k);
     cell_t c = cell_get(w, k[0], k[1], k[2]);
     brick_t* b = B(c);
     int erase = 0;
@@ -303,7 +326,7 @@ static void alg_layer_initial_depth(world_t* w) {
       b->type[c.o] = set_fluid(b->type[c.o]);
     }
     if (!erase) {
-      if (keep != q) memmove(w->pos + 3 * keep, w->pos + 3 * q, 24);
+      particle_move(w, keep, q);
       ++keep;
     }
   }
@@ -487,7 +510,7 @@ static void alg_gravity(world_t* w, int ib) {
         cell_t n = cell_at(w, k[0], k[1], k[2]);
         apply = cell_valid(w, n) && is_fluid(B(n)->type[n.o]);
       }
-      if (apply) set_u(b, b->acc[ax], o, ax, b->acc[ax][o] + w->hdr.gravity, 0);
+      if (apply) set_u(b, b->u[ACC][ax], o, ax, b->u[ACC][ax][o] + w->hdr.gravity, 0);
     }
   }
 }
@@ -548,7 +571,7 @@ static void alg_convection(world_t* w, int ib) {
       int k[3];
       key_of(w, bi, o, k);
       for (int i = 0; i < 3; ++i)
-        if (conv_apply(w, bi, o, i)) set_u(b, b->acc[i], o, i, b->acc[i][o] + convection_speed(w, ib, k, i), 0);
+        if (conv_apply(w, bi, o, i)) set_u(b, b->u[ACC][i], o, i, b->u[ACC][i][o] + convection_speed(w, ib, k, i), 0);
     }
   }
 }
@@ -593,7 +616,7 @@ static void alg_viscosity(world_t* w, int ib) {
         }
         lap[i] = temp;
       }
-      for (int i = 0; i < 3; ++i) set_u(b, b->acc[i], o, i, b->acc[i][o] + lap[i] * nu, 0);
+      for (int i = 0; i < 3; ++i) set_u(b, b->u[ACC][i], o, i, b->u[ACC][i][o] + lap[i] * nu, 0);
     }
   }
 }
@@ -609,7 +632,7 @@ static void acc_zero(world_t* w) {
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o)
       if (w->b[bi]->exists[o])
-        for (int i = 0; i < 3; ++i) w->b[bi]->acc[i][o] = 0.0;
+        for (int i = 0; i < 3; ++i) w->b[bi]->u[ACC][i][o] = 0.0;
 }
 
 /* ------------------------------------------------------------- pressure */
@@ -799,7 +822,14 @@ static double dir_sum(world_t* w, int ib, const int k[3]) {
  * composition Algorithms_Solve_Pressure_Dirichlet::Divergence_Projection
  * (src/Algorithms_Solve_Pressure_Dirichlet.h:171-233): b -= the Dirichlet sum,
  * and Dirichlet air cells take their boundary pressure. */
-static void project_with(world_t* w, const csr_t* A, int ib) {
+/* The projection of vector field f (a speed buffer, or ACC for the force
+ * projection of Algorithms_Solve_Pressure_Force, src/Algorithms_Solve_Pressure_Force.h:16-24,
+ * where Speed_GetRef() returns the acceleration); the Dirichlet pressures read
+ * speed buffer idir (Speed_GetRef(-1, false), src/Policy_Dirichlet_Boundary.h:100-102). */
+static void project_field(world_t* w, const csr_t* A, int f, int idir);
+static void project_with(world_t* w, const csr_t* A, int ib) { project_field(w, A, ib, ib); }
+static void project_field(world_t* w, const csr_t* A, int f, int idir) {
+  const int ib = f;
   int64_t n = A->n;
   double* b = (double*)malloc(8 * (n + 1));
   double* x = (double*)malloc(8 * (n + 1));
@@ -807,7 +837,7 @@ static void project_with(world_t* w, const csr_t* A, int ib) {
     int k[3];
     key_of(w, A->bi[r], A->o[r], k);
     b[r] = divergence(w, ib, k);
-    if (w->viscous) b[r] -= dir_sum(w, ib, k);
+    if (w->viscous) b[r] -= dir_sum(w, idir, k);
   }
   solve(w, A, b, x);
   for (int64_t bi = 0; bi < w->nb; ++bi)
@@ -819,7 +849,7 @@ static void project_with(world_t* w, const csr_t* A, int ib) {
       } else if (w->viscous) {
         int k[3];
         key_of(w, bi, o, k);
-        br->p[o] = dir_boundary(w, k) ? dir_pressure(w, ib, k) : 0.0;
+        br->p[o] = dir_boundary(w, k) ? dir_pressure(w, idir, k) : 0.0;
       } else {
         br->p[o] = 0.0;
       }
@@ -860,7 +890,7 @@ static void alg_rk2(world_t* w) {
     for (int o = 0; o < 512; ++o) {
       brick_t* b = w->b[bi];
       if (!b->exists[o]) continue;
-      for (int i = 0; i < 3; ++i) b->u[1][i][o] = b->u[0][i][o] + b->acc[i][o] * dt;
+      for (int i = 0; i < 3; ++i) b->u[1][i][o] = b->u[0][i][o] + b->u[ACC][i][o] * dt;
     }
   acc_zero(w);
   project_with(w, &A, 1);
@@ -870,7 +900,7 @@ static void alg_rk2(world_t* w) {
       brick_t* b = w->b[bi];
       if (!b->exists[o]) continue;
       for (int i = 0; i < 3; ++i) {
-        double v = 0.5 * b->u[0][i][o] + 0.5 * b->u[1][i][o] + 0.5 * b->acc[i][o] * dt;
+        double v = 0.5 * b->u[0][i][o] + 0.5 * b->u[1][i][o] + 0.5 * b->u[ACC][i][o] * dt;
         set_u(b, b->u[0][i], o, i, v, 0);
       }
     }
@@ -897,7 +927,7 @@ static int lay_of(world_t* w, int x, int y, int z, int* valid) {
  * level, each face between a layer-lay cell and a cell of layer >= lay (or a
  * missing one on the minus side) gets the mean of the parallel or collinear
  * faces that touch a lower layer. n == 0 yields 0/0 as in the reference. */
-static void alg_extrapolate(world_t* w) {
+static void alg_extrapolate_f(world_t* w, int fld) {
   keylist set = {0}, set2 = {0};
   for (int64_t bi = 0; bi < w->nb; ++bi)
     for (int o = 0; o < 512; ++o) {
@@ -936,21 +966,21 @@ static void alg_extrapolate(world_t* w) {
             for (int s2 = -1; s2 <= 1; s2 += 2) {
               if (s2 == -1 && j == i) {
                 int l3 = lay_of(w, K[0] - e[0], K[1] - e[1], K[2] - e[2], &v3);
-                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, i, K, 0, 0, 0); }
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, fld, i, K, 0, 0, 0); }
               } else if (s2 == 1 && j == i) {
                 int l3 = lay_of(w, K[0] + 2 * e[0], K[1] + 2 * e[1], K[2] + 2 * e[2], &v3);
-                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, i, K, 2 * e[0], 2 * e[1], 2 * e[2]); }
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, fld, i, K, 2 * e[0], 2 * e[1], 2 * e[2]); }
               } else {
                 int d3[3] = {e[0] + s2 * f[0], e[1] + s2 * f[1], e[2] + s2 * f[2]};
                 int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
                 int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
                 int l4 = lay_of(w, K[0] + d4[0], K[1] + d4[1], K[2] + d4[2], &v4);
-                if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d3[0], d3[1], d3[2]); }
+                if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, fld, i, K, d3[0], d3[1], d3[2]); }
               }
             }
           }
           cell_t c2 = cell_at(w, K[0] + e[0], K[1] + e[1], K[2] + e[2]);
-          set_u(B(c2), B(c2)->u[0][i], c2.o, i, val / n, 0);
+          set_u(B(c2), B(c2)->u[fld][i], c2.o, i, val / n, 0);
         }
         /* -1 direction: face u_i(neigh) with neigh2 = K - e_i */
         l2 = lay_of(w, K[0] - e[0], K[1] - e[1], K[2] - e[2], &v2);
@@ -972,20 +1002,20 @@ static void alg_extrapolate(world_t* w) {
               for (int s2 = -1; s2 <= 1; s2 += 2) {
                 if (s2 == 1 && j == i) {
                   int l3 = lay_of(w, K[0] + f[0], K[1] + f[1], K[2] + f[2], &v3);
-                  if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, f[0], f[1], f[2]); }
+                  if (v3 && l3 < lay) { ++n; val += rd_u(w, fld, j, K, f[0], f[1], f[2]); }
                 } else if (s2 == -1 && j == i) {
                   int l3 = lay_of(w, K[0] - 2 * f[0], K[1] - 2 * f[1], K[2] - 2 * f[2], &v3);
-                  if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, -f[0], -f[1], -f[2]); }
+                  if (v3 && l3 < lay) { ++n; val += rd_u(w, fld, j, K, -f[0], -f[1], -f[2]); }
                 } else {
                   int d3[3] = {-e[0] + s2 * f[0], -e[1] + s2 * f[1], -e[2] + s2 * f[2]};
                   int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
                   int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
                   int l4 = lay_of(w, K[0] + d4[0], K[1] + d4[1], K[2] + d4[2], &v4);
-                  if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d4[0], d4[1], d4[2]); }
+                  if (v3 && v4 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, fld, i, K, d4[0], d4[1], d4[2]); }
                 }
               }
             }
-            set_u(B(c), B(c)->u[0][i], c.o, i, val / n, 0);
+            set_u(B(c), B(c)->u[fld][i], c.o, i, val / n, 0);
           }
         } else {
           int n = 0;
@@ -995,7 +1025,7 @@ static void alg_extrapolate(world_t* w) {
             for (int s2 = -1; s2 <= 1; s2 += 2) {
               if (s2 == 1 && j == i) {
                 int l3 = lay_of(w, K[0] + f[0], K[1] + f[1], K[2] + f[2], &v3);
-                if (v3 && l3 < lay) { ++n; val += rd_u(w, 0, j, K, f[0], f[1], f[2]); }
+                if (v3 && l3 < lay) { ++n; val += rd_u(w, fld, j, K, f[0], f[1], f[2]); }
               } else if (s2 == -1 && j == i) {
               } else {
                 int d4[3] = {s2 * f[0], s2 * f[1], s2 * f[2]};
@@ -1003,12 +1033,12 @@ static void alg_extrapolate(world_t* w) {
                 if (v4) {
                   int d3[3] = {d4[0] - e[0], d4[1] - e[1], d4[2] - e[2]};
                   int l3 = lay_of(w, K[0] + d3[0], K[1] + d3[1], K[2] + d3[2], &v3);
-                  if (v3 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, 0, i, K, d4[0], d4[1], d4[2]); }
+                  if (v3 && (l3 < lay || l4 < lay)) { ++n; val += rd_u(w, fld, i, K, d4[0], d4[1], d4[2]); }
                 }
               }
             }
           }
-          set_u(B(c), B(c)->u[0][i], c.o, i, val / n, 0);
+          set_u(B(c), B(c)->u[fld][i], c.o, i, val / n, 0);
         }
       }
     }
@@ -1019,6 +1049,8 @@ static void alg_extrapolate(world_t* w) {
   free(set.k); free(set2.k);
 }
 
+static void alg_extrapolate(world_t* w) { alg_extrapolate_f(w, 0); }
+
 /* ------------------------------------------------------------- particles */
 /* Speed read through grid[key] semantics: the interpolation's m_grid[key]
  * creates the base cell (src/Policy_Speed_Interpolation_Linear_Symmetric.h:115). */
@@ -1028,7 +1060,7 @@ static double interp_rec(world_t* w, const double* d, int i, const int k[3], int
   else { w0 = 1 - d[i]; w1 = d[i]; }
   int k1[3] = {k[0] + (i == 0), k[1] + (i == 1), k[2] + (i == 2)};
   if (i < 2) return w0 * interp_rec(w, d, i + 1, k, comp, sym) + w1 * interp_rec(w, d, i + 1, k1, comp, sym);
-  return w0 * rd_u(w, 0, comp, k, 0, 0, 0) + w1 * rd_u(w, 0, comp, k1, 0, 0, 0);
+  return w0 * rd_u(w, w->ispeed, comp, k, 0, 0, 0) + w1 * rd_u(w, w->ispeed, comp, k1, 0, 0, 0);
 }
 
 /* Get_Speed of Policy_Speed_Interpolation_Linear_Symmetric
@@ -1138,6 +1170,131 @@ static void alg_mirror(world_t* w) {
   free(s.k);
 }
 
+/* ------------------------------------------------------------ pipeline B */
+/* src/Algorithms_Create_Interior_Depth.h:20-40: the stage form of the refill
+ * (no particles): inflow cells still empty get layer 0 and SetFluid, interior
+ * cells get layer 0. */
+static void alg_create_interior_depth(world_t* w) {
+  for (int64_t bi = 0; bi < w->nb; ++bi) {
+    brick_t* b = w->b[bi];
+    for (int o = 0; o < 512; ++o) {
+      if (!b->exists[o]) continue;
+      if (b->type[o] == MAC_INFLOW && b->layer[o] == -1) {
+        b->layer[o] = 0;
+        b->type[o] = set_fluid(b->type[o]);
+      } else if (b->type[o] == MAC_INTERIOR) {
+        b->layer[o] = 0;
+      }
+    }
+  }
+}
+
+/* One stage's Policy::Do() of test/Jet3.cpp:642-675: Algorithms<solve_grid,
+ * force projection, extrapolation of the acceleration>, where solve_grid =
+ * Algorithms<init2, Gravity, Convection, Viscosity> and init2 the depth
+ * topology with Create_Interior_Depth and Algorithms_Extrapolate (the
+ * boundary-condition extrapolation is not composed). The force projection
+ * (src/Algorithms_Solve_Pressure_Force.h:16-24) assembles, projects the
+ * acceleration with Dirichlet pressures from the current speed buffer, and
+ * Algorithms_Accel_To_Speed (src/Algorithms_Accel_To_Speed.h:26-31) runs the
+ * extrapolation on the acceleration. */
+static void stage_solve_grid_force(world_t* w) {
+  alg_initialize_depth(w);
+  alg_layer_initial_depth(w);
+  alg_create_interior_depth(w);
+  alg_update_layer_depth(w);
+  alg_delete(w);
+  alg_extrapolate_f(w, w->ispeed);
+  grid_forces(w, w->ispeed);
+  csr_t A;
+  assemble(w, &A);
+  project_field(w, &A, ACC, w->ispeed);
+  csr_free(&A);
+  alg_extrapolate_f(w, ACC);
+}
+
+/* Algorithms_RungeKutta_all::Do (src/Algorithms_RungeKutta_all.h:35-156) with
+ * Policy_Move_Particle (src/Policy_Move_Particle.h:24-56): four stages over
+ * speed buffers 0..2 and particle positions 0..2 in the reference's order
+ * (the grid update of a stage comes before its particle update, which reads
+ * the updated speed; the stage-2/3 update of position 1 reads the speed at the
+ * position 2 just written). Forced sets except the final speed. */
+static void alg_rk_all(world_t* w) {
+  const double dt = w->hdr.dt;
+  const int sym = w->hdr.interp_symmetric != 0;
+  w->ispeed = 0;
+  w->imove = 0;
+  acc_zero(w);
+  for (int stage = 1; stage <= 4; ++stage) {
+    stage_solve_grid_force(w);
+    for (int64_t bi = 0; bi < w->nb; ++bi) {
+      brick_t* b = w->b[bi];
+      for (int o = 0; o < 512; ++o) {
+        if (!b->exists[o]) continue;
+        for (int i = 0; i < 3; ++i) {
+          const double a = b->u[ACC][i][o];
+          if (stage == 1) {
+            b->u[2][i][o] = b->u[0][i][o] + a * dt * 0.5;
+            b->u[1][i][o] = b->u[0][i][o] + a * dt * 1. / 6.;
+          } else if (stage == 2) {
+            b->u[2][i][o] = b->u[0][i][o] + a * dt * 0.5;
+            b->u[1][i][o] = b->u[1][i][o] + a * dt * 1. / 3.;
+          } else if (stage == 3) {
+            b->u[2][i][o] = b->u[0][i][o] + a * dt;
+            b->u[1][i][o] = b->u[1][i][o] + a * dt * 1. / 3.;
+          } else {
+            set_u(b, b->u[0][i], o, i, b->u[1][i][o] + a * dt * 1. / 6., 0);
+          }
+        }
+      }
+    }
+    for (int64_t q = 0; q < w->np; ++q) {
+      double* p0 = pbuf(w, 0, q);
+      double* p1 = pbuf(w, 1, q);
+      double* p2 = pbuf(w, 2, q);
+      double v[3];
+      if (stage == 1) {
+        get_speed(w, p0, v, sym);
+        for (int i = 0; i < 3; ++i) p2[i] = p0[i] + dt * 0.5 * v[i];
+        get_speed(w, p0, v, sym);
+        for (int i = 0; i < 3; ++i) p1[i] = p0[i] + dt * 1.0 / 6.0 * v[i];
+      } else if (stage == 2 || stage == 3) {
+        const double s2 = stage == 2 ? dt * 0.5 : dt;
+        get_speed(w, p2, v, sym);
+        for (int i = 0; i < 3; ++i) p2[i] = p0[i] + s2 * v[i];
+        get_speed(w, p2, v, sym);
+        for (int i = 0; i < 3; ++i) p1[i] = p1[i] + dt * 1.0 / 3.0 * v[i];
+      } else {
+        get_speed(w, p2, v, sym);
+        for (int i = 0; i < 3; ++i) p0[i] = p1[i] + dt * 1.0 / 6.0 * v[i];
+      }
+    }
+    if (stage < 4) acc_zero(w);
+    if (stage == 1) {
+      w->hdr.t += 0.5 * dt;
+      w->ispeed = 2;
+      w->imove = 2;
+    } else if (stage == 3) {
+      w->hdr.t += 0.5 * dt;
+    }
+  }
+  w->ispeed = 0;
+  w->imove = 0;
+}
+
+/* The per-step init of pipeline B (test/Jet3.cpp:546 without the jet's own
+ * particle filter and the boundary-condition extrapolation): the depth
+ * topology with the refill, dt, and Algorithms_Extrapolate on speed 0. */
+static void alg_init_b(world_t* w) {
+  alg_initialize_depth(w);
+  alg_layer_initial_depth(w);
+  alg_create_fluid_depth(w);
+  alg_update_layer_depth(w);
+  alg_delete(w);
+  alg_dt(w);
+  alg_extrapolate_f(w, 0);
+}
+
 /* --------------------------------------------------------------- driver */
 static world_t* world_from_file(const mac_state_file* st) {
   world_t* w = (world_t*)calloc(1, sizeof(world_t));
@@ -1152,7 +1309,7 @@ static world_t* world_from_file(const mac_state_file* st) {
     memcpy(b->exists, st->exists + base, 512);
     for (int k = 0; k < 2; ++k)
       for (int i = 0; i < 3; ++i) memcpy(b->u[k][i], st->u[k][i] + base, 512 * 8);
-    for (int i = 0; i < 3; ++i) memcpy(b->acc[i], st->acc[i] + base, 512 * 8);
+    for (int i = 0; i < 3; ++i) memcpy(b->u[ACC][i], st->acc[i] + base, 512 * 8);
     memcpy(b->p, st->p + base, 512 * 8);
     memcpy(b->flags, st->flags + base, 512);
     memcpy(b->type, st->type + base, 512);
@@ -1187,7 +1344,7 @@ static void world_to_file(world_t* w, mac_state_file* st) {
     memcpy(st->exists + base, b->exists, 512);
     for (int k = 0; k < 2; ++k)
       for (int i = 0; i < 3; ++i) memcpy(st->u[k][i] + base, b->u[k][i], 512 * 8);
-    for (int i = 0; i < 3; ++i) memcpy(st->acc[i] + base, b->acc[i], 512 * 8);
+    for (int i = 0; i < 3; ++i) memcpy(st->acc[i] + base, b->u[ACC][i], 512 * 8);
     memcpy(st->p + base, b->p, 512 * 8);
     memcpy(st->flags + base, b->flags, 512);
     memcpy(st->type + base, b->type, 512);
@@ -1200,7 +1357,7 @@ static void world_to_file(world_t* w, mac_state_file* st) {
 
 static void world_free(world_t* w) {
   for (int64_t i = 0; i < w->nb; ++i) free(w->b[i]);
-  free(w->b); free(w->hkeys); free(w->hval); free(w->pos); free(w);
+  free(w->b); free(w->hkeys); free(w->hval); free(w->pos); free(w->pos1); free(w->pos2); free(w);
 }
 
 static int64_t fluid_count(world_t* w) {
@@ -1271,6 +1428,19 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
       alg_move(w, sym);
       w->hdr.t += w->hdr.dt;
       fcs += fluid_count(w);
+    } else if (!strcmp(cmd, "bstep")) {
+      w->viscous = 1;
+      ++w->seed;
+      alg_init_b(w);
+      alg_rk_all(w);
+      fcs += fluid_count(w);
+    } else if (!strcmp(cmd, "binit")) {
+      w->viscous = 1;
+      ++w->seed;
+      alg_init_b(w);
+    } else if (!strcmp(cmd, "bode")) {
+      w->viscous = 1;
+      alg_rk_all(w);
     } else if (!strcmp(cmd, "vstep")) {
       w->viscous = 1;
       ++w->seed;

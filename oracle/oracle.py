@@ -17,6 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libmac_oracle.so")
 REF = os.path.join(HERE, "_ref", "mac_ref")
 REF_DEPTH = os.path.join(HERE, "_ref", "mac_ref_depth")
+REF_B = os.path.join(HERE, "_ref", "mac_ref_b")
+PIPELINE_B = ("bstep", "binit", "bode")
 
 _lib = None
 
@@ -95,8 +97,10 @@ def _depth_mode(path: str) -> int:
 
 def run_ref(cmd: str, in_path: str, out_path: str, arg=None, timeout: float = 600.0) -> str:
     """Runs the reference's own code on a state (``cmd`` as in ``ref_world.cpp``);
-    a state in the depth composition goes to the depth build of the runner."""
-    args = [REF_DEPTH if _depth_mode(in_path) else REF, cmd, in_path, out_path]
+    a state in the depth composition goes to the depth build of the runner, the
+    pipeline-B commands to the build with three speed buffers."""
+    exe = REF_B if cmd in PIPELINE_B else (REF_DEPTH if _depth_mode(in_path) else REF)
+    args = [exe, cmd, in_path, out_path]
     if arg is not None:
         args.append(str(arg))
     out = subprocess.run(args, capture_output=True, text=True, timeout=timeout)

@@ -139,6 +139,13 @@
 #include "Algorithms_Create_Fluid_Particle_Depth.h"
 #include "Algorithms_Update_CellType_Layer_Depth.h"
 #endif
+#ifdef MAC_PIPELINE_B
+#include "Algorithms_Create_Interior_Depth.h"
+#include "Algorithms_Solve_Pressure_Force.h"
+#include "Algorithms_Accel_To_Speed.h"
+#include "Policy_Move_Particle.h"
+#include "Algorithms_RungeKutta_all.h"
+#endif
 
 #ifdef MAC_WITH_GPU
 // The C++ drop-in layer of the device path; compiled in only for _ref/mac_ref_gpu.
@@ -283,7 +290,11 @@ static int run(int argc, char** argv) {
   typedef double type_data_value;
   const int N = MAC_BRICK;
   const int NStock = N * N * N;
+#ifdef MAC_PIPELINE_B
+  const int NBSpeed = 3;  // Algorithms_RungeKutta_all needs 3 speeds (src/Algorithms_RungeKutta_all.h:6)
+#else
   const int NBSpeed = 2;
+#endif
 
   typedef Data_Base_Dim_Type<type_data_value, DIM> type_Data_Type;
   type_Data_Type m_data_type;
@@ -392,7 +403,11 @@ static int run(int argc, char** argv) {
   typedef Data_Grid_Data<type_interface_constant, type_Data_Base> type_grid_data;
   type_grid_data m_grid_data(m_type_interface_constant, data_base);
 
+#ifdef MAC_PIPELINE_B
+  typedef Data_Particle<type_Data_Base, 3> type_particle;  // pos0..pos2 of the RK4 over particles
+#else
   typedef Data_Particle<type_Data_Base> type_particle;
+#endif
   typedef Data_Particles_List<type_particle, type_Data_Base> type_particles;
   type_particles particles(data_base);
   typedef Data_Topology<type_particles, type_grid_data> type_topology;
@@ -586,6 +601,43 @@ static int run(int argc, char** argv) {
   typedef Algorithms_RungeKutta_RK2_TVD<type_data_ref, type_pol_ODE_v> type_alg_ODE_v;
   type_alg_ODE_v m_alg_ODE_v(m_data_ref, m_pol_ODE_v);
 
+#ifdef MAC_PIPELINE_B
+  // Pipeline B, test/Jet3.cpp:546-675 (no SPLIT, VISCOSITY): the per-step init
+  // with dt and the extrapolation, then Algorithms_RungeKutta_all over
+  // Policies<Algorithms<solve_grid, force projection, extrapolation of the
+  // acceleration>, Policy_Move_Particle>, where solve_grid re-runs the topology
+  // (with Create_Interior_Depth) at every stage before gravity, convection and
+  // viscosity. Deviations: the Dirichlet projection solves with the stand-in
+  // policy instead of pyamg (Algorithmes_Solve_Pressure_Dirichlet_Pyamg.h
+  // assembles the same system with the opposite sign), and
+  // Algorithm_Extrapolate_Boundary_Condition is left out of both
+  // extrapolations (its result depends on the hash map's visiting order).
+  typedef Algorithms_Create_Interior_Depth<type_data_ref, type_pol_init> type_alg_create_interior;
+  type_alg_create_interior m_alg_create_interior(m_data_ref, m_pol_init);
+  typedef Algorithms<type_alg_initialize_mac, type_alg_layer_initial, type_alg_create, type_alg_update_celltype, type_alg_delete, type_alg_dt, type_alg_extrapolate> type_alg_init_b;
+  type_alg_init_b m_alg_init_b(m_alg_initialize_mac, m_alg_layer_initial, m_alg_create, m_alg_update_celltype, m_alg_delete, m_alg_dt, m_alg_extrapolate);
+  typedef Algorithms<type_alg_initialize_mac, type_alg_layer_initial, type_alg_create_interior, type_alg_update_celltype, type_alg_delete, type_alg_extrapolate> type_alg_init2;
+  type_alg_init2 m_alg_init2(m_alg_initialize_mac, m_alg_layer_initial, m_alg_create_interior, m_alg_update_celltype, m_alg_delete, m_alg_extrapolate);
+  typedef Algorithms<type_alg_init2, type_alg_gravity, type_alg_convection, type_alg_viscosity> type_alg_solve_grid_b;
+  type_alg_solve_grid_b m_alg_solve_grid_b(m_alg_init2, m_alg_gravity, m_alg_convection, m_alg_viscosity);
+  typedef Algorithms_Solve_Pressure_Force<type_data_ref, type_alg_solve_pressure_v> type_alg_force_pressure;
+  type_alg_force_pressure m_alg_force_pressure(m_data_ref, m_alg_solve_pressure_v);
+  typedef Algorithms<type_alg_extrapolate> type_alg_extrap_only;
+  type_alg_extrap_only m_alg_extrap_only(m_alg_extrapolate);
+  typedef Algorithms_Accel_To_Speed<type_data_ref, type_alg_extrap_only> type_alg_extrap_force;
+  type_alg_extrap_force m_alg_extrap_force(m_data_ref, m_alg_extrap_only);
+  typedef Algorithms<type_alg_solve_grid_b, type_alg_force_pressure, type_alg_extrap_force> type_alg_solve_grid_force;
+  type_alg_solve_grid_force m_alg_solve_grid_force(m_alg_solve_grid_b, m_alg_force_pressure, m_alg_extrap_force);
+  typedef Policies<type_pol_interp_sym> type_pol_move_b;
+  type_pol_move_b m_pol_move_b(m_pol_interp_sym);
+  typedef Policy_Move_Particle<type_data_ref, type_pol_move_b> type_pol_move2;
+  type_pol_move2 m_pol_move2(m_data_ref, m_pol_move_b);
+  typedef Policies<type_alg_solve_grid_force, type_pol_move2> type_pol_ODE_b;
+  type_pol_ODE_b m_pol_ODE_b(m_alg_solve_grid_force, m_pol_move2);
+  typedef Algorithms_RungeKutta_all<type_data_ref, type_pol_ODE_b> type_alg_ODE_b;
+  type_alg_ODE_b m_alg_ODE_b(m_data_ref, m_pol_ODE_b);
+#endif
+
   typedef Policy_Advance_Ode_RungeKutta<type_data_ref> type_pol_advance;
   type_pol_advance m_pol_advance;
   typedef Policies<type_pol_advance, type_pol_interp_sym> type_pol_move;
@@ -702,6 +754,17 @@ static int run(int argc, char** argv) {
       m_alg_do_pressure_v.Do();
     } else if (cmd == "vode") {
       m_alg_ODE_v.Do();
+#ifdef MAC_PIPELINE_B
+    } else if (cmd == "bstep") {
+      ++g_refill_seed;
+      m_alg_init_b.Do();
+      m_alg_ODE_b.Do();
+    } else if (cmd == "binit") {
+      ++g_refill_seed;
+      m_alg_init_b.Do();
+    } else if (cmd == "bode") {
+      m_alg_ODE_b.Do();
+#endif
     } else if (cmd == "vstep") {
       ++g_refill_seed;
       m_alg_init.Do();

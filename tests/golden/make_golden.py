@@ -36,7 +36,15 @@ Policy_Add_Particle_Cube(1) refill) of a 24x24x32 jet over a 12-cell pool
   d_ref_s11.npz        one step from d_ref_s10
   d_ref_s20.npz        ten steps from d_ref_s10
 
-Usage: python tests/golden/make_golden.py [--viscous-only | --depth-only]
+Pipeline-B fixtures (oracle/_ref/mac_ref_b: Algorithms_RungeKutta_all over the
+depth world, test/Jet3.cpp:546-675, viscosity 1e-3), from d_ref_s10:
+
+  b_ref_i10.npz        after the pipeline-B per-step init (depth topology, dt,
+                       extrapolation)
+  b_ref_s11.npz        one pipeline-B step
+  b_ref_s15.npz        five pipeline-B steps
+
+Usage: python tests/golden/make_golden.py [--viscous-only | --depth-only | --b-only]
 """
 from __future__ import annotations
 
@@ -90,6 +98,17 @@ def depth(t, out):
         State.read(t("d" + name)).save_npz(out("d_ref_" + name))
 
 
+def pipeline_b(t, out):
+    s = State.load_npz(out("d_ref_s10"))
+    s.params.viscosity = VISCOSITY
+    s.write(t("bs10"))
+    oracle.run_ref("binit", t("bs10"), t("bi10"))
+    oracle.run_ref("bstep", t("bs10"), t("bs11"), 1)
+    oracle.run_ref("bstep", t("bs10"), t("bs15"), 5)
+    for name in ("i10", "s11", "s15"):
+        State.read(t("b" + name)).save_npz(out("b_ref_" + name))
+
+
 def main():
     oracle.build()
     if not oracle.have_ref():
@@ -104,6 +123,10 @@ def main():
     if "--depth-only" in sys.argv:
         depth(t, out)
         print("depth fixtures written to", HERE)
+        return
+    if "--b-only" in sys.argv:
+        pipeline_b(t, out)
+        print("pipeline-B fixtures written to", HERE)
         return
     s = jet_world()
     s.write(t("setup"))
@@ -126,6 +149,7 @@ def main():
     oracle.run_ref("csc", t("t30"), t("junk"), os.path.join(HERE, "c1_ref_t30_csc.bin"))
     viscous(t, out)
     depth(t, out)
+    pipeline_b(t, out)
     print("fixtures written to", HERE)
 
 

@@ -92,3 +92,34 @@ def test_planted_depth_mistakes_are_caught(golden, run_oracle, planted):
         compare_topology(got, ref)
         assert compare_particles(got, ref) == 0.0
     assert not np.array_equal(got.pos.shape, ref.pos.shape) or planted == "interior"
+
+
+# ------------------------------------------------------------ pipeline B
+def _b_input(golden):
+    s = golden("d_ref_s10")
+    s.params.viscosity = 1e-3
+    return s
+
+
+def test_pipeline_b_init_bit_exact(golden, run_oracle):
+    """The per-step init of test/Jet3.cpp:546 (depth topology, dt, extrapolation)."""
+    got, _ = run_oracle("binit", _b_input(golden))
+    ref = golden("b_ref_i10")
+    compare_topology(got, ref)
+    assert compare_particles(got, ref) == 0.0
+    _exact_fields(got, ref, ("u0x", "u0y", "u0z", "p"))
+    assert got.params.dt == ref.params.dt
+
+
+def test_pipeline_b_steps_track_reference(golden, run_oracle):
+    """Algorithms_RungeKutta_all over grid and particles
+    (src/Algorithms_RungeKutta_all.h:35-156) with the stage topology, the force
+    projection and the extrapolation of the acceleration: one and five steps."""
+    for n, name in ((1, "b_ref_s11"), (5, "b_ref_s15")):
+        got, _ = run_oracle("bstep", _b_input(golden), n=n)
+        ref = golden(name)
+        compare_topology(got, ref)
+        e = field_errors(got, ref, ("u0x", "u0y", "u0z", "p"))
+        assert max(e.values()) <= 1e-12, (n, e)
+        compare_particles(got, ref, atol=1e-13)
+        assert got.params.t == ref.params.t
