@@ -86,7 +86,12 @@ typedef struct {
   /* inflow (and interior) refill: 0 = 8 jittered particles per cell,
    * n >= 1 = Policy_Add_Particle_Cube(n), (2n+1)^3 particles per cell */
   int32_t refill_cube;
-  int32_t reserved0;
+  /* 0: pipeline A, the step of test/TestJetDEau_Basic.cpp:434-441 (RK2-TVD,
+   * extrapolation, particle RK4); 1: pipeline B, the step of test/Jet3.cpp:713-726
+   * (per-step init with the extrapolation, then Algorithms_RungeKutta_all over
+   * grid and particles with the topology re-run, the force projection and the
+   * extrapolation of the acceleration at every stage); needs depth_mode. */
+  int32_t pipeline;
 } mac_params;
 
 /* Host view of a world, arrays owned by the caller. Brick b holds cells
@@ -168,6 +173,10 @@ int mac_pressure_project(void* ctx, int ispeed);
 /* Algorithms_RungeKutta_RK2_TVD::Do with Policy = Algorithms<Gravity, Convection> +
  * Algorithms_Solve_Pressure (src/Algorithms_RungeKutta_RK2_TVD.h:20-66) */
 int mac_rk2tvd(void* ctx);
+/* src/Algorithms_RungeKutta_all.h:35-156 with the policy of test/Jet3.cpp:642-675
+ * (pipeline B only: mac_params.pipeline = 1): four stages of topology, forces,
+ * force projection and extrapolation, moving grid speeds and particles */
+int mac_rungekutta_all(void* ctx);
 /* src/Algorithms_Extrapolate.h:25-233 */
 int mac_extrapolate(void* ctx);
 /* Algorithms_Move_Particles + Policy_Advance_Ode_RungeKutta + Get_Speed

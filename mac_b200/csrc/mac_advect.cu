@@ -106,10 +106,12 @@ __device__ inline double laplacian(const double* __restrict__ Ui, const int* sn,
 // is fluid (src/Policy_Gravity.h:14-34); convection uses the same rule on axis
 // i (src/Policy_Convection_Apply_If.h:41-61). With a viscosity, Algorithms_Viscosity
 // (src/Algorithms_Viscosity.h:24-30) then adds viscosity * Laplacian.
+// base: the acceleration the contributions add to (0 after the forced zero;
+// pipeline B's stage forces add to what a re-created cell holds).
 __device__ inline double face_accel(const double* const* U, const int* sn, const int8_t* __restrict__ lay,
                                     const uint8_t* __restrict__ type, int64_t c, uint8_t fl, int x, int y, int z,
-                                    int i, const Params& P) {
-  if (fl & (1u << i)) return 0.0;
+                                    int i, const Params& P, double base = 0.0) {
+  if (fl & (1u << i)) return base;
   bool fluid = is_fluid(type[c]);
   bool apply = fluid;
   if (!fluid && lay[c] != kEmpty) {
@@ -118,7 +120,7 @@ __device__ inline double face_accel(const double* const* U, const int* sn, const
     int64_t n = cidx(sn, m[0], m[1], m[2]);
     apply = n >= 0 && lay[n] != kMissing && is_fluid(type[n]);
   }
-  double a = 0.0;
+  double a = base;
   if (i == P.gaxis) {
     bool g = fluid;
     if (!fluid && lay[c] != kEmpty) {
@@ -177,6 +179,47 @@ __global__ void __launch_bounds__(256) k_forces(const int* __restrict__ blist, i
   }
 }
 
+// Pipeline B's Algorithms<Gravity, Convection, Viscosity> of a stage: acc +=
+// the forces of speed field U, through the non-forced Set, for every existing
+// cell (src/Algorithms_Gravity.h:15-28, src/Algorithms_Convection.h:18-37,
+// src/Algorithms_Viscosity.h:24-30).
+__global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ blist, int nlive,
+                                                    const int* __restrict__ nbr, const int8_t* __restrict__ lay,
+                                                    const uint8_t* __restrict__ type, const uint8_t* __restrict__ flags,
+                                                    const double* __restrict__ ux, const double* __restrict__ uy,
+                                                    const double* __restrict__ uz, double* ax, double* ay, double* az,
+                                                    Params P) {
+  __shared__ int sn[kNbr];
+  const double* U[3] = {ux, uy, uz};
+  double* A[3] = {ax, ay, az};
+  for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
+    int b = blist[bi];
+    if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
+    __syncthreads();
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      int64_t c = (int64_t)b * kCells + o;
+      if (lay[c] == kMissing) continue;
+      int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+      uint8_t fl = flags[c];
+      double a[3];
+      for (int i = 0; i < 3; ++i) a[i] = face_accel(U, sn, lay, type, c, fl, x, y, z, i, P, A[i][c]);
+      for (int i = 0; i < 3; ++i) A[i][c] = a[i];
+    }
+    __syncthreads();
+  }
+}
+
+int forces_add(Ctx* c, const double* const* U) {
+  if (c->nlive_host == 0) return MAC_OK;
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  prof_begin(c, PH_FORCES);
+  k_forces_add<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
+                                                     U[0], U[1], U[2], c->f64 + AX * cap, c->f64 + AY * cap,
+                                                     c->f64 + AZ * cap, c->dp); MAC_COUNT(c);
+  prof_end(c, PH_FORCES);
+  return check(cudaGetLastError());
+}
+
 int forces(Ctx* c, int ib) {
   if (c->nlive_host == 0) return MAC_OK;
   size_t cap = (size_t)c->cap_bricks * kCells;
@@ -213,7 +256,8 @@ __device__ inline int8_t lay_i(const int8_t* __restrict__ lay, int64_t i) { retu
 
 __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ blist, int nlive, const int* __restrict__ nbr,
                                                      const int8_t* __restrict__ lay, const uint8_t* __restrict__ flags,
-                                                     double* f64, size_t cap, int L) {
+                                                     double* fx, double* fy, double* fz, int L) {
+  double* const F[3] = {fx, fy, fz};
   __shared__ int sn[kNbr];
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
     int b = blist[bi];
@@ -233,7 +277,7 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
         bool vA = lA >= 0;
         bool write = (vA && lA == L && lB >= L) || (lB == L && (!vA || lA >= L));
         if (!write) continue;
-        const double* Ui = f64 + (size_t)(U0X + i) * cap;
+        const double* Ui = F[i];
         int n = 0;
         double val = 0;
         for (int j = 0; j < 3; ++j) {
@@ -273,23 +317,31 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
             }
           }
         }
-        f64[(size_t)(U0X + i) * cap + c] = val / n;
+        F[i][c] = val / n;
       }
     }
     __syncthreads();
   }
 }
 
-int extrapolate(Ctx* c) {
+// Algorithms_Extrapolate on the vector field F (speed buffer 0 in pipeline A;
+// the stage speed and, through Algorithms_Accel_To_Speed, the acceleration in
+// pipeline B).
+int extrapolate_field(Ctx* c, double* const* F) {
   if (c->nlive_host == 0) return MAC_OK;
-  size_t cap = (size_t)c->cap_bricks * kCells;
   prof_begin(c, PH_EXTRAPOLATE);
   for (int L = 1; L <= c->dp.layer_max + 1; ++L) {
-    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, c->f64,
-                                                        cap, L); MAC_COUNT(c);
+    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, F[0], F[1],
+                                                        F[2], L); MAC_COUNT(c);
   }
   prof_end(c, PH_EXTRAPOLATE);
   return check(cudaGetLastError());
+}
+
+int extrapolate(Ctx* c) {
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  double* F[3] = {c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap};
+  return extrapolate_field(c, F);
 }
 
 // ---------------------------------------------------------------- particles
@@ -610,6 +662,163 @@ __global__ void __launch_bounds__(256) k_move_stray(double* px, double* py, doub
     pz[q] = pos[2];
   }
   if (bad) atomicAdd(bad_count, 1ull);
+}
+
+// ------------------------------------------------------------ pipeline B
+// The grid and particle updates of Algorithms_RungeKutta_all::Do
+// (src/Algorithms_RungeKutta_all.h:35-156), stage by stage, in the reference's
+// expression order: stage 1 u2 = u0 + a dt 0.5, u1 = u0 + a dt 1/6; stage 2
+// u2 = u0 + a dt 0.5, u1 += a dt 1/3; stage 3 u2 = u0 + a dt, u1 += a dt 1/3
+// (all forced Sets); stage 4 u0 = u1 + a dt 1/6 through the non-forced Set.
+__global__ void __launch_bounds__(256) k_acc_zero(const int* __restrict__ blist, int nlive,
+                                                  const int8_t* __restrict__ lay, double* ax, double* ay, double* az) {
+  for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
+    size_t base = (size_t)blist[bi] * kCells;
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      size_t c = base + o;
+      if (lay[c] == kMissing) continue;
+      ax[c] = 0.0;
+      ay[c] = 0.0;
+      az[c] = 0.0;
+    }
+  }
+}
+
+struct Fields3 {
+  double* f[3][3];  // speed buffers 0..2, components x..z
+  double* a[3];     // acceleration
+};
+
+__global__ void __launch_bounds__(256) k_grid_stage(const int* __restrict__ blist, int nlive,
+                                                    const int8_t* __restrict__ lay, const uint8_t* __restrict__ flags,
+                                                    Fields3 F, const Scalars* __restrict__ ds, int stage) {
+  const double dt = ds->dt;
+  for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
+    size_t base = (size_t)blist[bi] * kCells;
+    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+      size_t c = base + o;
+      if (lay[c] == kMissing) continue;
+      const uint8_t fl = flags[c];
+      for (int i = 0; i < 3; ++i) {
+        const double a = F.a[i][c];
+        const double u0 = F.f[0][i][c];
+        if (stage == 1) {
+          F.f[2][i][c] = u0 + a * dt * 0.5;
+          F.f[1][i][c] = u0 + a * dt * 1. / 6.;
+        } else if (stage == 2) {
+          F.f[2][i][c] = u0 + a * dt * 0.5;
+          F.f[1][i][c] = F.f[1][i][c] + a * dt * 1. / 3.;
+        } else if (stage == 3) {
+          F.f[2][i][c] = u0 + a * dt;
+          F.f[1][i][c] = F.f[1][i][c] + a * dt * 1. / 3.;
+        } else if (!(fl & (1u << i))) {
+          F.f[0][i][c] = F.f[1][i][c] + a * dt * 1. / 6.;
+        }
+      }
+    }
+  }
+}
+
+// Policy_Move_Particle's particle updates (src/Policy_Move_Particle.h:24-56,
+// the speed from Policy_Speed_Interpolation_Linear[_Symmetric]::Get_Speed of
+// the stage's speed field U): stage 1 p2 = p0 + dt 0.5 v(p0), p1 = p0 + dt/6 v(p0);
+// stages 2 and 3 p2 = p0 + s v(p2) (s = dt 0.5, dt), then p1 += dt/3 v(p2 new);
+// stage 4 p0 = p1 + dt/6 v(p2).
+struct PartBufs {
+  double* p[3][3];  // positions 0..2, components x..z
+};
+
+__global__ void __launch_bounds__(256) k_particle_stage(PartBufs B, const int* __restrict__ nbr,
+                                                        const unsigned long long* __restrict__ hk,
+                                                        const int* __restrict__ hv, int64_t hcap,
+                                                        const int8_t* __restrict__ lay, const double* __restrict__ ux,
+                                                        const double* __restrict__ uy, const double* __restrict__ uz,
+                                                        Params P, const Scalars* __restrict__ ds, int stage,
+                                                        unsigned long long* bad_count) {
+  const double dt = ds->dt;
+  const int64_t n = ds->np;
+  const double* U[3] = {ux, uy, uz};
+  int bad = 0;
+  auto speed = [&](const double* pos, double* v) {
+    PBase pb;
+    for (int i = 0; i < 3; ++i) pb.key[i] = fdiv8((int)lround(pos[i] * P.ih[i]));
+    pb.b = hash_find(hk, hv, hcap, pack_key(pb.key[0], pb.key[1], pb.key[2]));
+    GlobalField f{pb, nbr, hk, hv, hcap, lay, U};
+    get_speed(pos, v, f, P, P.interp_sym, &bad);
+  };
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    double p0[3], p1[3], p2[3], v[3];
+    for (int i = 0; i < 3; ++i) p0[i] = B.p[0][i][q];
+    if (stage == 1) {
+      speed(p0, v);
+      for (int i = 0; i < 3; ++i) {
+        B.p[2][i][q] = p0[i] + dt * 0.5 * v[i];
+        B.p[1][i][q] = p0[i] + dt * 1.0 / 6.0 * v[i];
+      }
+    } else if (stage == 2 || stage == 3) {
+      const double s = stage == 2 ? dt * 0.5 : dt;
+      for (int i = 0; i < 3; ++i) p2[i] = B.p[2][i][q];
+      speed(p2, v);
+      for (int i = 0; i < 3; ++i) p2[i] = p0[i] + s * v[i];
+      speed(p2, v);
+      for (int i = 0; i < 3; ++i) {
+        B.p[2][i][q] = p2[i];
+        p1[i] = B.p[1][i][q];
+        B.p[1][i][q] = p1[i] + dt * 1.0 / 3.0 * v[i];
+      }
+    } else {
+      for (int i = 0; i < 3; ++i) p2[i] = B.p[2][i][q];
+      speed(p2, v);
+      for (int i = 0; i < 3; ++i) B.p[0][i][q] = B.p[1][i][q] + dt * 1.0 / 6.0 * v[i];
+    }
+  }
+  if (bad) atomicAdd(bad_count, 1ull);
+}
+
+__global__ void k_half_time(Scalars* ds) { ds->t += 0.5 * ds->dt; }
+
+int rk_all_stage_update(Ctx* c, int stage, const double* const* U) {
+  cudaStream_t st = c->stream;
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  Fields3 F;
+  for (int i = 0; i < 3; ++i) {
+    F.f[0][i] = c->f64 + (size_t)(U0X + i) * cap;
+    F.f[1][i] = c->f64 + (size_t)(U1X + i) * cap;
+    F.f[2][i] = c->u2 + (size_t)i * cap;
+    F.a[i] = c->f64 + (size_t)(AX + i) * cap;
+  }
+  if (c->nlive_host > 0) {
+    k_grid_stage<<<c->nlive_host, 256, 0, st>>>(c->blist, c->nlive_host, c->lay, c->flags, F, c->ds, stage); MAC_COUNT(c);
+  }
+  if (c->np_host > 0) {
+    PartBufs B;
+    B.p[0][0] = c->px;
+    B.p[0][1] = c->py;
+    B.p[0][2] = c->pz;
+    for (int k = 0; k < 2; ++k)
+      for (int i = 0; i < 3; ++i) B.p[k + 1][i] = c->pbuf[k][i];
+    int g = grid_for(c->np_host, 256);
+    if (g > 148 * 16) g = 148 * 16;
+    prof_begin(c, PH_MOVE);
+    k_particle_stage<<<g, 256, 0, st>>>(B, c->nbr, c->hkeys, c->hval, c->hcap, c->lay, U[0], U[1], U[2], c->dp, c->ds,
+                                        stage, &c->ds->bad_reads); MAC_COUNT(c);
+    prof_end(c, PH_MOVE);
+  }
+  if (stage < 4 && c->nlive_host > 0) {
+    k_acc_zero<<<c->nlive_host, 256, 0, st>>>(c->blist, c->nlive_host, c->lay, F.a[0], F.a[1], F.a[2]); MAC_COUNT(c);
+  }
+  if (stage == 1 || stage == 3) {
+    k_half_time<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
+  }
+  return check(cudaGetLastError());
+}
+
+int acc_zero(Ctx* c) {
+  if (c->nlive_host == 0) return MAC_OK;
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  k_acc_zero<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->lay, c->f64 + AX * cap,
+                                                   c->f64 + AY * cap, c->f64 + AZ * cap); MAC_COUNT(c);
+  return check(cudaGetLastError());
 }
 
 int move_particles(Ctx* c) {

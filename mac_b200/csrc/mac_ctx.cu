@@ -176,7 +176,9 @@ static void free_all(Ctx* c) {
   free_solver(c);
   cudaFree(c->bkey); cudaFree(c->lay); cudaFree(c->type); cudaFree(c->flags); cudaFree(c->f64);
   cudaFree(c->pdir);
-  cudaFree(c->depth); cudaFree(c->pkeep);
+  cudaFree(c->depth); cudaFree(c->pkeep); cudaFree(c->u2);
+  for (int k = 0; k < 2; ++k)
+    for (int i = 0; i < 3; ++i) { cudaFree(c->pbuf[k][i]); cudaFree(c->pbuf2[k][i]); }
   cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
@@ -199,6 +201,7 @@ static int create(const mac_params* p, Ctx** out) {
   if (!(p->viscosity >= 0) || !std::isfinite(p->viscosity)) return MAC_ERR_INVALID;
   if (p->refill_cube < 0 || p->refill_cube > 4) return MAC_ERR_INVALID;
   if (p->depth_mode && (p->depth_interior < 0 || p->depth_remove < 0)) return MAC_ERR_INVALID;
+  if (p->pipeline < 0 || p->pipeline > 1 || (p->pipeline == 1 && !p->depth_mode)) return MAC_ERR_INVALID;
   if (p->device < 0 || p->device >= ndev) return MAC_ERR_INVALID;
   MAC_CUDA(cudaSetDevice(p->device));
   Ctx* c = new (std::nothrow) Ctx();
@@ -227,6 +230,7 @@ static int create(const mac_params* p, Ctx** out) {
   c->dp.depth_interior = p->depth_interior;
   c->dp.depth_remove = p->depth_remove;
   c->dp.refill_cube = p->refill_cube;
+  c->dp.pipeline = p->pipeline;
   for (int i = 0; i < 3; ++i) c->dp.lih2[i] = std::pow(c->dp.ih[i], 2);
   c->cap_bricks = p->max_bricks;
   c->cap_particles = p->max_particles;
@@ -246,6 +250,14 @@ static int create(const mac_params* p, Ctx** out) {
   if (p->depth_mode) {
     A(dalloc(&c->depth, nc));
     A(dalloc(&c->pkeep, (size_t)c->cap_particles));
+  }
+  if (p->pipeline == 1) {
+    A(dalloc(&c->u2, 3 * nc));
+    for (int k = 0; k < 2; ++k)
+      for (int i = 0; i < 3; ++i) {
+        A(dalloc(&c->pbuf[k][i], (size_t)c->cap_particles));
+        A(dalloc(&c->pbuf2[k][i], (size_t)c->cap_particles));
+      }
   }
   A(dalloc(&c->nbr, kNbr * c->cap_bricks));
   A(dalloc(&c->blist, c->cap_bricks));
@@ -330,6 +342,9 @@ static int upload(Ctx* c, const mac_host_state* s) {
   }
   if (cap > nc) MAC_CUDA(cudaMemsetAsync(c->lay + nc, 0xFE, cap - nc, st));
   if (cap > nc && c->depth) MAC_CUDA(cudaMemsetAsync(c->depth + nc, 0xFF, 2 * (cap - nc), st));
+  // speed buffer 2 is not part of a state: the prototype value everywhere
+  if (c->u2) MAC_CUDA(cudaMemsetAsync(c->u2, 0, 8 * 3 * cap, st));
+  c->imove = 0;
   k_init_lists<<<grid_for(c->cap_bricks, 256), 256, 0, st>>>(c->blist, c->freelist, nb, (int)c->cap_bricks); MAC_COUNT(c);
   // particles, through a bounded staging buffer (solver vector pd)
   int64_t np = s->nparticles;

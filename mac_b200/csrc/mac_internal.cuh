@@ -98,6 +98,7 @@ struct Params {
   double nu, lih2[3];
   // depth composition (Policy_Depth) and the refill policy (0: jitter8, n: cube(n))
   int depth_mode, depth_interior, depth_remove, refill_cube;
+  int pipeline;  // 0: pipeline A (RK2-TVD + particle RK4); 1: pipeline B (Algorithms_RungeKutta_all)
   // inverse diagonal of the level-0 operator by active faces per axis
   // (index ax + 3 ay + 9 az, each 0..2); 0 when no face is active
   double dtab[27];
@@ -134,6 +135,12 @@ struct Ctx {
   double* pdir = nullptr;     // [cap*512] Dirichlet air pressure, NaN off the boundary (viscous only)
   int16_t* depth = nullptr;   // [cap*512] distance to the surface, -1 empty (depth composition only)
   uint8_t* pkeep = nullptr;   // [max_particles] removal marks of the particle pass (depth composition only)
+  // pipeline B (Algorithms_RungeKutta_all): speed buffer 2, particle positions
+  // 1 and 2 with their compaction scratch, and the position the topology reads
+  double* u2 = nullptr;       // [3][cap*512]
+  double* pbuf[2][3] = {};    // [max_particles] each
+  double* pbuf2[2][3] = {};
+  int imove = 0;              // 0 or 2 (Data_Particle::imove_particle)
   int* nbr = nullptr;         // [cap][27]
   int* blist = nullptr;       // live bricks (current)
   int* blist2 = nullptr;      // scratch for compaction
@@ -459,6 +466,12 @@ int read_scalars(Ctx* c);
 int forces(Ctx* c, int ib);
 int rk2tvd(Ctx* c);
 int project(Ctx* c, int ib);
+int project_field(Ctx* c, double* const* U, const double* const* D);
+int extrapolate_field(Ctx* c, double* const* F);
+int forces_add(Ctx* c, const double* const* U);
+int rk_all_stage_update(Ctx* c, int stage, const double* const* U);
+int acc_zero(Ctx* c);
+int topology_stage(Ctx* c);
 int setup_system(Ctx* c);
 int extrapolate(Ctx* c);
 int move_particles(Ctx* c);

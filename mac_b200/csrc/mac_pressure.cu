@@ -652,6 +652,19 @@ static void precondition(Ctx* c) {
 }
 
 int project(Ctx* c, int ib) {
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  double* U[3] = {c->f64 + (size_t)(3 * ib) * cap, c->f64 + (size_t)(3 * ib + 1) * cap,
+                  c->f64 + (size_t)(3 * ib + 2) * cap};
+  return project_field(c, U, U);
+}
+
+// The projection of vector field U (Divergence_Projection: divergence,
+// solve, pressure write-back, gradient correction of U). D is the speed
+// field the Dirichlet air pressures of the viscous composition read
+// (Speed_GetRef(-1, false), src/Policy_Dirichlet_Boundary.h:100-102): U
+// itself, except in the force projection of pipeline B
+// (src/Algorithms_Solve_Pressure_Force.h:16-24), where U is the acceleration.
+int project_field(Ctx* c, double* const* U, const double* const* D) {
   if (!c->system_ready) {
     int rc = setup_system(c);
     if (rc) return rc;
@@ -659,14 +672,12 @@ int project(Ctx* c, int ib) {
   int nd = c->ndom_host;
   cudaStream_t st = c->stream;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  double* U[3] = {c->f64 + (size_t)(3 * ib) * cap, c->f64 + (size_t)(3 * ib + 1) * cap,
-                  c->f64 + (size_t)(3 * ib + 2) * cap};
   int status = MAC_OK;
   int rc;
   // the viscous composition projects with Dirichlet air pressures
   double* pdir = c->dp.nu > 0 ? c->pdir : nullptr;
   if (pdir && nd == 0 && c->nlive_host > 0) {
-    k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, U[0], U[1], U[2], pdir,
+    k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, D[0], D[1], D[2], pdir,
                                                c->dp); MAC_COUNT(c);
   }
   if (nd > 0) {
@@ -674,7 +685,7 @@ int project(Ctx* c, int ib) {
     double rtol2 = c->prm.rtol * c->prm.rtol;
     prof_begin(c, PH_DIVERGENCE);
     if (pdir) {
-      k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, U[0], U[1], U[2], pdir,
+      k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, D[0], D[1], D[2], pdir,
                                                  c->dp); MAC_COUNT(c);
     }
     k_divergence<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,

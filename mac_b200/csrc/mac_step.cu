@@ -26,8 +26,53 @@ int rk2tvd(Ctx* c) {
 
 __global__ void k_advance_time(Scalars* ds) { ds->t += ds->dt; }
 
+// Algorithms_RungeKutta_all::Do (src/Algorithms_RungeKutta_all.h:35-156) with
+// the policy of test/Jet3.cpp:642-675: the acceleration is zeroed, then each
+// of the four stages runs the stage topology at the current particle position
+// (init2), Algorithms_Extrapolate on the stage speed, gravity + convection (+
+// viscosity) into the acceleration, the force projection of the acceleration
+// (Dirichlet pressures from the stage speed), Algorithms_Extrapolate on the
+// acceleration, and the stage's grid and particle updates. The stage speed is
+// buffer 0 in stage 1 and buffer 2 after it; the topology reads position 0 in
+// stage 1 and position 2 after it.
+int rk_all(Ctx* c) {
+  if (c->dp.pipeline != 1) return MAC_ERR_INVALID;
+  size_t cap = (size_t)c->cap_bricks * kCells;
+  double* U0[3] = {c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap};
+  double* U2[3] = {c->u2, c->u2 + cap, c->u2 + 2 * cap};
+  double* A[3] = {c->f64 + AX * cap, c->f64 + AY * cap, c->f64 + AZ * cap};
+  int rc, status = MAC_OK;
+  c->imove = 0;
+  if ((rc = acc_zero(c))) return rc;
+  for (int stage = 1; stage <= 4; ++stage) {
+    double* const* S = stage == 1 ? U0 : U2;
+    if ((rc = topology_stage(c))) return rc;
+    if ((rc = extrapolate_field(c, S))) return rc;
+    if ((rc = forces_add(c, S))) return rc;
+    int sp = project_field(c, A, S);
+    if (sp && sp != MAC_ERR_NOT_CONVERGED) return sp;
+    if (sp) status = sp;
+    if ((rc = extrapolate_field(c, A))) return rc;
+    if ((rc = rk_all_stage_update(c, stage, S))) return rc;
+    if (stage == 1) c->imove = 2;
+  }
+  c->imove = 0;
+  return status;
+}
+
+// One step of test/Jet3.cpp:720-726 (pipeline B): the per-step init (the depth
+// topology with dt, then Algorithms_Extrapolate) and Algorithms_RungeKutta_all,
+// which moves the particles itself.
+static int step_b(Ctx* c) {
+  int rc = topology_rebuild(c, false);
+  if (rc) return rc;
+  if ((rc = extrapolate(c))) return rc;
+  return rk_all(c);
+}
+
 // One step of test/TestJetDEau_Basic.cpp:434-441.
 static int step(Ctx* c) {
+  if (c->dp.pipeline == 1) return step_b(c);
   int rc = topology_rebuild(c, false);
   if (rc) return rc;
   int ode = rk2tvd(c);
@@ -222,6 +267,10 @@ int mac_pressure_project(void* ctx, int ispeed) {
 int mac_rk2tvd(void* ctx) {
   CTX_OR_FAIL();
   return mac::rk2tvd(c);
+}
+int mac_rungekutta_all(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::rk_all(c);
 }
 int mac_extrapolate(void* ctx) {
   CTX_OR_FAIL();

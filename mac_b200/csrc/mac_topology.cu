@@ -112,7 +112,7 @@ __global__ void k_bbox_reset(Scalars* ds) {
 __global__ void k_alloc_bricks(const int* __restrict__ newslots, const unsigned long long* __restrict__ hk,
                                int* hv, int* bkey, int* blist, const int* __restrict__ freelist,
                                int8_t* lay, uint8_t* type, uint8_t* flags, double* f64, int16_t* depth,
-                               size_t cap_cells, int64_t cap_bricks, Scalars* ds) {
+                               double* u2, size_t cap_cells, int64_t cap_bricks, Scalars* ds) {
   __shared__ int sb;
   int n = ds->nnew;
   if (n > cap_bricks) n = (int)cap_bricks;
@@ -145,6 +145,8 @@ __global__ void k_alloc_bricks(const int* __restrict__ newslots, const unsigned 
         type[c] = MAC_CELL_AIR;
         flags[c] = 0;
         if (depth) depth[c] = -1;
+        if (u2)
+          for (int f = 0; f < 3; ++f) u2[(size_t)f * cap_cells + c] = 0.0;
         for (int f = 0; f < NF64; ++f) f64[(size_t)f * cap_cells + c] = 0.0;
       }
     }
@@ -221,10 +223,15 @@ __global__ void k_mark_particles(const double* __restrict__ px, const double* __
 // src/Algorithms_Layer_Initial_With_Particle_Depth.h:33-36): kept particles are
 // packed into the second position arrays with one atomic per warp. The order
 // changes; nothing depends on the particle order.
-__global__ void k_compact_particles(const double* __restrict__ px, const double* __restrict__ py,
-                                    const double* __restrict__ pz, const uint8_t* __restrict__ pkeep,
-                                    double* __restrict__ qx, double* __restrict__ qy, double* __restrict__ qz,
-                                    Scalars* ds) {
+// Up to three position buffers (pipeline B carries positions 0..2 of every
+// particle) move together.
+struct PartMove {
+  const double* src[9];
+  double* dst[9];
+  int n;  // 3 or 9 arrays
+};
+
+__global__ void k_compact_particles(PartMove M, const uint8_t* __restrict__ pkeep, Scalars* ds) {
   const int64_t n = ds->np;
   const int lane = threadIdx.x & 31;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
@@ -236,9 +243,7 @@ __global__ void k_compact_particles(const double* __restrict__ px, const double*
     w = __shfl_sync(0xffffffffu, w, 0);
     if (keep) {
       const unsigned long long i = w + __popc(m & ((1u << lane) - 1u));
-      qx[i] = px[q];
-      qy[i] = py[q];
-      qz[i] = pz[q];
+      for (int a = 0; a < M.n; ++a) M.dst[a][i] = M.src[a][q];
     }
   }
 }
@@ -285,10 +290,13 @@ __device__ inline void jitter8(unsigned long long seed, int kx, int ky, int kz, 
 // (src/Algorithms_Create_Fluid_Particle_Depth.h:21-43): an interior cell with
 // an empty layer no deeper than the removal depth is refilled too, and every
 // interior cell gets layer 0.
+// no_particles: the stage form Algorithms_Create_Interior_Depth
+// (src/Algorithms_Create_Interior_Depth.h:20-40), which sets the layers (and
+// SetFluid on inflow cells) without adding particles.
 __global__ void k_refill(const int* __restrict__ blist, const int* __restrict__ bkey, int8_t* lay,
                          const uint8_t* __restrict__ type, const int16_t* __restrict__ depth, double* px,
                          double* py, double* pz, int64_t cap_particles, unsigned long long seed, Params P,
-                         Scalars* ds) {
+                         Scalars* ds, int no_particles) {
   int n = ds->nlive;
   const int side = 2 * P.refill_cube + 1;
   const int per = P.refill_cube > 0 ? side * side * side : 8;
@@ -308,6 +316,10 @@ __global__ void k_refill(const int* __restrict__ blist, const int* __restrict__ 
         }
       }
       if (!refill) continue;
+      if (no_particles) {
+        lay[base + o] = 0;
+        continue;
+      }
       int kx = bkey[3 * b] * 8 + (o & 7), ky = bkey[3 * b + 1] * 8 + ((o >> 3) & 7),
           kz = bkey[3 * b + 2] * 8 + (o >> 6);
       unsigned long long pos = atomicAdd((unsigned long long*)&ds->np, (unsigned long long)per);
@@ -642,7 +654,7 @@ int rebuild_index(Ctx* c) {
 static void alloc_new(Ctx* c) {
   cudaStream_t st = c->stream;
   k_alloc_bricks<<<kTopoBlocks, 256, 0, st>>>(c->newslots, c->hkeys, c->hval, c->bkey, c->blist, c->freelist,
-                                               c->lay, c->type, c->flags, c->f64, c->depth,
+                                               c->lay, c->type, c->flags, c->f64, c->depth, c->u2,
                                                (size_t)c->cap_bricks * kCells, c->cap_bricks, c->ds); MAC_COUNT(c);
 }
 
@@ -657,20 +669,40 @@ int topo_layer_initial(Ctx* c) {
   int g = kTopoBlocks * 2;
   k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   uint8_t* keep = c->dp.depth_mode ? c->pkeep : nullptr;
-  k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
+  // the position the topology reads (Data_Particle::imove_particle): 0, or 2
+  // during pipeline B's stages 2-4
+  const double* kx = c->imove == 2 ? c->pbuf[1][0] : c->px;
+  const double* ky = c->imove == 2 ? c->pbuf[1][1] : c->py;
+  const double* kz = c->imove == 2 ? c->pbuf[1][2] : c->pz;
+  k_mark_particles<<<g, 256, 0, st>>>(kx, ky, kz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
                                       c->cap_bricks, c->lay, c->type, c->depth, keep, c->ds, 0); MAC_COUNT(c);
   k_note_missing<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   alloc_new(c);
   k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
-  k_mark_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
+  k_mark_particles<<<g, 256, 0, st>>>(kx, ky, kz, c->dp, c->hkeys, c->hval, c->hcap, c->newslots,
                                       c->cap_bricks, c->lay, c->type, c->depth, keep, c->ds, 1); MAC_COUNT(c);
   k_clear_note<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   if (keep) {
-    k_compact_particles<<<g, 256, 0, st>>>(c->px, c->py, c->pz, keep, c->px2, c->py2, c->pz2, c->ds); MAC_COUNT(c);
+    PartMove M;
+    M.src[0] = c->px; M.src[1] = c->py; M.src[2] = c->pz;
+    M.dst[0] = c->px2; M.dst[1] = c->py2; M.dst[2] = c->pz2;
+    M.n = 3;
+    if (c->dp.pipeline == 1) {
+      for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 3; ++i) {
+          M.src[3 + 3 * k + i] = c->pbuf[k][i];
+          M.dst[3 + 3 * k + i] = c->pbuf2[k][i];
+        }
+      M.n = 9;
+    }
+    k_compact_particles<<<g, 256, 0, st>>>(M, keep, c->ds); MAC_COUNT(c);
     k_compact_particles_done<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
     std::swap(c->px, c->px2);
     std::swap(c->py, c->py2);
     std::swap(c->pz, c->pz2);
+    if (c->dp.pipeline == 1)
+      for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 3; ++i) std::swap(c->pbuf[k][i], c->pbuf2[k][i]);
   }
   c->system_ready = false;
   return check(cudaGetLastError());
@@ -678,7 +710,7 @@ int topo_layer_initial(Ctx* c) {
 
 int topo_create_fluid(Ctx* c) {
   k_refill<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->bkey, c->lay, c->type, c->depth, c->px, c->py, c->pz,
-                                                c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds); MAC_COUNT(c);
+                                                c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds, 0); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
@@ -750,6 +782,21 @@ int topo_finish(Ctx* c) {
   int rc = read_scalars(c);
   c->stats.fluid_cells = c->hs->nfluid;
   return rc;
+}
+
+// init2 of pipeline B's stages (test/Jet3.cpp:549): the depth topology with
+// Create_Interior_Depth and no time step, at the current particle buffer.
+int topology_stage(Ctx* c) {
+  int rc;
+  prof_begin(c, PH_TOPOLOGY);
+  if ((rc = topo_initialize(c))) return rc;
+  if ((rc = topo_layer_initial(c))) return rc;
+  k_refill<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->bkey, c->lay, c->type, c->depth, c->px, c->py, c->pz,
+                                                c->cap_particles, (unsigned long long)c->seed, c->dp, c->ds, 1); MAC_COUNT(c);
+  if ((rc = topo_update_layer(c))) return rc;
+  if ((rc = topo_delete(c))) return rc;
+  prof_end(c, PH_TOPOLOGY);
+  return read_scalars(c);  // live bricks and particles; the fluid count stays the step's
 }
 
 int topology_rebuild(Ctx* c, bool first_init_order) {

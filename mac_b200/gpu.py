@@ -36,7 +36,7 @@ class mac_params(ctypes.Structure):
                 ("max_bricks", ctypes.c_int64), ("max_particles", ctypes.c_int64), ("device", ctypes.c_int32),
                 ("div_check", ctypes.c_int32), ("viscosity", ctypes.c_double), ("depth_mode", ctypes.c_int32),
                 ("depth_max", ctypes.c_int32), ("depth_interior", ctypes.c_int32), ("depth_remove", ctypes.c_int32),
-                ("refill_cube", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
+                ("refill_cube", ctypes.c_int32), ("pipeline", ctypes.c_int32)]
 
 
 _P = ctypes.POINTER
@@ -62,7 +62,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_upload_state", "mac_query_sizes", "mac_download_state", "mac_initialize_maccell",
            "mac_layer_initial_with_particle", "mac_create_fluid_particle", "mac_update_celltype_layer",
            "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
-           "mac_pressure_project", "mac_rk2tvd", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
+           "mac_pressure_project", "mac_rk2tvd", "mac_rungekutta_all", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
            "mac_stream", "mac_launch_count", "mac_set_profiling", "mac_get_profile",
            "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc",
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
@@ -96,6 +96,7 @@ def load(path: str = LIB_PATH):
     lib.mac_download_state.argtypes = [vp, _P(mac_host_state)]
     for n in ["mac_initialize_maccell", "mac_layer_initial_with_particle", "mac_create_fluid_particle",
               "mac_update_celltype_layer", "mac_delete_maccell", "mac_topology_rebuild", "mac_rk2tvd",
+              "mac_rungekutta_all",
               "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync", "mac_csc_clean"]:
         getattr(lib, n).argtypes = [vp]
     lib.mac_calculate_time_step.argtypes = [vp, _P(ctypes.c_double)]
@@ -159,7 +160,7 @@ def make_params(pr: Params, max_bricks: int, max_particles: int, solver="mgpcg64
     p.device = device
     p.div_check = int(div_check)
     p.viscosity = float(getattr(pr, "viscosity", 0.0))
-    for k in ("depth_mode", "depth_max", "depth_interior", "depth_remove", "refill_cube"):
+    for k in ("depth_mode", "depth_max", "depth_interior", "depth_remove", "refill_cube", "pipeline"):
         setattr(p, k, int(getattr(pr, k, 0)))
     return p
 
@@ -334,6 +335,11 @@ class Context:
 
     def rk2tvd(self, allow_not_converged=False):
         return self._check(self.lib.mac_rk2tvd(self.h), "mac_rk2tvd", allow=(-4,) if allow_not_converged else ())
+
+    def rungekutta_all(self, allow_not_converged=False):
+        """Algorithms_RungeKutta_all of pipeline B (contexts created with pipeline=1)."""
+        return self._check(self.lib.mac_rungekutta_all(self.h), "mac_rungekutta_all",
+                           allow=(-4,) if allow_not_converged else ())
 
     def extrapolate(self):
         return self._check(self.lib.mac_extrapolate(self.h), "mac_extrapolate")

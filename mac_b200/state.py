@@ -62,6 +62,9 @@ class Params:
     depth_remove: int = 0
     # inflow refill: 0 = 8 jittered particles, n >= 1 = Policy_Add_Particle_Cube(n)
     refill_cube: int = 0
+    # 0: pipeline A step (RK2-TVD); 1: pipeline B step (Algorithms_RungeKutta_all),
+    # a run-time choice, not stored in state files
+    pipeline: int = 0
 
 
 @dataclasses.dataclass
