@@ -214,22 +214,90 @@ __device__ inline int64_t lidx(const int* __restrict__ nbr, int b, int x, int y,
   return (int64_t)nb * (D * D * D) + (x - D * dx) + D * (y - D * dy) + D * D * (z - D * dz);
 }
 
+// Brick-level kernels run 256 threads over 256 / D^3 bricks; the bricks and
+// their six face neighbours are read once per block into shared memory, so no
+// thread chains a brick-table load before its own loads.
+template <int D>
+struct LBricks {
+  static constexpr int N = D * D * D;
+  static constexpr int BPB = 256 / N;  // bricks per block
+};
+
+// sbr[7 * j + k]: local brick j's pool index (k = 0) and its face neighbours
+// -x, +x, -y, +y, -z, +z (k = 1..6), -1 when absent or past the list.
+template <int D>
+__device__ inline void load_lbricks(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr, int* sbr) {
+  constexpr int BPB = LBricks<D>::BPB;
+  for (int t = threadIdx.x; t < 7 * BPB; t += blockDim.x) {
+    const int j = t / 7, k = t % 7;
+    const int gb = blockIdx.x * BPB + j;
+    int v = -1;
+    if (gb < nd) {
+      const int b = dbl[gb];
+      if (k == 0) {
+        v = b;
+      } else {
+        const int f = k - 1;
+        const int d = (f & 1) ? 1 : -1;
+        const int ax = f >> 1;
+        v = nbr[(size_t)b * kNbr + nbr_index(ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0)];
+      }
+    }
+    sbr[t] = v;
+  }
+}
+
+// Pool index of cell (x, y, z) of local brick row sb (coordinates may leave the
+// brick by one cell along one axis), -1 if that brick is absent.
+template <int D>
+__device__ inline int64_t lidx_s(const int* sb, int x, int y, int z) {
+  int k = 0;
+  if (x < 0) { k = 1; x += D; }
+  else if (x >= D) { k = 2; x -= D; }
+  else if (y < 0) { k = 3; y += D; }
+  else if (y >= D) { k = 4; y -= D; }
+  else if (z < 0) { k = 5; z += D; }
+  else if (z >= D) { k = 6; z -= D; }
+  const int nb = sb[k];
+  if (nb < 0) return -1;
+  return (int64_t)nb * (D * D * D) + x + D * y + D * D * z;
+}
+
 // Weights w: 6 slots of ncap entries: [0..2] left faces, [3] diagonal, [4] inverse, [5] Dirichlet part.
-template <class T, int D>
-__device__ inline double apply_l(const T* __restrict__ e, const T* __restrict__ w, size_t ncap,
-                                 const int* __restrict__ nbr, int b, int x, int y, int z, size_t i, double ec) {
-  double s = (double)w[3 * ncap + i] * ec;
+// The six neighbour indices of cell (x, y, z) (-1 absent): [2a] = -e_a, [2a+1] = +e_a.
+template <int D>
+__device__ inline void lnbrs(const int* sb, int x, int y, int z, int64_t* n) {
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double wl = (double)w[a * ncap + i];
     int p[3] = {x, y, z};
     p[a] -= 1;
-    if (wl != 0) s -= wl * (double)e[lidx<D>(nbr, b, p[0], p[1], p[2])];
+    n[2 * a] = lidx_s<D>(sb, p[0], p[1], p[2]);
     p[a] += 2;
-    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
-    if (n >= 0) {
-      double wr = (double)w[a * ncap + n];
-      if (wr != 0) s -= wr * (double)e[n];
-    }
+    n[2 * a + 1] = lidx_s<D>(sb, p[0], p[1], p[2]);
+  }
+}
+
+// M e at cell i: every load is issued before any term is tested (a missing
+// neighbour reads cell i itself and drops out through its zero weight), then
+// the terms are summed in the fixed order.
+template <class T, int D>
+__device__ inline double apply_l(const T* __restrict__ e, const T* __restrict__ w, size_t ncap,
+                                 const int64_t* n, size_t i, double ec) {
+  double wl[3], wr[3], el[3], er[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
+    const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+    wl[a] = (double)w[a * ncap + i];
+    el[a] = (double)e[jl];
+    wr[a] = n[2 * a + 1] < 0 ? 0.0 : (double)w[a * ncap + jr];
+    er[a] = (double)e[jr];
+  }
+  double s = (double)w[3 * ncap + i] * ec;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (wl[a] != 0) s -= wl[a] * el[a];
+    if (wr[a] != 0) s -= wr[a] * er[a];
   }
   return s;
 }
@@ -239,9 +307,13 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
                                               T* __restrict__ e) {
   constexpr int N = D * D * D;
+  __shared__ int sbr[7 * LBricks<D>::BPB];
+  load_lbricks<D>(dbl, nd, nbr, sbr);
+  __syncthreads();
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= (int64_t)nd * N) return;
-  int b = dbl[g / N];
+  const int* sb = sbr + 7 * (threadIdx.x / N);
+  int b = sb[0];
   int o = (int)(g % N);
   size_t i = (size_t)b * N + o;
   double dinv = (double)w[4 * ncap + i];
@@ -250,21 +322,25 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
     return;
   }
   int x = o % D, y = (o / D) % D, z = o / (D * D);
-  double s = (2.0 - kOmega) * (double)r[i];
+  int64_t n[6];
+  lnbrs<D>(sb, x, y, z, n);
+  double wl[3], wr[3], dl[3], dr[3], rl[3], rr[3];
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double wl = (double)w[a * ncap + i];
-    int p[3] = {x, y, z};
-    p[a] -= 1;
-    if (wl != 0) {
-      int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
-      s += wl * kOmega * (double)w[4 * ncap + n] * (double)r[n];
-    }
-    p[a] += 2;
-    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
-    if (n >= 0) {
-      double wr = (double)w[a * ncap + n];
-      if (wr != 0) s += wr * kOmega * (double)w[4 * ncap + n] * (double)r[n];
-    }
+    const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
+    const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+    wl[a] = (double)w[a * ncap + i];
+    dl[a] = (double)w[4 * ncap + jl];
+    rl[a] = (double)r[jl];
+    wr[a] = n[2 * a + 1] < 0 ? 0.0 : (double)w[a * ncap + jr];
+    dr[a] = (double)w[4 * ncap + jr];
+    rr[a] = (double)r[jr];
+  }
+  double s = (2.0 - kOmega) * (double)r[i];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (wl[a] != 0) s += wl[a] * kOmega * dl[a] * rl[a];
+    if (wr[a] != 0) s += wr[a] * kOmega * dr[a] * rr[a];
   }
   e[i] = (T)(kOmega * dinv * s);
 }
@@ -287,20 +363,27 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
                                                    DenseGrid g3) {
   constexpr int H = D / 2;
   constexpr int N = D * D * D;
+  __shared__ int sbr[7 * LBricks<D>::BPB];
+  load_lbricks<D>(dbl, nd, nbr, sbr);
+  __syncthreads();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = g < (int64_t)nd * N;  // nd * N is a multiple of 8: groups are whole
+  const int* sb = sbr + 7 * (threadIdx.x / N);
   double v = 0;
   int b = 0, p = 0;
   if (live) {
-    b = dbl[g / N];
+    b = sb[0];
     const int o = (int)(g % N);
     p = o >> 3;
     const int k = o & 7;
     const int X = p % H, Y = (p / H) % H, Z = p / (H * H);
     const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
     const size_t i = (size_t)b * N + x + D * y + D * D * z;
-    if ((double)w[4 * ncap + i] != 0)
-      v = (double)r[i] - apply_l<T, D>(e, w, ncap, nbr, b, x, y, z, i, (double)e[i]);
+    if ((double)w[4 * ncap + i] != 0) {
+      int64_t n[6];
+      lnbrs<D>(sb, x, y, z, n);
+      v = (double)r[i] - apply_l<T, D>(e, w, ncap, n, i, (double)e[i]);
+    }
   }
   v = sum8(v);
   if (live && (threadIdx.x & 7) == 0) {
@@ -318,9 +401,21 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
                                                  const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3) {
   constexpr int N = D * D * D;
   constexpr int H = D / 2;
+  __shared__ int sbr[7 * LBricks<D>::BPB];
+  __shared__ int64_t sdi[7 * LBricks<D>::BPB];  // D = 2: dense level-3 index of each table brick
+  load_lbricks<D>(dbl, nd, nbr, sbr);
+  __syncthreads();
+  if (WITH_COARSE && D == 2) {
+    for (int t = threadIdx.x; t < 7 * LBricks<D>::BPB; t += blockDim.x) {
+      const int bb = sbr[t];
+      sdi[t] = bb < 0 ? 0 : g3.index(bkey[3 * bb], bkey[3 * bb + 1], bkey[3 * bb + 2]);
+    }
+    __syncthreads();
+  }
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= (int64_t)nd * N) return;
-  int b = dbl[g / N];
+  const int* sb = sbr + 7 * (threadIdx.x / N);
+  int b = sb[0];
   int o = (int)(g % N);
   size_t i = (size_t)b * N + o;
   double dinv = (double)w[4 * ncap + i];
@@ -329,33 +424,48 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     return;
   }
   int x = o % D, y = (o / D) % D, z = o / (D * D);
-  auto ev = [&](int64_t n) -> double {
-    double v = (double)e[n];
+  // slot of each neighbour's brick in the shared table (0 = this brick)
+  int64_t n[6];
+  int k[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int c[3] = {x, y, z};
+    n[2 * a] = lidx_s<D>(sb, a == 0 ? x - 1 : x, a == 1 ? y - 1 : y, a == 2 ? z - 1 : z);
+    n[2 * a + 1] = lidx_s<D>(sb, a == 0 ? x + 1 : x, a == 1 ? y + 1 : y, a == 2 ? z + 1 : z);
+    k[2 * a] = c[a] == 0 ? 1 + 2 * a : 0;
+    k[2 * a + 1] = c[a] == D - 1 ? 2 + 2 * a : 0;
+  }
+  // e plus the coarse correction at cell j of the brick in slot kk
+  auto ev = [&](int64_t j, int kk) -> double {
+    double v = (double)e[j];
     if (WITH_COARSE) {
-      int nb = (int)(n / N);
-      int no = (int)(n % N);
       if (D == 2) {
-        v += (double)ec[g3.index(bkey[3 * nb], bkey[3 * nb + 1], bkey[3 * nb + 2])];
+        v += (double)ec[sdi[7 * (threadIdx.x / N) + kk]];
       } else {
-        int xx = no % D, yy = (no / D) % D, zz = no / (D * D);
+        const int nb = (int)(j / N), no = (int)(j % N);
+        const int xx = no % D, yy = (no / D) % D, zz = no / (D * D);
         v += (double)ec[(size_t)nb * H * H * H + (xx >> 1) + H * (yy >> 1) + H * H * (zz >> 1)];
       }
     }
     return v;
   };
-  double ecc = ev((int64_t)i);
-  double s = (double)w[3 * ncap + i] * ecc;
+  double wl[3], wr[3], vl[3], vr[3];
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double wl = (double)w[a * ncap + i];
-    int p[3] = {x, y, z};
-    p[a] -= 1;
-    if (wl != 0) s -= wl * ev(lidx<D>(nbr, b, p[0], p[1], p[2]));
-    p[a] += 2;
-    int64_t n = lidx<D>(nbr, b, p[0], p[1], p[2]);
-    if (n >= 0) {
-      double wr = (double)w[a * ncap + n];
-      if (wr != 0) s -= wr * ev(n);
-    }
+    const bool hl = n[2 * a] >= 0, hr = n[2 * a + 1] >= 0;
+    const int64_t jl = hl ? n[2 * a] : (int64_t)i;
+    const int64_t jr = hr ? n[2 * a + 1] : (int64_t)i;
+    wl[a] = (double)w[a * ncap + i];
+    vl[a] = ev(jl, hl ? k[2 * a] : 0);
+    wr[a] = hr ? (double)w[a * ncap + jr] : 0.0;
+    vr[a] = ev(jr, hr ? k[2 * a + 1] : 0);
+  }
+  double ecc = ev((int64_t)i, 0);
+  double s = (double)w[3 * ncap + i] * ecc;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (wl[a] != 0) s -= wl[a] * vl[a];
+    if (wr[a] != 0) s -= wr[a] * vr[a];
   }
   eout[i] = (T)(ecc + kOmega * dinv * ((double)r[i] - s));
 }
