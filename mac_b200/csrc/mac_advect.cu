@@ -511,31 +511,64 @@ __device__ inline void rk4(double* pos, const F& field, const Params& P, double 
   for (int i = 0; i < 3; ++i) pos[i] = res[i];
 }
 
-// Particles are binned by the brick of their cell each step (counting sort,
-// order inside a brick unspecified; every particle moves independently, so
-// the order changes no result).
+// Particles are binned by the brick of their cell each step, and inside a
+// brick's bin by cell (counting sort over 512 * brick + cell; the order inside
+// a cell is unspecified). Every particle moves independently, so the order
+// changes no result; cell order makes the lanes of a warp read the same
+// staged stencil values, which shared memory serves as broadcasts.
 __global__ void k_bin_count(const double* __restrict__ px, const double* __restrict__ py,
                             const double* __restrict__ pz, int64_t np, Params P,
                             const unsigned long long* __restrict__ hk, const int* __restrict__ hv, int64_t hcap,
-                            int* pbrick, int* bcount, int stray) {
-  // Whole warps iterate together so the lanes that share a brick can add
-  // their count with one atomic (the array is mostly sorted by brick already).
+                            int* pbrick, int* ccount, int stray) {
+  // Whole warps iterate together so the lanes that share a cell can add their
+  // count with one atomic (the array stays mostly sorted from the last step).
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < np; q0 += stride) {
     int64_t q = q0 + (threadIdx.x & 31);
-    int b = -2;
+    int key = -2;
     if (q < np) {
-      int bx = fdiv8((int)lround(px[q] * P.ih[0]));
-      int by = fdiv8((int)lround(py[q] * P.ih[1]));
-      int bz = fdiv8((int)lround(pz[q] * P.ih[2]));
-      b = hash_find(hk, hv, hcap, pack_key(bx, by, bz));
-      if (b < 0) b = stray;
-      pbrick[q] = b;
+      const int kx = (int)lround(px[q] * P.ih[0]);
+      const int ky = (int)lround(py[q] * P.ih[1]);
+      const int kz = (int)lround(pz[q] * P.ih[2]);
+      int b = hash_find(hk, hv, hcap, pack_key(fdiv8(kx), fdiv8(ky), fdiv8(kz)));
+      key = b < 0 ? stray * kCells : b * kCells + (kx & 7) + 8 * (ky & 7) + 64 * (kz & 7);
+      pbrick[q] = key;
     }
-    unsigned peers = __match_any_sync(0xffffffffu, b);
+    unsigned peers = __match_any_sync(0xffffffffu, key);
     int leader = __ffs(peers) - 1;
-    if (b >= 0 && (int)(threadIdx.x & 31) == leader) atomicAdd(&bcount[b], __popc(peers));
+    if (key >= 0 && (int)(threadIdx.x & 31) == leader) atomicAdd(&ccount[key], __popc(peers));
   }
+}
+
+// Per brick of the live list (and the no-brick slot in the last block):
+// exclusive scan of its 512 cell counts in place, and the brick total.
+__global__ void __launch_bounds__(512) k_cell_scan(const int* __restrict__ blist, int nlive, int stray, int* ccount,
+                                                   int* bcount) {
+  __shared__ int ws[16];
+  const int b = blockIdx.x < nlive ? blist[blockIdx.x] : stray;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int v = ccount[(size_t)b * kCells + t];
+  int x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < 16 ? ws[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < 16; d <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += y;
+    }
+    if (lane < 16) ws[lane] = w;
+  }
+  __syncthreads();
+  const int incl = x + (wid > 0 ? ws[wid - 1] : 0);
+  ccount[(size_t)b * kCells + t] = incl - v;
+  if (t == kCells - 1) bcount[b] = incl;
 }
 
 // Exclusive scan of n counts (one block of 1024 threads).
@@ -568,14 +601,14 @@ __global__ void k_bin_scatter(const double* __restrict__ px, const double* __res
   int lane = threadIdx.x & 31;
   for (int64_t q0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); q0 < np; q0 += stride) {
     int64_t q = q0 + lane;
-    int b = q < np ? pbrick[q] : -2;
-    unsigned peers = __match_any_sync(0xffffffffu, b);
+    int key = q < np ? pbrick[q] : -2;
+    unsigned peers = __match_any_sync(0xffffffffu, key);
     int leader = __ffs(peers) - 1;
     int base = 0;
-    if (b >= 0 && lane == leader) base = atomicAdd(&cursor[b], __popc(peers));
+    if (key >= 0 && lane == leader) base = atomicAdd(&cursor[key], __popc(peers));
     base = __shfl_sync(0xffffffffu, base, leader);
-    if (b >= 0) {
-      int64_t pos = off[b] + base + __popc(peers & ((1u << lane) - 1));
+    if (key >= 0) {
+      int64_t pos = off[key / kCells] + base + __popc(peers & ((1u << lane) - 1));
       qx[pos] = px[q];
       qy[pos] = py[q];
       qz[pos] = pz[q];
@@ -832,10 +865,11 @@ int move_particles(Ctx* c) {
   unsigned long long* bad = &c->ds->bad_reads;
   prof_begin(c, PH_MOVE);
   int rc = check(cudaMemsetAsync(c->bcount, 0, sizeof(int) * (c->cap_bricks + 1), st));
-  if (!rc) rc = check(cudaMemsetAsync(c->bcursor, 0, sizeof(int) * (c->cap_bricks + 1), st));
+  if (!rc) rc = check(cudaMemsetAsync(c->bcursor, 0, sizeof(int) * (c->cap_bricks + 1) * kCells, st));
   if (rc) return rc;
-  k_bin_count<<<g, 256, 0, st>>>(c->px, c->py, c->pz, np, c->dp, c->hkeys, c->hval, c->hcap, c->pbrick, c->bcount,
+  k_bin_count<<<g, 256, 0, st>>>(c->px, c->py, c->pz, np, c->dp, c->hkeys, c->hval, c->hcap, c->pbrick, c->bcursor,
                                  stray); MAC_COUNT(c);
+  k_cell_scan<<<c->nlive_host + 1, kCells, 0, st>>>(c->blist, c->nlive_host, stray, c->bcursor, c->bcount); MAC_COUNT(c);
   k_bin_scan<<<1, 1024, 0, st>>>(c->bcount, c->boff, stray + 1); MAC_COUNT(c);
   k_bin_scatter<<<g, 256, 0, st>>>(c->px, c->py, c->pz, np, c->pbrick, c->boff, c->bcursor, c->px2, c->py2,
                                    c->pz2); MAC_COUNT(c);

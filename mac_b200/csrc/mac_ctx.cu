@@ -276,7 +276,7 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->pz2, c->cap_particles));
   A(dalloc(&c->pbrick, c->cap_particles));
   A(dalloc(&c->bcount, c->cap_bricks + 1));
-  A(dalloc(&c->bcursor, c->cap_bricks + 1));
+  A(dalloc(&c->bcursor, (size_t)(c->cap_bricks + 1) * kCells));
   A(dalloc(&c->boff, c->cap_bricks + 2));
   A(dalloc(&c->ds, 1));
   if (rc == MAC_OK) A(check(cudaMallocHost((void**)&c->hs, sizeof(Scalars))));

@@ -158,9 +158,9 @@ struct Ctx {
   double* px2 = nullptr;      // binned copy (swapped with px each move)
   double* py2 = nullptr;
   double* pz2 = nullptr;
-  int* pbrick = nullptr;      // brick of each particle's cell
+  int* pbrick = nullptr;      // 512 * brick + cell of each particle's cell (brick cap: no brick)
   int* bcount = nullptr;      // [cap+1] particles per brick (last: no brick)
-  int* bcursor = nullptr;     // [cap+1]
+  int* bcursor = nullptr;     // [(cap+1)*512] particles per (brick, cell), then each cell's running slot
   int64_t* boff = nullptr;    // [cap+2] bin offsets
   // pressure system and solver
   uint16_t* fmask = nullptr;  // [cap*512] face classes of the level-0 operator
