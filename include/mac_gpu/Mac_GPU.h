@@ -20,7 +20,12 @@
  * and unpacks it again when Algorithms_To_Host_GPU runs (before any host
  * algorithm, output or checkpoint that reads the world). Requires a chunk edge
  * N = 8 (the device bricks are 8^3) and the four-material cell type
- * (src/Data_CellType_Fluid_Air_Solid_Inflow.h).
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow.h), or the cell type of the depth
+ * composition (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.h, whose
+ * 0-pressure material no algorithm sets) with a Data_Chunk_Depth: the session
+ * detects the interior material and the depth chunk and carries both, so
+ * mac_params.depth_mode / .pipeline worlds (test/Jet3.cpp) run through the
+ * same classes plus Algorithms_RungeKutta_all_GPU.
  *
  * Errors follow the reference's convention for its solver policy
  * (src/Policy_Solve_Linear_Umfpack.h:15-21): the status is printed and the run
@@ -48,6 +53,60 @@ inline int report(int rc, const char* what) {
 }
 
 inline int chunk_of(int v) { return v >= 0 ? v / MAC_BRICK_EDGE : (v + 1) / MAC_BRICK_EDGE - 1; }
+
+/* Whether the cell type's material enum has the interior material
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.h). */
+template <class M, class = void>
+struct has_interior : std::false_type {};
+template <class M>
+struct has_interior<M, decltype((void)M::Interior)> : std::true_type {};
+
+template <class M>
+uint8_t interior_or_air(M m, std::true_type) { return m == M::Interior ? (uint8_t)MAC_CELL_INTERIOR : (uint8_t)MAC_CELL_AIR; }
+template <class M>
+uint8_t interior_or_air(M, std::false_type) { return MAC_CELL_AIR; }
+template <class M>
+M interior_material(std::true_type) { return M::Interior; }
+template <class M>
+M interior_material(std::false_type) { return M::Air; }
+
+/* Material to MAC_CELL_* (MaterialToInt, src/Data_CellType_Fluid_Air_Solid_Inflow.tpp:3-18). */
+template <class M>
+uint8_t to_code(M m) {
+  if (m == M::Fluid) return MAC_CELL_FLUID;
+  if (m == M::Solid) return MAC_CELL_SOLID;
+  if (m == M::Inflow) return MAC_CELL_INFLOW;
+  return interior_or_air(m, has_interior<M>());
+}
+template <class M>
+M from_code(uint8_t c) {
+  switch (c) {
+    case MAC_CELL_FLUID: return M::Fluid;
+    case MAC_CELL_SOLID: return M::Solid;
+    case MAC_CELL_INFLOW: return M::Inflow;
+    case MAC_CELL_INTERIOR: return interior_material<M>(has_interior<M>());
+    default: return M::Air;
+  }
+}
+
+/* Whether the world's chunk carries a depth (src/Data_Chunk_Depth.h). */
+template <class C, class = void>
+struct has_depth : std::false_type {};
+template <class C>
+struct has_depth<C, decltype((void)std::declval<C&>().Depth_GetPointer())> : std::true_type {};
+
+template <class C>
+void pack_depth(C& ch, int32_t* d, std::true_type) {
+  for (int o = 0; o < MAC_BRICK_CELLS; ++o) d[o] = ch.Depth_GetPointer()[o].GetDepth();
+}
+template <class C>
+void pack_depth(C&, int32_t*, std::false_type) {}
+template <class C>
+void unpack_depth(C& ch, const int32_t* d, std::true_type) {
+  for (int o = 0; o < MAC_BRICK_CELLS; ++o) ch.Depth_GetPointer()[o].SetDepth(d[o]);
+}
+template <class C>
+void unpack_depth(C&, const int32_t*, std::false_type) {}
 
 }  // namespace mac_gpu_detail
 
@@ -108,6 +167,9 @@ class Mac_GPU_Session {
   typedef typename type_Data_Topology::type_particle_list type_particle_list;
   typedef typename type_Data_Topology::type_particle type_particle;
   typedef typename type_particle::type_data_vector type_data_vector;
+  typedef typename std::remove_reference<decltype(
+      std::declval<type_Data_Grid&>().DirectAcessChunk(std::declval<const type_key&>()))>::type type_chunk;
+  typedef mac_gpu_detail::has_depth<type_chunk> type_has_depth;
 
   DataRef m_data;
   void* m_ctx = nullptr;
@@ -122,7 +184,7 @@ class Mac_GPU_Session {
   }
 
   struct Host {
-    std::vector<int32_t> keys, layer;
+    std::vector<int32_t> keys, layer, depth;
     std::vector<uint8_t> exists, flags, type;
     std::vector<double> f[10], pos;  // u0x..u1z, ax..az, p
     mac_host_state view{};
@@ -147,7 +209,8 @@ class Mac_GPU_Session {
       view.type = type.data();
       view.layer = layer.data();
       view.pos = pos.data();
-      view.depth = nullptr;  // the reference world of this layer carries no depth
+      depth.assign(type_has_depth::value ? nc : 0, -1);
+      view.depth = type_has_depth::value ? depth.data() : nullptr;
     }
   };
 
@@ -206,12 +269,11 @@ class Mac_GPU_Session {
         auto& ct = ch.CellType_GetPointer()[o];
         if (ct.GetIsNoDelete()) fl |= MAC_FLAG_NODELETE;
         h.flags[i] = fl;
-        typedef typename std::remove_reference<decltype(ct)>::type::Material_Type Mat;
-        h.type[i] = ct.m_mat == Mat::Fluid ? MAC_CELL_FLUID
-                    : ct.m_mat == Mat::Solid ? MAC_CELL_SOLID
-                    : ct.m_mat == Mat::Inflow ? MAC_CELL_INFLOW : MAC_CELL_AIR;
+        h.type[i] = mac_gpu_detail::to_code(ct.m_mat);
         h.layer[i] = ch.Layer_GetPointer()[o].GetLayer();
       }
+      if (type_has_depth::value)
+        mac_gpu_detail::pack_depth(ch, h.depth.data() + (size_t)b * MAC_BRICK_CELLS, type_has_depth());
       ++b;
     }
     int64_t q = 0;
@@ -283,15 +345,12 @@ class Mac_GPU_Session {
         ch.Pressure_GetPointer()[o].Pressure_Set(h.f[9][i]);
         auto& ct = ch.CellType_GetPointer()[o];
         typedef typename std::remove_reference<decltype(ct)>::type::Material_Type Mat;
-        switch (h.type[i]) {
-          case MAC_CELL_FLUID: ct.m_mat = Mat::Fluid; break;
-          case MAC_CELL_SOLID: ct.m_mat = Mat::Solid; break;
-          case MAC_CELL_INFLOW: ct.m_mat = Mat::Inflow; break;
-          default: ct.m_mat = Mat::Air; break;
-        }
+        ct.m_mat = mac_gpu_detail::from_code<Mat>(h.type[i]);
         ct.SetIsNoDelete((h.flags[i] & MAC_FLAG_NODELETE) != 0);
         ch.Layer_GetPointer()[o].SetLayer(h.layer[i]);
       }
+      if (type_has_depth::value)
+        mac_gpu_detail::unpack_depth(ch, h.depth.data() + (size_t)b * MAC_BRICK_CELLS, type_has_depth());
     }
     type_particle_list& plist = m_data.m_data.GetTopologyData().GetRefToParticleList();
     while (plist.size()) plist.pop_back();
@@ -365,7 +424,11 @@ MAC_GPU_ALGORITHM(Algorithms_RungeKutta_RK2_TVD_GPU, mac_rk2tvd(c))
 MAC_GPU_ALGORITHM(Algorithms_Extrapolate_GPU, mac_extrapolate(c))
 /* src/Algorithms_Move_Particles.h:22-36 */
 MAC_GPU_ALGORITHM(Algorithms_Move_Particles_GPU, mac_move_particles(c))
-/* One pipeline-A step, test/TestJetDEau_Basic.cpp:434-441 (t += dt included). */
+/* src/Algorithms_RungeKutta_all.h:35-156 with the policy of test/Jet3.cpp:642-675
+ * (a context created with mac_params.pipeline = 1) */
+MAC_GPU_ALGORITHM(Algorithms_RungeKutta_all_GPU, mac_rungekutta_all(c))
+/* One step: pipeline A, test/TestJetDEau_Basic.cpp:434-441 (t += dt included),
+ * or, with mac_params.pipeline = 1, pipeline B, test/Jet3.cpp:720-726. */
 MAC_GPU_ALGORITHM(Algorithms_Step_GPU, mac_step(c))
 
 #undef MAC_GPU_ALGORITHM

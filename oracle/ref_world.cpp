@@ -674,6 +674,14 @@ static int run(int argc, char** argv) {
   gprm.layer_max = st.hdr.layer_max;
   gprm.interp_symmetric = st.hdr.interp_symmetric;
   gprm.viscosity = st.hdr.viscosity;
+  gprm.depth_mode = st.hdr.depth_mode;
+  gprm.depth_max = st.hdr.depth_max;
+  gprm.depth_interior = st.hdr.depth_interior;
+  gprm.depth_remove = st.hdr.depth_remove;
+  gprm.refill_cube = st.hdr.refill_cube;
+#ifdef MAC_PIPELINE_B
+  gprm.pipeline = 1;  // Algorithms_Step_GPU runs the pipeline-B step of this world
+#endif
   gprm.rtol = g_cg_rtol;
   gprm.max_iters = 5000;
   gprm.max_bricks = 8192;

@@ -2,7 +2,10 @@
 world: oracle/_ref/mac_ref_gpu composes the unmodified reference headers and
 swaps in (a) Policy_Solve_Linear_GPU as the solver policy of the reference's
 Algorithms_Solve_Pressure, (b) Algorithms_Step_GPU + Algorithms_To_Host_GPU for
-the pipeline-A step. Results are compared with the reference's own outputs
+the pipeline-A step. oracle/_ref/mac_ref_b_gpu is the depth world of
+test/Jet3.cpp (interior cells, depth chunk, three speed buffers) whose
+Algorithms_Step_GPU runs pipeline B: the session carries the interior material
+and the depths across. Results are compared with the reference's own outputs
 (committed fixtures) at the tolerances of the device parity tests.
 
 The binary is built from the reference sources by oracle/Makefile (target
@@ -23,13 +26,16 @@ P_TOL = 1e-9
 U_TOL = 1e-10
 
 
-def _run(cmd, state, tmp_path, n=None, rtol="1e-13"):
+BIN_B = os.path.join(HERE, "..", "oracle", "_ref", "mac_ref_b_gpu")
+
+
+def _run(cmd, state, tmp_path, n=None, rtol="1e-13", binary=BIN):
     from mac_b200.state import State
-    if not os.path.exists(BIN):
-        pytest.skip("oracle/_ref/mac_ref_gpu is not built (needs the reference sources)")
+    if not os.path.exists(binary):
+        pytest.skip(f"{os.path.basename(binary)} is not built (needs the reference sources)")
     src, dst = str(tmp_path / "in.state"), str(tmp_path / "out.state")
     state.write(src)
-    args = [BIN, cmd, src, dst] + ([str(n)] if n is not None else [])
+    args = [binary, cmd, src, dst] + ([str(n)] if n is not None else [])
     out = subprocess.run(args, capture_output=True, text=True, timeout=600,
                          env=dict(os.environ, MAC_REF_RTOL=rtol))
     assert out.returncode == 0, out.stderr + out.stdout
@@ -54,3 +60,15 @@ def test_reference_world_steps_on_device(golden, tmp_path):
     compare_particles(got, ref, atol=1e-12)
     assert abs(got.params.t - ref.params.t) <= 1e-15
     assert got.params.step == ref.params.step
+
+
+def test_reference_depth_world_runs_pipeline_b_on_device(golden, tmp_path):
+    s = golden("d_ref_s10")
+    s.params.viscosity = 1e-3
+    got = _run("gpustep", s, tmp_path, n=1, binary=BIN_B)
+    ref = golden("b_ref_s11")
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("p", "u0x", "u0y", "u0z"))
+    assert e["p"] <= P_TOL and max(e["u0x"], e["u0y"], e["u0z"]) <= U_TOL, e
+    compare_particles(got, ref, atol=1e-12)
+    assert abs(got.params.t - ref.params.t) <= 1e-15
