@@ -360,15 +360,17 @@ __device__ inline void stage_h1(V* s, int b, const int64_t* sb, V zero, F val) {
 
 // The same staging of a plain array: the brick's own 512 cells with 16-byte
 // vector loads (thread t takes cells 4t..4t+3, half a row), the face halos
-// with scalar loads; the values land in s as doubles.
-__device__ inline void load4(const double* p, double* v) {
+// with scalar loads; the values land in s converted to its element type S.
+template <class V>
+__device__ inline void load4(const double* p, V* v) {
   const double2 a = *reinterpret_cast<const double2*>(p);
   const double2 c = *reinterpret_cast<const double2*>(p + 2);
-  v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+  v[0] = (V)a.x; v[1] = (V)a.y; v[2] = (V)c.x; v[3] = (V)c.y;
 }
-__device__ inline void load4(const float* p, double* v) {
+template <class V>
+__device__ inline void load4(const float* p, V* v) {
   const float4 a = *reinterpret_cast<const float4*>(p);
-  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[0] = (V)a.x; v[1] = (V)a.y; v[2] = (V)a.z; v[3] = (V)a.w;
 }
 
 // Only the face halos of stage_h1 (value 0 where the neighbour brick is absent).
@@ -390,12 +392,12 @@ __device__ inline void stage_h1_halo(double* s, const int64_t* sb, F val) {
   }
 }
 
-template <class T>
-__device__ inline void stage_arr(double* s, const T* __restrict__ a, int b, const int64_t* sb) {
+template <class S, class T>
+__device__ inline void stage_arr(S* s, const T* __restrict__ a, int b, const int64_t* sb) {
   static_assert(kBT * 4 == kCells, "one 4-cell vector per thread");
   {
     const int o = 4 * threadIdx.x;
-    double v[4];
+    S v[4];
     load4(a + (int64_t)b * kCells + o, v);
     const int si = s1_of(o);
 #pragma unroll
@@ -413,7 +415,7 @@ __device__ inline void stage_arr(double* s, const T* __restrict__ a, int b, cons
       case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
       default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
     }
-    s[s1(x, y, z)] = gi < 0 ? 0.0 : (double)a[gi];
+    s[s1(x, y, z)] = gi < 0 ? (S)0 : (S)a[gi];
   }
 }
 

@@ -12,7 +12,9 @@
 // Smoother: weighted Jacobi (two sweeps before and after the coarse
 // correction); the levels from 4 down are solved by one thread block in
 // shared memory, the coarsest (at most 64 cells) exactly with an inverse built
-// at set-up. Storage type T is double (plain form) or float (mixed form).
+// at set-up. T is the storage and arithmetic type of every level: double
+// (plain form) or float (mixed form); the fine residual r and the
+// preconditioned residual z the CG iteration exchanges stay double.
 #include <cstdio>
 #include <cstring>
 
@@ -41,12 +43,13 @@ __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const
                                               const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                               T* __restrict__ e, Params P) {
   __shared__ int64_t sb[6];
-  __shared__ double sr[kS1];  // w D^-1 r of the brick and its face halo
+  __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
   __shared__ uint16_t sm[kCells];
+  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
-  stage_h1(sr, b, sb, 0.0, [&](int64_t i) { return kOmega * P.dtab[active_index(fmask[i])] * r[i]; });
+  stage_h1(sr, b, sb, (T)0, [&](int64_t i) { return om * (T)P.dtab[active_index(fmask[i])] * (T)r[i]; });
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) sm[threadIdx.x + kBT * k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
   __syncthreads();
@@ -55,17 +58,17 @@ __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
     uint16_t m = sm[o];
-    double out = 0;
+    T out = 0;
     if (m & kDomainBit) {
       int si = s1_of(o);
-      double dinv = P.dtab[active_index(m)];
-      double s = (2.0 - kOmega) * r[c];
+      T dinv = (T)P.dtab[active_index(m)];
+      T s = (T)(2.0 - kOmega) * (T)r[c];
 #pragma unroll
       for (int f = 0; f < 6; ++f)
-        if (m & (1u << f)) s += P.ih2[f >> 1] * sr[si + s1_off(f)];
-      out = kOmega * dinv * s;
+        if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
+      out = om * dinv * s;
     }
-    e[c] = (T)out;
+    e[c] = out;
   }
 }
 
@@ -75,8 +78,9 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P) {
   __shared__ int64_t sb[6];
-  __shared__ double res[kCells];
-  __shared__ double se[kS1];
+  __shared__ T res[kCells];
+  __shared__ T se[kS1];
+  const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
@@ -87,17 +91,17 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
     uint16_t m = fmask[c];
-    double v = 0;
+    T v = 0;
     if (m & kDomainBit) {
       int si = s1_of(o);
-      double ec = se[si];
-      double me = 0;
+      T ec = se[si];
+      T me = 0;
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
-        if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * ec;
-        if (m & (1u << f)) me -= P.ih2[f >> 1] * se[si + s1_off(f)];
+        if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
+        if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
       }
-      v = r[c] - me;
+      v = (T)r[c] - me;
     }
     res[o] = v;
   }
@@ -106,9 +110,9 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   if (o < 64) {
     int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
     int base = 2 * X + 16 * Y + 128 * Z;
-    double s = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] + res[base + 65] +
-               res[base + 72] + res[base + 73];
-    r1[(size_t)b * 64 + o] = (T)s;
+    T s = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] + res[base + 65] +
+          res[base + 72] + res[base + 73];
+    r1[(size_t)b * 64 + o] = s;
   }
 }
 
@@ -121,8 +125,9 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P) {
   __shared__ int64_t sb[6];
-  __shared__ double se[kS1];  // e (plus the coarse correction when FIRST) with face halo
-  __shared__ double s1p[64 + 96];  // FIRST: level-1 parents of the brick (64) and of its face halos (6 x 16)
+  __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
+  __shared__ T s1p[64 + 96];  // FIRST: level-1 parents of the brick (64) and of its face halos (6 x 16)
+  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   __syncthreads();
@@ -131,9 +136,9 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
     // parents staged once: own level-1 cells, then for face f the 4x4 level-1
     // cells of the neighbour brick next to it
     for (int j = threadIdx.x; j < 160; j += kBT) {
-      double v;
+      T v;
       if (j < 64) {
-        v = (double)e1[(size_t)b * 64 + j];
+        v = e1[(size_t)b * 64 + j];
       } else {
         const int f = (j - 64) >> 4, p = (j - 64) & 3, q = ((j - 64) >> 2) & 3;
         const int64_t base = sb[f];
@@ -146,7 +151,7 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
           case 4: l = p + 4 * q + 48; break;
           default: l = p + 4 * q; break;
         }
-        v = base < 0 ? 0.0 : (double)e1[(base >> 9) * 64 + l];
+        v = base < 0 ? (T)0 : e1[(base >> 9) * 64 + l];
       }
       s1p[j] = v;
     }
@@ -184,20 +189,20 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
       continue;
     }
     int si = s1_of(o);
-    double epc = se[si];
-    double me = 0;
+    T epc = se[si];
+    T me = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      if (m & (1u << (8 + f))) me += P.ih2[f >> 1] * epc;
-      if (m & (1u << f)) me -= P.ih2[f >> 1] * se[si + s1_off(f)];
+      if (m & (1u << (8 + f))) me += ih2[f >> 1] * epc;
+      if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
     }
     double rc = r[c];
-    double out = epc + kOmega * P.dtab[active_index(m)] * (rc - me);
+    T out = epc + om * (T)P.dtab[active_index(m)] * ((T)rc - me);
     if (FIRST) {
-      eout[c] = (T)out;
+      eout[c] = out;
     } else {
-      z[c] = out;
-      rz += rc * out;
+      z[c] = (double)out;
+      rz += rc * (double)out;
     }
   }
   if (!FIRST) block_sum<kBT>(rz, 0.0, partial);
@@ -281,19 +286,19 @@ __device__ inline void lnbrs(const int* sb, int x, int y, int z, int64_t* n) {
 // neighbour reads cell i itself and drops out through its zero weight), then
 // the terms are summed in the fixed order.
 template <class T, int D>
-__device__ inline double apply_l(const T* __restrict__ e, const T* __restrict__ w, size_t ncap,
-                                 const int64_t* n, size_t i, double ec) {
-  double wl[3], wr[3], el[3], er[3];
+__device__ inline T apply_l(const T* __restrict__ e, const T* __restrict__ w, size_t ncap,
+                                 const int64_t* n, size_t i, T ec) {
+  T wl[3], wr[3], el[3], er[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
     const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
-    wl[a] = (double)w[a * ncap + i];
-    el[a] = (double)e[jl];
-    wr[a] = n[2 * a + 1] < 0 ? 0.0 : (double)w[a * ncap + jr];
-    er[a] = (double)e[jr];
+    wl[a] = w[a * ncap + i];
+    el[a] = e[jl];
+    wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr];
+    er[a] = e[jr];
   }
-  double s = (double)w[3 * ncap + i] * ec;
+  T s = w[3 * ncap + i] * ec;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (wl[a] != 0) s -= wl[a] * el[a];
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
   int b = sb[0];
   int o = (int)(g % N);
   size_t i = (size_t)b * N + o;
-  double dinv = (double)w[4 * ncap + i];
+  T dinv = w[4 * ncap + i];
   if (dinv == 0) {
     e[i] = (T)0;
     return;
@@ -324,29 +329,30 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
   int x = o % D, y = (o / D) % D, z = o / (D * D);
   int64_t n[6];
   lnbrs<D>(sb, x, y, z, n);
-  double wl[3], wr[3], dl[3], dr[3], rl[3], rr[3];
+  T wl[3], wr[3], dl[3], dr[3], rl[3], rr[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
     const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
-    wl[a] = (double)w[a * ncap + i];
-    dl[a] = (double)w[4 * ncap + jl];
-    rl[a] = (double)r[jl];
-    wr[a] = n[2 * a + 1] < 0 ? 0.0 : (double)w[a * ncap + jr];
-    dr[a] = (double)w[4 * ncap + jr];
-    rr[a] = (double)r[jr];
+    wl[a] = w[a * ncap + i];
+    dl[a] = w[4 * ncap + jl];
+    rl[a] = r[jl];
+    wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr];
+    dr[a] = w[4 * ncap + jr];
+    rr[a] = r[jr];
   }
-  double s = (2.0 - kOmega) * (double)r[i];
+  T s = (T)(2.0 - kOmega) * r[i];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    if (wl[a] != 0) s += wl[a] * kOmega * dl[a] * rl[a];
-    if (wr[a] != 0) s += wr[a] * kOmega * dr[a] * rr[a];
+    if (wl[a] != 0) s += wl[a] * (T)kOmega * dl[a] * rl[a];
+    if (wr[a] != 0) s += wr[a] * (T)kOmega * dr[a] * rr[a];
   }
-  e[i] = (T)(kOmega * dinv * s);
+  e[i] = (T)kOmega * dinv * s;
 }
 
 // Sum over aligned groups of 8 lanes; the result is valid in the group's first lane.
-__device__ inline double sum8(double v) {
+template <class V>
+__device__ inline V sum8(V v) {
   v += __shfl_down_sync(0xffffffffu, v, 4, 8);
   v += __shfl_down_sync(0xffffffffu, v, 2, 8);
   v += __shfl_down_sync(0xffffffffu, v, 1, 8);
@@ -369,7 +375,7 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = g < (int64_t)nd * N;  // nd * N is a multiple of 8: groups are whole
   const int* sb = sbr + 7 * (threadIdx.x / N);
-  double v = 0;
+  T v = 0;
   int b = 0, p = 0;
   if (live) {
     b = sb[0];
@@ -379,10 +385,10 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
     const int X = p % H, Y = (p / H) % H, Z = p / (H * H);
     const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
     const size_t i = (size_t)b * N + x + D * y + D * D * z;
-    if ((double)w[4 * ncap + i] != 0) {
+    if (w[4 * ncap + i] != 0) {
       int64_t n[6];
       lnbrs<D>(sb, x, y, z, n);
-      v = (double)r[i] - apply_l<T, D>(e, w, ncap, n, i, (double)e[i]);
+      v = r[i] - apply_l<T, D>(e, w, ncap, n, i, e[i]);
     }
   }
   v = sum8(v);
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
   int b = sb[0];
   int o = (int)(g % N);
   size_t i = (size_t)b * N + o;
-  double dinv = (double)w[4 * ncap + i];
+  T dinv = w[4 * ncap + i];
   if (dinv == 0) {
     eout[i] = (T)0;
     return;
@@ -436,38 +442,38 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     k[2 * a + 1] = c[a] == D - 1 ? 2 + 2 * a : 0;
   }
   // e plus the coarse correction at cell j of the brick in slot kk
-  auto ev = [&](int64_t j, int kk) -> double {
-    double v = (double)e[j];
+  auto ev = [&](int64_t j, int kk) -> T {
+    T v = e[j];
     if (WITH_COARSE) {
       if (D == 2) {
-        v += (double)ec[sdi[7 * (threadIdx.x / N) + kk]];
+        v += ec[sdi[7 * (threadIdx.x / N) + kk]];
       } else {
         const int nb = (int)(j / N), no = (int)(j % N);
         const int xx = no % D, yy = (no / D) % D, zz = no / (D * D);
-        v += (double)ec[(size_t)nb * H * H * H + (xx >> 1) + H * (yy >> 1) + H * H * (zz >> 1)];
+        v += ec[(size_t)nb * H * H * H + (xx >> 1) + H * (yy >> 1) + H * H * (zz >> 1)];
       }
     }
     return v;
   };
-  double wl[3], wr[3], vl[3], vr[3];
+  T wl[3], wr[3], vl[3], vr[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const bool hl = n[2 * a] >= 0, hr = n[2 * a + 1] >= 0;
     const int64_t jl = hl ? n[2 * a] : (int64_t)i;
     const int64_t jr = hr ? n[2 * a + 1] : (int64_t)i;
-    wl[a] = (double)w[a * ncap + i];
+    wl[a] = w[a * ncap + i];
     vl[a] = ev(jl, hl ? k[2 * a] : 0);
-    wr[a] = hr ? (double)w[a * ncap + jr] : 0.0;
+    wr[a] = hr ? w[a * ncap + jr] : (T)0;
     vr[a] = ev(jr, hr ? k[2 * a + 1] : 0);
   }
-  double ecc = ev((int64_t)i, 0);
-  double s = (double)w[3 * ncap + i] * ecc;
+  T ecc = ev((int64_t)i, 0);
+  T s = w[3 * ncap + i] * ecc;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (wl[a] != 0) s -= wl[a] * vl[a];
     if (wr[a] != 0) s -= wr[a] * vr[a];
   }
-  eout[i] = (T)(ecc + kOmega * dinv * ((double)r[i] - s));
+  eout[i] = ecc + (T)kOmega * dinv * (r[i] - s);
 }
 
 // ------------------------------------------------------------ dense levels
@@ -484,18 +490,18 @@ struct DView {
 };
 
 template <class T>
-__device__ inline double dense_apply(const DView<T>& L, const T* e, int64_t i, int x, int y, int z, double ec) {
+__device__ inline T dense_apply(const DView<T>& L, const T* e, int64_t i, int x, int y, int z, T ec) {
   int64_t n = L.n;
-  double s = (double)L.w[3 * n + i] * ec;
+  T s = L.w[3 * n + i] * ec;
   int c[3] = {x, y, z};
   int dim[3] = {L.nx, L.ny, L.nz};
   int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
   for (int a = 0; a < 3; ++a) {
-    double wl = (double)L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) s -= wl * (double)e[i - stride[a]];
+    T wl = L.w[a * n + i];
+    if (wl != 0 && c[a] > 0) s -= wl * e[i - stride[a]];
     if (c[a] + 1 < dim[a]) {
-      double wr = (double)L.w[a * n + i + stride[a]];
-      if (wr != 0) s -= wr * (double)e[i + stride[a]];
+      T wr = L.w[a * n + i + stride[a]];
+      if (wr != 0) s -= wr * e[i + stride[a]];
     }
   }
   return s;
@@ -507,7 +513,7 @@ __global__ void kd_pre(DView<T> L) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   int64_t n = L.n;
-  double dinv = (double)L.w[4 * n + i];
+  T dinv = L.w[4 * n + i];
   if (dinv == 0) {
     L.e[i] = (T)0;
     return;
@@ -516,16 +522,16 @@ __global__ void kd_pre(DView<T> L) {
   int c[3] = {x, y, z};
   int dim[3] = {L.nx, L.ny, L.nz};
   int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  double s = (2.0 - kOmega) * (double)L.r[i];
+  T s = (T)(2.0 - kOmega) * L.r[i];
   for (int a = 0; a < 3; ++a) {
-    double wl = (double)L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) s += wl * kOmega * (double)L.w[4 * n + i - stride[a]] * (double)L.r[i - stride[a]];
+    T wl = L.w[a * n + i];
+    if (wl != 0 && c[a] > 0) s += wl * (T)kOmega * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
     if (c[a] + 1 < dim[a]) {
-      double wr = (double)L.w[a * n + i + stride[a]];
-      if (wr != 0) s += wr * kOmega * (double)L.w[4 * n + i + stride[a]] * (double)L.r[i + stride[a]];
+      T wr = L.w[a * n + i + stride[a]];
+      if (wr != 0) s += wr * (T)kOmega * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
     }
   }
-  L.e[i] = (T)(kOmega * dinv * s);
+  L.e[i] = (T)kOmega * dinv * s;
 }
 
 // One thread per (coarse cell, child), the 8 children on adjacent lanes.
@@ -534,14 +540,14 @@ __global__ void kd_restrict(DView<T> F, DView<T> C) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t I = g >> 3;
   const int k = (int)(g & 7);
-  double s = 0;
+  T s = 0;
   if (I < C.n) {
     const int XY = (int)(I / C.nx);
     const int X = (int)(I - (int64_t)XY * C.nx), Y = XY % C.ny, Z = XY / C.ny;
     const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
     if (x < F.nx && y < F.ny && z < F.nz) {
       const int64_t i = F.at(x, y, z);
-      if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, F.e, i, x, y, z, (double)F.e[i]);
+      if (F.w[4 * F.n + i] != 0) s = F.r[i] - dense_apply(F, F.e, i, x, y, z, F.e[i]);
     }
   }
   s = sum8(s);
@@ -553,38 +559,38 @@ __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   int64_t n = L.n;
-  double dinv = (double)L.w[4 * n + i];
+  T dinv = L.w[4 * n + i];
   if (dinv == 0) {
     eout[i] = (T)0;
     return;
   }
   int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
-  auto ev = [&](int64_t j, int xx, int yy, int zz) -> double {
-    double v = (double)ein[j];
-    if (WITH_COARSE) v += (double)C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
+  auto ev = [&](int64_t j, int xx, int yy, int zz) -> T {
+    T v = ein[j];
+    if (WITH_COARSE) v += C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
     return v;
   };
   int c[3] = {x, y, z};
   int dim[3] = {L.nx, L.ny, L.nz};
   int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  double ec = ev(i, x, y, z);
-  double s = (double)L.w[3 * n + i] * ec;
+  T ec = ev(i, x, y, z);
+  T s = L.w[3 * n + i] * ec;
   for (int a = 0; a < 3; ++a) {
     int p[3] = {x, y, z};
-    double wl = (double)L.w[a * n + i];
+    T wl = L.w[a * n + i];
     if (wl != 0 && c[a] > 0) {
       p[a] = c[a] - 1;
       s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
     }
     if (c[a] + 1 < dim[a]) {
-      double wr = (double)L.w[a * n + i + stride[a]];
+      T wr = L.w[a * n + i + stride[a]];
       if (wr != 0) {
         p[a] = c[a] + 1;
         s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
       }
     }
   }
-  eout[i] = (T)(ec + kOmega * dinv * ((double)L.r[i] - s));
+  eout[i] = ec + (T)kOmega * dinv * (L.r[i] - s);
 }
 
 // ------------------------------------------- coarse V-cycle in one block
@@ -606,44 +612,44 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce
   const T* __restrict__ w = L.w;
   const T* __restrict__ r = L.r;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double dinv = (double)w[4 * n + i];
+    const T dinv = w[4 * n + i];
     if (dinv == 0) {
       eout[i] = (T)0;
       continue;
     }
     if (first) {
-      eout[i] = (T)(kOmega * dinv * (double)r[i]);
+      eout[i] = (T)kOmega * dinv * r[i];
       continue;
     }
     const int xy = i / nx;
     const int x = i - xy * nx, y = xy % ny, z = xy / ny;
-    auto ev = [&](int j, int xx, int yy, int zz) -> double {
-      double v = (double)ein[j];
-      if (ce) v += (double)ce[(xx >> 1) + cnx * ((yy >> 1) + cny * (zz >> 1))];
+    auto ev = [&](int j, int xx, int yy, int zz) -> T {
+      T v = ein[j];
+      if (ce) v += ce[(xx >> 1) + cnx * ((yy >> 1) + cny * (zz >> 1))];
       return v;
     };
     const int c[3] = {x, y, z};
     const int dim[3] = {nx, ny, nz};
     const int stride[3] = {1, nx, nx * ny};
-    const double ec = ev(i, x, y, z);
-    double s = (double)w[3 * n + i] * ec;
+    const T ec = ev(i, x, y, z);
+    T s = w[3 * n + i] * ec;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       int p[3] = {x, y, z};
-      const double wl = (double)w[a * n + i];
+      const T wl = w[a * n + i];
       if (wl != 0 && c[a] > 0) {
         p[a] = c[a] - 1;
         s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
       }
       if (c[a] + 1 < dim[a]) {
-        const double wr = (double)w[a * n + i + stride[a]];
+        const T wr = w[a * n + i + stride[a]];
         if (wr != 0) {
           p[a] = c[a] + 1;
           s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
         }
       }
     }
-    eout[i] = (T)(ec + kOmega * dinv * ((double)r[i] - s));
+    eout[i] = ec + (T)kOmega * dinv * (r[i] - s);
   }
 }
 
@@ -655,14 +661,14 @@ __device__ void blk_restrict(const DView<T>& F, const T* fe, const DView<T>& C) 
   const int total = ((int)C.n * 8 + 31) & ~31;
   for (int g = threadIdx.x; g < total; g += blockDim.x) {
     const int I = g >> 3, k = g & 7;
-    double s = 0;
+    T s = 0;
     if (I < (int)C.n) {
       const int XY = I / C.nx;
       const int X = I - XY * C.nx, Y = XY % C.ny, Z = XY / C.ny;
       const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
       if (x < F.nx && y < F.ny && z < F.nz) {
         const int i = x + F.nx * (y + F.ny * z);
-        if ((double)F.w[4 * F.n + i] != 0) s = (double)F.r[i] - dense_apply(F, fe, i, x, y, z, (double)fe[i]);
+        if (F.w[4 * F.n + i] != 0) s = F.r[i] - dense_apply(F, fe, i, x, y, z, fe[i]);
       }
     }
     s = sum8(s);
