@@ -180,29 +180,34 @@ def reduce_over_ranks(seconds: float, count: float, device) -> tuple:
 
 
 # ------------------------------------------------------------- our arm
-def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8):
+def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8, cg_iterations=0):
     """Achieved GB/s per phase from algorithmic bytes (every array element a
     kernel must touch, read or written once) over the measured event times.
-    A "launch" is one timed region of the phase (one V-cycle, one CG update)."""
+    A "launch" is one timed region of the phase (one particle move, one SpMV),
+    except for the V-cycle phase: its regions hold one V-cycle per CG
+    iteration, whose first kernel also applies the iteration's update
+    x += alpha p, r -= alpha q, and one region per solve with the last update
+    alone, so its launch is one CG iteration (a V-cycle and an update)."""
     unk = ctx_stats["unknowns"]
     # V-cycle: per cell of a level, 2 pre + 2 post sweeps of 17 B, residual 25 B,
     # restriction 8 B and prolongation 16 B at FP64 (117 B), the levels adding
-    # up to 8/7 of the finest; FP32 storage halves it.
+    # up to 8/7 of the finest; FP32 storage halves it. The update: x, p, r, q
+    # read, x, r written, 48 B at FP64.
     vc = 117.0 * 8.0 / 7.0 * (mg_bytes / 8.0)
     models = {
-        # phase: (bytes per launch, description)
-        "move": (48.0 * np_count, "48 B per particle (read + write 3 FP64 positions)"),
-        "vcycle": (vc * unk, f"{vc:.1f} B per unknown per V-cycle (levels 0.. at {mg_bytes} B per value)"),
-        "spmv": (34.0 * unk, "34 B per unknown (read z, p_old 16, face mask 2, write p, q 16)"),
-        "cg_vector": (24.0 * unk, "24 B per unknown per region (x, p, r, q read, x, r written: 48 B "
-                                   "per iteration over its 2 regions)"),
-        "forces": (75.0 * n_exist, "75 B per existing cell (mean of stage 1: 51, stage 2: 99)"),
-        "gradient": (67.0 * n_exist, "67 B per existing cell (x 8, flags 3, p 8, u read+write 48)"),
-        "divergence": (42.0 * unk, "42 B per unknown (u 24, mask 2, rhs 8, x 8)"),
+        # phase: (bytes per launch, description, launches or None for the region count)
+        "move": (48.0 * np_count, "48 B per particle (read + write 3 FP64 positions)", None),
+        "vcycle": ((vc + 48.0) * unk, f"{vc + 48.0:.1f} B per unknown per CG iteration: a V-cycle ({vc:.1f} B, "
+                   f"levels 0.. at {mg_bytes} B per value) and the update it applies (48 B)", cg_iterations),
+        "spmv": (34.0 * unk, "34 B per unknown (read z, p_old 16, face mask 2, write p, q 16)", None),
+        "forces": (75.0 * n_exist, "75 B per existing cell (mean of stage 1: 51, stage 2: 99)", None),
+        "gradient": (67.0 * n_exist, "67 B per existing cell (x 8, flags 3, p 8, u read+write 48)", None),
+        "divergence": (42.0 * unk, "42 B per unknown (u 24, mask 2, rhs 8, x 8)", None),
     }
     out = {}
-    for ph, (nbytes, desc) in models.items():
+    for ph, (nbytes, desc, count) in models.items():
         ms, n = prof.get(ph, (0.0, 0))
+        n = count if count else n
         if n:
             out[ph] = {"ms_total": ms, "launches": n, "avg_ms": ms / n,
                        "gbs": nbytes / (ms / n * 1e-3) / 1e9, "bytes_per_launch": nbytes, "model": desc}
@@ -333,6 +338,7 @@ def run_ours(args, rank, world, local_rank):
     e1 = torch.cuda.Event(enable_timing=True)
     fluid_steps = 0
     iters = []
+    it0 = ctx.stats()["total_iterations"]
     e0.record(stream)
     for _ in range(args.steps):
         ctx.step()
@@ -348,6 +354,7 @@ def run_ours(args, rank, world, local_rank):
     prof = ctx.profile()
     ctx.set_profiling(False)
     st = ctx.stats()
+    cg_iterations = st["total_iterations"] - it0
     sec, total_fluid_steps = reduce_over_ranks(ms / 1e3, fluid_steps, f"cuda:{dev}")
     value = total_fluid_steps / sec
 
@@ -378,7 +385,7 @@ def run_ours(args, rank, world, local_rank):
            "d2h_bytes_per_step": bo // e2e_steps, "steps": e2e_steps}
 
     n_exist = int(st["live_bricks"] * 512)  # upper bound of existing cells (slots of live bricks)
-    rl = roofline_models(st, prof, st["particles"], n_exist, 4 if args.solver == "mixed" else 8)
+    rl = roofline_models(st, prof, st["particles"], n_exist, 4 if args.solver == "mixed" else 8, cg_iterations)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

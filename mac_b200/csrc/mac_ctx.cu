@@ -186,6 +186,9 @@ static void free_all(Ctx* c) {
   cudaFree(c->bcount); cudaFree(c->bcursor); cudaFree(c->boff);
   cudaFree(c->ds);
   if (c->hs) cudaFreeHost(c->hs);
+  if (c->hs_lag) cudaFreeHost(c->hs_lag);
+  for (cudaEvent_t e : c->ev_lag)
+    if (e) cudaEventDestroy(e);
   cudaFree(c->csc_off); cudaFree(c->csc_ind); cudaFree(c->csc_val); cudaFree(c->csc_vec);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -280,6 +283,8 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->boff, c->cap_bricks + 2));
   A(dalloc(&c->ds, 1));
   if (rc == MAC_OK) A(check(cudaMallocHost((void**)&c->hs, sizeof(Scalars))));
+  if (rc == MAC_OK) A(check(cudaMallocHost((void**)&c->hs_lag, 2 * sizeof(Scalars))));
+  for (int k = 0; k < 2 && rc == MAC_OK; ++k) A(check(cudaEventCreateWithFlags(&c->ev_lag[k], cudaEventDisableTiming)));
   if (rc == MAC_OK) A(alloc_solver(c));
   if (rc == MAC_OK) {
     A(check(cudaMemsetAsync(c->ds, 0, sizeof(Scalars), c->stream)));

@@ -167,6 +167,8 @@ struct Ctx {
   double* x = nullptr;        // solution (pressure in domain)
   double* b = nullptr;        // right-hand side
   double* r = nullptr;
+  double* r2 = nullptr;       // the residual's second buffer: a V-cycle that finishes the
+                              // previous CG iteration writes the new r there
   double* z = nullptr;
   double* pd = nullptr;       // search direction
   double* pd2 = nullptr;      // its previous value (the update reads neighbours' old p)
@@ -198,6 +200,8 @@ struct Ctx {
   // scalars
   Scalars* ds = nullptr;      // device
   Scalars* hs = nullptr;      // pinned host mirror
+  Scalars* hs_lag = nullptr;  // [2] pinned: the scalars after the last two CG iterations
+  cudaEvent_t ev_lag[2] = {};
   int nlive_host = 0;
   int64_t np_host = 0;
   mac_stats stats{};
@@ -374,8 +378,8 @@ __device__ inline void load4(const float* p, V* v) {
 }
 
 // Only the face halos of stage_h1 (value 0 where the neighbour brick is absent).
-template <class F>
-__device__ inline void stage_h1_halo(double* s, const int64_t* sb, F val) {
+template <class S, class F>
+__device__ inline void stage_h1_halo(S* s, const int64_t* sb, F val) {
   for (int j = threadIdx.x; j < 384; j += kBT) {
     int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
     int x, y, z;
@@ -388,7 +392,7 @@ __device__ inline void stage_h1_halo(double* s, const int64_t* sb, F val) {
       case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
       default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
     }
-    s[s1(x, y, z)] = gi < 0 ? 0.0 : val(gi);
+    s[s1(x, y, z)] = gi < 0 ? (S)0 : (S)val(gi);
   }
 }
 
@@ -418,6 +422,10 @@ __device__ inline void stage_arr(S* s, const T* __restrict__ a, int b, const int
     s[s1(x, y, z)] = gi < 0 ? (S)0 : (S)a[gi];
   }
 }
+
+// Kernels of an iterative solve that the host enqueues ahead of its
+// convergence check do nothing once the solve is done (done == nullptr: run).
+__device__ inline bool solve_done(const int32_t* done) { return done != nullptr && *done != 0; }
 
 // Sum over an NT-thread block of two values into partial[blockIdx.x] and
 // partial[gridDim.x + blockIdx.x] (fixed order).
@@ -480,7 +488,11 @@ int move_particles(Ctx* c);
 int alloc_solver(Ctx* c);
 void free_solver(Ctx* c);
 int mg_setup(Ctx* c);
-void mg_vcycle(Ctx* c);
+// update = 1: the V-cycle's first kernel also applies the previous CG
+// iteration's x += alpha p, r -= alpha q and its convergence test. part: 1 =
+// that first kernel (and the test), 2 = the rest of the V-cycle, 3 = all.
+void mg_vcycle(Ctx* c, int update, int part);
+void cg_finish_update(Ctx* c);
 int mg_configure(Ctx* c);
 
 }  // namespace mac

@@ -17,6 +17,7 @@
 // preconditioned residual z the CG iteration exchanges stay double.
 #include <cstdio>
 #include <cstring>
+#include <utility>
 
 #include "mac_internal.cuh"
 
@@ -38,20 +39,49 @@ __device__ inline int64_t parent1(int64_t n) {
 // ---------------------------------------------------------------- level 0
 // Two Jacobi sweeps from zero, fused: e1 = w D^-1 r, e = e1 + w D^-1 (r - M e1)
 // = w D^-1 ((2 - w) r + sum_f ih2_f e1(n_f)).
+// With update (every CG iteration but the first) the kernel first finishes
+// the previous iteration over all cells of the brick: x += alpha p and
+// r = rin - alpha q into rout with the block's partial r.r. rout is not rin,
+// so a block staging its face halos reads the old r of its neighbours and
+// forms their new r on the fly with the same expression.
 template <class T>
 __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
-                                              const uint16_t* __restrict__ fmask, const double* __restrict__ r,
-                                              T* __restrict__ e, Params P) {
+                                              const uint16_t* __restrict__ fmask, const double* __restrict__ rin,
+                                              double* __restrict__ rout, double* __restrict__ x,
+                                              const double* __restrict__ p, const double* __restrict__ q,
+                                              double* partial, const Scalars* ds, int update, T* __restrict__ e,
+                                              Params P) {
+  if (solve_done(&ds->done)) return;
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
   __shared__ uint16_t sm[kCells];
   const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const double al = update ? ds->alpha : 0.0;
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  __syncthreads();
-  stage_h1(sr, b, sb, (T)0, [&](int64_t i) { return om * (T)P.dtab[active_index(fmask[i])] * (T)r[i]; });
+  double rv[kCPT];
+  double rr = 0;
 #pragma unroll
-  for (int k = 0; k < kCPT; ++k) sm[threadIdx.x + kBT * k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
+  for (int k = 0; k < kCPT; ++k) {
+    const int o = threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + o;
+    double v = rin[c];
+    if (update) {
+      v = v - al * q[c];
+      rout[c] = v;
+      x[c] += al * p[c];
+      rr += v * v;
+    }
+    rv[k] = v;
+    const uint16_t m = fmask[c];
+    sm[o] = m;
+    sr[s1_of(o)] = om * (T)P.dtab[active_index(m)] * (T)v;
+  }
+  __syncthreads();
+  stage_h1_halo(sr, sb, [&](int64_t i) {
+    const double v = update ? rin[i] - al * q[i] : rin[i];
+    return om * (T)P.dtab[active_index(fmask[i])] * (T)v;
+  });
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
@@ -62,7 +92,7 @@ __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const
     if (m & kDomainBit) {
       int si = s1_of(o);
       T dinv = (T)P.dtab[active_index(m)];
-      T s = (T)(2.0 - kOmega) * (T)r[c];
+      T s = (T)(2.0 - kOmega) * (T)rv[k];
 #pragma unroll
       for (int f = 0; f < 6; ++f)
         if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
@@ -70,13 +100,16 @@ __global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const
     }
     e[c] = out;
   }
+  if (update) block_sum<kBT>(rr, 0.0, partial);
 }
 
 // res = r - M e on the brick, summed over 2x2x2 children into level 1.
 template <class T>
 __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
-                                                   const T* __restrict__ e, T* __restrict__ r1, Params P) {
+                                                   const T* __restrict__ e, T* __restrict__ r1, Params P,
+                                                   const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T res[kCells];
   __shared__ T se[kS1];
@@ -123,7 +156,9 @@ template <class T, bool FIRST>
 __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
-                                               double* __restrict__ z, double* partial, Params P) {
+                                               double* __restrict__ z, double* partial, Params P,
+                                               const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
   __shared__ T s1p[64 + 96];  // FIRST: level-1 parents of the brick (64) and of its face halos (6 x 16)
@@ -310,7 +345,8 @@ __device__ inline T apply_l(const T* __restrict__ e, const T* __restrict__ w, si
 template <class T, int D>
 __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
-                                              T* __restrict__ e) {
+                                              T* __restrict__ e, const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
   load_lbricks<D>(dbl, nd, nbr, sbr);
@@ -366,7 +402,8 @@ template <class T, int D>
 __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                                    const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                    const T* __restrict__ r, const T* __restrict__ e, T* __restrict__ rc,
-                                                   DenseGrid g3) {
+                                                   DenseGrid g3, const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   constexpr int H = D / 2;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
@@ -404,7 +441,9 @@ template <class T, int D, bool WITH_COARSE>
 __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                                  const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                  const T* __restrict__ r, const T* __restrict__ e,
-                                                 const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3) {
+                                                 const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3,
+                                                 const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   constexpr int N = D * D * D;
   constexpr int H = D / 2;
   __shared__ int sbr[7 * LBricks<D>::BPB];
@@ -509,7 +548,8 @@ __device__ inline T dense_apply(const DView<T>& L, const T* e, int64_t i, int x,
 
 // Device-wide dense kernels for level 3.
 template <class T>
-__global__ void kd_pre(DView<T> L) {
+__global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   int64_t n = L.n;
@@ -536,7 +576,8 @@ __global__ void kd_pre(DView<T> L) {
 
 // One thread per (coarse cell, child), the 8 children on adjacent lanes.
 template <class T>
-__global__ void kd_restrict(DView<T> F, DView<T> C) {
+__global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t I = g >> 3;
   const int k = (int)(g & 7);
@@ -555,7 +596,9 @@ __global__ void kd_restrict(DView<T> F, DView<T> C) {
 }
 
 template <class T, bool WITH_COARSE>
-__global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__ eout, DView<T> C) {
+__global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__ eout, DView<T> C,
+                          const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   int64_t n = L.n;
@@ -745,7 +788,9 @@ __device__ void blk_copy(T* dst, const T* src, int64_t n) {
 
 template <class T>
 __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem, const double* __restrict__ inv,
-                                                        const int* __restrict__ inv_ok) {
+                                                        const int* __restrict__ inv_ok,
+                                                        const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // Level descriptors live in shared memory (one copy per block); which of a
   // level's two correction buffers is current is a bit in a register.
@@ -1024,8 +1069,9 @@ static int mg_setup_t(Ctx* c) {
 
 int mg_setup(Ctx* c) { return c->mg_float ? mg_setup_t<float>(c) : mg_setup_t<double>(c); }
 
+// part: 1 = the head (first kernel, with update the convergence test), 2 = the rest.
 template <class T>
-static void mg_vcycle_t(Ctx* c) {
+static void mg_vcycle_t(Ctx* c, int update, int part) {
   cudaStream_t st = c->stream;
   int nd = c->ndom_host;
   size_t ncap1 = (size_t)c->cap_bricks * 64, ncap2 = (size_t)c->cap_bricks * 8;
@@ -1042,46 +1088,59 @@ static void mg_vcycle_t(Ctx* c) {
   DView<T> d3 = dview<T>(c, 0);
   int g1 = grid_for((int64_t)nd * 64, 256), g2 = grid_for((int64_t)nd * 8, 256);
   DenseGrid G = c->g3;
-  // down
-  k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, c->dp); MAC_COUNT(c);
-  k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp); MAC_COUNT(c);
-  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1); MAC_COUNT(c);
-  kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G); MAC_COUNT(c);
-  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2); MAC_COUNT(c);
-  kl_restrict<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G); MAC_COUNT(c);
+  const int32_t* dn = &c->ds->done;
+  // down (with update: finish the previous CG iteration into r2, which becomes r)
+  if (part & 1) {
+    k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
+                                  update, e0, c->dp); MAC_COUNT(c);
+    if (update) {
+      std::swap(c->r, c->r2);
+      cg_finish_update(c);
+    }
+  }
+  if (!(part & 2)) return;
+  k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
+  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1, dn); MAC_COUNT(c);
+  kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
+  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2, dn); MAC_COUNT(c);
+  kl_restrict<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
     DView<T> d4 = dview<T>(c, 1);
-    kd_pre<T><<<grid_for(d3.n, 256), 256, 0, st>>>(d3); MAC_COUNT(c);
-    kd_restrict<T><<<grid_for(8 * d4.n, 256), 256, 0, st>>>(d3, d4); MAC_COUNT(c);
+    kd_pre<T><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, dn); MAC_COUNT(c);
+    kd_restrict<T><<<grid_for(8 * d4.n, 256), 256, 0, st>>>(d3, d4, dn); MAC_COUNT(c);
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
     S.lo = 1;
     S.hi = c->ndense;
     int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
-    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem, c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
-    kd_jacobi<T, true><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e, d3.e2, d4); MAC_COUNT(c);
-    kd_jacobi<T, false><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e2, d3.e, d4); MAC_COUNT(c);
+    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem, c->coarse_inv, c->coarse_ok,
+                                                                      dn); MAC_COUNT(c);
+    kd_jacobi<T, true><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
+    kd_jacobi<T, false><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
   } else {
     DenseSet<T> S;
     S.L[0] = d3;
     S.lo = 0;
     S.hi = 1;
-    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0, c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
+    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
   // up
-  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G); MAC_COUNT(c);
-  kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G); MAC_COUNT(c);
-  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G); MAC_COUNT(c);
-  kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G); MAC_COUNT(c);
-  k0_post<T, true><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp); MAC_COUNT(c);
+  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, dn); MAC_COUNT(c);
+  kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
+                                             dn); MAC_COUNT(c);
+  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, dn); MAC_COUNT(c);
+  kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
+                                             dn); MAC_COUNT(c);
+  k0_post<T, true><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
+                                       dn); MAC_COUNT(c);
   k0_post<T, false><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
-                                         c->dp); MAC_COUNT(c);
+                                        c->dp, dn); MAC_COUNT(c);
 }
 
-void mg_vcycle(Ctx* c) {
-  if (c->mg_float) mg_vcycle_t<float>(c);
-  else mg_vcycle_t<double>(c);
+void mg_vcycle(Ctx* c, int update, int part) {
+  if (c->mg_float) mg_vcycle_t<float>(c, update, part);
+  else mg_vcycle_t<double>(c, update, part);
 }
 
 int mg_configure(Ctx* c) {

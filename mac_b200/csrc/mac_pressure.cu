@@ -40,6 +40,7 @@ int alloc_solver(Ctx* c) {
   A(dalloc(&c->x, nc));
   A(dalloc(&c->b, nc));
   A(dalloc(&c->r, nc));
+  A(dalloc(&c->r2, nc));
   A(dalloc(&c->z, nc));
   A(dalloc(&c->pd, nc));
   A(dalloc(&c->pd2, nc));
@@ -70,7 +71,7 @@ int alloc_solver(Ctx* c) {
 }
 
 void free_solver(Ctx* c) {
-  cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->z); cudaFree(c->pd);
+  cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->r2); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
   cudaFree(c->zold);
   cudaFree(c->coarse_inv);
@@ -647,8 +648,15 @@ static void precondition(Ctx* c) {
   if (c->prm.solver == MAC_SOLVER_CG_FP64) {
     k_jacobi_prec<<<c->ndom_host, 512, 0, c->stream>>>(c->dbl, c->fmask, c->r, c->z, c->partial, c->dp); MAC_COUNT(c);
   } else {
-    mg_vcycle(c);
+    mg_vcycle(c, 0, 3);
   }
+}
+
+// Convergence test after the update the V-cycle's first kernel applied (its
+// partial r.r are in c->partial).
+void cg_finish_update(Ctx* c) {
+  k_fin_rr<<<1, 1024, 0, c->stream>>>(c->partial, c->ndom_host, c->ds, c->prm.rtol * c->prm.rtol,
+                                      c->prm.max_iters); MAC_COUNT(c);
 }
 
 int project(Ctx* c, int ib) {
@@ -705,10 +713,38 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
     constexpr int kStallWindow = 8, kLearnedMax = 200;
     std::vector<double> hist;
     c->stats.learned_iterations = 0;
+    // The multigrid forms fold x += alpha p, r -= alpha q and the convergence
+    // test into the next V-cycle's first kernel. The host reads each
+    // iteration's scalars one iteration late, with the next iteration already
+    // enqueued, so the device does not wait for the host between iterations.
+    // Once the residual's contraction predicts convergence within two
+    // iterations ("near"), the host instead tests right after each V-cycle's
+    // first kernel and enqueues the rest only if the solve goes on, so no
+    // V-cycle runs past convergence (its kernels would return at once, but
+    // some twenty empty launches still cost about 0.1 ms).
+    const bool mg = c->prm.solver != MAC_SOLVER_CG_FP64;
+    bool lagged = false;  // the fold was used: the final scalars are read at the end
+    bool near = false;
+    int ahead = 0;        // readbacks enqueued while not near
+    double rr_prev = -1;  // r.r of the iteration before the last one read back
     while (true) {
+      const bool fold = mg && !learned;
       prof_begin(c, PH_VCYCLE);
       if (learned) {
         if ((rc = learned_precondition(c, first))) return rc;
+      } else if (fold) {
+        lagged = true;
+        const int update = first ? 0 : 1;
+        mg_vcycle(c, update, 1);
+        if (near && update) {
+          rc = read_scalars(c);
+          if (rc || c->hs->done) {
+            prof_end(c, PH_VCYCLE);
+            if (rc) return rc;
+            break;
+          }
+        }
+        mg_vcycle(c, 0, 2);
       } else {
         precondition(c);
       }
@@ -726,9 +762,30 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
       first = 0;
       prof_begin(c, PH_CGVEC);
       k_fin_alpha<<<1, 1024, 0, st>>>(c->partial, nd, c->ds); MAC_COUNT(c);
-      k_axpy<<<nd, 512, 0, st>>>(c->dbl, c->x, c->r, c->pd, c->q, c->partial, c->ds); MAC_COUNT(c);
-      k_fin_rr<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2, c->prm.max_iters); MAC_COUNT(c);
+      if (!fold) {
+        k_axpy<<<nd, 512, 0, st>>>(c->dbl, c->x, c->r, c->pd, c->q, c->partial, c->ds); MAC_COUNT(c);
+        k_fin_rr<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2, c->prm.max_iters); MAC_COUNT(c);
+      }
       prof_end(c, PH_CGVEC);
+      if (fold) {
+        if (near) continue;  // tested after the next V-cycle's first kernel
+        const int s = ahead & 1;
+        rc = check(cudaMemcpyAsync(&c->hs_lag[s], c->ds, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+        if (!rc) rc = check(cudaEventRecord(c->ev_lag[s], st));
+        if (rc) return rc;
+        if (ahead++ == 0) continue;
+        if ((rc = check(cudaEventSynchronize(c->ev_lag[s ^ 1])))) return rc;
+        const Scalars& h = c->hs_lag[s ^ 1];
+        if (h.done) break;
+        // r.r two tests after the one read back, at the last contraction
+        if (rr_prev > 0) {
+          const double q = h.rr / rr_prev;
+          near = h.rr * q * q <= 4.0 * rtol2 * h.bnorm2;
+        }
+        if (h.iters + 2 >= c->prm.max_iters) near = true;
+        rr_prev = h.rr;
+        continue;
+      }
       rc = read_scalars(c);
       if (rc) return rc;
       if (learned) c->stats.learned_iterations = c->hs->iters;
@@ -747,6 +804,7 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
         }
       }
     }
+    if (lagged && (rc = read_scalars(c))) return rc;
     double relres = c->hs->bnorm2 > 0 ? sqrt(c->hs->rr / c->hs->bnorm2) : 0.0;
     c->stats.iterations = c->hs->iters;
     c->stats.total_iterations += c->hs->iters;
