@@ -27,42 +27,69 @@ __device__ inline int64_t cidx(const int* sn, int x, int y, int z) {
 // (src/Offset_Base_Neighbour.h:14-33) reads 0 here.
 __device__ inline double rdv(const double* __restrict__ U, int64_t i) { return i < 0 ? 0.0 : U[i]; }
 
-struct Fields {
-  const double* u[3];  // speed buffer read by the stencil
+// The brick of a force kernel and its halo in shared memory, slot s1(x, y, z)
+// for coordinates -1..8: the three speed components (0 where the brick is not
+// live, as rdv reads), the layer (kMissing there) and the material. The
+// stencils below read the brick, its face halos and the edge cells
+// c - e_i + e_j; corner slots are never read and stay unset.
+struct Stage {
+  double u[3][kS1];
+  int8_t lay[kS1];
+  uint8_t type[kS1];
 };
+
+__device__ inline void stage_forces(Stage& S, const double* const* U, const int* sn, const int8_t* __restrict__ lay,
+                                    const uint8_t* __restrict__ type) {
+  for (int t = threadIdx.x; t < kS1; t += blockDim.x) {
+    const int x = t % 10 - 1, y = (t / 10) % 10 - 1, z = t / 100 - 1;
+    if ((x < 0 || x > 7) + (y < 0 || y > 7) + (z < 0 || z > 7) > 2) continue;
+    const int64_t i = cidx(sn, x, y, z);
+    S.u[0][t] = rdv(U[0], i);
+    S.u[1][t] = rdv(U[1], i);
+    S.u[2][t] = rdv(U[2], i);
+    S.lay[t] = i < 0 ? kMissing : lay[i];
+    S.type[t] = i < 0 ? (uint8_t)0 : type[i];
+  }
+}
+
+__device__ inline double su(const Stage& S, int j, int x, int y, int z) { return S.u[j][s1(x, y, z)]; }
+
+// The cell at (x, y, z) exists and is fluid (false where its brick is not live).
+__device__ inline bool fluid_at(const Stage& S, int x, int y, int z) {
+  const int t = s1(x, y, z);
+  return S.lay[t] != kMissing && is_fluid(S.type[t]);
+}
 
 // Get_Speed_At_Bound (src/Policy_Speed_Interpolation_Linear_Symmetric.h:120-127,
 // identical in src/Policy_Speed_Interpolation_Linear.h:107-114).
-__device__ inline double speed_at_bound(const double* const* U, const int* sn, int x, int y, int z, int i, int j) {
-  int c[3] = {x, y, z};
-  if (i == j) return rdv(U[j], cidx(sn, x, y, z));
+__device__ inline double speed_at_bound(const Stage& S, int x, int y, int z, int i, int j) {
+  if (i == j) return su(S, j, x, y, z);
   int cj[3] = {x, y, z}, ci[3] = {x, y, z}, cij[3] = {x, y, z};
   cj[j] += 1;
   ci[i] -= 1;
   cij[i] -= 1;
   cij[j] += 1;
-  double a = rdv(U[j], cidx(sn, c[0], c[1], c[2]));
-  double b = rdv(U[j], cidx(sn, cj[0], cj[1], cj[2]));
-  double d = rdv(U[j], cidx(sn, ci[0], ci[1], ci[2]));
-  double e = rdv(U[j], cidx(sn, cij[0], cij[1], cij[2]));
+  double a = su(S, j, x, y, z);
+  double b = su(S, j, cj[0], cj[1], cj[2]);
+  double d = su(S, j, ci[0], ci[1], ci[2]);
+  double e = su(S, j, cij[0], cij[1], cij[2]);
   return 0.25 * (((a + b) + d) + e);
 }
 
 // Policy_Upwind_1_Order::Get_Convection_Speed(neigh, i) (src/Policy_Upwind_1_Order.h:18-38,58-66).
-__device__ inline double convection(const double* const* U, const int* sn, int x, int y, int z, int i,
-                                    const Params& P) {
+__device__ inline double convection(const Stage& S, int x, int y, int z, int i, const Params& P) {
   double ret = 0;
-  double U1 = rdv(U[i], cidx(sn, x, y, z));
+  double U1 = su(S, i, x, y, z);
   for (int j = 0; j < 3; ++j) {
-    double Ub = speed_at_bound(U, sn, x, y, z, i, j);
+    double Ub = speed_at_bound(S, x, y, z, i, j);
     int m[3] = {x, y, z};
     if (Ub > 0) {
       m[j] -= 1;
-      double U2 = rdv(U[i], cidx(sn, m[0], m[1], m[2]));
+      double U2 = su(S, i, m[0], m[1], m[2]);
       Ub *= (U1 - U2) * P.ih[j];
     } else {
       m[j] += 1;
-      double U2 = rdv(U[i], cidx(sn, m[0], m[1], m[2]));
+      double U2 = su(S, i, m[0], m[1], m[2]);
       Ub *= (U2 - U1) * P.ih[j];
     }
     ret -= Ub;
@@ -73,29 +100,24 @@ __device__ inline double convection(const double* const* U, const int* sn, int x
 // Policy_Viscosity_Apply_If::Get_Viscosity_Apply_If (src/Policy_Viscosity_Apply_If.h:15-42):
 // a fluid cell, or a cell with a layer one of whose -e_j neighbours (any axis)
 // exists and is fluid. One answer for the three faces of the cell.
-__device__ inline bool viscosity_applies(const int* sn, const int8_t* __restrict__ lay,
-                                         const uint8_t* __restrict__ type, int64_t c, bool fluid, int x, int y,
-                                         int z) {
+__device__ inline bool viscosity_applies(const Stage& S, bool fluid, int x, int y, int z) {
   if (fluid) return true;
-  if (lay[c] == kEmpty) return false;
-  for (int j = 0; j < 3; ++j) {
-    int64_t n = cidx(sn, x - (j == 0), y - (j == 1), z - (j == 2));
-    if (n >= 0 && lay[n] != kMissing && is_fluid(type[n])) return true;
-  }
+  if (S.lay[s1(x, y, z)] == kEmpty) return false;
+  for (int j = 0; j < 3; ++j)
+    if (fluid_at(S, x - (j == 0), y - (j == 1), z - (j == 2))) return true;
   return false;
 }
 
 // Policy_Laplacian_Speed::Get_Laplacian_Speed(neigh, i) (src/Policy_Laplacian_Speed.h:22-36):
 // per axis j, -2 u(c)/h_j^2 + u(c+e_j)/h_j^2 + u(c-e_j)/h_j^2 with h_j^-2 = pow(1/h_j, 2),
 // accumulated in that order.
-__device__ inline double laplacian(const double* __restrict__ Ui, const int* sn, int x, int y, int z,
-                                   const Params& P) {
+__device__ inline double laplacian(const Stage& S, int i, int x, int y, int z, const Params& P) {
   double t = 0;
-  const double uc = rdv(Ui, cidx(sn, x, y, z));
+  const double uc = su(S, i, x, y, z);
   for (int j = 0; j < 3; ++j) {
     t -= 2 * uc * P.lih2[j];
-    t += rdv(Ui, cidx(sn, x + (j == 0), y + (j == 1), z + (j == 2))) * P.lih2[j];
-    t += rdv(Ui, cidx(sn, x - (j == 0), y - (j == 1), z - (j == 2))) * P.lih2[j];
+    t += su(S, i, x + (j == 0), y + (j == 1), z + (j == 2)) * P.lih2[j];
+    t += su(S, i, x - (j == 0), y - (j == 1), z - (j == 2)) * P.lih2[j];
   }
   return t;
 }
@@ -108,44 +130,33 @@ __device__ inline double laplacian(const double* __restrict__ Ui, const int* sn,
 // (src/Algorithms_Viscosity.h:24-30) then adds viscosity * Laplacian.
 // base: the acceleration the contributions add to (0 after the forced zero;
 // pipeline B's stage forces add to what a re-created cell holds).
-__device__ inline double face_accel(const double* const* U, const int* sn, const int8_t* __restrict__ lay,
-                                    const uint8_t* __restrict__ type, int64_t c, uint8_t fl, int x, int y, int z,
-                                    int i, const Params& P, double base = 0.0) {
+__device__ inline double face_accel(const Stage& S, uint8_t fl, int x, int y, int z, int i, const Params& P,
+                                    double base = 0.0) {
   if (fl & (1u << i)) return base;
-  bool fluid = is_fluid(type[c]);
-  bool apply = fluid;
-  if (!fluid && lay[c] != kEmpty) {
-    int m[3] = {x, y, z};
-    m[i] -= 1;
-    int64_t n = cidx(sn, m[0], m[1], m[2]);
-    apply = n >= 0 && lay[n] != kMissing && is_fluid(type[n]);
-  }
+  const int sc = s1(x, y, z);
+  bool fluid = is_fluid(S.type[sc]);
+  // convection and gravity on axis i: the cell is fluid, or it has a layer
+  // and its -e_i neighbour exists and is fluid
+  bool apply = fluid || (S.lay[sc] != kEmpty && fluid_at(S, x - (i == 0), y - (i == 1), z - (i == 2)));
   double a = base;
-  if (i == P.gaxis) {
-    bool g = fluid;
-    if (!fluid && lay[c] != kEmpty) {
-      int m[3] = {x, y, z};
-      m[i] -= 1;
-      int64_t n = cidx(sn, m[0], m[1], m[2]);
-      g = n >= 0 && lay[n] != kMissing && is_fluid(type[n]);
-    }
-    if (g) a = a + P.g;
-  }
-  if (apply) a = a + convection(U, sn, x, y, z, i, P);
-  if (P.nu != 0.0 && viscosity_applies(sn, lay, type, c, fluid, x, y, z))
-    a = a + laplacian(U[i], sn, x, y, z, P) * P.nu;
+  if (i == P.gaxis && apply) a = a + P.g;
+  if (apply) a = a + convection(S, x, y, z, i, P);
+  if (P.nu != 0.0 && viscosity_applies(S, fluid, x, y, z)) a = a + laplacian(S, i, x, y, z, P) * P.nu;
   return a;
 }
 
 // mode 0: acc = forces(u[ib]); mode 1: RK stage 1 (src/Algorithms_RungeKutta_RK2_TVD.h:31-43):
 // u1 = u0 + a(u0)*dt, forced; mode 2: stage 2 (:45-58 after the first projection):
 // acc = a(u1) and u0 = 0.5*u0 + 0.5*u1 + 0.5*acc*dt through the non-forced Set.
+// The speed field read by the stencils is staged per brick; the kernels write
+// other arrays only, so no block reads what another writes.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_forces(const int* __restrict__ blist, int nlive, const int* __restrict__ nbr,
                                                 const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
                                                 const uint8_t* __restrict__ flags, double* f64, size_t cap,
                                                 int ib, Params P, const Scalars* __restrict__ ds) {
   __shared__ int sn[kNbr];
+  __shared__ Stage S;
   const double dt = ds->dt;
   const double* U[3];
   for (int i = 0; i < 3; ++i) U[i] = f64 + (size_t)((MODE == 2 ? 1 : (MODE == 1 ? 0 : ib)) * 3 + i) * cap;
@@ -153,23 +164,25 @@ __global__ void __launch_bounds__(256) k_forces(const int* __restrict__ blist, i
     int b = blist[bi];
     if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
+    stage_forces(S, U, sn, lay, type);
+    __syncthreads();
     for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
       int64_t c = (int64_t)b * kCells + o;
-      if (lay[c] == kMissing) continue;
       int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+      if (S.lay[s1(x, y, z)] == kMissing) continue;
       uint8_t fl = flags[c];
       double a[3];
-      for (int i = 0; i < 3; ++i) a[i] = face_accel(U, sn, lay, type, c, fl, x, y, z, i, P);
+      for (int i = 0; i < 3; ++i) a[i] = face_accel(S, fl, x, y, z, i, P);
       if (MODE == 0) {
         for (int i = 0; i < 3; ++i) f64[(size_t)(AX + i) * cap + c] = a[i];
       } else if (MODE == 1) {
         for (int i = 0; i < 3; ++i)
-          f64[(size_t)(U1X + i) * cap + c] = f64[(size_t)(U0X + i) * cap + c] + a[i] * dt;
+          f64[(size_t)(U1X + i) * cap + c] = S.u[i][s1(x, y, z)] + a[i] * dt;
       } else {
         for (int i = 0; i < 3; ++i) {
           f64[(size_t)(AX + i) * cap + c] = a[i];
           if (!(fl & (1u << i))) {
-            double u0 = f64[(size_t)(U0X + i) * cap + c], u1 = f64[(size_t)(U1X + i) * cap + c];
+            double u0 = f64[(size_t)(U0X + i) * cap + c], u1 = S.u[i][s1(x, y, z)];
             f64[(size_t)(U0X + i) * cap + c] = 0.5 * u0 + 0.5 * u1 + 0.5 * a[i] * dt;
           }
         }
@@ -190,19 +203,22 @@ __global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ blis
                                                     const double* __restrict__ uz, double* ax, double* ay, double* az,
                                                     Params P) {
   __shared__ int sn[kNbr];
+  __shared__ Stage S;
   const double* U[3] = {ux, uy, uz};
   double* A[3] = {ax, ay, az};
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
     int b = blist[bi];
     if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
+    stage_forces(S, U, sn, lay, type);
+    __syncthreads();
     for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
       int64_t c = (int64_t)b * kCells + o;
-      if (lay[c] == kMissing) continue;
       int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+      if (S.lay[s1(x, y, z)] == kMissing) continue;
       uint8_t fl = flags[c];
       double a[3];
-      for (int i = 0; i < 3; ++i) a[i] = face_accel(U, sn, lay, type, c, fl, x, y, z, i, P, A[i][c]);
+      for (int i = 0; i < 3; ++i) a[i] = face_accel(S, fl, x, y, z, i, P, A[i][c]);
       for (int i = 0; i < 3; ++i) A[i][c] = a[i];
     }
     __syncthreads();
@@ -254,16 +270,48 @@ int rk_stage(Ctx* c, int stage) {
 // level is race-free. n == 0 gives 0/0 like the reference.
 __device__ inline int8_t lay_i(const int8_t* __restrict__ lay, int64_t i) { return i < 0 ? kMissing : lay[i]; }
 
+__device__ inline uint32_t layer_bit(int l) { return 1u << (l < 31 ? l : 31); }
+
+// The layers present in each live brick (bit l for layer l), so that a level's
+// launch skips the bricks it cannot write.
+__global__ void __launch_bounds__(256) k_layer_mask(const int* __restrict__ blist, const int8_t* __restrict__ lay,
+                                                    uint32_t* __restrict__ lmask) {
+  __shared__ uint32_t sw[8];
+  const int b = blist[blockIdx.x];
+  uint32_t m = 0;
+  for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+    const int8_t l = lay[(int64_t)b * kCells + o];
+    if (l >= 0) m |= layer_bit(l);
+  }
+  m = __reduce_or_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; ++w) m |= sw[w];
+    lmask[b] = m;
+  }
+}
+
+// A face of a cell in brick b is written at level L only when its cell or the
+// cell behind it (-e_i) has layer L, so only when b or one of its -x, -y, -z
+// face neighbours holds a layer-L cell; other bricks are skipped whole.
 __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ blist, int nlive, const int* __restrict__ nbr,
                                                      const int8_t* __restrict__ lay, const uint8_t* __restrict__ flags,
-                                                     double* fx, double* fy, double* fz, int L) {
+                                                     const uint32_t* __restrict__ lmask, double* fx, double* fy,
+                                                     double* fz, int L) {
   double* const F[3] = {fx, fy, fz};
   __shared__ int sn[kNbr];
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
     int b = blist[bi];
     if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
-    for (int o = threadIdx.x; o < kCells; o += blockDim.x) {
+    uint32_t near = lmask[b];
+    for (int i = 0; i < 3; ++i) {
+      const int nb = sn[nbr_index(i == 0 ? -1 : 0, i == 1 ? -1 : 0, i == 2 ? -1 : 0)];
+      if (nb >= 0) near |= lmask[nb];
+    }
+    const bool skip = !(near & layer_bit(L));
+    for (int o = skip ? kCells : threadIdx.x; o < kCells; o += blockDim.x) {
       int64_t c = (int64_t)b * kCells + o;
       int8_t lB = lay[c];
       if (lB < 0) continue;  // c must exist with a layer
@@ -330,9 +378,10 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
 int extrapolate_field(Ctx* c, double* const* F) {
   if (c->nlive_host == 0) return MAC_OK;
   prof_begin(c, PH_EXTRAPOLATE);
+  k_layer_mask<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->lay, c->lmask); MAC_COUNT(c);
   for (int L = 1; L <= c->dp.layer_max + 1; ++L) {
-    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, F[0], F[1],
-                                                        F[2], L); MAC_COUNT(c);
+    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, c->lmask,
+                                                        F[0], F[1], F[2], L); MAC_COUNT(c);
   }
   prof_end(c, PH_EXTRAPOLATE);
   return check(cudaGetLastError());

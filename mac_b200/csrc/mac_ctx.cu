@@ -183,7 +183,7 @@ static void free_all(Ctx* c) {
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
   cudaFree(c->px2); cudaFree(c->py2); cudaFree(c->pz2); cudaFree(c->pbrick);
-  cudaFree(c->bcount); cudaFree(c->bcursor); cudaFree(c->boff);
+  cudaFree(c->bcount); cudaFree(c->bcursor); cudaFree(c->boff); cudaFree(c->lmask);
   cudaFree(c->ds);
   if (c->hs) cudaFreeHost(c->hs);
   if (c->hs_lag) cudaFreeHost(c->hs_lag);
@@ -279,6 +279,7 @@ static int create(const mac_params* p, Ctx** out) {
   A(dalloc(&c->pz2, c->cap_particles));
   A(dalloc(&c->pbrick, c->cap_particles));
   A(dalloc(&c->bcount, c->cap_bricks + 1));
+  A(dalloc(&c->lmask, c->cap_bricks));
   A(dalloc(&c->bcursor, (size_t)(c->cap_bricks + 1) * kCells));
   A(dalloc(&c->boff, c->cap_bricks + 2));
   A(dalloc(&c->ds, 1));

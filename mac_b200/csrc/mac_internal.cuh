@@ -160,6 +160,7 @@ struct Ctx {
   double* pz2 = nullptr;
   int* pbrick = nullptr;      // 512 * brick + cell of each particle's cell (brick cap: no brick)
   int* bcount = nullptr;      // [cap+1] particles per brick (last: no brick)
+  uint32_t* lmask = nullptr;  // [cap] per live brick: bit l set when a cell has layer l (l >= 31 on bit 31)
   int* bcursor = nullptr;     // [(cap+1)*512] particles per (brick, cell), then each cell's running slot
   int64_t* boff = nullptr;    // [cap+2] bin offsets
   // pressure system and solver
