@@ -340,27 +340,33 @@ __device__ inline int s1_off(int f) {
   return (f & 1) ? mag : -mag;
 }
 
-template <class V, class F>
-__device__ inline void stage_h1(V* s, int b, const int64_t* sb, V zero, F val) {
-#pragma unroll
-  for (int k = 0; k < kCPT; ++k) {
-    int o = threadIdx.x + kBT * k;
-    s[s1_of(o)] = val((int64_t)b * kCells + o);
+// The face halos: 384 slots, three per thread. Thread t takes position
+// (u, v) = (t & 7, (t >> 3) & 7) on the three faces of sign t >> 6 (0: -x,
+// -y, -z; 1: +x, +y, +z), one per axis a; the element is cell off of face
+// neighbour f's brick (the row of that brick next to this one) and lands in
+// staging slot `slot`.
+static_assert(kBT == 128, "the halo map gives each of 128 threads three slots");
+struct HaloSlot {
+  int slot;  // staging slot
+  int f;     // face: 2 * axis + sign (the index into the face bases)
+  int off;   // cell within the neighbour brick
+};
+__device__ inline HaloSlot halo_slot(int a) {
+  const int t = threadIdx.x & 63, sg = threadIdx.x >> 6, u = t & 7, v = t >> 3;
+  const int e = sg ? 8 : -1, w = sg ? 0 : 7;
+  HaloSlot h;
+  h.f = 2 * a + sg;
+  if (a == 0) {
+    h.slot = s1(e, u, v);
+    h.off = w + 8 * u + 64 * v;
+  } else if (a == 1) {
+    h.slot = s1(u, e, v);
+    h.off = u + 8 * w + 64 * v;
+  } else {
+    h.slot = s1(u, v, e);
+    h.off = u + 8 * v + 64 * w;
   }
-  for (int j = threadIdx.x; j < 384; j += kBT) {
-    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
-    int x, y, z;
-    int64_t gi;
-    switch (f) {
-      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
-      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
-      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
-      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
-      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
-      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
-    }
-    s[s1(x, y, z)] = gi < 0 ? zero : val(gi);
-  }
+  return h;
 }
 
 // The same staging of a plain array: the brick's own 512 cells with 16-byte
@@ -378,50 +384,32 @@ __device__ inline void load4(const float* p, V* v) {
   v[0] = (V)a.x; v[1] = (V)a.y; v[2] = (V)a.z; v[3] = (V)a.w;
 }
 
-// Only the face halos of stage_h1 (value 0 where the neighbour brick is absent).
+// The face halos of a brick staging: s[slot] = val(global index), 0 where the
+// neighbour brick is absent; all three loads are issued before any store.
 template <class S, class F>
 __device__ inline void stage_h1_halo(S* s, const int64_t* sb, F val) {
-  for (int j = threadIdx.x; j < 384; j += kBT) {
-    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
-    int x, y, z;
-    int64_t gi;
-    switch (f) {
-      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
-      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
-      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
-      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
-      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
-      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
-    }
-    s[s1(x, y, z)] = gi < 0 ? (S)0 : (S)val(gi);
+  S hv[3];
+  int hs[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const HaloSlot h = halo_slot(a);
+    hs[a] = h.slot;
+    hv[a] = sb[h.f] < 0 ? (S)0 : (S)val(sb[h.f] + h.off);
   }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) s[hs[a]] = hv[a];
 }
 
 template <class S, class T>
 __device__ inline void stage_arr(S* s, const T* __restrict__ a, int b, const int64_t* sb) {
   static_assert(kBT * 4 == kCells, "one 4-cell vector per thread");
-  {
-    const int o = 4 * threadIdx.x;
-    S v[4];
-    load4(a + (int64_t)b * kCells + o, v);
-    const int si = s1_of(o);
+  const int o = 4 * threadIdx.x;
+  S v[4];
+  load4(a + (int64_t)b * kCells + o, v);
+  stage_h1_halo(s, sb, [&](int64_t i) { return a[i]; });
+  const int si = s1_of(o);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) s[si + q] = v[q];
-  }
-  for (int j = threadIdx.x; j < 384; j += kBT) {
-    int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
-    int x, y, z;
-    int64_t gi;
-    switch (f) {
-      case 0: x = -1; y = u; z = v; gi = sb[0] < 0 ? -1 : sb[0] + 7 + 8 * y + 64 * z; break;
-      case 1: x = 8; y = u; z = v; gi = sb[1] < 0 ? -1 : sb[1] + 8 * y + 64 * z; break;
-      case 2: y = -1; x = u; z = v; gi = sb[2] < 0 ? -1 : sb[2] + x + 56 + 64 * z; break;
-      case 3: y = 8; x = u; z = v; gi = sb[3] < 0 ? -1 : sb[3] + x + 64 * z; break;
-      case 4: z = -1; x = u; y = v; gi = sb[4] < 0 ? -1 : sb[4] + x + 8 * y + 448; break;
-      default: z = 8; x = u; y = v; gi = sb[5] < 0 ? -1 : sb[5] + x + 8 * y; break;
-    }
-    s[s1(x, y, z)] = gi < 0 ? (S)0 : (S)a[gi];
-  }
+  for (int q = 0; q < 4; ++q) s[si + q] = v[q];
 }
 
 // Kernels of an iterative solve that the host enqueues ahead of its

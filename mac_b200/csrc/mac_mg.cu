@@ -116,14 +116,21 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  uint16_t mk[kCPT];
+  double rk[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    const int64_t c = (int64_t)b * kCells + threadIdx.x + kBT * k;
+    mk[k] = fmask[c];
+    rk[k] = r[c];
+  }
   __syncthreads();
   stage_arr(se, e, b, sb);
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
-    int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = fmask[c];
+    uint16_t m = mk[k];
     T v = 0;
     if (m & kDomainBit) {
       int si = s1_of(o);
@@ -134,7 +141,7 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
         if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
         if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
       }
-      v = (T)r[c] - me;
+      v = (T)rk[k] - me;
     }
     res[o] = v;
   }
@@ -149,9 +156,14 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   }
 }
 
+// Level-1 parent (within its brick's 64) of cell `off` of a level-0 brick.
+__device__ inline int parent_off(int off) { return ((off & 7) >> 1) + 4 * (((off >> 3) & 7) >> 1) + 16 * (off >> 7); }
+
 // Post-smoothing at level 0. FIRST: ep = e + P e1 (coarse correction added on
-// the fly), out = ep + w D^-1 (r - M ep) into eout. Otherwise a plain sweep
-// writing the FP64 preconditioned residual z and the block's partial r.z.
+// the fly, the level-1 parent of every staged cell read as it is staged), out
+// = ep + w D^-1 (r - M ep) into eout. Otherwise a plain sweep writing the FP64
+// preconditioned residual z and the block's partial r.z. The cells' r and
+// face masks are loaded first, so they are in flight during the staging.
 template <class T, bool FIRST>
 __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                const uint16_t* __restrict__ fmask, const double* __restrict__ r,
@@ -161,55 +173,34 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
-  __shared__ T s1p[64 + 96];  // FIRST: level-1 parents of the brick (64) and of its face halos (6 x 16)
   const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  __syncthreads();
-  stage_arr(se, e, b, sb);
-  if (FIRST) {
-    // parents staged once: own level-1 cells, then for face f the 4x4 level-1
-    // cells of the neighbour brick next to it
-    for (int j = threadIdx.x; j < 160; j += kBT) {
-      T v;
-      if (j < 64) {
-        v = e1[(size_t)b * 64 + j];
-      } else {
-        const int f = (j - 64) >> 4, p = (j - 64) & 3, q = ((j - 64) >> 2) & 3;
-        const int64_t base = sb[f];
-        int l;
-        switch (f) {
-          case 0: l = 3 + 4 * p + 16 * q; break;
-          case 1: l = 4 * p + 16 * q; break;
-          case 2: l = p + 12 + 16 * q; break;
-          case 3: l = p + 16 * q; break;
-          case 4: l = p + 4 * q + 48; break;
-          default: l = p + 4 * q; break;
-        }
-        v = base < 0 ? (T)0 : e1[(base >> 9) * 64 + l];
-      }
-      s1p[j] = v;
-    }
-    __syncthreads();
+  uint16_t mk[kCPT];
+  double rk[kCPT];
 #pragma unroll
-    for (int k = 0; k < kCPT; ++k) {
-      const int o = threadIdx.x + kBT * k;
-      const int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
-      se[s1_of(o)] += s1p[(x >> 1) + 4 * (y >> 1) + 16 * (z >> 1)];
-    }
-    for (int j = threadIdx.x; j < 384; j += kBT) {
-      const int f = j >> 6, t = j & 63, u = t & 7, v = t >> 3;
-      int x, y, z;
-      switch (f) {
-        case 0: x = -1; y = u; z = v; break;
-        case 1: x = 8; y = u; z = v; break;
-        case 2: y = -1; x = u; z = v; break;
-        case 3: y = 8; x = u; z = v; break;
-        case 4: z = -1; x = u; y = v; break;
-        default: z = 8; x = u; y = v; break;
-      }
-      se[s1(x, y, z)] += s1p[64 + 16 * f + (u >> 1) + 4 * (v >> 1)];
-    }
+  for (int k = 0; k < kCPT; ++k) {
+    const int64_t c = (int64_t)b * kCells + threadIdx.x + kBT * k;
+    mk[k] = fmask[c];
+    rk[k] = r[c];
+  }
+  if (FIRST) {
+    // the brick: cells 4t..4t+3 of one row share two level-1 parents
+    const int o4 = 4 * threadIdx.x;
+    T v[4];
+    load4(e + (int64_t)b * kCells + o4, v);
+    const int p0 = parent_off(o4);
+    const T c0 = e1[(size_t)b * 64 + p0], c1 = e1[(size_t)b * 64 + p0 + 1];
+    __syncthreads();
+    stage_h1_halo(se, sb, [&](int64_t i) { return e[i] + e1[(i >> 9) * 64 + parent_off((int)(i & 511))]; });
+    const int si = s1_of(o4);
+    se[si] = v[0] + c0;
+    se[si + 1] = v[1] + c0;
+    se[si + 2] = v[2] + c1;
+    se[si + 3] = v[3] + c1;
+  } else {
+    __syncthreads();
+    stage_arr(se, e, b, sb);
   }
   __syncthreads();
   double rz = 0;
@@ -217,7 +208,7 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = fmask[c];
+    uint16_t m = mk[k];
     if (!(m & kDomainBit)) {
       if (FIRST) eout[c] = (T)0;
       else z[c] = 0.0;
@@ -231,7 +222,7 @@ __global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, cons
       if (m & (1u << (8 + f))) me += ih2[f >> 1] * epc;
       if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
     }
-    double rc = r[c];
+    double rc = rk[k];
     T out = epc + om * (T)P.dtab[active_index(m)] * ((T)rc - me);
     if (FIRST) {
       eout[c] = out;
