@@ -459,44 +459,39 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     eout[i] = (T)0;
     return;
   }
-  int x = o % D, y = (o / D) % D, z = o / (D * D);
-  // slot of each neighbour's brick in the shared table (0 = this brick)
-  int64_t n[6];
-  int k[6];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const int c[3] = {x, y, z};
-    n[2 * a] = lidx_s<D>(sb, a == 0 ? x - 1 : x, a == 1 ? y - 1 : y, a == 2 ? z - 1 : z);
-    n[2 * a + 1] = lidx_s<D>(sb, a == 0 ? x + 1 : x, a == 1 ? y + 1 : y, a == 2 ? z + 1 : z);
-    k[2 * a] = c[a] == 0 ? 1 + 2 * a : 0;
-    k[2 * a + 1] = c[a] == D - 1 ? 2 + 2 * a : 0;
-  }
-  // e plus the coarse correction at cell j of the brick in slot kk
-  auto ev = [&](int64_t j, int kk) -> T {
-    T v = e[j];
+  const int x = o % D, y = (o / D) % D, z = o / (D * D);
+  // e plus the coarse correction at local cell (lx, ly, lz) of the brick in
+  // table slot k (0 = this brick)
+  auto ev = [&](int k, int lx, int ly, int lz) -> T {
+    const int nb = sb[k];
+    T v = e[(size_t)nb * N + lx + D * ly + D * D * lz];
     if (WITH_COARSE) {
-      if (D == 2) {
-        v += ec[sdi[7 * (threadIdx.x / N) + kk]];
-      } else {
-        const int nb = (int)(j / N), no = (int)(j % N);
-        const int xx = no % D, yy = (no / D) % D, zz = no / (D * D);
-        v += ec[(size_t)nb * H * H * H + (xx >> 1) + H * (yy >> 1) + H * H * (zz >> 1)];
-      }
+      if (D == 2) v += ec[sdi[7 * (threadIdx.x / N) + k]];
+      else v += ec[(size_t)nb * H * H * H + (lx >> 1) + H * (ly >> 1) + H * H * (lz >> 1)];
     }
     return v;
   };
+  // the six neighbours: slot and local coordinates (an absent neighbour reads
+  // this cell and drops out through its zero weight)
   T wl[3], wr[3], vl[3], vr[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const bool hl = n[2 * a] >= 0, hr = n[2 * a + 1] >= 0;
-    const int64_t jl = hl ? n[2 * a] : (int64_t)i;
-    const int64_t jr = hr ? n[2 * a + 1] : (int64_t)i;
+    const int c[3] = {x, y, z};
+    int pl[3] = {x, y, z}, pr[3] = {x, y, z};
+    int kl = 0, kr = 0;
+    if (c[a] > 0) pl[a] = c[a] - 1;
+    else { kl = 1 + 2 * a; pl[a] = D - 1; }
+    if (c[a] < D - 1) pr[a] = c[a] + 1;
+    else { kr = 2 + 2 * a; pr[a] = 0; }
+    const bool hl = sb[kl] >= 0, hr = sb[kr] >= 0;
+    if (!hl) { kl = 0; pl[0] = x; pl[1] = y; pl[2] = z; }
+    if (!hr) { kr = 0; pr[0] = x; pr[1] = y; pr[2] = z; }
     wl[a] = w[a * ncap + i];
-    vl[a] = ev(jl, hl ? k[2 * a] : 0);
-    wr[a] = hr ? w[a * ncap + jr] : (T)0;
-    vr[a] = ev(jr, hr ? k[2 * a + 1] : 0);
+    vl[a] = ev(kl, pl[0], pl[1], pl[2]);
+    wr[a] = hr ? w[a * ncap + (size_t)sb[kr] * N + pr[0] + D * pr[1] + D * D * pr[2]] : (T)0;
+    vr[a] = ev(kr, pr[0], pr[1], pr[2]);
   }
-  T ecc = ev((int64_t)i, 0);
+  T ecc = ev(0, x, y, z);
   T s = w[3 * ncap + i] * ecc;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -772,9 +767,23 @@ __global__ void __launch_bounds__(1024) kd_coarsest_inverse(DView<T> L, double* 
   if (threadIdx.x == 0) *ok = 1;
 }
 
+// Block-wide copy with eight independent loads per thread in flight before
+// their stores (one block moves the coarse levels' weights, ~100 KB, into
+// shared memory every V-cycle: a load-store chain per element would pay the
+// memory latency once per element).
 template <class T>
 __device__ void blk_copy(T* dst, const T* src, int64_t n) {
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  constexpr int U = 8;
+  const int64_t step = blockDim.x;
+  int64_t i = threadIdx.x;
+  for (; i + (U - 1) * step < n; i += U * step) {
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = src[i + u * step];
+#pragma unroll
+    for (int u = 0; u < U; ++u) dst[i + u * step] = v[u];
+  }
+  for (; i < n; i += step) dst[i] = src[i];
 }
 
 template <class T>
@@ -828,13 +837,21 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
     const int l = hi - 1;
     const DView<T>& L = SL[l];
     if (*inv_ok && L.n <= 64) {
+      // row i of inv r by the 16 lanes i*16..i*16+15 (j = lane part + 16 q),
+      // summed over the lanes with shuffles; the block holds 1024 threads
       const int n = (int)L.n;
-      if ((int)threadIdx.x < n) {
-        const int i = threadIdx.x;
-        double s = 0.0;
-        for (int j = 0; j < n; ++j) s += inv[i * 64 + j] * (double)L.r[j];
-        cur(l)[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
+      const int i = threadIdx.x >> 4, p = threadIdx.x & 15;
+      double s = 0.0;
+      if (i < n) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int j = p + 16 * q;
+          if (j < n) s += inv[i * 64 + j] * (double)L.r[j];
+        }
       }
+#pragma unroll
+      for (int m = 8; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m, 16);
+      if (i < n && p == 0) cur(l)[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
       __syncthreads();
     } else {
       blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true);

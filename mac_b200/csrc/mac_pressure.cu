@@ -318,28 +318,30 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   __shared__ double sp[kS1];  // the new direction on the brick and its face halo
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  __syncthreads();
-  double be = first ? 0.0 : ds->beta;
-  if (first) {
-    stage_arr(sp, z, b, sb);
-  } else {
-    // p = z + beta p_old: the brick with vector loads of both, the halo with scalars
-    const int o4 = 4 * threadIdx.x;
-    double vz[4], vp[4];
-    load4(z + (int64_t)b * kCells + o4, vz);
-    load4(pold + (int64_t)b * kCells + o4, vp);
-    const int si = s1_of(o4);
+  const double be = first ? 0.0 : ds->beta;
+  // the cells' face masks and the brick's z and p_old (16-byte vector loads)
+  // are in flight before the barrier the halo staging waits on
+  uint16_t mk[kCPT];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sp[si + q] = vz[q] + be * vp[q];
-    stage_h1_halo(sp, sb, [&](int64_t i) { return z[i] + be * pold[i]; });
-  }
+  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
+  const int o4 = 4 * threadIdx.x;
+  double vz[4], vp[4] = {0.0, 0.0, 0.0, 0.0};
+  load4(z + (int64_t)b * kCells + o4, vz);
+  if (!first) load4(pold + (int64_t)b * kCells + o4, vp);
+  __syncthreads();
+  // p = z (first) or z + beta p_old, on the brick and its face halo
+  if (first) stage_h1_halo(sp, sb, [&](int64_t i) { return z[i]; });
+  else stage_h1_halo(sp, sb, [&](int64_t i) { return z[i] + be * pold[i]; });
+  const int si4 = s1_of(o4);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) sp[si4 + k] = first ? vz[k] : vz[k] + be * vp[k];
   __syncthreads();
   double pq = 0;
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = fmask[c];
+    uint16_t m = mk[k];
     if (!(m & kDomainBit)) {
       pnew[c] = 0.0;
       q[c] = 0.0;
