@@ -36,6 +36,32 @@ __device__ inline int64_t parent1(int64_t n) {
   return (n >> 9) * 64 + ((o & 7) >> 1) + 4 * (((o >> 3) & 7) >> 1) + 16 * ((o >> 6) >> 1);
 }
 
+// Coordinates of cell i of an nx x ny x nz grid of n cells. Below 2^24 cells
+// the quotients come from float reciprocals with one exact correction step
+// each (the product's error stays under one unit there); larger grids divide
+// in 64 bits.
+__device__ inline int qdiv(int i, int d, float rd) {
+  int q = (int)((float)i * rd);
+  const int r = i - q * d;
+  if (r < 0) --q;
+  else if (r >= d) ++q;
+  return q;
+}
+__device__ inline void coords3(int64_t i, int nx, int ny, int64_t n, int& x, int& y, int& z) {
+  if (n < (int64_t)(1 << 24)) {
+    const int ii = (int)i;
+    const int xy = qdiv(ii, nx, 1.0f / (float)nx);
+    x = ii - xy * nx;
+    z = qdiv(xy, ny, 1.0f / (float)ny);
+    y = xy - z * ny;
+  } else {
+    const int64_t xy = i / nx;
+    x = (int)(i - xy * nx);
+    z = (int)(xy / ny);
+    y = (int)(xy - (int64_t)z * ny);
+  }
+}
+
 // ---------------------------------------------------------------- level 0
 // Two Jacobi sweeps from zero, fused: e1 = w D^-1 r, e = e1 + w D^-1 (r - M e1)
 // = w D^-1 ((2 - w) r + sum_f ih2_f e1(n_f)).
@@ -278,33 +304,23 @@ __device__ inline void load_lbricks(const int* __restrict__ dbl, int nd, const i
   }
 }
 
-// Pool index of cell (x, y, z) of local brick row sb (coordinates may leave the
-// brick by one cell along one axis), -1 if that brick is absent.
-template <int D>
-__device__ inline int64_t lidx_s(const int* sb, int x, int y, int z) {
-  int k = 0;
-  if (x < 0) { k = 1; x += D; }
-  else if (x >= D) { k = 2; x -= D; }
-  else if (y < 0) { k = 3; y += D; }
-  else if (y >= D) { k = 4; y -= D; }
-  else if (z < 0) { k = 5; z += D; }
-  else if (z >= D) { k = 6; z -= D; }
-  const int nb = sb[k];
-  if (nb < 0) return -1;
-  return (int64_t)nb * (D * D * D) + x + D * y + D * D * z;
-}
-
 // Weights w: 6 slots of ncap entries: [0..2] left faces, [3] diagonal, [4] inverse, [5] Dirichlet part.
 // The six neighbour indices of cell (x, y, z) (-1 absent): [2a] = -e_a, [2a+1] = +e_a.
 template <int D>
 __device__ inline void lnbrs(const int* sb, int x, int y, int z, int64_t* n) {
+  constexpr int N = D * D * D;
+  const int c[3] = {x, y, z};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    int p[3] = {x, y, z};
-    p[a] -= 1;
-    n[2 * a] = lidx_s<D>(sb, p[0], p[1], p[2]);
-    p[a] += 2;
-    n[2 * a + 1] = lidx_s<D>(sb, p[0], p[1], p[2]);
+    int pl[3] = {x, y, z}, pr[3] = {x, y, z};
+    int kl = 0, kr = 0;
+    if (c[a] > 0) pl[a] = c[a] - 1;
+    else { kl = 1 + 2 * a; pl[a] = D - 1; }
+    if (c[a] < D - 1) pr[a] = c[a] + 1;
+    else { kr = 2 + 2 * a; pr[a] = 0; }
+    const int bl = sb[kl], br = sb[kr];
+    n[2 * a] = bl < 0 ? -1 : (int64_t)bl * N + pl[0] + D * pl[1] + D * D * pl[2];
+    n[2 * a + 1] = br < 0 ? -1 : (int64_t)br * N + pr[0] + D * pr[1] + D * D * pr[2];
   }
 }
 
@@ -544,7 +560,8 @@ __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
     L.e[i] = (T)0;
     return;
   }
-  int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+  int x, y, z;
+  coords3(i, L.nx, L.ny, L.n, x, y, z);
   int c[3] = {x, y, z};
   int dim[3] = {L.nx, L.ny, L.nz};
   int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
@@ -569,8 +586,8 @@ __global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ 
   const int k = (int)(g & 7);
   T s = 0;
   if (I < C.n) {
-    const int XY = (int)(I / C.nx);
-    const int X = (int)(I - (int64_t)XY * C.nx), Y = XY % C.ny, Z = XY / C.ny;
+    int X, Y, Z;
+    coords3(I, C.nx, C.ny, C.n, X, Y, Z);
     const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
     if (x < F.nx && y < F.ny && z < F.nz) {
       const int64_t i = F.at(x, y, z);
@@ -593,7 +610,8 @@ __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__
     eout[i] = (T)0;
     return;
   }
-  int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((int64_t)L.nx * L.ny));
+  int x, y, z;
+  coords3(i, L.nx, L.ny, L.n, x, y, z);
   auto ev = [&](int64_t j, int xx, int yy, int zz) -> T {
     T v = ein[j];
     if (WITH_COARSE) v += C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
@@ -640,6 +658,7 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const T* __restrict__ w = L.w;
   const T* __restrict__ r = L.r;
+  const float rnx = 1.0f / (float)nx, rny = 1.0f / (float)ny;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const T dinv = w[4 * n + i];
     if (dinv == 0) {
@@ -650,8 +669,8 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce
       eout[i] = (T)kOmega * dinv * r[i];
       continue;
     }
-    const int xy = i / nx;
-    const int x = i - xy * nx, y = xy % ny, z = xy / ny;
+    const int xy = qdiv(i, nx, rnx);
+    const int x = i - xy * nx, z = qdiv(xy, ny, rny), y = xy - z * ny;
     auto ev = [&](int j, int xx, int yy, int zz) -> T {
       T v = ein[j];
       if (ce) v += ce[(xx >> 1) + cnx * ((yy >> 1) + cny * (zz >> 1))];
@@ -692,8 +711,8 @@ __device__ void blk_restrict(const DView<T>& F, const T* fe, const DView<T>& C) 
     const int I = g >> 3, k = g & 7;
     T s = 0;
     if (I < (int)C.n) {
-      const int XY = I / C.nx;
-      const int X = I - XY * C.nx, Y = XY % C.ny, Z = XY / C.ny;
+      int X, Y, Z;
+      coords3(I, C.nx, C.ny, C.n, X, Y, Z);
       const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
       if (x < F.nx && y < F.ny && z < F.nz) {
         const int i = x + F.nx * (y + F.ny * z);
