@@ -1,0 +1,74 @@
+"""Where the pressure solve's CG loop stops, on a 64^3 pool + spheres world.
+
+The multigrid forms apply each iteration's update x += alpha p, r -= alpha q
+and its convergence test inside the next V-cycle's first kernel, read the
+done flag one iteration late and, near convergence, test right after that
+kernel; the Jacobi-CG form keeps one host read per iteration. In every form a
+cap of k iterations stops the solve after exactly k updates of x, more
+iterations bring the iterate closer to the converged one, and a right-hand
+side of zero takes no iteration and leaves the pressure at zero.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+N = 64
+
+
+@pytest.fixture(scope="module")
+def pool64():
+    from mac_b200.state import pool_spheres_world
+    from mac_b200.world import setup_passes
+    return setup_passes(pool_spheres_world(N, r_range=(6.0 * N / 128, 20.0 * N / 128)))
+
+
+def _ctx(s, solver, rtol, max_iters):
+    from mac_b200.gpu import Context
+    return Context(s.params, max_bricks=int(s.nbricks * 1.2) + 64, max_particles=1024, solver=solver, rtol=rtol,
+                   max_iters=max_iters)
+
+
+@pytest.mark.parametrize("solver", ["mixed", "mgpcg64", "cg64"])
+@pytest.mark.parametrize("cap", [1, 2, 5])
+def test_iteration_cap_is_exact(pool64, solver, cap):
+    with _ctx(pool64, solver, 1e-14, cap) as ctx:
+        ctx.upload(pool64)
+        ctx.project(0, allow_not_converged=True)
+        st = ctx.stats()
+    assert st["iterations"] == cap
+    assert st["relres"] > 1e-14
+
+
+@pytest.mark.parametrize("solver", ["mixed", "mgpcg64"])
+def test_capped_solves_approach_the_converged_one(pool64, solver):
+    """More iterations bring the pressure closer to the converged solve's (the
+    capped solves' iterates are the loop's own, not ones a late stop skipped)."""
+    ps = []
+    for cap in (3, 6, 9, 200):
+        with _ctx(pool64, solver, 1e-12, cap) as ctx:
+            ctx.upload(pool64)
+            ctx.project(0, allow_not_converged=True)
+            got = ctx.download()
+        ex = got.exists.astype(bool)
+        ps.append(got.f64["p"][ex].copy())
+    ref = ps[-1]
+    err = [float(np.linalg.norm(p - ref) / np.linalg.norm(ref)) for p in ps[:-1]]
+    assert err[0] > err[1] > err[2], err
+    assert err[2] < 1e-3, err
+
+
+@pytest.mark.parametrize("solver", ["mixed", "mgpcg64", "cg64"])
+def test_zero_rhs_takes_no_iteration(pool64, solver):
+    z = copy.copy(pool64)
+    z.f64 = {k: (np.zeros_like(v) if k.startswith("u") else v) for k, v in pool64.f64.items()}
+    with _ctx(z, solver, 1e-10, 100) as ctx:
+        ctx.upload(z)
+        ctx.project(0)
+        st = ctx.stats()
+        got = ctx.download()
+    assert st["iterations"] == 0
+    ex = got.exists.astype(bool)
+    assert np.all(got.f64["p"][ex] == 0.0)
