@@ -63,6 +63,9 @@ __device__ inline void coords3(int64_t i, int nx, int ny, int64_t n, int& x, int
 }
 
 // ---------------------------------------------------------------- level 0
+// The level-0 sweeps wait mostly on memory latency; in the FP32 form their
+// register caps let 16 blocks of 128 threads share an SM without spills (the
+// FP64 pre-sweep takes 12; the FP64 post-sweeps would spill under any cap).
 // Two Jacobi sweeps from zero, fused: e1 = w D^-1 r, e = e1 + w D^-1 (r - M e1)
 // = w D^-1 ((2 - w) r + sum_f ih2_f e1(n_f)).
 // With update (every CG iteration but the first) the kernel first finishes
@@ -71,7 +74,7 @@ __device__ inline void coords3(int64_t i, int nx, int ny, int64_t n, int& x, int
 // so a block staging its face halos reads the old r of its neighbours and
 // forms their new r on the fly with the same expression.
 template <class T>
-__global__ void __launch_bounds__(kBT) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                               const uint16_t* __restrict__ fmask, const double* __restrict__ rin,
                                               double* __restrict__ rout, double* __restrict__ x,
                                               const double* __restrict__ p, const double* __restrict__ q,
@@ -191,7 +194,7 @@ __device__ inline int parent_off(int off) { return ((off & 7) >> 1) + 4 * (((off
 // preconditioned residual z and the block's partial r.z. The cells' r and
 // face masks are loaded first, so they are in flight during the staging.
 template <class T, bool FIRST>
-__global__ void __launch_bounds__(kBT) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
                                                const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P,
