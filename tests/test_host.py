@@ -96,3 +96,25 @@ def test_cpu_reference_arm_runs(tmp_path):
     v, kind, secs, fcs, wall = bench.cpu_reference_run(1, 1, str(tmp_path))
     assert v > 0 and fcs > 0
     assert kind in ("reference", "port")
+
+
+def test_roofline_models_count_cg_iterations():
+    """The V-cycle phase's regions hold one V-cycle per CG iteration (with the
+    update its first kernel applies) plus one update-only region per solve, so
+    its launch is a CG iteration: bytes per launch (V-cycle + 48 B update per
+    unknown) over the phase time divided by the iteration count."""
+    sys.path.insert(0, ROOT)
+    import bench
+    stats = {"unknowns": 1_000_000}
+    # 10 steps, 2 solves each, 18 iterations per solve: 360 V-cycles in 380 regions
+    prof = {"vcycle": (150.0, 380), "spmv": (36.0, 360), "move": (40.0, 10)}
+    rl = bench.roofline_models(stats, prof, 8_000_000, 2_000_000, mg_bytes=4, cg_iterations=360)
+    vc = 117.0 * 8.0 / 7.0 * 0.5
+    assert rl["vcycle"]["launches"] == 360
+    assert abs(rl["vcycle"]["bytes_per_launch"] - (vc + 48.0) * 1e6) < 1e-3
+    assert abs(rl["vcycle"]["gbs"] - (vc + 48.0) * 1e6 / (150.0 / 360 * 1e-3) / 1e9) < 1e-9
+    # the other phases count their timed regions
+    assert rl["spmv"]["launches"] == 360 and rl["move"]["launches"] == 10
+    assert abs(rl["move"]["bytes_per_launch"] - 48.0 * 8_000_000) < 1e-3
+    # the CG scalars move no bulk data and carry no bytes model
+    assert "cg_vector" not in rl
