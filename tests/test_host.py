@@ -1,6 +1,6 @@
 """Host-side checks that need no GPU: the C-ABI library and its exports, the
 state container, the multi-rank reduction of bench.py (gloo, two ranks), the
-CPU reference arm of the benchmark."""
+CPU reference arm of the benchmark and its roofline accounting."""
 import ctypes
 import os
 import re
