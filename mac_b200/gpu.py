@@ -293,7 +293,11 @@ class Context:
         self._check(self.lib.mac_query_sizes(self.h, ctypes.byref(nb), ctypes.byref(npart)), "mac_query_sizes")
         return nb.value, npart.value
 
-    def download(self, host: HostState | None = None) -> State:
+    def download(self, host: HostState | None = None, to_state: bool = True):
+        """Reads the device state through mac_download_state into ``host`` (a
+        new HostState if it is missing or too small). Returns it as a State
+        (key-sorted copies of the arrays), or, with ``to_state=False``, the
+        HostState itself with the arrays as the C-ABI wrote them."""
         nb, npart = self.sizes()
         if host is None or host.nbricks < nb or len(host.pos) < 3 * npart:
             host = HostState(nb, npart, depth=bool(self.params.depth_mode))
@@ -302,7 +306,7 @@ class Context:
         self._check(self.lib.mac_download_state(self.h, ctypes.byref(st)), "mac_download_state")
         host.nbricks, host.nparticles = st.nbricks, st.nparticles
         host.t, host.dt, host.step = st.t, st.dt, st.step
-        return host.to_state(self.params)
+        return host.to_state(self.params) if to_state else host
 
     def stats(self) -> dict:
         s = mac_stats()
