@@ -4,10 +4,14 @@ the reference itself):
 
 * particle -> key: test/TestAlgorithm_Layer_Initial_With_Particle.h:106-123
 * air layers around one fluid cell: test/TestAlgorithms_Update_CellType_Layer.h:103-149
-* upwind convection -1.0 / 0.11: test/old/TestPolicy_Upwind_1_Order.h:99-104
+* upwind convection -1.0 / 0.11 / -1.25: test/old/TestPolicy_Upwind_1_Order.h:99-104,214-215
 * staggered interpolation 1, 1.5, 1.4: test/old/TestPolicy_Speed_Interpolation_Linear.h:100-120
 * divergence and gradient of simple fields: test/old/TestPolicy_Divergence.h,
   test/old/TestPolicy_Gradiant.h (values -1, -10, 1)
+* RK4 particle moves 0.1 / 0.01: test/old/TestAlgorithms_Move_Particles.h:159-567
+* the projection of a five-cell plus, 1.25 / 0.2499999999999998890 / 0.75:
+  test/old/TestAlgorithms_Solve_Pressure.h:449-470 (2D cases embedded in one
+  layer of cells between Neumann faces)
 """
 import numpy as np
 import pytest
@@ -115,3 +119,74 @@ def test_brick_layout_and_floor_division():
     assert bk == {(-1, 0, 0), (-2, 0, 0), (0, 0, 0), (1, 0, 0)}
     ck = s.cell_keys()[s.exists.astype(bool)]
     assert sorted(map(tuple, ck.tolist())) == sorted(map(tuple, keys.tolist()))
+
+
+def _cells(entries, params):
+    """entries: {(x, y, z): (type, flags, (ux, uy, uz))}."""
+    keys = np.array(list(entries.keys()), dtype=np.int64)
+    vals = list(entries.values())
+    return from_cells(params, keys, np.array([v[0] for v in vals], np.uint8), np.array([v[1] for v in vals], np.uint8),
+                      np.array([v[2] for v in vals], np.float64))
+
+
+def _at(s, k, field):
+    keys = s.cell_keys()
+    hit = (keys[..., 0] == k[0]) & (keys[..., 1] == k[1]) & (keys[..., 2] == k[2]) & s.exists.astype(bool)
+    return s.f64[field][hit].item()
+
+
+def test_upwind_known_answer_diagonal(oracle_lib, tmp_path):
+    """test/old/TestPolicy_Upwind_1_Order.h:106-215 (2D): speeds zero on a 3x3
+    block except (1, 1) = (1, 1); the convection of both components there is
+    -1.25 (x: U = 1, backward difference 1; y: U at the bound = 1/4, backward
+    difference 1). Here a 3x3x3 block of fluid cells, the middle layer as the
+    2D case; the z term vanishes (U_z = 0)."""
+    cells = {(x, y, z): (FLUID, 0, (0.0, 0.0, 0.0)) for x in range(3) for y in range(3) for z in (-1, 0, 1)}
+    cells[(1, 1, 0)] = (FLUID, 0, (1.0, 1.0, 0.0))
+    p = _write(_cells(cells, Params(h=(1.0, 1.0, 1.0), gravity=0.0)), tmp_path)
+    assert abs(oracle_lib.probe(p, "convection", key=(1, 1, 0), i=0) - (-1.25)) < EPS
+    assert abs(oracle_lib.probe(p, "convection", key=(1, 1, 0), i=1) - (-1.25)) < EPS
+
+
+@pytest.mark.parametrize("stage", ["movelin", "move"])
+@pytest.mark.parametrize("h,dt,want", [(1.0, 0.1, 0.1), (0.1, 0.01, 0.01)])
+def test_particle_move_known_answers(run_oracle, stage, h, dt, want):
+    """test/old/TestAlgorithms_Move_Particles.h:49-567: a uniform unit speed,
+    a particle at the origin moved by RK4 over dt: 0.1 at h = 1, dt = 0.1 and
+    0.01 at h = 0.1, dt = 0.01, in every component (the reference's linear
+    interpolation; the symmetric one gives the same on a uniform field)."""
+    cells = {(x, y, z): (FLUID, 0, (1.0, 1.0, 1.0))
+             for x in range(-2, 3) for y in range(-2, 3) for z in range(-2, 3)}
+    pr = Params(h=(h, h, h), gravity=0.0, dt=dt)
+    s = _cells(cells, pr)
+    s.pos = np.zeros((1, 3))
+    got, st = run_oracle(stage, s)
+    assert np.allclose(got.pos[0], [want, want, want], rtol=0, atol=1e-10), got.pos[0]
+    assert st["invalid_reads"] == 0
+
+
+def test_projection_known_answers(run_oracle):
+    """test/old/TestAlgorithms_Solve_Pressure.h:202-470 (2D): a plus of five
+    fluid cells, (0, 0) at speed (2, 2) and its four neighbours at (1, 1), air
+    (p = 0) around. After the projection (0, 0) has (1.25, 1.25), (1, 0) has
+    (1.25, 0.25), (0, 1) has (0.25, 1.25) and (-1, 0), (0, -1) have (0.75,
+    0.75). Here the plus lies in the layer z = 0 between solid layers whose
+    faces towards it are const (Neumann), so the z terms drop out of the
+    operator and the 3D projection is the 2D one."""
+    plus = {(0, 0): (2.0, 2.0), (1, 0): (1.0, 1.0), (-1, 0): (1.0, 1.0), (0, 1): (1.0, 1.0), (0, -1): (1.0, 1.0)}
+    cells = {}
+    for x in range(-2, 3):
+        for y in range(-2, 3):
+            u = plus.get((x, y))
+            cells[(x, y, 0)] = (FLUID if u else 0, 4, (u[0], u[1], 0.0) if u else (0.0, 0.0, 0.0))
+            cells[(x, y, -1)] = (2, 0, (0.0, 0.0, 0.0))  # solid below
+            cells[(x, y, 1)] = (2, 4, (0.0, 0.0, 0.0))   # solid above, its -z face const
+    got, st = run_oracle("project", _cells(cells, Params(h=(1.0, 1.0, 1.0), gravity=0.0)))
+    want = {(0, 0): (1.25, 1.25), (1, 0): (1.25, 0.24999999999999988898), (0, 1): (0.24999999999999988898, 1.25),
+            (-1, 0): (0.75, 0.75), (0, -1): (0.75, 0.75)}
+    for (x, y), (wx, wy) in want.items():
+        assert abs(_at(got, (x, y, 0), "u0x") - wx) < 1e-10, (x, y)
+        assert abs(_at(got, (x, y, 0), "u0y") - wy) < 1e-10, (x, y)
+        assert _at(got, (x, y, 0), "u0z") == 0.0
+    assert abs(_at(got, (0, 0, 0), "p") - 1.0) < 1e-10
+    assert st["relres"] <= 1e-14
