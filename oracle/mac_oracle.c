@@ -1536,3 +1536,17 @@ void mac_oracle_jitter8(uint64_t seed, int kx, int ky, int kz, int s, double hx,
                         double hz, double* out) {
   mac_jitter8_position(seed, kx, ky, kz, s, hx, hy, hz, out);
 }
+
+/* The material rules, exported so the tests can check them against the
+ * reference's own truth tables (test/TestData_CellType_Fluid_Air_Solid_Inflow*.h,
+ * test/Test_Data_CellType_Domain_Fluid.h): out[0] GetIsFluid, out[1] GetIsAir,
+ * out[2] GetIsInDomain, out[3] the material after SetAir, out[4] after SetFluid
+ * (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior.tpp:178-193). */
+void mac_oracle_material(int code, int* out) {
+  const uint8_t t = (uint8_t)code;
+  out[0] = is_fluid(t);
+  out[1] = is_air(t);
+  out[2] = in_domain(t);
+  out[3] = set_air(t);
+  out[4] = set_fluid(t);
+}

@@ -84,6 +84,15 @@ def jitter8(seed, k, s, h):
     return [out[0], out[1], out[2]]
 
 
+def material(code: int) -> dict:
+    """The oracle's material rules for one material code: the predicates and
+    the results of SetAir / SetFluid."""
+    out = (ctypes.c_int * 5)()
+    lib().mac_oracle_material(int(code), out)
+    return {"is_fluid": bool(out[0]), "is_air": bool(out[1]), "in_domain": bool(out[2]),
+            "after_set_air": out[3], "after_set_fluid": out[4]}
+
+
 def have_ref() -> bool:
     return os.path.exists(REF)
 

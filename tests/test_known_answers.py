@@ -12,6 +12,9 @@ the reference itself):
 * the projection of a five-cell plus, 1.25 / 0.2499999999999998890 / 0.75:
   test/old/TestAlgorithms_Solve_Pressure.h:449-470 (2D cases embedded in one
   layer of cells between Neumann faces)
+* the material predicates and setters: test/TestData_CellType_Fluid_Air_Solid_Inflow*.h,
+  test/Test_Data_CellType_Domain_Fluid.h
+* in-chunk neighbour offsets: test/Test_Offset.h
 """
 import numpy as np
 import pytest
@@ -190,3 +193,51 @@ def test_projection_known_answers(run_oracle):
         assert _at(got, (x, y, 0), "u0z") == 0.0
     assert abs(_at(got, (0, 0, 0), "p") - 1.0) < 1e-10
     assert st["relres"] <= 1e-14
+
+
+# material: (GetIsFluid, GetIsAir) from test/TestData_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.h:29-58
+# (the 0_Pres material of that variant is not on this path)
+MATERIAL_TABLE = {"Air": (False, True), "Fluid": (True, False), "Solid": (False, True),
+                  "Inflow": (True, False), "Interior": (True, False)}
+
+
+def test_material_rules_match_the_reference_tables(oracle_lib):
+    from mac_b200.state import AIR, INFLOW, INTERIOR, SOLID
+    code = {"Air": AIR, "Fluid": FLUID, "Solid": SOLID, "Inflow": INFLOW, "Interior": INTERIOR}
+    # MaterialToInt: Fluid 1, Air 0 (test/TestData_CellType_Fluid_Air_Solid_Inflow.h:19-20)
+    assert code["Fluid"] == 1 and code["Air"] == 0
+    for name, (fluid, air) in MATERIAL_TABLE.items():
+        m = oracle_lib.material(code[name])
+        assert m["is_fluid"] == fluid and m["is_air"] == air, name
+        # the solve's domain is the fluid cells (test/Test_Data_CellType_Domain_Fluid.h:22-23)
+        assert m["in_domain"] == fluid, name
+    # SetFluid puts an air cell in the domain, SetAir takes it out
+    # (test/Test_Data_CellType_Domain_Fluid.h:29-32)
+    assert oracle_lib.material(oracle_lib.material(AIR)["after_set_fluid"])["in_domain"]
+    assert not oracle_lib.material(oracle_lib.material(FLUID)["after_set_air"])["in_domain"]
+    # the setters are sticky: SetAir changes only fluid and interior cells, SetFluid
+    # only air and interior cells (src/Data_CellType_Fluid_Air_Solid_Inflow_Interior.tpp:178-193)
+    for name in MATERIAL_TABLE:
+        m = oracle_lib.material(code[name])
+        assert m["after_set_air"] == (AIR if name in ("Fluid", "Interior") else code[name]), name
+        assert m["after_set_fluid"] == (FLUID if name in ("Air", "Interior") else code[name]), name
+
+
+def test_brick_neighbour_offsets_match_the_offset_tests():
+    """test/Test_Offset.h:30-43 (N = 4, 3D): from offset 0 the +x, +y, +z
+    neighbours stay in the chunk at offsets 1, N, N^2 and the -x, -y, -z ones
+    leave it, wrapping to N-1, N(N-1), N^2(N-1). The device's 8^3 bricks follow
+    the same rule with N = 8: 1, 8, 64 inside, 7, 56, 448 in the neighbour brick."""
+    pr = Params()
+    cases = {(1, 0, 0): ((0, 0, 0), 1), (0, 1, 0): ((0, 0, 0), 8), (0, 0, 1): ((0, 0, 0), 64),
+             (-1, 0, 0): ((-1, 0, 0), 7), (0, -1, 0): ((0, -1, 0), 56), (0, 0, -1): ((0, 0, -1), 448)}
+    keys = np.array([[0, 0, 0]] + [list(k) for k in cases], dtype=np.int64)
+    s = from_cells(pr, keys, np.zeros(len(keys)), np.zeros(len(keys)), np.zeros((len(keys), 3)))
+    where = {}
+    for b, bk in enumerate(s.keys.tolist()):
+        for off in np.flatnonzero(s.exists[b]):
+            x, y, z = off % 8, (off // 8) % 8, off // 64
+            where[(bk[0] * 8 + x, bk[1] * 8 + y, bk[2] * 8 + z)] = (tuple(bk), int(off))
+    assert where[(0, 0, 0)] == ((0, 0, 0), 0)
+    for k, want in cases.items():
+        assert where[k] == want, k
