@@ -9,7 +9,8 @@ stencils and both particle moves, and within solver rounding on the
 projection and a full step (both solve to a relative residual of 1e-14). The
 same holds for the viscous composition on two of the worlds (viscosity 2e-3),
 and for the depth composition on two pool worlds with other Policy_Depth
-rules, one of which also runs pipeline B's init and step. Skipped where the
+rules, one of which also runs pipeline B's init and step, and for a small
+lateral jet (side-wall inflow aimed 15 degrees up). Skipped where the
 reference runners are not built.
 """
 import pytest
@@ -251,3 +252,55 @@ def test_pipeline_b_init_and_step(ref_depth, run_oracle):
     e = field_errors(got, r["bs7"], ("u0x", "u0y", "u0z", "p"))
     assert max(e.values()) <= 1e-12, e
     compare_particles(got, r["bs7"], atol=1e-13)
+
+
+# ---------------------------------------------------------------- lateral
+# a small lateral jet (side-wall inflow aimed 15 degrees up, as the 384x192x192
+# configuration), run through the same checks
+LATERAL = dict(nx=32, ny=20, nz=20, h=0.05, r_inflow=4.0, speed=2.0, angle_deg=15.0)
+
+
+@pytest.fixture(scope="module")
+def ref_lateral(tmp_path_factory):
+    import oracle
+    from mac_b200.state import State, lateral_jet_world
+    oracle.build()
+    if not oracle.have_ref():
+        pytest.skip("reference runners (oracle/_ref) not built")
+    d = tmp_path_factory.mktemp("livel")
+    t = lambda n: str(d / f"lateral_{n}.state")  # noqa: E731
+    lateral_jet_world(**LATERAL).write(t("setup"))
+    oracle.run_ref("firstinit", t("setup"), t("s0"))
+    oracle.run_ref("step", t("s0"), t("s8"), SPIN_UP)
+    oracle.run_ref("topology", t("s8"), t("t8"))
+    for st in ("forces", "extrapolate", "move"):
+        oracle.run_ref(st, t("t8"), t("t8_" + st))
+    oracle.run_ref("step", t("s8"), t("s9"), 1)
+    return {k: State.read(t(k)) for k in ("setup", "s0", "s8", "t8", "t8_forces", "t8_extrapolate", "t8_move", "s9")}
+
+
+def test_lateral_jet_bit_exact_and_step(ref_lateral, run_oracle):
+    from mac_b200.state import INFLOW
+    r = ref_lateral
+    got, _ = run_oracle("firstinit", r["setup"])
+    compare_topology(got, r["s0"])
+    _exact(got, r["s0"])
+    assert compare_particles(got, r["s0"]) == 0.0
+    got, _ = run_oracle("topology", r["s8"])
+    compare_topology(got, r["t8"])
+    _exact(got, r["t8"])
+    assert compare_particles(got, r["t8"]) == 0.0
+    for stage in ("forces", "extrapolate", "move"):
+        got, st = run_oracle(stage, r["t8"])
+        compare_topology(got, r["t8_" + stage])
+        _exact(got, r["t8_" + stage])
+        assert compare_particles(got, r["t8_" + stage]) == 0.0
+        assert st["invalid_reads"] == 0
+    got, _ = run_oracle("step", r["s8"])
+    compare_topology(got, r["s9"])
+    e = field_errors(got, r["s9"], ("u0x", "u0y", "u0z", "p"))
+    assert max(e.values()) <= 1e-12, e
+    compare_particles(got, r["s9"], atol=1e-14)
+    # the side-wall inflow is there and has produced fluid
+    ex = r["s8"].exists.astype(bool)
+    assert (r["s8"].type[ex] == INFLOW).sum() > 40 and r["s8"].nparticles > 1000
