@@ -227,7 +227,7 @@ def _peaks():
         return {}
 
 
-def poisson_solves(dev, reps=3):
+def poisson_solves(dev, mg_sweeps=2, reps=3):
     """Standalone pressure solve of the 128^3 pool + 12 spheres world (solid box,
     face speeds uniform in [-1, 1]) to a relative residual of 1e-10: device time
     of one projection and of its solve (system set-up + CG iterations), per
@@ -256,6 +256,7 @@ def poisson_solves(dev, reps=3):
     for name, solver, rtol in forms:
         with Context(s.params, max_bricks=8192, max_particles=1024, solver=solver, rtol=rtol, max_iters=1000,
                      device=dev) as ctx:
+            ctx.set_multigrid(mg_sweeps)
             if net is not None:
                 ctx.set_preconditioner(net)
             stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
@@ -302,6 +303,68 @@ def poisson_solves(dev, reps=3):
     return res
 
 
+SOLVER_NAMES = {"mgpcg64": "plain FP64 MG-PCG", "mixed": "FP32 MG in FP64 PCG", "cg64": "FP64 Jacobi-PCG",
+                "learned": "learned preconditioner in FP64 flexible CG (FP64 MG-PCG fall-back)",
+                "learned_mixed": "learned preconditioner in FP64 flexible CG (FP32 MG fall-back)"}
+
+
+def solver_forms(args, dev, params, host, wl, steps=5, warmup=2):
+    """The same spun-up jet state (host, pinned) stepped with each solver form
+    in turn: device ms per step (CUDA events on the library's stream), fluid
+    cell-steps/s, CG iterations per solve, and the step-time ratios against
+    the plain FP64 MG-PCG form (the denominator of the learned + mixed
+    target)."""
+    import torch
+    from mac_b200.gpu import Context
+    forms = ["mgpcg64", "mixed"]
+    net = None
+    if os.path.exists(WEIGHTS):
+        from mac_b200.unet import UNet
+        net = UNet(dev)
+        net.load(WEIGHTS)
+        forms.append("learned_mixed")
+    out = {"steps": steps, "warmup": warmup, "rtol": 1e-8, "mg_sweeps0": args.mg_sweeps}
+    for form in forms:
+        with Context(params, max_bricks=wl[8], max_particles=wl[9], solver=form, rtol=1e-8, max_iters=1000,
+                     device=dev, div_check=True) as ctx:
+            ctx.set_multigrid(args.mg_sweeps)
+            if form.startswith("learned"):
+                ctx.set_preconditioner(net)
+            ctx.upload(None, host)
+            stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+            for _ in range(warmup):
+                ctx.step()
+            ctx.sync()
+            it0 = ctx.stats()["total_iterations"]
+            fb0 = ctx.stats()["fallbacks"]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            fluid = 0
+            learned_its = []
+            e0.record(stream)
+            for _ in range(steps):
+                ctx.step()
+                st = ctx.stats()
+                fluid += st["fluid_cells"]
+                learned_its.append(st["learned_iterations"])
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            st = ctx.stats()
+            r = {"solver": SOLVER_NAMES[form], "ms_per_step": round(ms / steps, 3),
+                 "value": fluid / (ms * 1e-3), "cg_iters_per_solve": (st["total_iterations"] - it0) / (2 * steps),
+                 "relres_last": st["relres"], "max_div_last": st["max_div"]}
+            if form.startswith("learned"):
+                r["fallback_solves"] = st["fallbacks"] - fb0
+                r["learned_iters_last"] = learned_its[-1] if learned_its else 0
+            out[form] = r
+        log(f"[forms] {form}: {out[form]}")
+    if net is not None:
+        net.close()
+    base = out["mgpcg64"]["ms_per_step"]
+    out["speedup_vs_mgpcg64"] = {f: round(base / out[f]["ms_per_step"], 3) for f in forms}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from mac_b200.gpu import Context, HostState
@@ -315,10 +378,17 @@ def run_ours(args, rank, world, local_rank):
     log(f"[rank {rank}] world built in {time.perf_counter() - t0:.1f}s: {s.nbricks} bricks, {s.nparticles} particles")
     ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
                   device=dev, div_check=True, warm_start=args.warm_start)
+    ctx.set_multigrid(args.mg_sweeps)
+    if args.solver.startswith("learned"):
+        from mac_b200.unet import UNet
+        net_main = UNet(dev)
+        net_main.load(WEIGHTS)
+        ctx.set_preconditioner(net_main)
     t0 = time.perf_counter()
     first_init(ctx, s)
     ctx.sync()
     log(f"[rank {rank}] first init {time.perf_counter() - t0:.1f}s")
+    params = s.params
     del s
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
 
@@ -416,8 +486,7 @@ def run_ours(args, rank, world, local_rank):
         "dtype": "f64", "data": "synthetic (seeded spun-up jet state)",
         "config": {"workload": f"jet {wl[0]}x{wl[1]}x{wl[2]} h={wl[3]} inflow r={wl[4]:g} w={wl[5]}, pool depth "
                                f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
-                   "solver": {"mgpcg64": "plain FP64 MG-PCG", "mixed": "FP32 MG in FP64 PCG",
-                              "cg64": "FP64 Jacobi-PCG"}[args.solver],
+                   "solver": SOLVER_NAMES[args.solver], "mg_sweeps0": args.mg_sweeps,
                    "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
@@ -429,8 +498,11 @@ def run_ours(args, rank, world, local_rank):
                                                  for k, v in rl.items()},
     }
     ctx.close()
+    if rank == 0 and not args.no_forms:
+        out["solver_forms"] = solver_forms(args, dev, params, host, wl)
+    del host
     if rank == 0 and not args.no_poisson:
-        out["poisson"] = poisson_solves(dev)
+        out["poisson"] = poisson_solves(dev, args.mg_sweeps)
     return out
 
 
@@ -442,9 +514,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="jet256")
-    ap.add_argument("--solver", choices=["mgpcg64", "mixed", "cg64"], default="mixed",
+    ap.add_argument("--solver", choices=sorted(SOLVER_NAMES), default="mixed",
                     help="projection solver: mixed = FP64 CG with the FP32 multigrid (default), "
-                         "mgpcg64 = plain FP64 MG-PCG, cg64 = FP64 Jacobi-PCG")
+                         "mgpcg64 = plain FP64 MG-PCG, cg64 = FP64 Jacobi-PCG, learned[_mixed] = the network "
+                         "in flexible CG")
+    ap.add_argument("--mg-sweeps", type=int, choices=[1, 2], default=2,
+                    help="Jacobi sweeps before and after the coarse correction on the finest multigrid level")
+    ap.add_argument("--no-forms", action="store_true", help="skip stepping the jet with every solver form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

@@ -27,7 +27,8 @@ enum {
   MAC_ERR_NOT_CONVERGED = -4, /* iterative solve hit max_iters */
   MAC_ERR_NO_DEVICE = -5,     /* no CUDA device */
   MAC_ERR_OUT_OF_MEMORY = -6,
-  MAC_ERR_TIMEOUT = -7
+  MAC_ERR_TIMEOUT = -7,
+  MAC_ERR_MATRIX = -8         /* matrix not of the form the solver handles */
 };
 
 /* Pressure solver of the projection. */
@@ -207,7 +208,13 @@ int mac_get_profile(void* ctx, double* ms, int64_t* count, int nphase);
 /* ---- drop-in linear solver: the Policy_Solve_Linear_Umfpack member functions
  * (src/Policy_Solve_Linear_Umfpack.h:28-70) over the CSC arrays the reference assembles
  * in Algorithms_Solve_Pressure::Init_Iteration (src/Algorithms_Solve_Pressure.h:52-152).
- * The matrix is symmetric and negative definite; solved by FP64 Jacobi-PCG on the device. ---- */
+ * mac_csc_factorize checks the arrays (MAC_ERR_INVALID: offsets not starting at 0 or
+ * decreasing, a row index outside [0, n)) and the matrix's form: the symmetric matrix
+ * with a negative diagonal the reference assembles is solved by FP64 Jacobi-PCG on the
+ * device; any other matrix (the general LU of Umfpack takes any non-singular one) by
+ * FP64 Jacobi-preconditioned BiCGStab on a row-major copy. Both stop at
+ * ||b - A x|| <= rtol ||b|| (mac_params.rtol) or return MAC_ERR_NOT_CONVERGED after
+ * max_iters or on a breakdown, with x the last finite iterate. ---- */
 int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value);
 int mac_csc_solve(void* ctx, int n, const double* b, double* x);
 int mac_csc_clean(void* ctx);
@@ -256,6 +263,14 @@ int mac_set_preconditioner_net(void* ctx, void* net);
  * 0 turns it off. Default 0.8. */
 int mac_set_learned_smoothing(void* ctx, double omega);
 
+/* Multigrid preconditioner of the MG-PCG solvers (no counterpart in the
+ * reference, which factorises with Umfpack): weighted-Jacobi sweeps before and
+ * after the coarse correction on the finest level, 1 or 2 (default 2). One
+ * sweep fuses the pre-sweep with the residual's restriction, so a V-cycle
+ * reads the fine grid twice instead of four times; the CG iteration count may
+ * rise. The preconditioner stays symmetric either way. */
+int mac_set_multigrid(void* ctx, int sweeps0);
+
 /* ---- allocation-free CSC solve (no counterpart in the reference) ----
  * The same FP64 Jacobi-PCG as mac_csc_factorize + mac_csc_solve, for callers
  * that must not allocate device memory: a host program whose device memory is
@@ -265,6 +280,10 @@ int mac_set_learned_smoothing(void* ctx, double omega);
  *
  * - offset/indice/value (CSC, as mac_csc_factorize), b and x are DEVICE
  *   pointers owned by the caller; x is overwritten (the solve starts from 0).
+ * - The matrix must be the symmetric matrix with a negative diagonal that the
+ *   reference assembles (the solve is CG); the call checks this on the device
+ *   first and returns MAC_ERR_MATRIX otherwise (use mac_csc_factorize for other
+ *   matrices). The arrays must form a valid CSC matrix of n columns.
  * - Work vectors live in one fixed device array of MAC_NOALLOC_MAX_N rows per
  *   device; n > MAC_NOALLOC_MAX_N returns MAC_ERR_CAPACITY and touches nothing.
  *   Its reduction slots must be zero before each reduction, and the call clears
@@ -273,8 +292,10 @@ int mac_set_learned_smoothing(void* ctx, double omega);
  *   device and returns after the solve has finished (it reads the CG scalars
  *   on the host every iteration).
  * - The first call on a device looks up the array's address with
- *   cudaGetSymbolAddress; make that first call before any stream capture
- *   begins on that device.
+ *   cudaGetSymbolAddress; the driver then places the array (2.5 MiB) in device
+ *   memory, so that first call needs that much free. A call with n = 0 does
+ *   only this set-up: make it on each device before handing its memory to
+ *   another allocator, and before any stream capture begins on that device.
  * - All calls on one device share the array: two calls in flight at the same
  *   time on one device (other streams or host threads) race and corrupt each
  *   other's result. Serialise them.

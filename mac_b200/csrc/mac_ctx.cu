@@ -465,6 +465,7 @@ const char* mac_error_string(int code) {
     case MAC_ERR_NO_DEVICE: return "no CUDA device";
     case MAC_ERR_OUT_OF_MEMORY: return "out of device memory";
     case MAC_ERR_TIMEOUT: return "timeout";
+    case MAC_ERR_MATRIX: return "matrix not of the form the solver handles";
     default: return "unknown error";
   }
 }

@@ -183,6 +183,7 @@ struct Ctx {
   void* mg_w[kLevels] = {};   // [4][cells]: left-face weights x,y,z and Dirichlet diagonal
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
+  int mg_sweeps0 = 2;         // Jacobi sweeps before and after the coarse correction at level 0 (1 or 2)
   // learned preconditioner (flexible CG): the network and the previous z
   void* unet = nullptr;
   double* zold = nullptr;
@@ -212,7 +213,11 @@ struct Ctx {
   int* csc_off = nullptr;
   int* csc_ind = nullptr;
   double* csc_val = nullptr;
-  double* csc_vec = nullptr;   // [7][n] + scalars
+  double* csc_vec = nullptr;   // [7][n] + scalars (CG), [11][n] + scalars (BiCGStab)
+  int csc_general = 0;         // 1: not the symmetric negative-diagonal form, solved by BiCGStab
+  int* csr_off = nullptr;      // row-major copy for BiCGStab
+  int* csr_ind = nullptr;
+  double* csr_val = nullptr;
   long long launches = 0;      // kernels launched by this context
   struct Prof* prof = nullptr; // per-phase event timing (null when off)
 };

@@ -263,6 +263,135 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
   if (!FIRST) block_sum<kBT>(rz, 0.0, partial);
 }
 
+// ---- level 0 with one sweep before and after the coarse correction.
+// Pre-sweep, residual and restriction in one pass: with e = w D^-1 r (one
+// Jacobi sweep from zero, pointwise) the residual r - M e needs only the
+// staged w D^-1 r of the brick and its face halo, which k0_pre's staging
+// already forms; the sum over 2x2x2 children goes to level 1. e is not
+// stored: the post-sweep recomputes it from r. The CG update is folded in as
+// in k0_pre.
+template <class T>
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict(
+    const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
+    const double* __restrict__ rin, double* __restrict__ rout, double* __restrict__ x, const double* __restrict__ p,
+    const double* __restrict__ q, double* partial, const Scalars* ds, int update, T* __restrict__ r1, Params P) {
+  if (solve_done(&ds->done)) return;
+  __shared__ int64_t sb[6];
+  __shared__ T sr[kS1];    // e = w D^-1 r of the brick and its face halo
+  __shared__ T res[kCells];
+  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const double al = update ? ds->alpha : 0.0;
+  int b = dbl[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  double rv[kCPT];
+  uint16_t mk[kCPT];
+  double rr = 0;
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    const int o = threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + o;
+    double v = rin[c];
+    if (update) {
+      v = v - al * q[c];
+      rout[c] = v;
+      x[c] += al * p[c];
+      rr += v * v;
+    }
+    rv[k] = v;
+    const uint16_t m = fmask[c];
+    mk[k] = m;
+    sr[s1_of(o)] = om * (T)P.dtab[active_index(m)] * (T)v;
+  }
+  __syncthreads();
+  stage_h1_halo(sr, sb, [&](int64_t i) {
+    const double v = update ? rin[i] - al * q[i] : rin[i];
+    return om * (T)P.dtab[active_index(fmask[i])] * (T)v;
+  });
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    const int o = threadIdx.x + kBT * k;
+    const uint16_t m = mk[k];
+    T v = 0;
+    if (m & kDomainBit) {
+      const int si = s1_of(o);
+      const T ec = sr[si];
+      T me = 0;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
+        if (m & (1u << f)) me -= ih2[f >> 1] * sr[si + s1_off(f)];
+      }
+      v = (T)rv[k] - me;
+    }
+    res[o] = v;
+  }
+  __syncthreads();
+  const int o = threadIdx.x;
+  if (o < 64) {
+    const int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
+    const int base = 2 * X + 16 * Y + 128 * Z;
+    r1[(size_t)b * 64 + o] = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] +
+                             res[base + 65] + res[base + 72] + res[base + 73];
+  }
+  if (update) block_sum<kBT>(rr, 0.0, partial);
+}
+
+// The one post-sweep: ep = w D^-1 r + P e1 (pre-sweep recomputed, coarse
+// correction added, on the brick and its face halo), z = ep + w D^-1 (r - M ep)
+// in FP64 with the block's partial r.z.
+template <class T>
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
+    const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
+    const double* __restrict__ r, const T* __restrict__ e1, double* __restrict__ z, double* partial, Params P,
+    const int32_t* __restrict__ done) {
+  if (solve_done(done)) return;
+  __shared__ int64_t sb[6];
+  __shared__ T se[kS1];
+  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  int b = dbl[blockIdx.x];
+  load_face_bases(nbr, b, sb);
+  uint16_t mk[kCPT];
+  double rk[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    const int o = threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + o;
+    mk[k] = fmask[c];
+    rk[k] = r[c];
+    se[s1_of(o)] = om * (T)P.dtab[active_index(mk[k])] * (T)rk[k] + e1[(size_t)b * 64 + parent_off(o)];
+  }
+  __syncthreads();
+  stage_h1_halo(se, sb, [&](int64_t i) {
+    return om * (T)P.dtab[active_index(fmask[i])] * (T)r[i] + e1[(i >> 9) * 64 + parent_off((int)(i & 511))];
+  });
+  __syncthreads();
+  double rz = 0;
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) {
+    const int o = threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + o;
+    const uint16_t m = mk[k];
+    if (!(m & kDomainBit)) {
+      z[c] = 0.0;
+      continue;
+    }
+    const int si = s1_of(o);
+    const T epc = se[si];
+    T me = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (m & (1u << (8 + f))) me += ih2[f >> 1] * epc;
+      if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
+    }
+    const double rc = rk[k];
+    const T out = epc + om * (T)P.dtab[active_index(m)] * ((T)rc - me);
+    z[c] = (double)out;
+    rz += rc * (double)out;
+  }
+  block_sum<kBT>(rz, 0.0, partial);
+}
+
 // ------------------------------------------------------- levels 1, 2 (bricks)
 template <int D>
 __device__ inline int64_t lidx(const int* __restrict__ nbr, int b, int x, int y, int z) {
@@ -1120,16 +1249,24 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   DenseGrid G = c->g3;
   const int32_t* dn = &c->ds->done;
   // down (with update: finish the previous CG iteration into r2, which becomes r)
+  const bool one = c->mg_sweeps0 == 1;
   if (part & 1) {
-    k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
-                                  update, e0, c->dp); MAC_COUNT(c);
+    if (one) {
+      k0_pre_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
+                                             c->ds, update, r1, c->dp); MAC_COUNT(c);
+    } else {
+      k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
+                                    update, e0, c->dp); MAC_COUNT(c);
+    }
     if (update) {
       std::swap(c->r, c->r2);
       cg_finish_update(c);
     }
   }
   if (!(part & 2)) return;
-  k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
+  if (!one) {
+    k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
+  }
   kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1, dn); MAC_COUNT(c);
   kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
   kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2, dn); MAC_COUNT(c);
@@ -1162,6 +1299,10 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, dn); MAC_COUNT(c);
   kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
                                              dn); MAC_COUNT(c);
+  if (one) {
+    k0_post_one<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
+    return;
+  }
   k0_post<T, true><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
                                        dn); MAC_COUNT(c);
   k0_post<T, false><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,

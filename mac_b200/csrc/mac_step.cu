@@ -1,7 +1,9 @@
 // Step orchestration and the stage entry points of the C-ABI, plus the
 // drop-in CSC linear solver (the Policy_Solve_Linear_* member functions).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "mac_internal.cuh"
 
@@ -85,8 +87,8 @@ static int step(Ctx* c) {
 }
 
 // ------------------------------------------------------- drop-in CSC solver
-// The reference's assembled matrix is symmetric, so its CSC arrays read as CSR
-// rows: y_j = sum_k value[k] * x[indice[k]] over column j.
+// A symmetric matrix's CSC arrays read as CSR rows: y_j = sum_k value[k] *
+// x[indice[k]] over column j (the CG path; mac_csc_factorize checks symmetry).
 __global__ void k_csc_spmv(int n, const int* __restrict__ off, const int* __restrict__ ind,
                            const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
                            double* partial_dot, const double* __restrict__ pdot) {
@@ -158,9 +160,12 @@ __global__ void k_csc_vec(int n, int mode, const double* b, double* x, double* r
   }
 }
 
-static int csc_solve(Ctx* c, const double* hb, double* hx) {
+// CG breakdown: p.q of zero, or not finite, means the direction carries no
+// information (a singular or indefinite system, or a zero row with b != 0).
+static inline bool cg_breakdown(double pq) { return !(pq != 0.0 && std::isfinite(pq)); }
+
+static int csc_solve_cg(Ctx* c, const double* hb, double* hx) {
   int n = c->csc_n;
-  if (n <= 0) return MAC_OK;
   cudaStream_t st = c->stream;
   double* v = c->csc_vec;
   double *b = v, *x = v + n, *r = v + 2 * (size_t)n, *z = v + 3 * (size_t)n, *p = v + 4 * (size_t)n,
@@ -184,6 +189,7 @@ static int csc_solve(Ctx* c, const double* hb, double* hx) {
     k_csc_spmv<<<g, 256, 0, st>>>(n, c->csc_off, c->csc_ind, c->csc_val, p, q, scal + 3, p); MAC_COUNT(c);
     cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st);
     if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+    if (cg_breakdown(hs[3])) break;  // x keeps the last finite iterate
     double alpha = rz / hs[3];
     k_csc_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, z, p, q, dinv, scal, alpha); MAC_COUNT(c);
     k_csc_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, z, p, q, dinv, scal, 0); MAC_COUNT(c);
@@ -204,6 +210,217 @@ static int csc_solve(Ctx* c, const double* hb, double* hx) {
   c->stats.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
   c->stats.unknowns = n;
   return (bb > 0 && !(rr <= rtol * rtol * bb)) ? MAC_ERR_NOT_CONVERGED : MAC_OK;
+}
+
+// ---- general (non-symmetric) matrices: Jacobi-preconditioned BiCGStab on
+// the row-major copy built at factorisation. A x is a row-wise product, so
+// every y_i is summed in a fixed order.
+__global__ void k_csr_spmv_dot(int n, const int* __restrict__ off, const int* __restrict__ ind,
+                               const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                               const double* __restrict__ w0, const double* __restrict__ w1, double* scal) {
+  double a0 = 0, a1 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int k = off[i]; k < off[i + 1]; ++k) s += val[k] * x[ind[k]];
+    y[i] = s;
+    a0 += w0[i] * s;
+    if (w1) a1 += w1[i] * s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(scal, a0);
+    if (w1) atomicAdd(scal + 1, a1);
+  }
+}
+
+// The diagonal's inverse from the row-major copy (1 where the diagonal is 0).
+__global__ void k_csr_dinv(int n, const int* __restrict__ off, const int* __restrict__ ind,
+                           const double* __restrict__ val, double* dinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = 0;
+    for (int k = off[i]; k < off[i + 1]; ++k)
+      if (ind[k] == i) d += val[k];
+    dinv[i] = d != 0 ? 1.0 / d : 1.0;
+  }
+}
+
+// BiCGStab vector steps (van der Vorst 1992, right preconditioning K = diag):
+// mode 0: r = rh = b, x = 0, p = v = 0; scal[2] += b.b
+// mode 1: p = r + beta (p - omega v); y = K^-1 p
+// mode 2: s = r - alpha v; z = K^-1 s; scal[2] += s.s
+// mode 3: x += alpha y + omega z; r = s - omega t; scal[2] += r.r, scal[3] += rh.r
+__global__ void k_bicg_vec(int n, int mode, const double* __restrict__ b, double* x, double* r,
+                           double* rh, double* p, double* v, double* y, double* s,
+                           double* z, const double* __restrict__ t, const double* __restrict__ dinv, double* scal,
+                           double alpha, double beta, double omega) {
+  double a0 = 0, a1 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (mode == 0) {
+      const double bv = b[i];
+      r[i] = bv;
+      rh[i] = bv;
+      x[i] = 0.0;
+      p[i] = 0.0;
+      v[i] = 0.0;
+      a0 += bv * bv;
+    } else if (mode == 1) {
+      const double pv = r[i] + beta * (p[i] - omega * v[i]);
+      p[i] = pv;
+      y[i] = dinv[i] * pv;
+    } else if (mode == 2) {
+      const double sv = r[i] - alpha * v[i];
+      s[i] = sv;
+      z[i] = dinv[i] * sv;
+      a0 += sv * sv;
+    } else {
+      x[i] += alpha * y[i] + omega * z[i];
+      const double rv = s[i] - omega * t[i];
+      r[i] = rv;
+      a0 += rv * rv;
+      a1 += rh[i] * rv;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+  }
+  if ((threadIdx.x & 31) == 0 && mode != 1) {
+    atomicAdd(scal + 2, a0);
+    if (mode == 3) atomicAdd(scal + 3, a1);
+  }
+}
+
+static int csc_solve_bicgstab(Ctx* c, const double* hb, double* hx) {
+  const int n = c->csc_n;
+  const size_t N = (size_t)n;
+  cudaStream_t st = c->stream;
+  double* w = c->csc_vec;
+  double *b = w, *x = w + N, *r = w + 2 * N, *rh = w + 3 * N, *p = w + 4 * N, *v = w + 5 * N, *y = w + 6 * N,
+         *s = w + 7 * N, *z = w + 8 * N, *t = w + 9 * N, *dinv = w + 10 * N, *scal = w + 11 * N;
+  int g = grid_for(n, 256);
+  if (g > 1184) g = 1184;
+  double hs[8];
+  auto read = [&]() {
+    int e = check(cudaMemcpyAsync(hs, scal, 64, cudaMemcpyDeviceToHost, st));
+    return e ? e : check(cudaStreamSynchronize(st));
+  };
+  int rc = check(cudaMemcpyAsync(b, hb, 8 * N, cudaMemcpyHostToDevice, st));
+  if (rc) return rc;
+  k_csr_dinv<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, dinv); MAC_COUNT(c);
+  cudaMemsetAsync(scal, 0, 64, st);
+  k_bicg_vec<<<g, 256, 0, st>>>(n, 0, b, x, r, rh, p, v, y, s, z, t, dinv, scal, 0, 0, 0); MAC_COUNT(c);
+  if ((rc = read())) return rc;
+  const double bb = hs[2], rtol2 = c->prm.rtol * c->prm.rtol;
+  double rr = bb, rho = bb, rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  int it = 0;
+  bool first = true;
+  while (bb > 0 && it < c->prm.max_iters) {
+    const double beta = first ? 0.0 : (rho / rho_prev) * (alpha / omega);
+    first = false;
+    k_bicg_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, rh, p, v, y, s, z, t, dinv, scal, 0, beta, omega); MAC_COUNT(c);
+    cudaMemsetAsync(scal, 0, 64, st);
+    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, y, v, rh, nullptr, scal); MAC_COUNT(c);
+    if ((rc = read())) return rc;
+    const double rhv = hs[0];
+    if (cg_breakdown(rhv)) break;
+    alpha = rho / rhv;
+    cudaMemsetAsync(scal, 0, 64, st);
+    k_bicg_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, rh, p, v, y, s, z, t, dinv, scal, alpha, 0, 0); MAC_COUNT(c);
+    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, z, t, s, t, scal); MAC_COUNT(c);
+    if ((rc = read())) return rc;
+    const double ts = hs[0], tt = hs[1], ss = hs[2];
+    ++it;
+    if (ss <= rtol2 * bb || cg_breakdown(tt)) {
+      // converged on the half step (or t = 0): x += alpha y, r = s
+      k_bicg_vec<<<g, 256, 0, st>>>(n, 3, b, x, r, rh, p, v, y, s, z, t, dinv, scal, alpha, 0, 0); MAC_COUNT(c);
+      rr = ss;
+      break;
+    }
+    omega = ts / tt;
+    cudaMemsetAsync(scal, 0, 64, st);
+    k_bicg_vec<<<g, 256, 0, st>>>(n, 3, b, x, r, rh, p, v, y, s, z, t, dinv, scal, alpha, 0, omega); MAC_COUNT(c);
+    if ((rc = read())) return rc;
+    rr = hs[2];
+    if (rr <= rtol2 * bb) break;
+    rho_prev = rho;
+    rho = hs[3];
+    if (cg_breakdown(rho) || omega == 0.0) break;
+  }
+  if ((rc = check(cudaMemcpyAsync(hx, x, 8 * N, cudaMemcpyDeviceToHost, st)))) return rc;
+  if ((rc = check(cudaStreamSynchronize(st)))) return rc;
+  c->stats.iterations = it;
+  c->stats.total_iterations += it;
+  c->stats.solves += 1;
+  c->stats.relres = bb > 0 ? std::sqrt(rr / bb) : 0.0;
+  c->stats.unknowns = n;
+  return (bb > 0 && !(rr <= rtol2 * bb)) ? MAC_ERR_NOT_CONVERGED : MAC_OK;
+}
+
+static int csc_solve(Ctx* c, const double* hb, double* hx) {
+  if (c->csc_n <= 0) return MAC_OK;
+  return c->csc_general ? csc_solve_bicgstab(c, hb, hx) : csc_solve_cg(c, hb, hx);
+}
+
+// Host-side checks of a CSC matrix at factorisation. csc_valid: offsets start
+// at 0 and never decrease, row indices lie in [0, n). csc_symmetric_negdiag:
+// the matrix equals its transpose entry by entry and every diagonal entry is
+// negative, the form Algorithms_Solve_Pressure::Init_Iteration assembles
+// (src/Algorithms_Solve_Pressure.h:103-136), whose negation CG can solve.
+static bool csc_valid(int n, const int* off, const int* ind) {
+  if (off[0] != 0) return false;
+  for (int j = 0; j < n; ++j)
+    if (off[j + 1] < off[j]) return false;
+  for (int k = 0; k < off[n]; ++k)
+    if (ind[k] < 0 || ind[k] >= n) return false;
+  return true;
+}
+
+struct Entry {
+  int i, j;
+  double v;
+  bool operator<(const Entry& o) const { return i != o.i ? i < o.i : (j != o.j ? j < o.j : v < o.v); }
+  bool operator==(const Entry& o) const { return i == o.i && j == o.j && v == o.v; }
+};
+
+static bool csc_symmetric_negdiag(int n, const int* off, const int* ind, const double* val) {
+  const int nnz = off[n];
+  std::vector<Entry> a(nnz), at(nnz);
+  std::vector<int> diag(n, 0);
+  for (int j = 0; j < n; ++j)
+    for (int k = off[j]; k < off[j + 1]; ++k) {
+      a[k] = {ind[k], j, val[k]};
+      at[k] = {j, ind[k], val[k]};
+      if (ind[k] == j) {
+        if (!(val[k] < 0)) return false;
+        diag[j] += 1;
+      }
+    }
+  for (int j = 0; j < n; ++j)
+    if (diag[j] != 1) return false;
+  std::sort(a.begin(), a.end());
+  std::sort(at.begin(), at.end());
+  return a == at;
+}
+
+// Row-major copy (CSR) of a CSC matrix, rows in column order.
+static void csc_to_csr(int n, const int* off, const int* ind, const double* val, std::vector<int>& roff,
+                       std::vector<int>& rind, std::vector<double>& rval) {
+  const int nnz = off[n];
+  roff.assign(n + 1, 0);
+  for (int k = 0; k < nnz; ++k) roff[ind[k] + 1] += 1;
+  for (int i = 0; i < n; ++i) roff[i + 1] += roff[i];
+  rind.resize(nnz);
+  rval.resize(nnz);
+  std::vector<int> cur(roff.begin(), roff.end() - 1);
+  for (int j = 0; j < n; ++j)
+    for (int k = off[j]; k < off[j + 1]; ++k) {
+      const int q = cur[ind[k]]++;
+      rind[q] = j;
+      rval[q] = val[k];
+    }
 }
 
 }  // namespace mac
@@ -298,25 +515,50 @@ int mac_set_learned_smoothing(void* ctx, double omega) {
   return MAC_OK;
 }
 
+int mac_set_multigrid(void* ctx, int sweeps0) {
+  CTX_OR_FAIL();
+  if (sweeps0 != 1 && sweeps0 != 2) return MAC_ERR_INVALID;
+  c->mg_sweeps0 = sweeps0;
+  return MAC_OK;
+}
+
 int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value) {
   CTX_OR_FAIL();
   if (n < 0 || (n > 0 && (!offset || !indice || !value))) return MAC_ERR_INVALID;
   mac_csc_clean(ctx);
   if (n == 0) return MAC_OK;
+  if (!mac::csc_valid(n, offset, indice)) return MAC_ERR_INVALID;
   int nnz = offset[n];
+  // The reference's pressure matrix (symmetric, negative diagonal) goes to
+  // Jacobi-CG; any other matrix Policy_Solve_Linear_Umfpack would factorise
+  // goes to Jacobi-BiCGStab on a row-major copy.
+  const bool general = !mac::csc_symmetric_negdiag(n, offset, indice, value);
+  const size_t nvec = general ? 11 : 7;
   int rc = mac::check(cudaMalloc((void**)&c->csc_off, 4 * (size_t)(n + 1)));
   if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_ind, 4 * (size_t)(nnz ? nnz : 1)));
   if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_val, 8 * (size_t)(nnz ? nnz : 1)));
-  if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_vec, 8 * (size_t)(7 * (size_t)n + 8)));
+  if (!rc) rc = mac::check(cudaMalloc((void**)&c->csc_vec, 8 * (size_t)(nvec * (size_t)n + 8)));
   if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_off, offset, 4 * (size_t)(n + 1), cudaMemcpyHostToDevice, c->stream));
   if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_ind, indice, 4 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
   if (!rc) rc = mac::check(cudaMemcpyAsync(c->csc_val, value, 8 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+  std::vector<int> roff, rind;
+  std::vector<double> rval;
+  if (general && !rc) {
+    mac::csc_to_csr(n, offset, indice, value, roff, rind, rval);
+    rc = mac::check(cudaMalloc((void**)&c->csr_off, 4 * (size_t)(n + 1)));
+    if (!rc) rc = mac::check(cudaMalloc((void**)&c->csr_ind, 4 * (size_t)(nnz ? nnz : 1)));
+    if (!rc) rc = mac::check(cudaMalloc((void**)&c->csr_val, 8 * (size_t)(nnz ? nnz : 1)));
+    if (!rc) rc = mac::check(cudaMemcpyAsync(c->csr_off, roff.data(), 4 * (size_t)(n + 1), cudaMemcpyHostToDevice, c->stream));
+    if (!rc) rc = mac::check(cudaMemcpyAsync(c->csr_ind, rind.data(), 4 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+    if (!rc) rc = mac::check(cudaMemcpyAsync(c->csr_val, rval.data(), 8 * (size_t)nnz, cudaMemcpyHostToDevice, c->stream));
+  }
   if (!rc) rc = mac::check(cudaStreamSynchronize(c->stream));
   if (rc) {
     mac_csc_clean(ctx);
     return rc;
   }
   c->csc_n = n;
+  c->csc_general = general ? 1 : 0;
   return MAC_OK;
 }
 
@@ -332,6 +574,13 @@ int mac_csc_clean(void* ctx) {
   cudaFree(c->csc_ind);
   cudaFree(c->csc_val);
   cudaFree(c->csc_vec);
+  cudaFree(c->csr_off);
+  cudaFree(c->csr_ind);
+  cudaFree(c->csr_val);
+  c->csr_off = nullptr;
+  c->csr_ind = nullptr;
+  c->csr_val = nullptr;
+  c->csc_general = 0;
   c->csc_off = nullptr;
   c->csc_ind = nullptr;
   c->csc_val = nullptr;

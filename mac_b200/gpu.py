@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libmac_gpu.so")
 
 MAC_OK = 0
 ERRORS = {-1: "invalid", -2: "cuda", -3: "capacity", -4: "not converged", -5: "no device",
-          -6: "out of memory", -7: "timeout"}
+          -6: "out of memory", -7: "timeout", -8: "matrix form"}
 SOLVERS = {"mgpcg64": 0, "mixed": 1, "cg64": 2, "learned": 3, "learned_mixed": 4}
 
 
@@ -68,7 +68,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
            "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
-           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_unet_set_loss", "mac_unet_time_forward"]
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_unet_set_loss", "mac_unet_time_forward"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -128,6 +128,7 @@ def load(path: str = LIB_PATH):
     lib.mac_unet_launch_count.argtypes = [vp, _P(i64)]
     lib.mac_set_preconditioner_net.argtypes = [vp, vp]
     lib.mac_set_learned_smoothing.argtypes = [vp, f64]
+    lib.mac_set_multigrid.argtypes = [vp, i32]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
     lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
     _lib = lib
@@ -386,6 +387,10 @@ class Context:
 
     def set_learned_smoothing(self, omega):
         self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
+
+    def set_multigrid(self, sweeps0):
+        """Jacobi sweeps before and after the coarse correction on the finest level (1 or 2)."""
+        self._check(self.lib.mac_set_multigrid(self.h, int(sweeps0)), "mac_set_multigrid")
 
     # ---- drop-in CSC solver
     def csc_solve(self, offset, indice, value, b):

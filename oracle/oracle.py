@@ -21,12 +21,15 @@ REF_B = os.path.join(HERE, "_ref", "mac_ref_b")
 PIPELINE_B = ("bstep", "binit", "bode")
 
 _lib = None
+# The reference checkout's sources, read in place by the Makefile's _ref
+# targets (MAC_REF_SRC overrides the checkout's location).
+REF_SRC = os.environ.get("MAC_REF_SRC", "/root/reference/src")
 
 
 def build(quiet: bool = True) -> None:
     """Builds the restatement (and the reference runner when the reference
     sources are present)."""
-    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    out = subprocess.run(["make", "-C", HERE, "all", f"REF_SRC={REF_SRC}"], capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

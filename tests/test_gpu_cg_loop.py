@@ -25,16 +25,18 @@ def pool64():
     return setup_passes(pool_spheres_world(N, r_range=(6.0 * N / 128, 20.0 * N / 128)))
 
 
-def _ctx(s, solver, rtol, max_iters):
+def _ctx(s, solver, rtol, max_iters, sweeps=2):
     from mac_b200.gpu import Context
-    return Context(s.params, max_bricks=int(s.nbricks * 1.2) + 64, max_particles=1024, solver=solver, rtol=rtol,
-                   max_iters=max_iters)
+    c = Context(s.params, max_bricks=int(s.nbricks * 1.2) + 64, max_particles=1024, solver=solver, rtol=rtol,
+                max_iters=max_iters)
+    c.set_multigrid(sweeps)
+    return c
 
 
-@pytest.mark.parametrize("solver", ["mixed", "mgpcg64", "cg64"])
+@pytest.mark.parametrize("solver,sweeps", [("mixed", 2), ("mgpcg64", 2), ("cg64", 2), ("mixed", 1), ("mgpcg64", 1)])
 @pytest.mark.parametrize("cap", [1, 2, 5])
-def test_iteration_cap_is_exact(pool64, solver, cap):
-    with _ctx(pool64, solver, 1e-14, cap) as ctx:
+def test_iteration_cap_is_exact(pool64, solver, sweeps, cap):
+    with _ctx(pool64, solver, 1e-14, cap, sweeps) as ctx:
         ctx.upload(pool64)
         ctx.project(0, allow_not_converged=True)
         st = ctx.stats()
@@ -42,13 +44,13 @@ def test_iteration_cap_is_exact(pool64, solver, cap):
     assert st["relres"] > 1e-14
 
 
-@pytest.mark.parametrize("solver", ["mixed", "mgpcg64"])
-def test_capped_solves_approach_the_converged_one(pool64, solver):
+@pytest.mark.parametrize("solver,sweeps", [("mixed", 2), ("mgpcg64", 2), ("mixed", 1)])
+def test_capped_solves_approach_the_converged_one(pool64, solver, sweeps):
     """More iterations bring the pressure closer to the converged solve's (the
     capped solves' iterates are the loop's own, not ones a late stop skipped)."""
     ps = []
     for cap in (3, 6, 9, 200):
-        with _ctx(pool64, solver, 1e-12, cap) as ctx:
+        with _ctx(pool64, solver, 1e-12, cap, sweeps) as ctx:
             ctx.upload(pool64)
             ctx.project(0, allow_not_converged=True)
             got = ctx.download()

@@ -1,6 +1,8 @@
 """Standalone pressure solve on the 128^3 pool + 12 spheres world (solid box,
 air above, face speeds uniform in [-1, 1]): the device projection with the
-plain FP64 MG-PCG and with the mixed form (FP32 multigrid inside FP64 CG)
+plain FP64 MG-PCG and with the mixed form (FP32 multigrid inside FP64 CG),
+each with one and with two Jacobi sweeps around the finest level's coarse
+correction,
 against the oracle's FP64 projection (CG to a relative residual of 1e-14) of
 the same world.
 
@@ -56,18 +58,20 @@ def oracle_projection(pool_world, tmp_path_factory):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("sweeps", [1, 2])
 @pytest.mark.parametrize("solver", ["mgpcg64", "mixed"])
 @pytest.mark.parametrize("rtol,p_tol,u_tol", [(1e-12, 1e-9, 1e-10), (1e-10, 1e-8, 1e-9)])
-def test_pool_projection_against_oracle(pool_world, oracle_projection, solver, rtol, p_tol, u_tol):
+def test_pool_projection_against_oracle(pool_world, oracle_projection, solver, rtol, p_tol, u_tol, sweeps):
     from mac_b200.gpu import Context
     with Context(pool_world.params, max_bricks=8192, max_particles=1024, solver=solver, rtol=rtol,
                  max_iters=500) as ctx:
+        ctx.set_multigrid(sweeps)
         ctx.upload(pool_world)
         ctx.project(0)
         st = ctx.stats()
         got = ctx.download()
     e = field_errors(got, oracle_projection, ("p", "u0x", "u0y", "u0z"))
-    print(f"{solver} rtol {rtol:g}: iterations {st['iterations']}, relres {st['relres']:.2e}, errors {e}")
+    print(f"{solver} sweeps {sweeps} rtol {rtol:g}: iterations {st['iterations']}, relres {st['relres']:.2e}, errors {e}")
     assert st["relres"] <= rtol
     assert e["p"] <= p_tol, e
     assert max(e["u0x"], e["u0y"], e["u0z"]) <= u_tol, e

@@ -1,13 +1,18 @@
-"""The allocation-free CSC solve (mac_csc_solve_noalloc) against the
-context-based drop-in solve (mac_csc_factorize + mac_csc_solve), both called
-through the C-ABI on the reference's own assembled pressure matrices (the CSC
-arrays Algorithms_Solve_Pressure::Init_Iteration builds, dumped from the
-reference for the 32x32x64 jet at step 30).
+"""The allocation-free CSC solve (mac_csc_solve_noalloc), for callers that
+cannot allocate device memory, against the context-based drop-in solve
+(mac_csc_factorize + mac_csc_solve) and against the reference's own solution,
+all called through the C-ABI on the reference's own assembled pressure
+matrices (the CSC arrays Algorithms_Solve_Pressure::Init_Iteration builds,
+dumped from the reference for the 32x32x64 jet at step 30, with the solution
+its linear-solver policy returned).
 
-Both run the same FP64 Jacobi-PCG to a relative residual of 1e-12; their
-block-level reductions finish in different orders, so the solutions agree to
-a relative L2 error of 1e-10 rather than bit for bit. The solve is called
-twice in a row on the same scratch to show that nothing carries over.
+Both device solves run the same FP64 Jacobi-PCG to a relative residual of
+1e-12; their block-level reductions finish in different orders, so the
+solutions agree to a relative L2 error of 1e-10 rather than bit for bit, and
+each is within 1e-10 of the reference's solution. The solve is called twice
+in a row on the same scratch to show that nothing carries over, and the
+device's allocated and free memory are checked unchanged across those two
+calls: the property the entry point exists for.
 """
 import ctypes
 import os
@@ -33,8 +38,8 @@ def _systems():
         ind = np.frombuffer(raw, dtype="<i4", count=nnz, offset=off); off += 4 * nnz
         val = np.frombuffer(raw, dtype="<f8", count=nnz, offset=off); off += 8 * nnz
         b = np.frombuffer(raw, dtype="<f8", count=n, offset=off); off += 8 * n
-        off += 8 * n  # the reference's solution, not needed here
-        yield ptr, ind, val, b
+        xref = np.frombuffer(raw, dtype="<f8", count=n, offset=off); off += 8 * n
+        yield ptr, ind, val, b, xref
 
 
 def _context_solve(ptr, ind, val, b):
@@ -45,10 +50,9 @@ def _context_solve(ptr, ind, val, b):
         return ctx.csc_solve(ptr, ind, val, b)
 
 
-def _noalloc_solve(lib, stream, dev_arrays, n):
-    import torch
+def _noalloc_solve(lib, stream, dev_arrays, d_x, n):
     d_ptr, d_ind, d_val, d_b = dev_arrays
-    d_x = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+    d_x.fill_(float("nan"))
     its = ctypes.c_int(-1)
     rel = ctypes.c_double(-1.0)
     rc = lib.mac_csc_solve_noalloc(stream, n, d_ptr.data_ptr(), d_ind.data_ptr(), d_val.data_ptr(),
@@ -56,7 +60,7 @@ def _noalloc_solve(lib, stream, dev_arrays, n):
                                    ctypes.byref(rel))
     assert rc == 0, lib.mac_error_string(rc)
     assert 0 < its.value < 5000 and rel.value <= RTOL
-    return d_x.cpu().numpy()
+    return d_x
 
 
 def test_noalloc_solve_matches_context_solve():
@@ -65,18 +69,50 @@ def test_noalloc_solve_matches_context_solve():
     lib = load()
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
+    s = ctypes.c_void_p(stream.cuda_stream)
+    # set-up call: resolves the work array on this device before anything is measured
+    assert lib.mac_csc_solve_noalloc(s, 0, None, None, None, None, None, RTOL, 1, None, None) == 0
     checked = 0
-    for ptr, ind, val, b in _systems():
+    for ptr, ind, val, b, xref in _systems():
         n = len(b)
         assert n <= 65536
         want = _context_solve(ptr, ind, val, b)
+        assert np.linalg.norm(want - xref) / np.linalg.norm(xref) <= X_TOL
         dev = tuple(torch.from_numpy(np.array(a)).cuda() for a in (ptr, ind, val, b))
+        d_x = torch.empty((n,), dtype=torch.float64, device="cuda")
+        _noalloc_solve(lib, s, dev, d_x, n)  # warm-up: every kernel of the solve loaded
+        torch.cuda.synchronize()
+        alloc0 = torch.cuda.memory_allocated()
+        free0, _ = torch.cuda.mem_get_info()
+        got = []
         for _ in range(2):
-            got = _noalloc_solve(lib, ctypes.c_void_p(stream.cuda_stream), dev, n)
-            err = np.linalg.norm(got - want) / np.linalg.norm(want)
-            assert err <= X_TOL, err
+            _noalloc_solve(lib, s, dev, d_x, n)
+            stream.synchronize()
+            got.append(d_x.cpu().numpy())
+        assert torch.cuda.memory_allocated() == alloc0
+        assert torch.cuda.mem_get_info()[0] == free0
+        for x in got:
+            assert np.linalg.norm(x - want) / np.linalg.norm(want) <= X_TOL
+            assert np.linalg.norm(x - xref) / np.linalg.norm(xref) <= X_TOL
         checked += 1
     assert checked >= 1
+
+
+def test_noalloc_rejects_a_nonsymmetric_matrix():
+    import torch
+    from mac_b200.gpu import load
+    lib = load()
+    torch.cuda.set_device(0)
+    # 3x3, negative diagonal, A[0,1] = 1 but A[1,0] = 2: not the form CG solves
+    ptr = torch.tensor([0, 2, 4, 5], dtype=torch.int32, device="cuda")
+    ind = torch.tensor([0, 1, 0, 1, 2], dtype=torch.int32, device="cuda")
+    val = torch.tensor([-4.0, 2.0, 1.0, -4.0, -4.0], dtype=torch.float64, device="cuda")
+    b = torch.ones(3, dtype=torch.float64, device="cuda")
+    x = torch.zeros(3, dtype=torch.float64, device="cuda")
+    rc = lib.mac_csc_solve_noalloc(None, 3, ptr.data_ptr(), ind.data_ptr(), val.data_ptr(), b.data_ptr(),
+                                   x.data_ptr(), RTOL, 100, None, None)
+    torch.cuda.synchronize()
+    assert rc == -8  # MAC_ERR_MATRIX
 
 
 def test_noalloc_rejects_oversize_and_bad_arguments():
