@@ -106,6 +106,12 @@ typedef struct {
   double* u[2][3];      /* two speed buffers (src/Data_Chunk_Speed.h:13) */
   double* acc[3];       /* acceleration buffer */
   double* p;            /* pressure */
+  /* Any of u[1][*], acc[*] and p may be NULL: that field is left out of the
+   * transfer (upload zeroes it on the device, download skips it). Pipeline A's
+   * step writes speed buffer 1 and the acceleration before it reads them
+   * (RK2-TVD's stage buffers, src/Algorithms_RungeKutta_RK2_TVD.h:25-55) and
+   * the pressure of every existing cell (read first only with warm_start), so
+   * a caller that does not look at them need not move them. */
   uint8_t* flags;       /* MAC_FLAG_* */
   uint8_t* type;        /* MAC_CELL_* */
   int32_t* layer;       /* -1 empty */
@@ -141,6 +147,14 @@ const char* mac_error_string(int code);
 int mac_upload_state(void* ctx, const mac_host_state* s);
 int mac_query_sizes(void* ctx, int64_t* nbricks, int64_t* nparticles);
 int mac_download_state(void* ctx, mac_host_state* s);
+/* One FP64 cell field of every live brick, [nbricks][512] in the brick order of
+ * mac_download_state (the order of the last mac_upload_state until a topology pass
+ * runs): for host integrators that keep the world on the host and project on the
+ * device (Algorithms_Solve_Pressure_GPU in include/mac_gpu/Mac_GPU.h). */
+enum { MAC_FIELD_U0X = 0, MAC_FIELD_U0Y, MAC_FIELD_U0Z, MAC_FIELD_U1X, MAC_FIELD_U1Y, MAC_FIELD_U1Z,
+       MAC_FIELD_AX, MAC_FIELD_AY, MAC_FIELD_AZ, MAC_FIELD_P };
+int mac_upload_field(void* ctx, int field, const double* data);
+int mac_download_field(void* ctx, int field, double* data);
 
 /* ---- topology rebuild: Algorithms<Initialize_MacCell, Layer_Initial_With_Particle,
  *      Create_Fluid_Particle, Update_CellType_Layer, Delete_MacCell, Calculate_Time_Step>
@@ -171,6 +185,22 @@ int mac_forces(void* ctx, int ispeed);
  * End_Iteration of Algorithms_Solve_Pressure (src/Algorithms_Do_Pressure.h:16-21,
  * src/Algorithms_Solve_Pressure.h:44-222) */
 int mac_pressure_project(void* ctx, int ispeed);
+/* Algorithms_Solve_Pressure at its composable interface, the three member
+ * functions the reference's integrators call through Policy::
+ * (src/Algorithms_Solve_Pressure.h:44,158,168; src/Algorithms_RungeKutta_RK2_TVD.h:29,50,60-61;
+ * src/Algorithms_Do_Pressure.h:16-21):
+ * - mac_pressure_init = Init_Iteration: numbers the domain cells' system from the
+ *   current cell types, existence and const faces (face classes, multigrid set-up);
+ * - mac_pressure_divergence_projection = Divergence_Projection on the system of the
+ *   last init: divergence of speed buffer ispeed (accel = 1: of the acceleration,
+ *   Speed_GetRef() with SetAccel_Instead_Speed(true), src/Data_Chunk_Speed.h:164-171,
+ *   with the viscous Dirichlet pressures read from speed buffer ispeed), solve,
+ *   pressure write-back, gradient correction; MAC_ERR_INVALID without an init;
+ * - mac_pressure_end = End_Iteration: drops the system.
+ * A topology pass between init and end invalidates the system (re-init). */
+int mac_pressure_init(void* ctx);
+int mac_pressure_divergence_projection(void* ctx, int ispeed, int accel);
+int mac_pressure_end(void* ctx);
 /* Algorithms_RungeKutta_RK2_TVD::Do with Policy = Algorithms<Gravity, Convection> +
  * Algorithms_Solve_Pressure (src/Algorithms_RungeKutta_RK2_TVD.h:20-66) */
 int mac_rk2tvd(void* ctx);
@@ -180,6 +210,14 @@ int mac_rk2tvd(void* ctx);
 int mac_rungekutta_all(void* ctx);
 /* src/Algorithms_Extrapolate.h:25-233 */
 int mac_extrapolate(void* ctx);
+/* Algorithm_Extrapolate_Boundary_Condition, 3D form, with Policy_Is_In_Domain_Speed
+ * (src/Algorithm_Extrapolate_Boundary_Condition.h:454-975, src/Policy_Is_In_Domain_Speed.h:15-48)
+ * on speed buffer ispeed: the reference's output-time stage (test/Lateral_jet_3.cpp:706-711).
+ * The reference visits its hash map's order, on which its result depends; the device
+ * visits the boundary cells by colour (key x, y, z mod 5), one colour at a time, the
+ * three-face corners last in reverse colour order: a fixed order whose result the oracle
+ * reproduces bit for bit. */
+int mac_extrapolate_boundary_condition(void* ctx, int ispeed);
 /* Algorithms_Move_Particles + Policy_Advance_Ode_RungeKutta + Get_Speed
  * (src/Algorithms_Move_Particles.h:22-36, src/Policy_Advance_ODE_RungeKutta.h:14-27,
  * src/Policy_Speed_Interpolation_Linear_Symmetric.h:79-119 or src/Policy_Speed_Interpolation_Linear.h:64-106) */

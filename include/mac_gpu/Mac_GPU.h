@@ -170,8 +170,10 @@ class Mac_GPU_Session {
   typedef typename std::remove_reference<decltype(
       std::declval<type_Data_Grid&>().DirectAcessChunk(std::declval<const type_key&>()))>::type type_chunk;
   typedef mac_gpu_detail::has_depth<type_chunk> type_has_depth;
+  typedef typename type_Data_Grid::type_data::type_chunk_speed type_chunk_speed;
 
   DataRef m_data;
+  std::vector<std::tuple<int, int, int>> m_order;  // chunk keys (x, y, z) in the device's brick order
   void* m_ctx = nullptr;
   bool m_on_device = false;
   int m_status = MAC_OK;
@@ -234,6 +236,14 @@ class Mac_GPU_Session {
   int ToDevice() {
     if (!m_ctx) return MAC_ERR_INVALID;
     if (m_on_device) return MAC_OK;
+    int rc = Upload();
+    m_on_device = rc == MAC_OK;
+    return rc;
+  }
+
+  /* Packs the host world and uploads it; the host copy stays the master. */
+  int Upload() {
+    if (!m_ctx) return MAC_ERR_INVALID;
     type_Data_Grid& grid = m_data.m_data.GetGridData();
     std::map<std::tuple<int, int, int>, int64_t> chunks;
     for (auto it = grid.begin(); it != grid.end(); ++it) {
@@ -246,8 +256,10 @@ class Mac_GPU_Session {
     Host h;
     h.size((int64_t)chunks.size(), (int64_t)plist.size());
     int64_t b = 0;
+    m_order.clear();
     for (auto& kv : chunks) {
       int cx = std::get<2>(kv.first), cy = std::get<1>(kv.first), cz = std::get<0>(kv.first);
+      m_order.emplace_back(cx, cy, cz);
       h.keys[3 * b] = cx;
       h.keys[3 * b + 1] = cy;
       h.keys[3 * b + 2] = cz;
@@ -285,10 +297,84 @@ class Mac_GPU_Session {
     h.view.t = timing.m_t;
     h.view.dt = timing.m_dt;
     h.view.step = m_step;
-    int rc = keep(mac_upload_state(m_ctx, &h.view), "mac_upload_state");
-    m_on_device = rc == MAC_OK;
-    return rc;
+    return keep(mac_upload_state(m_ctx, &h.view), "mac_upload_state");
   }
+
+  /* The projection with the world on the host, for the reference's own
+   * integrators (Algorithms_Solve_Pressure_GPU). Init uploads the world and
+   * builds the device system; each projection uploads the field it projects
+   * (the speed buffer type_chunk_speed::ispeed, or the acceleration when
+   * SetAccel_Instead_Speed(true) is in force, src/Data_Chunk_Speed.h:150-171),
+   * runs Divergence_Projection on the device and writes the projected field
+   * and the pressure back into the chunk grid. */
+  int ProjectionInit() {
+    if (m_on_device && ToHost()) return m_status;
+    int rc = Upload();
+    return rc ? rc : keep(mac_pressure_init(m_ctx), "mac_pressure_init");
+  }
+  int ProjectionRun() {
+    if (!m_ctx) return MAC_ERR_INVALID;
+    const int ispeed = type_chunk_speed::ispeed;
+    const bool accel = type_chunk_speed::GetAccel_Instead_Speed();
+    const size_t nc = m_order.size() * (size_t)MAC_BRICK_CELLS;
+    std::vector<double> buf(nc);
+    const int sfield = MAC_FIELD_U0X + 3 * ispeed;
+    const int target = accel ? (int)MAC_FIELD_AX : sfield;
+    int rc = MAC_OK;
+    for (int d = 1; d <= 3 && !rc; ++d) {
+      Field(ispeed, d, buf.data(), true);
+      rc = keep(mac_upload_field(m_ctx, sfield + d - 1, buf.data()), "mac_upload_field");
+      if (!rc && accel) {
+        Field(-1, d, buf.data(), true);
+        rc = keep(mac_upload_field(m_ctx, MAC_FIELD_AX + d - 1, buf.data()), "mac_upload_field");
+      }
+    }
+    if (rc) return rc;
+    const int st = keep(mac_pressure_divergence_projection(m_ctx, ispeed, accel ? 1 : 0),
+                        "mac_pressure_divergence_projection");
+    if (st && st != MAC_ERR_NOT_CONVERGED) return st;
+    for (int d = 1; d <= 3 && !rc; ++d) {
+      rc = keep(mac_download_field(m_ctx, target + d - 1, buf.data()), "mac_download_field");
+      if (!rc) Field(accel ? -1 : ispeed, d, buf.data(), false);
+    }
+    if (!rc) rc = keep(mac_download_field(m_ctx, MAC_FIELD_P, buf.data()), "mac_download_field");
+    if (!rc) Pressure(buf.data());
+    return rc ? rc : st;
+  }
+  int ProjectionEnd() { return keep(mac_pressure_end(m_ctx), "mac_pressure_end"); }
+
+ private:
+  /* Component d of speed buffer s (s = -1: the acceleration) of every cell, in
+   * the device's brick order: packed into v (to_device) or written from it. */
+  void Field(int s, int d, double* v, bool to_device) {
+    type_Data_Grid& grid = m_data.m_data.GetGridData();
+    for (size_t b = 0; b < m_order.size(); ++b) {
+      type_key ckey;
+      ckey.Set(1, std::get<0>(m_order[b]));
+      ckey.Set(2, std::get<1>(m_order[b]));
+      ckey.Set(3, std::get<2>(m_order[b]));
+      auto& ch = grid.DirectAcessChunk(ckey);
+      auto* f = s < 0 ? ch.Acceleration_GetPointer(0) : ch.Speed_GetPointer(s);
+      for (int o = 0; o < MAC_BRICK_CELLS; ++o) {
+        double& x = v[b * MAC_BRICK_CELLS + o];
+        if (to_device) x = f[o].Get(d);
+        else f[o].m_speed.Set(d, x);
+      }
+    }
+  }
+  void Pressure(const double* v) {
+    type_Data_Grid& grid = m_data.m_data.GetGridData();
+    for (size_t b = 0; b < m_order.size(); ++b) {
+      type_key ckey;
+      ckey.Set(1, std::get<0>(m_order[b]));
+      ckey.Set(2, std::get<1>(m_order[b]));
+      ckey.Set(3, std::get<2>(m_order[b]));
+      auto& ch = grid.DirectAcessChunk(ckey);
+      for (int o = 0; o < MAC_BRICK_CELLS; ++o) ch.Pressure_GetPointer()[o].Pressure_Set(v[b * MAC_BRICK_CELLS + o]);
+    }
+  }
+
+ public:
 
   /* Downloads the device world into the reference's chunk grid: chunks and
    * cells erased on the device are erased on the host, live chunks get all
@@ -422,6 +508,9 @@ MAC_GPU_ALGORITHM(Algorithms_Do_Pressure_GPU, mac_pressure_project(c, 0))
 MAC_GPU_ALGORITHM(Algorithms_RungeKutta_RK2_TVD_GPU, mac_rk2tvd(c))
 /* src/Algorithms_Extrapolate.h:25-233 */
 MAC_GPU_ALGORITHM(Algorithms_Extrapolate_GPU, mac_extrapolate(c))
+/* src/Algorithm_Extrapolate_Boundary_Condition.h:454-975 on speed 0, in the device's
+ * fixed colour order (mac_extrapolate_boundary_condition) */
+MAC_GPU_ALGORITHM(Algorithm_Extrapolate_Boundary_Condition_GPU, mac_extrapolate_boundary_condition(c, 0))
 /* src/Algorithms_Move_Particles.h:22-36 */
 MAC_GPU_ALGORITHM(Algorithms_Move_Particles_GPU, mac_move_particles(c))
 /* src/Algorithms_RungeKutta_all.h:35-156 with the policy of test/Jet3.cpp:642-675
@@ -432,6 +521,26 @@ MAC_GPU_ALGORITHM(Algorithms_RungeKutta_all_GPU, mac_rungekutta_all(c))
 MAC_GPU_ALGORITHM(Algorithms_Step_GPU, mac_step(c))
 
 #undef MAC_GPU_ALGORITHM
+
+/* Algorithms_Solve_Pressure at its composable interface
+ * (src/Algorithms_Solve_Pressure.h:44,158,168): Init_Iteration,
+ * Divergence_Projection and End_Iteration on the device, for the reference's
+ * own integrators, which call them through Policy:: between host loops over
+ * the speed buffers (src/Algorithms_RungeKutta_RK2_TVD.h:29,50,60-61), and for
+ * Algorithms_Do_Pressure (src/Algorithms_Do_Pressure.h:16-21). The world
+ * stays on the host; each projection moves only the field it projects and
+ * the pressure. In place of the reference's
+ *     Policies<type_alg_solve_grid, Algorithms_Solve_Pressure<DataRef, type_pol_pres>>
+ * a world composes
+ *     Policies<type_alg_solve_grid, Algorithms_Solve_Pressure_GPU<DataRef, Policy_Mac_GPU<DataRef>>>. */
+template <class DataRef, class Policy>
+class Algorithms_Solve_Pressure_GPU : public Policy {
+ public:
+  Algorithms_Solve_Pressure_GPU(DataRef data, const Policy& pol) : Policy(pol) { (void)data; }
+  void Init_Iteration() { this->Session().ProjectionInit(); }
+  void Divergence_Projection() { this->Session().ProjectionRun(); }
+  void End_Iteration() { this->Session().ProjectionEnd(); }
+};
 
 /* Brings the device world back into the reference's chunk grid; put it before
  * any host algorithm (output, checkpoint) that reads the world. */

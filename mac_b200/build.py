@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmac_gpu.so")
-SOURCES = ["mac_ctx.cu", "mac_topology.cu", "mac_advect.cu", "mac_pressure.cu", "mac_mg.cu", "mac_step.cu", "mac_noalloc.cu", "mac_unet.cu"]
+SOURCES = ["mac_ctx.cu", "mac_topology.cu", "mac_advect.cu", "mac_pressure.cu", "mac_mg.cu", "mac_step.cu", "mac_noalloc.cu", "mac_unet.cu",
+           "mac_extrap_bc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CONTRACT_OK = {"mac_mg.cu", "mac_unet.cu"}
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -438,14 +438,22 @@ struct GlobalField {
 // (its cells with a two-cell halo), falling back to the brick table outside it.
 constexpr int kStage = 12;
 constexpr int kStageCells = kStage * kStage * kStage;
+// Shared-memory layout of the staged field: slot x + kStage y + kStageZ z per
+// component, components kStageComp apart. A z-stride of kStage^2 = 144
+// doubles is a multiple of the 32 four-byte banks, so the 2x2x2 stencil's
+// z-pairs of neighbouring particles hit the same banks; one padding double per
+// z-plane moves them two banks apart.
+constexpr int kStageZ = kStage * kStage + 1;
+constexpr int kStageComp = kStageZ * kStage;
+__host__ __device__ constexpr int stage_slot(int x, int y, int z) { return x + kStage * y + kStageZ * z; }
 struct StagedField {
-  const double* s;        // [3][kStageCells]
+  const double* s;        // [3][kStageComp]
   int ox, oy, oz;         // cell key of stage slot (0,0,0)
   GlobalField g;
   __device__ double u(int k, int kx, int ky, int kz, int* bad) const {
     unsigned x = (unsigned)(kx - ox), y = (unsigned)(ky - oy), z = (unsigned)(kz - oz);
     if (x < (unsigned)kStage && y < (unsigned)kStage && z < (unsigned)kStage)
-      return s[k * kStageCells + (int)(x + kStage * (y + kStage * z))];
+      return s[k * kStageComp + stage_slot((int)x, (int)y, (int)z)];
     return g.u(k, kx, ky, kz, bad);
   }
   // The 2x2x2 stencil of component k at corner key (index n = 4X + 2Y + Z);
@@ -453,15 +461,15 @@ struct StagedField {
   __device__ void u8(int k, const int* key, double* out, int* bad) const {
     unsigned x = (unsigned)(key[0] - ox), y = (unsigned)(key[1] - oy), z = (unsigned)(key[2] - oz);
     if (x + 1 < (unsigned)kStage && y + 1 < (unsigned)kStage && z + 1 < (unsigned)kStage) {
-      const double* p = s + k * kStageCells + (int)(x + kStage * (y + kStage * z));
+      const double* p = s + k * kStageComp + stage_slot((int)x, (int)y, (int)z);
       out[0] = p[0];
-      out[1] = p[kStage * kStage];
+      out[1] = p[kStageZ];
       out[2] = p[kStage];
-      out[3] = p[kStage + kStage * kStage];
+      out[3] = p[kStage + kStageZ];
       out[4] = p[1];
-      out[5] = p[1 + kStage * kStage];
+      out[5] = p[1 + kStageZ];
       out[6] = p[1 + kStage];
-      out[7] = p[1 + kStage + kStage * kStage];
+      out[7] = p[1 + kStage + kStageZ];
       return;
     }
 #pragma unroll
@@ -677,7 +685,7 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
                                                      const double* __restrict__ ux, const double* __restrict__ uy,
                                                      const double* __restrict__ uz, Params P,
                                                      const Scalars* __restrict__ ds, unsigned long long* bad_count) {
-  __shared__ double s[3 * kStageCells];
+  __shared__ double s[3 * kStageComp];
   __shared__ int sn[kNbr];
   int b = blist[blockIdx.x];
   int64_t p0 = off[b], p1 = off[b + 1];
@@ -691,13 +699,14 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
     int lx = x - 2, ly = y - 2, lz = z - 2;  // local coordinates in brick b, -2..9
     int dx = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), dy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0), dz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
     int nb = sn[nbr_index(dx, dy, dz)];
+    const int j = stage_slot(x, y, z);
     if (nb < 0) {
-      s[i] = s[kStageCells + i] = s[2 * kStageCells + i] = 0.0;
+      s[j] = s[kStageComp + j] = s[2 * kStageComp + j] = 0.0;
     } else {
       int64_t gi = (int64_t)nb * kCells + (lx - 8 * dx) + 8 * (ly - 8 * dy) + 64 * (lz - 8 * dz);
-      s[i] = U[0][gi];
-      s[kStageCells + i] = U[1][gi];
-      s[2 * kStageCells + i] = U[2][gi];
+      s[j] = U[0][gi];
+      s[kStageComp + j] = U[1][gi];
+      s[2 * kStageComp + j] = U[2][gi];
     }
   }
   __syncthreads();

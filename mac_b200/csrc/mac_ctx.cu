@@ -95,6 +95,14 @@ __global__ void k_gather_bricks(T* __restrict__ out, const T* __restrict__ in, c
   out[i] = in[(size_t)blist[bi] * kCells + o];
 }
 
+// The inverse of k_gather_bricks: brick-ordered values into the pool.
+__global__ void k_scatter_bricks(double* __restrict__ out, const double* __restrict__ in,
+                                 const int* __restrict__ blist, int nlive) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nlive * kCells) return;
+  out[(size_t)blist[(int)(i >> 9)] * kCells + (i & 511)] = in[i];
+}
+
 __global__ void k_unpack_lay(const int8_t* __restrict__ lay, const int* __restrict__ blist, int nlive,
                              uint8_t* __restrict__ ex, int32_t* __restrict__ layer) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -190,6 +198,7 @@ static void free_all(Ctx* c) {
   for (cudaEvent_t e : c->ev_lag)
     if (e) cudaEventDestroy(e);
   cudaFree(c->csc_off); cudaFree(c->csc_ind); cudaFree(c->csc_val); cudaFree(c->csc_vec);
+  cudaFree(c->csr_off); cudaFree(c->csr_ind); cudaFree(c->csr_val); cudaFree(c->eb_work);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -325,13 +334,13 @@ static int upload(Ctx* c, const mac_host_state* s) {
     int32_t* tkeys = (int32_t*)c->r;
     MAC_CUDA(cudaMemcpyAsync(tkeys, s->keys, sizeof(int32_t) * 3 * nb, cudaMemcpyHostToDevice, st));
     k_set_keys<<<grid_for(3 * nb, 256), 256, 0, st>>>(c->bkey, tkeys, nb); MAC_COUNT(c);
-    for (int b = 0; b < 2; ++b)
-      for (int i = 0; i < 3; ++i)
-        MAC_CUDA(cudaMemcpyAsync(c->f64 + (size_t)(U0X + 3 * b + i) * cap, s->u[b][i], 8 * nc,
-                                 cudaMemcpyHostToDevice, st));
-    for (int i = 0; i < 3; ++i)
-      MAC_CUDA(cudaMemcpyAsync(c->f64 + (size_t)(AX + i) * cap, s->acc[i], 8 * nc, cudaMemcpyHostToDevice, st));
-    MAC_CUDA(cudaMemcpyAsync(c->f64 + (size_t)PRES * cap, s->p, 8 * nc, cudaMemcpyHostToDevice, st));
+    // a NULL stage buffer (speed 1, acceleration) is not transferred: zeroed here
+    for (int f = 0; f < NF64; ++f) {
+      const double* src = f < 6 ? s->u[f / 3][f % 3] : (f < 9 ? s->acc[f - 6] : s->p);
+      double* dst = c->f64 + (size_t)f * cap;
+      if (src) MAC_CUDA(cudaMemcpyAsync(dst, src, 8 * nc, cudaMemcpyHostToDevice, st));
+      else MAC_CUDA(cudaMemsetAsync(dst, 0, 8 * nc, st));
+    }
     MAC_CUDA(cudaMemcpyAsync(c->flags, s->flags, nc, cudaMemcpyHostToDevice, st));
     MAC_CUDA(cudaMemcpyAsync(c->type, s->type, nc, cudaMemcpyHostToDevice, st));
     uint8_t* tex = (uint8_t*)c->z;
@@ -390,6 +399,7 @@ static int download(Ctx* c, mac_host_state* s) {
     MAC_CUDA(cudaMemcpyAsync(s->keys, tk, 12 * (size_t)nb, cudaMemcpyDeviceToHost, st));
     for (int f = 0; f < NF64; ++f) {
       double* dst = f < 6 ? s->u[f / 3][f % 3] : (f < 9 ? s->acc[f - 6] : s->p);
+      if (!dst) continue;  // a field the caller leaves out
       k_gather_bricks<double><<<g, 256, 0, st>>>(tmp, c->f64 + (size_t)f * cap, c->blist, nb); MAC_COUNT(c);
       MAC_CUDA(cudaMemcpyAsync(dst, tmp, 8 * nc, cudaMemcpyDeviceToHost, st));
       MAC_CUDA(cudaStreamSynchronize(st));
@@ -426,6 +436,29 @@ static int download(Ctx* c, mac_host_state* s) {
   s->t = c->hs->t;
   s->dt = c->hs->dt;
   s->step = c->seed;
+  return MAC_OK;
+}
+
+// One FP64 cell field (MAC_FIELD_*) of every live brick, in the brick order of
+// mac_download_state (the order of the last upload while no topology pass has
+// run), through the solver vector q as staging.
+int field_transfer(Ctx* c, int field, const double* hin, double* hout) {
+  if (field < 0 || field >= NF64) return MAC_ERR_INVALID;
+  MAC_TRY(read_scalars(c));
+  const int nb = c->nlive_host;
+  if (nb == 0) return MAC_OK;
+  const size_t nc = (size_t)nb * kCells, cap = (size_t)c->cap_bricks * kCells;
+  cudaStream_t st = c->stream;
+  double* dst = c->f64 + (size_t)field * cap;
+  const int g = grid_for((int64_t)nc, 256);
+  if (hin) {
+    MAC_CUDA(cudaMemcpyAsync(c->q, hin, 8 * nc, cudaMemcpyHostToDevice, st));
+    k_scatter_bricks<<<g, 256, 0, st>>>(dst, c->q, c->blist, nb); MAC_COUNT(c);
+  } else {
+    k_gather_bricks<double><<<g, 256, 0, st>>>(c->q, dst, c->blist, nb); MAC_COUNT(c);
+    MAC_CUDA(cudaMemcpyAsync(hout, c->q, 8 * nc, cudaMemcpyDeviceToHost, st));
+  }
+  MAC_CUDA(cudaStreamSynchronize(st));
   return MAC_OK;
 }
 
@@ -509,6 +542,20 @@ int mac_query_sizes(void* ctx, int64_t* nbricks, int64_t* nparticles) {
   if (nbricks) *nbricks = c->nlive_host;
   if (nparticles) *nparticles = c->np_host;
   return rc;
+}
+
+int mac_upload_field(void* ctx, int field, const double* data) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !data) return MAC_ERR_INVALID;
+  cudaSetDevice(c->prm.device);
+  return mac::field_transfer(c, field, data, nullptr);
+}
+
+int mac_download_field(void* ctx, int field, double* data) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !data) return MAC_ERR_INVALID;
+  cudaSetDevice(c->prm.device);
+  return mac::field_transfer(c, field, nullptr, data);
 }
 
 int mac_download_state(void* ctx, mac_host_state* s) {

@@ -218,6 +218,7 @@ struct Ctx {
   int* csr_off = nullptr;      // row-major copy for BiCGStab
   int* csr_ind = nullptr;
   double* csr_val = nullptr;
+  int* eb_work = nullptr;      // boundary-condition extrapolation: colour counts and cursors
   long long launches = 0;      // kernels launched by this context
   struct Prof* prof = nullptr; // per-phase event timing (null when off)
 };

@@ -481,6 +481,28 @@ int mac_pressure_project(void* ctx, int ispeed) {
   int rc = mac::setup_system(c);
   return rc ? rc : mac::project(c, ispeed);
 }
+int mac_pressure_init(void* ctx) {
+  CTX_OR_FAIL();
+  return mac::setup_system(c);
+}
+int mac_pressure_divergence_projection(void* ctx, int ispeed, int accel) {
+  CTX_OR_FAIL();
+  if (ispeed < 0 || ispeed > 1 || (accel != 0 && accel != 1)) return MAC_ERR_INVALID;
+  if (!c->system_ready) return MAC_ERR_INVALID;  // mac_pressure_init first
+  const size_t cap = (size_t)c->cap_bricks * mac::kCells;
+  double* S[3];
+  double* A[3];
+  for (int i = 0; i < 3; ++i) {
+    S[i] = c->f64 + (size_t)(mac::U0X + 3 * ispeed + i) * cap;
+    A[i] = c->f64 + (size_t)(mac::AX + i) * cap;
+  }
+  return accel ? mac::project_field(c, A, S) : mac::project_field(c, S, S);
+}
+int mac_pressure_end(void* ctx) {
+  CTX_OR_FAIL();
+  c->system_ready = false;
+  return MAC_OK;
+}
 int mac_rk2tvd(void* ctx) {
   CTX_OR_FAIL();
   return mac::rk2tvd(c);

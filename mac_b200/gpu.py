@@ -59,10 +59,11 @@ class mac_stats(ctypes.Structure):
 
 
 EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_stats", "mac_error_string",
-           "mac_upload_state", "mac_query_sizes", "mac_download_state", "mac_initialize_maccell",
+           "mac_upload_state", "mac_query_sizes", "mac_download_state", "mac_upload_field", "mac_download_field",
+           "mac_pressure_init", "mac_pressure_divergence_projection", "mac_pressure_end", "mac_initialize_maccell",
            "mac_layer_initial_with_particle", "mac_create_fluid_particle", "mac_update_celltype_layer",
            "mac_delete_maccell", "mac_calculate_time_step", "mac_topology_rebuild", "mac_forces",
-           "mac_pressure_project", "mac_rk2tvd", "mac_rungekutta_all", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
+           "mac_pressure_project", "mac_extrapolate_boundary_condition", "mac_rk2tvd", "mac_rungekutta_all", "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync",
            "mac_stream", "mac_launch_count", "mac_set_profiling", "mac_get_profile",
            "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc",
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
@@ -97,11 +98,16 @@ def load(path: str = LIB_PATH):
     for n in ["mac_initialize_maccell", "mac_layer_initial_with_particle", "mac_create_fluid_particle",
               "mac_update_celltype_layer", "mac_delete_maccell", "mac_topology_rebuild", "mac_rk2tvd",
               "mac_rungekutta_all",
-              "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync", "mac_csc_clean"]:
+              "mac_extrapolate", "mac_move_particles", "mac_step", "mac_sync", "mac_csc_clean",
+              "mac_pressure_init", "mac_pressure_end"]:
         getattr(lib, n).argtypes = [vp]
     lib.mac_calculate_time_step.argtypes = [vp, _P(ctypes.c_double)]
     lib.mac_forces.argtypes = [vp, ctypes.c_int]
+    lib.mac_extrapolate_boundary_condition.argtypes = [vp, ctypes.c_int]
     lib.mac_pressure_project.argtypes = [vp, ctypes.c_int]
+    lib.mac_pressure_divergence_projection.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.mac_upload_field.argtypes = [vp, ctypes.c_int, _P(ctypes.c_double)]
+    lib.mac_download_field.argtypes = [vp, ctypes.c_int, _P(ctypes.c_double)]
     lib.mac_csc_factorize.argtypes = [vp, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_double)]
     lib.mac_csc_solve.argtypes = [vp, ctypes.c_int, _P(ctypes.c_double), _P(ctypes.c_double)]
     lib.mac_stream.argtypes = [vp, _P(vp)]
@@ -170,7 +176,13 @@ class HostState:
     """Host arrays laid out as mac_host_state expects (optionally in pinned
     memory); ``depth`` carries the per-cell depth of the depth composition."""
 
-    def __init__(self, nbricks: int, nparticles: int, pinned: bool = False, depth: bool = False):
+    # speed buffer 1 and the acceleration: RK2-TVD's stage buffers
+    STAGE = ("u1x", "u1y", "u1z", "ax", "ay", "az")
+
+    def __init__(self, nbricks: int, nparticles: int, pinned: bool = False, depth: bool = False,
+                 stage_buffers: bool = True):
+        """stage_buffers=False leaves speed buffer 1 and the acceleration out
+        (NULL in mac_host_state: not transferred either way)."""
         nc = nbricks * BRICK_CELLS
         if pinned:
             import torch
@@ -183,9 +195,11 @@ class HostState:
             u8 = lambda n: np.empty(n, np.uint8)
             i32 = lambda n: np.empty(n, np.int32)
         self.nbricks, self.nparticles = nbricks, nparticles
+        self.cap_bricks, self.cap_particles = nbricks, nparticles
         self.keys = i32(3 * max(nbricks, 1))
         self.exists = u8(max(nc, 1))
-        self.f64 = {n: f64(max(nc, 1)) for n in CELL_F64}
+        self.fields = [n for n in CELL_F64 if stage_buffers or n not in self.STAGE]
+        self.f64 = {n: f64(max(nc, 1)) for n in self.fields}
         self.flags = u8(max(nc, 1))
         self.type = u8(max(nc, 1))
         self.layer = i32(max(nc, 1))
@@ -198,7 +212,7 @@ class HostState:
         nb, nc = s.nbricks, s.nbricks * BRICK_CELLS
         self.keys[:3 * nb] = s.keys.reshape(-1)
         self.exists[:nc] = s.exists.reshape(-1)
-        for n in CELL_F64:
+        for n in self.fields:
             self.f64[n][:nc] = s.f64[n].reshape(-1)
         self.flags[:nc] = s.flags.reshape(-1)
         self.type[:nc] = s.type.reshape(-1)
@@ -213,7 +227,7 @@ class HostState:
     def nbytes(self) -> int:
         """Bytes of the current state content (what one transfer moves)."""
         nc = self.nbricks * BRICK_CELLS
-        per_cell = 1 + 8 * len(CELL_F64) + 1 + 1 + 4 + (4 if self.depth is not None else 0)
+        per_cell = 1 + 8 * len(self.fields) + 1 + 1 + 4 + (4 if self.depth is not None else 0)
         return 12 * self.nbricks + nc * per_cell + 24 * self.nparticles
 
     def c_struct(self) -> mac_host_state:
@@ -221,11 +235,12 @@ class HostState:
         h.nbricks, h.nparticles = self.nbricks, self.nparticles
         h.keys = _ptr(self.keys, ctypes.c_int32)
         h.exists = _ptr(self.exists, ctypes.c_uint8)
+        f = lambda n: _ptr(self.f64[n], ctypes.c_double) if n in self.f64 else None
         for b in range(2):
             for i in range(3):
-                h.u[b][i] = _ptr(self.f64[CELL_F64[3 * b + i]], ctypes.c_double)
+                h.u[b][i] = f(CELL_F64[3 * b + i])
         for i in range(3):
-            h.acc[i] = _ptr(self.f64[CELL_F64[6 + i]], ctypes.c_double)
+            h.acc[i] = f(CELL_F64[6 + i])
         h.p = _ptr(self.f64["p"], ctypes.c_double)
         h.flags = _ptr(self.flags, ctypes.c_uint8)
         h.type = _ptr(self.type, ctypes.c_uint8)
@@ -241,7 +256,8 @@ class HostState:
         pr = Params(**{**params.__dict__})
         pr.t, pr.dt, pr.step = self.t, self.dt, self.step
         return State(pr, self.keys[:3 * nb].reshape(nb, 3).copy(), self.exists[:nc].reshape(shp).copy(),
-                     {n: self.f64[n][:nc].reshape(shp).copy() for n in CELL_F64},
+                     {n: (self.f64[n][:nc].reshape(shp).copy() if n in self.f64 else np.zeros(shp))
+                      for n in CELL_F64},
                      self.flags[:nc].reshape(shp).copy(), self.type[:nc].reshape(shp).copy(),
                      self.layer[:nc].reshape(shp).copy(), np.full(shp, -1, np.int32),
                      self.pos[:3 * npart].reshape(npart, 3).copy(),
@@ -300,7 +316,7 @@ class Context:
         (key-sorted copies of the arrays), or, with ``to_state=False``, the
         HostState itself with the arrays as the C-ABI wrote them."""
         nb, npart = self.sizes()
-        if host is None or host.nbricks < nb or len(host.pos) < 3 * npart:
+        if host is None or host.cap_bricks < nb or host.cap_particles < npart:
             host = HostState(nb, npart, depth=bool(self.params.depth_mode))
         host.nbricks, host.nparticles = nb, npart
         st = host.c_struct()
@@ -331,12 +347,46 @@ class Context:
         self._check(self.lib.mac_calculate_time_step(self.h, ctypes.byref(v)), "mac_calculate_time_step")
         return v.value
 
+    def extrapolate_boundary_condition(self, ispeed=0):
+        """Algorithm_Extrapolate_Boundary_Condition (3D form) in the device's fixed colour order."""
+        return self._check(self.lib.mac_extrapolate_boundary_condition(self.h, ispeed),
+                           "mac_extrapolate_boundary_condition")
+
     def forces(self, ispeed=0):
         return self._check(self.lib.mac_forces(self.h, ispeed), "mac_forces")
 
     def project(self, ispeed=0, allow_not_converged=False):
         return self._check(self.lib.mac_pressure_project(self.h, ispeed), "mac_pressure_project",
                            allow=(-4,) if allow_not_converged else ())
+
+    # ---- the projection at Algorithms_Solve_Pressure's composable interface
+    def pressure_init(self):
+        """Init_Iteration (src/Algorithms_Solve_Pressure.h:44): the system of the current cells."""
+        self._check(self.lib.mac_pressure_init(self.h), "mac_pressure_init")
+
+    def divergence_projection(self, ispeed=0, accel=False, allow_not_converged=False):
+        """Divergence_Projection (src/Algorithms_Solve_Pressure.h:168) on the last init's system."""
+        return self._check(self.lib.mac_pressure_divergence_projection(self.h, ispeed, 1 if accel else 0),
+                           "mac_pressure_divergence_projection", allow=(-4,) if allow_not_converged else ())
+
+    def pressure_end(self):
+        """End_Iteration (src/Algorithms_Solve_Pressure.h:158)."""
+        self._check(self.lib.mac_pressure_end(self.h), "mac_pressure_end")
+
+    FIELDS = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
+
+    def upload_field(self, name, values):
+        """One FP64 cell field, [nbricks * 512] in the device's brick order (that of download())."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self.lib.mac_upload_field(self.h, self.FIELDS.index(name), _ptr(v, ctypes.c_double)),
+                    "mac_upload_field")
+
+    def download_field(self, name):
+        nb, _ = self.sizes()
+        out = np.empty(nb * BRICK_CELLS, np.float64)
+        self._check(self.lib.mac_download_field(self.h, self.FIELDS.index(name), _ptr(out, ctypes.c_double)),
+                    "mac_download_field")
+        return out
 
     def rk2tvd(self, allow_not_converged=False):
         return self._check(self.lib.mac_rk2tvd(self.h), "mac_rk2tvd", allow=(-4,) if allow_not_converged else ())

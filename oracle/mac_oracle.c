@@ -21,6 +21,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "solve3.h"
 #include "state_format.h"
 
 #define ACC 3 /* index of the acceleration among the brick's vector fields */
@@ -1114,6 +1115,352 @@ static void alg_move(world_t* w, int sym) {
 
 /* ---------------------------------------------------------- setup passes */
 /* src/Algorithms_Solid_To_Const.h:32-58 */
+/* ------------------------------------------- boundary-condition extrapolation
+ * Algorithm_Extrapolate_Boundary_Condition, 3D form
+ * (src/Algorithm_Extrapolate_Boundary_Condition.h:454-975, common part :52-252)
+ * with Policy_Is_In_Domain_Speed (src/Policy_Is_In_Domain_Speed.h:15-48), on
+ * speed buffer w->ispeed, every write through the non-forced Set (const faces
+ * keep their value).
+ *
+ * Visiting order. The reference visits its hash map's order, and a boundary
+ * cell's case writes faces that later cells read, so its result depends on
+ * that order. Here the order is fixed: cells by colour (x mod 5, y mod 5,
+ * z mod 5), colours in turn, keys in order within a colour; the stack of
+ * three-face corners is unwound in the reverse order (LIFO, :489-494). Every
+ * read and write of one cell's case lies within Chebyshev distance 2 of the
+ * cell, so two cells of one colour (5 or more apart on some axis) never touch
+ * the same face and a colour's cells commute: the device runs each colour in
+ * parallel and reaches the same values.
+ *
+ * Reference details kept: GetNeighbour(i, 0) is the -e_i neighbour (so
+ * apply_nan_extrap counts it twice), Apply_Div_3d keeps only the last
+ * tangential term, the n == 1 case's flag b is never cleared. An air or
+ * missing neighbour counts as "not a boundary" where the reference reads an
+ * unset counter; a read of a missing cell gives NaN (the reference would
+ * dereference a null chunk), a write to one is dropped. The 3x3 corner
+ * systems, which the reference hands to its Umfpack policy, are solved by
+ * Gaussian elimination with partial pivoting (mac_solve3, solve3.h; the device
+ * repeats its operations). */
+static int eb_valid(world_t* w, int x, int y, int z) { return cell_valid(w, cell_at(w, x, y, z)); }
+static int eb_air(world_t* w, int x, int y, int z) {
+  cell_t c = cell_at(w, x, y, z);
+  return !cell_valid(w, c) || is_air(B(c)->type[c.o]);
+}
+static double eb_u(world_t* w, const int k[3], int i) { /* i: 1..3 */
+  cell_t c = cell_at(w, k[0], k[1], k[2]);
+  return cell_valid(w, c) ? B(c)->u[w->ispeed][i - 1][c.o] : NAN;
+}
+static void eb_set(world_t* w, const int k[3], int i, double v) {
+  cell_t c = cell_at(w, k[0], k[1], k[2]);
+  if (cell_valid(w, c)) set_u(B(c), B(c)->u[w->ispeed][i - 1], c.o, i - 1, v, 0);
+}
+/* key + s e_i (i 1..3; s = 0 means -1, as the neighbour tables index (s + 1) >> 1) */
+static void eb_nb(const int k[3], int i, int s, int out[3]) {
+  out[0] = k[0]; out[1] = k[1]; out[2] = k[2];
+  out[i - 1] += s > 0 ? 1 : -1;
+}
+/* IsBoundary (:89-119): the air face-neighbours in (i, s) order; 0 for an air
+ * or missing cell */
+static int eb_boundary(world_t* w, const int k[3], int dir[6], int sign[6]) {
+  if (!eb_valid(w, k[0], k[1], k[2]) || eb_air(w, k[0], k[1], k[2])) return 0;
+  int n = 0;
+  for (int i = 1; i <= 3; ++i)
+    for (int s = -1; s <= 1; s += 2) {
+      int k2[3];
+      eb_nb(k, i, s, k2);
+      if (eb_valid(w, k2[0], k2[1], k2[2]) && eb_air(w, k2[0], k2[1], k2[2])) {
+        dir[n] = i;
+        sign[n] = s;
+        ++n;
+      }
+    }
+  return n;
+}
+static void eb_set_nan(world_t* w, const int k[3]) { /* apply_set_nan (:149-177) */
+  if (eb_air(w, k[0], k[1], k[2]) == 0) return;
+  for (int i = 1; i <= 3; ++i)
+    for (int s = -1; s <= 1; s += 2) {
+      int k2[3];
+      eb_nb(k, i, s, k2);
+      if (eb_valid(w, k2[0], k2[1], k2[2])) {
+        if (eb_air(w, k2[0], k2[1], k2[2])) eb_set(w, s == -1 ? k : k2, i, NAN);
+      } else if (s == -1) {
+        eb_set(w, k, i, NAN);
+      }
+    }
+}
+static int eb_in_domain(world_t* w, const int k[3], int d) { /* Get_Is_Speed_In_Domain */
+  int k2[3], k3[3];
+  eb_nb(k, d, -1, k2);
+  const int f1 = !eb_air(w, k[0], k[1], k[2]);
+  if (!eb_valid(w, k2[0], k2[1], k2[2])) return f1;
+  const int f2 = !eb_air(w, k2[0], k2[1], k2[2]);
+  if (f1 && f2) return 1;
+  if (!f1 && !f2) return 0;
+  if (f1) eb_nb(k, d, 1, k3);
+  else eb_nb(k2, d, -1, k3);
+  if (!eb_valid(w, k3[0], k3[1], k3[2])) return 1;
+  return eb_air(w, k3[0], k3[1], k3[2]);
+}
+static void eb_div(world_t* w, const int k[3], int d, int sign) { /* Apply_Div_3d (:912-932) */
+  int n[3];
+  eb_nb(k, d, 1, n);
+  double v = eb_u(w, k, d);
+  if (sign == -1) {
+    v = eb_u(w, n, d);
+    n[0] = k[0]; n[1] = k[1]; n[2] = k[2];
+  }
+  double res = 0;
+  for (int d2 = 1; d2 <= 3; ++d2) {
+    if (d2 == d) continue;
+    int k3[3];
+    eb_nb(k, d2, 1, k3);
+    res = w->ih[d2 - 1] * (eb_u(w, k3, d2) - eb_u(w, k, d2));
+  }
+  res = v - sign * res * w->h[d - 1];
+  eb_set(w, n, d, res);
+}
+static void eb_plane(world_t* w, const int a[3], const int b[3], int d, int sign, int d2) { /* Apply_3d_Plane (:897-911) */
+  int n[3] = {a[0], a[1], a[2]}, n2[3] = {b[0], b[1], b[2]};
+  if (sign == 1) {
+    eb_nb(a, d, 1, n);
+    eb_nb(b, d, 1, n2);
+  }
+  const double v1 = eb_u(w, n, d), v2 = eb_u(w, n2, d), v3 = eb_u(w, b, d2);
+  const double v = -sign * w->ih[d2 - 1] * w->h[d - 1] * (v2 - v1) + v3;
+  int k3[3];
+  eb_nb(b, d, sign, k3);
+  eb_set(w, k3, d2, v);
+}
+static void eb_plane45(world_t* w, const int k[3], int sa, int da, int sb, int db) { /* Apply_3d_Plane_45 (:934-952) */
+  int n1[3], n2[3];
+  eb_nb(k, da, 1, n1);
+  eb_nb(k, db, 1, n2);
+  double v1 = eb_u(w, k, da), v2 = eb_u(w, k, db);
+  if (sa == -1) {
+    v1 = eb_u(w, n1, da);
+    n1[0] = k[0]; n1[1] = k[1]; n1[2] = k[2];
+  }
+  if (sb == -1) {
+    v2 = eb_u(w, n2, db);
+    n2[0] = k[0]; n2[1] = k[1]; n2[2] = k[2];
+  }
+  eb_set(w, n1, da, v1);
+  eb_set(w, n2, db, v2);
+}
+/* Choose_Boundary_Case_3d (:793-890) for all but the n == 3 corners, which
+ * the caller keeps for eb_corner. */
+static void eb_choose(world_t* w, const int k[3], const int* dir, const int* sign, int n) {
+  if (n == 1) {
+    eb_div(w, k, dir[0], sign[0]);
+    for (int d2 = 1; d2 <= 3; ++d2) {
+      if (d2 == dir[0]) continue;
+      for (int i = -1; i <= 1; i += 2) {
+        int k2[3], dt[6], st[6];
+        eb_nb(k, d2, i, k2);
+        const int nt = eb_boundary(w, k2, dt, st);
+        if (nt == 1) eb_div(w, k2, dt[0], st[0]);
+        if (nt == 1 && dt[0] == dir[0]) {
+          if (i < 0) eb_plane(w, k2, k, dir[0], sign[0], d2);
+          else eb_plane(w, k, k2, dir[0], sign[0], d2);
+        }
+      }
+      int k3[3] = {k[0], k[1], k[2]};
+      if (sign[0] == 1) eb_nb(k, dir[0], 1, k3);
+      if (!eb_in_domain(w, k, dir[0])) eb_set(w, k3, dir[0], NAN);
+    }
+  } else if (n == 2) {
+    if (dir[0] != dir[1]) eb_plane45(w, k, sign[0], dir[0], sign[1], dir[1]);
+  } else if (n != 3) {
+    for (int i = 0; i < n; ++i) {
+      int k2[3] = {k[0], k[1], k[2]};
+      if (sign[i] == 1) eb_nb(k, dir[i], 1, k2);
+      if (!eb_in_domain(w, k2, dir[i])) eb_set(w, k2, dir[i], NAN);
+    }
+  }
+}
+/* The n == 3 corner signs (s1, s2, s3) or 0 when an axis repeats. */
+static int eb_corner_signs(const int* dir, const int* sign, int n, int s[3]) {
+  s[0] = s[1] = s[2] = 0;
+  for (int a = 1; a <= 3; ++a)
+    for (int i = 0; i < n; ++i)
+      if (dir[i] == a) {
+        s[a - 1] = sign[i];
+        break;
+      }
+  return s[0] != 0 && s[1] != 0 && s[2] != 0;
+}
+/* SolveMatrix (:571-775): the 3x3 system of CreateMatrix (:551-570; its CSC
+ * value[3 j + r] is A[r][j], so A below is row-major) with the right-hand
+ * side of the reference's terms, in their order. */
+static void eb_corner(world_t* w, const int k[3], int s1, int s2, int s3) {
+  const double* ih = w->ih;
+  const double A[9] = {
+      -s1 * 2 * ih[0] - s1 * 0.5 * ih[2], s2 * 2 * ih[1] + s2 * 0.5 * ih[2], -s3 * 0.5 * ih[0] + s2 * s3 * 0.5 * ih[1],
+      -s1 * 0.5 * ih[2] + s1 * 0.5 * ih[1], s2 * 2 * ih[1] + s2 * 0.5 * ih[1], -s3 * 2 * ih[2] - s3 * 0.5 * ih[0],
+      s1 * ih[0], s2 * ih[1], s3 * ih[2]};
+  int e1[3], e2[3], e3[3], m1[3], m2[3], m3[3], t[3];
+  eb_nb(k, 1, 1, e1);
+  eb_nb(k, 2, 1, e2);
+  eb_nb(k, 3, 1, e3);
+  eb_nb(k, 1, -s1, m1);
+  eb_nb(k, 2, -s2, m2);
+  eb_nb(k, 3, -s3, m3);
+#define U(key, i) eb_u(w, key, i)
+  double b[3], x[3];
+  b[0] = 0;
+  b[0] += s1 == 1 ? -2 * ih[0] * U(k, 1) : 2 * ih[0] * U(e1, 1);
+  b[0] += s2 == 1 ? 2 * ih[1] * U(k, 2) : -2 * ih[1] * U(e2, 2);
+  b[0] += s3 == 1 ? 0.5 * ih[0] * U(k, 3) : -0.5 * ih[0] * U(e3, 3);
+  eb_nb(m1, 3, 1, t);
+  b[0] += s3 * 0.5 * ih[0] * (-U(m1, 3) - U(t, 3));
+  b[0] += s1 == 1 ? 0.5 * ih[2] * U(k, 1) : -0.5 * ih[2] * U(e1, 1);
+  eb_nb(m3, 1, 1, t);
+  b[0] += s1 * 0.5 * ih[2] * (-U(m3, 1) - U(t, 1));
+  b[0] += s3 == 1 ? -0.5 * ih[1] * U(k, 3) : 0.5 * ih[1] * U(e3, 3);
+  eb_nb(m2, 3, 1, t);
+  b[0] += s3 * 0.5 * ih[1] * (U(m2, 3) + U(t, 3));
+  b[0] += s2 == 1 ? -0.5 * ih[2] * U(k, 2) : 0.5 * ih[2] * U(e2, 2);
+  eb_nb(m3, 2, 1, t);
+  b[0] += s2 * 0.5 * ih[2] * (U(m3, 2) + U(t, 2));
+  b[1] = 0;
+  b[1] += s3 == 1 ? -2 * ih[2] * U(k, 3) : 2 * ih[2] * U(m3, 3);
+  b[1] += s2 == 1 ? 2 * ih[1] * U(k, 2) : -2 * ih[1] * U(e2, 2);
+  b[1] += s3 == 1 ? 0.5 * ih[0] * U(k, 3) : -0.5 * ih[0] * U(e3, 3);
+  eb_nb(m1, 3, 1, t);
+  b[1] += s3 * 0.5 * ih[0] * (-U(m1, 3) - U(t, 3));
+  b[1] += s1 == 1 ? 0.5 * ih[2] * U(k, 1) : -0.5 * ih[2] * U(e1, 1);
+  eb_nb(m3, 1, 1, t);
+  b[1] += s1 * 0.5 * ih[2] * (-U(m3, 1) - U(t, 1));
+  b[1] += s1 == 1 ? -0.5 * ih[1] * U(k, 1) : -0.5 * ih[1] * U(e1, 1);
+  eb_nb(m2, 1, 1, t);
+  b[1] += s1 * 0.5 * ih[1] * (U(m2, 1) + U(t, 1));
+  b[1] += s2 == 1 ? -0.5 * ih[0] * U(k, 2) : 0.5 * ih[0] * U(e2, 2);
+  eb_nb(m1, 2, 1, t);
+  b[1] += s2 * 0.5 * ih[0] * (U(m1, 2) + U(t, 2));
+  b[2] = 0;
+  b[2] += s1 == 1 ? ih[0] * U(k, 1) : -ih[0] * U(e1, 1);
+  b[2] += s2 == 1 ? ih[1] * U(k, 2) : -ih[1] * U(e2, 2);
+  b[2] += s3 == 1 ? ih[2] * U(k, 3) : -ih[2] * U(e3, 3);
+#undef U
+  if (!isnan(b[0]) && !isnan(b[1]) && !isnan(b[2])) {
+    mac_solve3(A, b, x);
+  } else {
+    x[0] = x[1] = x[2] = NAN;
+  }
+  eb_set(w, s1 == 1 ? e1 : k, 1, x[0]);
+  eb_set(w, s2 == 1 ? e2 : k, 2, x[1]);
+  eb_set(w, s3 == 1 ? e3 : k, 3, x[2]);
+}
+/* apply_nan_extrap (:183-251) */
+static void eb_nan_extrap(world_t* w, const int k[3]) {
+  int tab[2][6], n = 0;
+  for (int i = 1; i <= 3; ++i) {
+    int e[3];
+    eb_nb(k, i, 1, e);
+    if (isnan(eb_u(w, k, i))) { tab[0][n] = i; tab[1][n] = 0; ++n; }
+    if (isnan(eb_u(w, e, i))) { tab[0][n] = i; tab[1][n] = 1; ++n; }
+  }
+  if (n == 0) return;
+  for (int j = 0; j < n; ++j) {
+    const int d = tab[0][j];
+    int k2[3] = {k[0], k[1], k[2]};
+    if (tab[1][j] == 1) eb_nb(k, d, 1, k2);
+    double vt = 0;
+    int nb = 0;
+    for (int d2 = 1; d2 <= 3; ++d2)
+      for (int s = -1; s <= 1; ++s) {
+        int k3[3];
+        eb_nb(k2, d2, s, k3);
+        const double add = eb_u(w, k3, d);
+        if (!isnan(add)) {
+          vt += add;
+          ++nb;
+        }
+      }
+    if (nb != 0) vt /= nb;
+    eb_set(w, k2, d, vt);
+  }
+  double div = 0;
+  for (int i = 1; i <= 3; ++i) {
+    int e[3];
+    eb_nb(k, i, 1, e);
+    div += w->ih[i - 1] * (eb_u(w, e, i) - eb_u(w, k, i));
+  }
+  const double cor = div / n;
+  for (int j = 0; j < n; ++j) {
+    const int d = tab[0][j], sg = tab[1][j];
+    int k2[3] = {k[0], k[1], k[2]};
+    if (sg == 1) eb_nb(k, d, 1, k2);
+    eb_set(w, k2, d, eb_u(w, k2, d) - (2 * sg - 1) * w->h[d - 1] * cor);
+  }
+}
+static int eb_mod5(int v) { return ((v % 5) + 5) % 5; }
+static int eb_color(const int* k) { return eb_mod5(k[0]) + 5 * eb_mod5(k[1]) + 25 * eb_mod5(k[2]); }
+static int cmp_color_key(const void* a, const void* b) {
+  const int* x = (const int*)a;
+  const int* y = (const int*)b;
+  const int cx = eb_color(x), cy = eb_color(y);
+  if (cx != cy) return cx < cy ? -1 : 1;
+  for (int i = 2; i >= 0; --i)
+    if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+  return 0;
+}
+static int cmp_color_key_rev(const void* a, const void* b) {
+  const int cx = eb_color((const int*)a), cy = eb_color((const int*)b);
+  if (cx != cy) return cx < cy ? -1 : 1;
+  return -cmp_color_key(a, b);
+}
+static int cmp_key_zyx(const void* a, const void* b) {
+  const int* x = (const int*)a;
+  const int* y = (const int*)b;
+  for (int i = 2; i >= 0; --i)
+    if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+  return 0;
+}
+/* order 0: colour-major, keys ascending within a colour (the device's order);
+ * 1: key order (z, then y, then x), within one chunk the reference's own order
+ * (offsets x + 8y + 64z), which the tests use to compare with the reference
+ * run on single-chunk worlds; 2: colour-major, keys descending within a
+ * colour (the tests check that it changes nothing). */
+static void alg_extrap_bc(world_t* w, int order) {
+  /* the existing cells in colour-major order */
+  int64_t n = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o) n += w->b[bi]->exists[o] != 0;
+  int* keys = (int*)malloc(sizeof(int) * 3 * (size_t)(n ? n : 1));
+  int64_t m = 0;
+  for (int64_t bi = 0; bi < w->nb; ++bi)
+    for (int o = 0; o < 512; ++o)
+      if (w->b[bi]->exists[o]) key_of(w, bi, o, keys + 3 * m++);
+  qsort(keys, (size_t)n, 3 * sizeof(int), order == 1 ? cmp_key_zyx : (order == 2 ? cmp_color_key_rev : cmp_color_key));
+  for (int64_t i = 0; i < n; ++i) eb_set_nan(w, keys + 3 * i);
+  int* corners = (int*)malloc(sizeof(int) * 6 * (size_t)(n ? n : 1));
+  int64_t nc = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    int dir[6], sign[6], s[3];
+    const int nn = eb_boundary(w, keys + 3 * i, dir, sign);
+    if (nn == 0) continue;
+    if (nn == 3) {
+      if (eb_corner_signs(dir, sign, nn, s)) {
+        memcpy(corners + 6 * nc, keys + 3 * i, 3 * sizeof(int));
+        memcpy(corners + 6 * nc + 3, s, 3 * sizeof(int));
+        ++nc;
+      }
+      continue;
+    }
+    eb_choose(w, keys + 3 * i, dir, sign, nn);
+  }
+  for (int64_t i = nc - 1; i >= 0; --i)
+    eb_corner(w, corners + 6 * i, corners[6 * i + 3], corners[6 * i + 4], corners[6 * i + 5]);
+  for (int64_t i = 0; i < n; ++i) {
+    int dir[6], sign[6];
+    if (eb_boundary(w, keys + 3 * i, dir, sign)) eb_nan_extrap(w, keys + 3 * i);
+  }
+  free(corners);
+  free(keys);
+}
+
 static void alg_solid_to_const(world_t* w) {
   keylist s = {0};
   for (int64_t bi = 0; bi < w->nb; ++bi)
@@ -1473,6 +1820,12 @@ int mac_oracle_run(const char* in_path, const char* out_path, const char* cmd, i
       alg_project(w);
     } else if (!strcmp(cmd, "extrapolate")) {
       alg_extrapolate(w);
+    } else if (!strcmp(cmd, "extrapbc")) {
+      alg_extrap_bc(w, 0);
+    } else if (!strcmp(cmd, "extrapbckey")) {
+      alg_extrap_bc(w, 1);
+    } else if (!strcmp(cmd, "extrapbcrev")) {
+      alg_extrap_bc(w, 2);
     } else if (!strcmp(cmd, "move")) {
       alg_move(w, 1);
     } else if (!strcmp(cmd, "movelin")) {

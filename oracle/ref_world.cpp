@@ -126,6 +126,9 @@
 #include "Algorithms_Viscosity.h"
 #include "Algorithms_Solve_Pressure_Dirichlet.h"
 #include "Policy_Add_Particle_Cube.h"
+#include "Policy_Is_In_Domain_Speed.h"
+#include <cassert>  // src/Algorithm_Extrapolate_Boundary_Condition.h:193 uses assert without including it
+#include "Algorithm_Extrapolate_Boundary_Condition.h"
 #ifdef MAC_DEPTH
 #include "Data_CellType_Fluid_Air_Solid_Inflow_Interior_0_Pres.h"
 #include "Data_CellType_Domain_Fluid_Without_0_Pres.h"
@@ -152,6 +155,7 @@
 #include "mac_gpu/Mac_GPU.h"
 #endif
 
+#include "solve3.h"
 #include "state_format.h"
 
 using namespace std;
@@ -218,6 +222,27 @@ class Policy_Solve_Linear_OracleCG {
     }
     dump(n, off, ind, val, b, x);
   }
+};
+
+// Linear-solver policy for the 3x3 corner systems of the boundary-condition
+// extrapolation (the member functions of Policy_Solve_Linear_Umfpack, with its
+// type_linear_solver typedef): the CSC matrix as a dense row-major array, solved
+// by the checkers' shared Gaussian elimination (solve3.h).
+class Policy_Solve_Linear_Dense3 {
+  double m_a[9];
+
+ public:
+  typedef Policy_Solve_Linear_Dense3 type_linear_solver;
+  void Solve_Linear_FactorizeMatrice(int n, int* off, int* ind, double* val) {
+    for (int i = 0; i < 9; ++i) m_a[i] = 0.0;
+    if (n != 3) return;
+    for (int j = 0; j < 3; ++j)
+      for (int k = off[j]; k < off[j + 1]; ++k) m_a[3 * ind[k] + j] = val[k];
+  }
+  void Solve_Linear(int n, int*, int*, double*, double* b, double* x) {
+    if (n == 3) mac_solve3(m_a, b, x);
+  }
+  void Solve_Linear_Clean() {}
 };
 
 // Shared counter-based jitter (same function in the oracle and on the GPU).
@@ -483,6 +508,16 @@ static int run(int argc, char** argv) {
   type_alg_solid m_alg_solid(m_data_ref, m_pol_empty);
   typedef Algorithms_Extrapolate<type_data_ref, type_pol_empty> type_alg_extrapolate;
   type_alg_extrapolate m_alg_extrapolate(m_data_ref, m_pol_empty);
+  // Algorithm_Extrapolate_Boundary_Condition (3D form) with the policies of
+  // test/Lateral_jet_3.cpp:491-498 that it reads: Policy_Is_In_Domain_Speed
+  // and the linear solver (here the dense 3x3 policy above).
+  typedef Policy_Is_In_Domain_Speed<type_data_ref> type_pol_in_domain_speed;
+  type_pol_in_domain_speed m_pol_in_domain_speed;
+  Policy_Solve_Linear_Dense3 m_pol_dense3;
+  typedef Policies<type_pol_in_domain_speed, Policy_Solve_Linear_Dense3> type_pol_extrap_bc;
+  type_pol_extrap_bc m_pol_extrap_bc(m_pol_in_domain_speed, m_pol_dense3);
+  typedef Algorithm_Extrapolate_Boundary_Condition<type_data_ref, type_pol_extrap_bc> type_alg_extrap_bc;
+  type_alg_extrap_bc m_alg_extrap_bc(m_data_ref, m_pol_extrap_bc);
 
   typedef Policy_Layer_Max<type_data_ref> type_pol_layer;
   type_pol_layer m_pol_layer(st.hdr.layer_max);
@@ -690,6 +725,20 @@ static int run(int argc, char** argv) {
   type_pol_gpu m_pol_gpu(m_data_ref, gprm, g_refill_seed);
   Algorithms_Step_GPU<type_data_ref, type_pol_gpu> m_alg_step_gpu(m_data_ref, m_pol_gpu);
   Algorithms_To_Host_GPU<type_data_ref, type_pol_gpu> m_alg_to_host_gpu(m_data_ref, m_pol_gpu);
+
+  // The reference's own RK2-TVD and Algorithms_Do_Pressure with the device
+  // projection at the composable interface (Init_Iteration,
+  // Divergence_Projection, End_Iteration): the host loops over the speed
+  // buffers stay the reference's, only the projections run on the device.
+  type_pol_gpu m_pol_gpu_proj(m_data_ref, gprm, g_refill_seed);
+  typedef Algorithms_Solve_Pressure_GPU<type_data_ref, type_pol_gpu> type_alg_solve_pressure_dev;
+  type_alg_solve_pressure_dev m_alg_solve_pressure_dev(m_data_ref, m_pol_gpu_proj);
+  typedef Policies<type_alg_solve_grid, type_alg_solve_pressure_dev> type_pol_ODE_dev;
+  type_pol_ODE_dev m_pol_ODE_dev(m_alg_solve_grid, m_alg_solve_pressure_dev);
+  typedef Algorithms_RungeKutta_RK2_TVD<type_data_ref, type_pol_ODE_dev> type_alg_ODE_dev;
+  type_alg_ODE_dev m_alg_ODE_dev(m_data_ref, m_pol_ODE_dev);
+  typedef Algorithms_Do_Pressure<type_data_ref, type_alg_solve_pressure_dev> type_alg_do_pressure_dev;
+  type_alg_do_pressure_dev m_alg_do_pressure_dev(m_data_ref, m_alg_solve_pressure_dev);
 #endif
 
   // The reference algorithms print timing lines on std::cout; keep them out of the way.
@@ -733,6 +782,9 @@ static int run(int argc, char** argv) {
       m_alg_do_pressure.Do();
     } else if (cmd == "extrapolate") {
       m_alg_extrapolate.Do();
+    } else if (cmd == "extrapbc") {
+      type_chunk_speed::ispeed = 0;
+      m_alg_extrap_bc.Do();
     } else if (cmd == "move") {
       m_alg_move.Do();
     } else if (cmd == "movelin") {
@@ -741,6 +793,21 @@ static int run(int argc, char** argv) {
     } else if (cmd == "gpuproject") {
       type_chunk_speed::ispeed = 0;
       m_alg_do_pressure_gpu.Do();
+    } else if (cmd == "gpuode") {
+      m_alg_ODE_dev.Do();
+      if (m_pol_gpu_proj.Session().Status() != MAC_OK) {
+        std::cout.rdbuf(saved);
+        fprintf(stderr, "device projection failed: %s\n", mac_error_string(m_pol_gpu_proj.Session().Status()));
+        return 1;
+      }
+    } else if (cmd == "gpudopressure") {
+      type_chunk_speed::ispeed = 0;
+      m_alg_do_pressure_dev.Do();
+      if (m_pol_gpu_proj.Session().Status() != MAC_OK) {
+        std::cout.rdbuf(saved);
+        fprintf(stderr, "device projection failed: %s\n", mac_error_string(m_pol_gpu_proj.Session().Status()));
+        return 1;
+      }
     } else if (cmd == "gpustep") {
       m_alg_step_gpu.Do();
       if (r + 1 == nrep) {

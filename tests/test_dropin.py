@@ -2,7 +2,9 @@
 world: oracle/_ref/mac_ref_gpu composes the unmodified reference headers and
 swaps in (a) Policy_Solve_Linear_GPU as the solver policy of the reference's
 Algorithms_Solve_Pressure, (b) Algorithms_Step_GPU + Algorithms_To_Host_GPU for
-the pipeline-A step. oracle/_ref/mac_ref_b_gpu is the depth world of
+the pipeline-A step, (c) Algorithms_Solve_Pressure_GPU as the projection the
+reference's own RK2-TVD and Algorithms_Do_Pressure call through
+Init_Iteration / Divergence_Projection / End_Iteration. oracle/_ref/mac_ref_b_gpu is the depth world of
 test/Jet3.cpp (interior cells, depth chunk, three speed buffers) whose
 Algorithms_Step_GPU runs pipeline B: the session carries the interior material
 and the depths across. Results are compared with the reference's own outputs
@@ -45,6 +47,26 @@ def _run(cmd, state, tmp_path, n=None, rtol="1e-13", binary=BIN):
 
 def test_reference_projection_with_device_solver_policy(golden, tmp_path):
     got = _run("gpuproject", golden("c1_ref_t30"), tmp_path, rtol="1e-14")
+    ref = golden("c1_ref_t30_project")
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("p", "u0x", "u0y", "u0z"))
+    assert e["p"] <= P_TOL and max(e["u0x"], e["u0y"], e["u0z"]) <= U_TOL, e
+
+
+def test_reference_rk2tvd_with_device_projection(golden, tmp_path):
+    """The reference's own Algorithms_RungeKutta_RK2_TVD (host loops over the
+    speed buffers, Init_Iteration / Divergence_Projection / End_Iteration
+    through Policy::) composed with Algorithms_Solve_Pressure_GPU."""
+    got = _run("gpuode", golden("c1_ref_t30"), tmp_path, rtol="1e-14")
+    ref = golden("c1_ref_t30_ode")
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("p", "u0x", "u0y", "u0z", "u1x", "u1y", "u1z"))
+    assert e["p"] <= P_TOL, e
+    assert max(e[k] for k in ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z")) <= U_TOL, e
+
+
+def test_reference_do_pressure_with_device_projection(golden, tmp_path):
+    got = _run("gpudopressure", golden("c1_ref_t30"), tmp_path, rtol="1e-14")
     ref = golden("c1_ref_t30_project")
     compare_topology(got, ref)
     e = field_errors(got, ref, ("p", "u0x", "u0y", "u0z"))

@@ -139,3 +139,69 @@ def test_first_init_matches_reference(golden):
     compare_topology(got, ref)
     _exact(got, ref, ("u0x", "u0y", "u0z", "p"))
     assert compare_particles(got, ref) == 0.0
+
+
+def test_composable_projection_in_a_host_rk2tvd(golden):
+    """Algorithms_RungeKutta_RK2_TVD (src/Algorithms_RungeKutta_RK2_TVD.h:20-66)
+    with its speed-buffer loops on the host and the projections at the
+    composable interface on the device (mac_pressure_init, then
+    mac_pressure_divergence_projection per stage, then mac_pressure_end), the
+    fields moved with mac_upload_field / mac_download_field: matches the
+    reference's own RK2-TVD output."""
+    t30 = golden("c1_ref_t30")
+    ref = golden("c1_ref_t30_ode")
+    with _ctx(t30) as ctx:
+        ctx.upload(t30)
+        dt = t30.params.dt
+        flags = ctx.download().flags.reshape(-1)
+        ctx.pressure_init()
+        ctx.forces(0)  # acc = 0, gravity + convection on speed 0
+        acc = {a: ctx.download_field("a" + a) for a in "xyz"}
+        u0 = {a: ctx.download_field("u0" + a) for a in "xyz"}
+        for a in "xyz":  # stage 1 (forced): u1 = u0 + acc dt
+            ctx.upload_field("u1" + a, u0[a] + acc[a] * dt)
+        ctx.divergence_projection(1)
+        ctx.forces(1)
+        acc = {a: ctx.download_field("a" + a) for a in "xyz"}
+        u1 = {a: ctx.download_field("u1" + a) for a in "xyz"}
+        for i, a in enumerate("xyz"):  # stage 2 (non-forced: const faces keep u0)
+            new = 0.5 * u0[a] + 0.5 * u1[a] + 0.5 * acc[a] * dt
+            const = (flags & (1 << i)) != 0
+            ctx.upload_field("u0" + a, np.where(const, u0[a], new))
+        ctx.divergence_projection(0)
+        ctx.pressure_end()
+        got = ctx.download()
+    compare_topology(got, ref)
+    e = field_errors(got, ref, ("p", "u0x", "u0y", "u0z", "u1x", "u1y", "u1z"))
+    assert e["p"] <= P_TOL, e
+    assert max(e[k] for k in ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z")) <= U_TOL, e
+
+
+def test_divergence_projection_needs_an_init(golden):
+    from mac_b200.gpu import MacError
+    t30 = golden("c1_ref_t30")
+    with _ctx(t30) as ctx:
+        ctx.upload(t30)
+        with pytest.raises(MacError):
+            ctx.divergence_projection(0)
+
+
+def test_stage_buffers_can_be_left_out_of_the_transfers(golden):
+    """NULL speed-1 and acceleration pointers in mac_host_state: the step
+    writes both before reading them, so a world uploaded without them steps to
+    the same speed 0, pressure, topology and particles bit for bit."""
+    from mac_b200.gpu import HostState
+    s30 = golden("c1_ref_s30")
+    with _ctx(s30) as ctx:
+        ctx.upload(s30)
+        ctx.step()
+        want = ctx.download()
+    lean = HostState(s30.nbricks + 64, s30.nparticles + 4096, stage_buffers=False).fill(s30)
+    with _ctx(s30) as ctx:
+        ctx.upload(None, lean)
+        ctx.step()
+        ctx.download(lean, to_state=False)
+        got = lean.to_state(s30.params)
+    compare_topology(got, want)
+    _exact(got, want, ("u0x", "u0y", "u0z", "p"))
+    assert compare_particles(got, want) == 0.0
