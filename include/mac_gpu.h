@@ -283,6 +283,11 @@ int mac_unet_adam_step(void* net, const float* grad, float lr);
  * each solved by plain FP64 CG for niter iterations from 0; pairs at iterations
  * 1, 2, 4, ... (nsnap). stats[0]: worst final relative residual, stats[1]: tscale. */
 int mac_unet_make_dataset(void* net, int nmasks, int size, int nsnap, int niter, uint64_t seed, double* stats);
+/* The same with the first nmasks_given masks supplied by the caller (host,
+ * nmasks_given x size^3 int8: 1 fluid, 0 air or missing, -1 solid), e.g. patches
+ * of jet states; the remaining nmasks - nmasks_given are random as above. */
+int mac_unet_make_dataset_ext(void* net, int nmasks, int size, int nsnap, int niter, uint64_t seed,
+                              const int8_t* masks, int nmasks_given, double* stats);
 int mac_unet_get_sample(void* net, int index, float* r, float* e, int8_t* mask);
 /* steps Adam steps on random batches of the training set; losses[steps] (may be NULL). */
 int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, float* losses);

@@ -1221,8 +1221,10 @@ static void adam(Net& t, float lr, cudaStream_t st) {
 // x_final - x_k at iterations k = 1, 2, 4, ... (nsnap of them) are kept.
 // Sample index = snapshot * nmasks + mask. stats: [0] largest final relative
 // residual, [1] target scale.
+// The first next masks come from ext (next x s^3 host bytes: 1 fluid, 0 air
+// or missing, -1 solid), the rest are random pools with spheres.
 static int make_dataset(Net& t, int nmasks, int s, int nsnap, int niter, uint64_t seed, double* stats,
-                        cudaStream_t st) {
+                        cudaStream_t st, const int8_t* ext = nullptr, int next = 0) {
   if (nmasks < 1 || s < 8 || s % 4 || nsnap < 1 || nsnap > 16 || niter < (1 << (nsnap - 1))) return MAC_ERR_INVALID;
   const size_t V1 = (size_t)s * s * s;
   const size_t S = (size_t)nmasks * nsnap;
@@ -1267,6 +1269,8 @@ static int make_dataset(Net& t, int nmasks, int s, int nsnap, int niter, uint64_
     const dim3 g(g1.x, nb);
     double *rr = sc, *rrn = sc + MB, *pq = sc + 2 * MB, *rr0 = sc + 3 * MB;
     k_mask_gen<<<g, 256, 0, st>>>(m, sph, nsph, s, (float)(0.4 * s));
+    for (int b = 0; b < nb; ++b)
+      if (m0 + b < next) cudaMemcpyAsync(m + (size_t)b * V1, ext + (size_t)(m0 + b) * V1, V1, cudaMemcpyHostToDevice, st);
     k_rhs_gen<<<g, 256, 0, st>>>(m, r, s, seed, (uint64_t)m0);
     cudaMemsetAsync(x, 0, nb * V1 * 8, st);
     cudaMemcpyAsync(p, r, nb * V1 * 8, cudaMemcpyDeviceToDevice, st);
@@ -1467,6 +1471,14 @@ int mac_unet_make_dataset(void* net, int nmasks, int size, int nsnap, int niter,
   if (!t) return MAC_ERR_INVALID;
   cudaSetDevice(t->device);
   return mac::unet::make_dataset(*t, nmasks, size, nsnap, niter, seed, stats, 0);
+}
+
+int mac_unet_make_dataset_ext(void* net, int nmasks, int size, int nsnap, int niter, uint64_t seed,
+                              const int8_t* masks, int nmasks_given, double* stats) {
+  Net* t = (Net*)net;
+  if (!t || nmasks_given < 0 || nmasks_given > nmasks || (nmasks_given > 0 && !masks)) return MAC_ERR_INVALID;
+  cudaSetDevice(t->device);
+  return mac::unet::make_dataset(*t, nmasks, size, nsnap, niter, seed, stats, 0, masks, nmasks_given);
 }
 
 int mac_unet_get_sample(void* net, int index, float* r, float* e, int8_t* mask) {

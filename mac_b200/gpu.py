@@ -68,7 +68,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_csc_factorize", "mac_csc_solve", "mac_csc_clean", "mac_csc_solve_noalloc",
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
-           "mac_unet_make_dataset", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
+           "mac_unet_make_dataset", "mac_unet_make_dataset_ext", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
            "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_unet_set_loss", "mac_unet_time_forward"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
@@ -129,6 +129,8 @@ def load(path: str = LIB_PATH):
                                        _P(f32)]
     lib.mac_unet_adam_step.argtypes = [vp, _P(f32), f32]
     lib.mac_unet_make_dataset.argtypes = [vp, i32, i32, i32, i32, ctypes.c_uint64, _P(f64)]
+    lib.mac_unet_make_dataset_ext.argtypes = [vp, i32, i32, i32, i32, ctypes.c_uint64, _P(ctypes.c_int8), i32,
+                                              _P(f64)]
     lib.mac_unet_get_sample.argtypes = [vp, i32, _P(f32), _P(f32), _P(ctypes.c_int8)]
     lib.mac_unet_train.argtypes = [vp, i32, i32, f32, ctypes.c_uint64, _P(f32)]
     lib.mac_unet_launch_count.argtypes = [vp, _P(i64)]

@@ -5,10 +5,14 @@
 
 Training pairs (residual, exact error) come from plain FP64 CG iterates on
 random fluid masks (a pool z < 0.4 size plus 12 spheres of radius 3..10 cells
-at size 64, solid box), generated on the device by mac_unet_make_dataset; the
-network is trained with Adam by the device's own forward and backward kernels
-(mac_unet_train). The saved file holds the FP32 parameters, the output scale
-and the loss curve; mac_b200.unet.UNet.load reads it back.
+at size 64, solid box) and on size^3 patches of jet states (--jet-masks: the
+32x32x64 jet every 5 steps of its first 100 from the first init, and
+patches centred on the free surface of the 256x256x512 jet after its first
+init and 10 steps, both stepped on the device), generated on the device by
+mac_unet_make_dataset[_ext]; the network is trained with Adam by the device's
+own forward and backward kernels (mac_unet_train). The saved file holds the
+FP32 parameters, the output scale and the loss curve; mac_b200.unet.UNet.load
+reads it back.
 """
 import argparse
 import json
@@ -17,10 +21,72 @@ import time
 
 import numpy as np
 
+from .state import FLUID_TYPES, SOLID
 from .unet import UNet
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "weights", "unet_pool64.npz")
+
+
+def state_mask(s, origin, size):
+    """The network's mask of the size^3 box at origin (cell keys): 1 fluid,
+    -1 solid, 0 air or no cell."""
+    ex = s.exists.astype(bool)
+    k = s.cell_keys()[ex] - np.asarray(origin)
+    t = s.type[ex]
+    inside = np.all((k >= 0) & (k < size), axis=1)
+    m = np.zeros((size, size, size), np.int8)
+    k, t = k[inside], t[inside]
+    val = np.where(np.isin(t, FLUID_TYPES), 1, np.where(t == SOLID, -1, 0)).astype(np.int8)
+    m[k[:, 2], k[:, 1], k[:, 0]] = val  # [z][y][x], x fastest
+    return m
+
+
+def surface_cells(s):
+    """Keys of fluid cells with a face neighbour that is not fluid."""
+    ex = s.exists.astype(bool)
+    keys = s.cell_keys()[ex]
+    lo = keys.min(axis=0) - 1
+    dims = keys.max(axis=0) - lo + 2
+    fl = np.zeros(dims[::-1], bool)
+    k = keys - lo
+    f = np.isin(s.type[ex], FLUID_TYPES)
+    fl[k[f, 2], k[f, 1], k[f, 0]] = True
+    inner = fl.copy()
+    for ax in range(3):
+        for d in (-1, 1):
+            inner &= np.roll(fl, d, axis=ax)
+    z, y, x = np.nonzero(fl & ~inner)
+    return np.stack([x, y, z], axis=1) + lo
+
+
+def jet_masks(n_big, size, device=0, seed=7):
+    """Patches of jet states for the training set (module docstring)."""
+    from .gpu import Context
+    from .state import jet_world
+    from .world import first_init
+    rng = np.random.default_rng(seed)
+    out = []
+    s = jet_world(32, 32, 64, h=0.05, r_inflow=4.0, w_inflow=1.0, seed=seed)
+    with Context(s.params, max_bricks=4096, max_particles=1 << 21, solver="mixed", rtol=1e-8, device=device) as ctx:
+        first_init(ctx, s)
+        for k in range(1, 101):
+            ctx.step()
+            if k % 5 == 0:
+                st = ctx.download()
+                out.append(state_mask(st, (-1 - (size - 34) // 2, -1 - (size - 34) // 2, -1), size))
+    s = jet_world(256, 256, 512, h=0.01, r_inflow=24.0, w_inflow=2.0, pool_depth=122, dt_max=0.01, seed=seed)
+    with Context(s.params, max_bricks=40000, max_particles=80_000_000, solver="mixed", rtol=1e-8,
+                 device=device) as ctx:
+        first_init(ctx, s)
+        del s
+        for _ in range(10):
+            ctx.step()
+        st = ctx.download()
+    surf = surface_cells(st)
+    for c in surf[rng.choice(len(surf), n_big, replace=False)]:
+        out.append(state_mask(st, c - size // 2, size))
+    return np.stack(out)
 
 
 def main():
@@ -36,11 +102,16 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--jet-masks", type=int, default=180,
+                    help="surface patches of the 256x256x512 jet added to the random masks (plus 20 of the "
+                         "32x32x64 jet); 0 for random masks only")
     a = ap.parse_args()
+    masks = jet_masks(a.jet_masks, a.size, a.device) if a.jet_masks > 0 else None
+    njet = 0 if masks is None else len(masks)
     with UNet(a.device, seed=a.seed) as net:
         net.set_loss(a.loss)
         t0 = time.perf_counter()
-        info = net.make_dataset(a.masks, a.size, a.snapshots, a.cg_iters, seed=1000 + a.seed)
+        info = net.make_dataset(a.masks + njet, a.size, a.snapshots, a.cg_iters, seed=1000 + a.seed, masks=masks)
         t_data = time.perf_counter() - t0
         print(f"training set: {info['samples']} pairs in {t_data:.1f}s, worst CG relres {info['worst_relres']:.1e}, "
               f"output scale {info['tscale']:.4g}", flush=True)
@@ -55,7 +126,8 @@ def main():
         losses = np.concatenate(losses)
         p, tscale = net.params()
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-        meta = {"masks": a.masks, "size": a.size, "snapshots": a.snapshots, "cg_iters": a.cg_iters, "steps": a.steps,
+        meta = {"masks": a.masks, "jet_masks": njet, "size": a.size, "snapshots": a.snapshots,
+                "cg_iters": a.cg_iters, "steps": a.steps,
                 "batch": a.batch, "lr": a.lr, "loss": a.loss, "seed": a.seed, "train_seconds": t_train,
                 "ms_per_step": 1e3 * t_train / a.steps, "dataset_seconds": t_data}
         np.savez_compressed(a.out, params=p, tscale=np.float32(tscale),

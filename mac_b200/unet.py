@@ -82,10 +82,18 @@ class UNet:
         self._check(self.lib.mac_unet_adam_step(self.h, g.ctypes.data_as(_P(ctypes.c_float)), float(lr)),
                     "mac_unet_adam_step")
 
-    def make_dataset(self, nmasks, size=64, nsnap=8, niter=1000, seed=1000):
+    def make_dataset(self, nmasks, size=64, nsnap=8, niter=1000, seed=1000, masks=None):
+        """nmasks masks of size^3: the given ones first (int8 [k][size][size][size]:
+        1 fluid, 0 air, -1 solid), random pools with spheres for the rest."""
         st = (ctypes.c_double * 2)()
-        self._check(self.lib.mac_unet_make_dataset(self.h, nmasks, size, nsnap, niter, seed, st),
-                    "mac_unet_make_dataset")
+        if masks is None:
+            self._check(self.lib.mac_unet_make_dataset(self.h, nmasks, size, nsnap, niter, seed, st),
+                        "mac_unet_make_dataset")
+        else:
+            m = np.ascontiguousarray(masks, dtype=np.int8).reshape(-1, size, size, size)
+            self._check(self.lib.mac_unet_make_dataset_ext(self.h, nmasks, size, nsnap, niter, seed,
+                                                           m.ctypes.data_as(_P(ctypes.c_int8)), len(m), st),
+                        "mac_unet_make_dataset_ext")
         self.size = size
         return {"worst_relres": st[0], "tscale": st[1], "samples": nmasks * nsnap}
 
