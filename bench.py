@@ -180,7 +180,7 @@ def reduce_over_ranks(seconds: float, count: float, device) -> tuple:
 
 
 # ------------------------------------------------------------- our arm
-def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8, cg_iterations=0):
+def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8, cg_iterations=0, sweeps0=2):
     """Achieved GB/s per phase from algorithmic bytes (every array element a
     kernel must touch, read or written once) over the measured event times.
     A "launch" is one timed region of the phase (one particle move, one SpMV),
@@ -193,7 +193,9 @@ def roofline_models(ctx_stats, prof, np_count, n_exist, mg_bytes=8, cg_iteration
     # restriction 8 B and prolongation 16 B at FP64 (117 B), the levels adding
     # up to 8/7 of the finest; FP32 storage halves it. The update: x, p, r, q
     # read, x, r written, 48 B at FP64.
-    vc = 117.0 * 8.0 / 7.0 * (mg_bytes / 8.0)
+    # With one sweep on the finest level its pre- and post-sweep count once each:
+    # (2 x 17 + 49) B there, the coarser levels (1/7 of 117 B) unchanged.
+    vc = ((4.0 * 17.0 + 49.0) * 8.0 / 7.0 if sweeps0 == 2 else 2.0 * 17.0 + 49.0 + 117.0 / 7.0) * (mg_bytes / 8.0)
     models = {
         # phase: (bytes per launch, description, launches or None for the region count)
         "move": (48.0 * np_count, "48 B per particle (read + write 3 FP64 positions)", None),
@@ -227,7 +229,7 @@ def _peaks():
         return {}
 
 
-def poisson_solves(dev, mg_sweeps=2, reps=3):
+def poisson_solves(dev, mg_sweeps=2, prefetch=True, reps=3):
     """Standalone pressure solve of the 128^3 pool + 12 spheres world (solid box,
     face speeds uniform in [-1, 1]) to a relative residual of 1e-10: device time
     of one projection and of its solve (system set-up + CG iterations), per
@@ -256,7 +258,7 @@ def poisson_solves(dev, mg_sweeps=2, reps=3):
     for name, solver, rtol in forms:
         with Context(s.params, max_bricks=8192, max_particles=1024, solver=solver, rtol=rtol, max_iters=1000,
                      device=dev) as ctx:
-            ctx.set_multigrid(mg_sweeps)
+            ctx.set_multigrid(mg_sweeps, prefetch)
             if net is not None:
                 ctx.set_preconditioner(net)
             stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
@@ -327,7 +329,7 @@ def solver_forms(args, dev, params, host, wl, steps=5, warmup=2):
     for form in forms:
         with Context(params, max_bricks=wl[8], max_particles=wl[9], solver=form, rtol=1e-8, max_iters=1000,
                      device=dev, div_check=True) as ctx:
-            ctx.set_multigrid(args.mg_sweeps)
+            ctx.set_multigrid(args.mg_sweeps, not args.no_prefetch)
             if form.startswith("learned"):
                 ctx.set_preconditioner(net)
             ctx.upload(None, host)
@@ -378,7 +380,7 @@ def run_ours(args, rank, world, local_rank):
     log(f"[rank {rank}] world built in {time.perf_counter() - t0:.1f}s: {s.nbricks} bricks, {s.nparticles} particles")
     ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
                   device=dev, div_check=True, warm_start=args.warm_start)
-    ctx.set_multigrid(args.mg_sweeps)
+    ctx.set_multigrid(args.mg_sweeps, not args.no_prefetch)
     if args.solver.startswith("learned"):
         from mac_b200.unet import UNet
         net_main = UNet(dev)
@@ -461,7 +463,8 @@ def run_ours(args, rank, world, local_rank):
                      "buffer 1 and the acceleration, RK2-TVD's stage buffers, left out)"}
 
     n_exist = int(st["live_bricks"] * 512)  # upper bound of existing cells (slots of live bricks)
-    rl = roofline_models(st, prof, st["particles"], n_exist, 4 if args.solver == "mixed" else 8, cg_iterations)
+    rl = roofline_models(st, prof, st["particles"], n_exist, 4 if args.solver == "mixed" else 8, cg_iterations,
+                         args.mg_sweeps)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -491,6 +494,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"jet {wl[0]}x{wl[1]}x{wl[2]} h={wl[3]} inflow r={wl[4]:g} w={wl[5]}, pool depth "
                                f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
                    "solver": SOLVER_NAMES[args.solver], "mg_sweeps0": args.mg_sweeps,
+                   "mg_prefetch": not args.no_prefetch,
                    "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
@@ -506,7 +510,7 @@ def run_ours(args, rank, world, local_rank):
         out["solver_forms"] = solver_forms(args, dev, params, host, wl)
     del host
     if rank == 0 and not args.no_poisson:
-        out["poisson"] = poisson_solves(dev, args.mg_sweeps)
+        out["poisson"] = poisson_solves(dev, args.mg_sweeps, not args.no_prefetch)
     return out
 
 
@@ -525,6 +529,8 @@ def main():
     ap.add_argument("--mg-sweeps", type=int, choices=[1, 2], default=2,
                     help="Jacobi sweeps before and after the coarse correction on the finest multigrid level")
     ap.add_argument("--no-forms", action="store_true", help="skip stepping the jet with every solver form")
+    ap.add_argument("--no-prefetch", action="store_true",
+                    help="run the V-cycle's first kernel one block per brick instead of prefetching bricks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

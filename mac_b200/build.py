@@ -7,7 +7,9 @@ the translation units whose results are compared with the reference bit for
 bit or hold the projection's FP64 arithmetic (topology, forces, extrapolation,
 particles, the step, the pressure system); the multigrid preconditioner and
 the network (CONTRACT_OK) only shape the CG iterates, whose FP64 residual
-decides convergence, and are built with contraction on.
+decides convergence, and are built with contraction on (the multigrid's first
+kernel also applies the CG update x += alpha p, r -= alpha q, which then
+rounds once per element instead of twice).
 """
 from __future__ import annotations
 

@@ -318,6 +318,7 @@ int read_scalars(Ctx* c) {
   c->stats.particles = c->hs->np;
   if (c->hs->err) {
     if (c->hs->err & (kErrBricks | kErrParticles | kErrHash | kErrPending)) return MAC_ERR_CAPACITY;
+    if (c->hs->err & kErrTimeout) return MAC_ERR_TIMEOUT;
     return MAC_ERR_INVALID;
   }
   return MAC_OK;

@@ -39,6 +39,7 @@ enum ErrBits : int {
   kErrParticles = 2,
   kErrHash = 4,
   kErrPending = 8,
+  kErrTimeout = 16,  // a bounded wait on an asynchronous copy ran out
 };
 
 // Field indices of the FP64 per-cell block.
@@ -184,6 +185,9 @@ struct Ctx {
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
   int mg_sweeps0 = 2;         // Jacobi sweeps before and after the coarse correction at level 0 (1 or 2)
+  int mg_bulk = 1;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
+  int bulk_grid = 0;          // its grid (blocks resident on all SMs at once)
+  int npart_head = 0;         // partial sums the V-cycle's first kernel left (its grid)
   // learned preconditioner (flexible CG): the network and the previous z
   void* unet = nullptr;
   double* zold = nullptr;

@@ -392,6 +392,204 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
   block_sum<kBT>(rz, 0.0, partial);
 }
 
+// ---- the V-cycle's first kernel with the bricks prefetched asynchronously.
+// A block walks the domain bricks j = blockIdx.x, blockIdx.x + G, ... (G
+// blocks resident on all SMs at once). While it works on one brick, one
+// thread has the next brick's CG vectors r, q, x, p (4 KB each, FP64) and its
+// face classes (1 KB) in flight into the other half of a two-stage shared
+// buffer: five cp.async.bulk copies completing on the stage's mbarrier. The
+// face halos are read with plain loads. The arithmetic is k0_pre's (two
+// sweeps, RESTRICT = false) or k0_pre_restrict's (one sweep with the residual
+// restricted to level 1, RESTRICT = true), value for value; only the block
+// partials of r.r sum several bricks. Every wait is bounded: a wait that runs
+// out sets kErrTimeout, waits once more for the copies in flight and returns.
+namespace bulk {
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+// global -> shared, 16-byte aligned addresses, size a multiple of 16
+__device__ __forceinline__ void copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   saddr(dst)),
+               "l"(src), "r"(bytes), "r"(saddr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool wait(uint64_t* bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 20); ++i)
+    if (try_wait(bar, parity)) return true;
+  return false;
+}
+}  // namespace bulk
+
+constexpr int kBulkVec = kCells * 8;                   // one FP64 vector of a brick
+constexpr int kBulkStage = 4 * kBulkVec + kCells * 2;  // r, q, x, p and the face classes
+
+template <class T>
+constexpr int bulk_smem() {
+  return 2 * kBulkStage + kS1 * (int)sizeof(T) + kCells * (int)sizeof(T);
+}
+
+template <class T, bool RESTRICT>
+__global__ void __launch_bounds__(kBT) k0_head_bulk(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ rin,
+                                                    double* __restrict__ rout, double* __restrict__ x,
+                                                    const double* __restrict__ p, const double* __restrict__ q,
+                                                    double* partial, Scalars* ds, int update, T* __restrict__ e,
+                                                    T* __restrict__ r1, Params P) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ int64_t sb[6];
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ int failed;
+  if (solve_done(&ds->done)) return;
+  T* sr = reinterpret_cast<T*>(smem + 2 * kBulkStage);  // w D^-1 r (brick and face halo)
+  T* res = sr + kS1;                                     // RESTRICT: the brick's residual
+  const int tid = threadIdx.x;
+  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const double al = update ? ds->alpha : 0.0;
+  const uint32_t bytes = update ? (uint32_t)kBulkStage : (uint32_t)(kBulkVec + kCells * 2);
+  auto issue = [&](int j, int st) {
+    const int64_t base = (int64_t)dbl[j] * kCells;
+    uint8_t* s = smem + st * kBulkStage;
+    bulk::expect_tx(&full[st], bytes);
+    bulk::copy(s, rin + base, kBulkVec, &full[st]);
+    if (update) {
+      bulk::copy(s + kBulkVec, q + base, kBulkVec, &full[st]);
+      bulk::copy(s + 2 * kBulkVec, x + base, kBulkVec, &full[st]);
+      bulk::copy(s + 3 * kBulkVec, p + base, kBulkVec, &full[st]);
+    }
+    bulk::copy(s + 4 * kBulkVec, fmask + base, kCells * 2, &full[st]);
+  };
+  if (tid == 0) {
+    bulk::mbar_init(&full[0]);
+    bulk::mbar_init(&full[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    failed = 0;
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < nd) issue(blockIdx.x, 0);
+  double rr = 0;
+  int it = 0;
+  bool next_issued = false;  // a copy into the other stage is in flight
+  for (int j = blockIdx.x; j < nd; j += gridDim.x, ++it) {
+    const int st = it & 1;
+    const int b = dbl[j];
+    load_face_bases(nbr, b, sb);
+    next_issued = j + (int)gridDim.x < nd;
+    if (tid == 0 && next_issued) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(j + gridDim.x, st ^ 1);
+    }
+    __syncthreads();
+    // the face halos with plain loads, all in flight before any store
+    stage_h1_halo(sr, sb, [&](int64_t i) {
+      const double v = update ? rin[i] - al * q[i] : rin[i];
+      return om * (T)P.dtab[active_index(fmask[i])] * (T)v;
+    });
+    if (!bulk::wait(&full[st], (uint32_t)((it >> 1) & 1))) {
+      atomicOr(&ds->err, kErrTimeout);
+      failed = 1;
+    }
+    __syncthreads();
+    if (failed) break;
+    const double* sR = reinterpret_cast<const double*>(smem + st * kBulkStage);
+    const double* sQ = sR + kCells;
+    const double* sX = sR + 2 * kCells;
+    const double* sP = sR + 3 * kCells;
+    const uint16_t* sM = reinterpret_cast<const uint16_t*>(sR + 4 * kCells);
+    double rv[kCPT];
+    uint16_t mk[kCPT];
+#pragma unroll
+    for (int k = 0; k < kCPT; ++k) {
+      const int o = tid + kBT * k;
+      const int64_t c = (int64_t)b * kCells + o;
+      double v = sR[o];
+      if (update) {
+        v = v - al * sQ[o];
+        rout[c] = v;
+        x[c] = sX[o] + al * sP[o];
+        rr += v * v;
+      }
+      rv[k] = v;
+      const uint16_t m = sM[o];
+      mk[k] = m;
+      sr[s1_of(o)] = om * (T)P.dtab[active_index(m)] * (T)v;
+    }
+    __syncthreads();
+    if (RESTRICT) {
+#pragma unroll
+      for (int k = 0; k < kCPT; ++k) {
+        const int o = tid + kBT * k;
+        const uint16_t m = mk[k];
+        T v = 0;
+        if (m & kDomainBit) {
+          const int si = s1_of(o);
+          const T ec = sr[si];
+          T me = 0;
+#pragma unroll
+          for (int f = 0; f < 6; ++f) {
+            if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
+            if (m & (1u << f)) me -= ih2[f >> 1] * sr[si + s1_off(f)];
+          }
+          v = (T)rv[k] - me;
+        }
+        res[o] = v;
+      }
+      __syncthreads();
+      if (tid < 64) {
+        const int X = tid & 3, Y = (tid >> 2) & 3, Z = tid >> 4;
+        const int base = 2 * X + 16 * Y + 128 * Z;
+        r1[(size_t)b * 64 + tid] = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] +
+                                   res[base + 65] + res[base + 72] + res[base + 73];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kCPT; ++k) {
+        const int o = tid + kBT * k;
+        const int64_t c = (int64_t)b * kCells + o;
+        const uint16_t m = mk[k];
+        T out = 0;
+        if (m & kDomainBit) {
+          const int si = s1_of(o);
+          const T dinv = (T)P.dtab[active_index(m)];
+          T s = (T)(2.0 - kOmega) * (T)rv[k];
+#pragma unroll
+          for (int f = 0; f < 6; ++f)
+            if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
+          out = om * dinv * s;
+        }
+        e[c] = out;
+      }
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    // the copies of this brick and of the next may still be in flight: wait
+    // for them (bounded) before the block's shared memory is given up
+    const int st = it & 1;
+    if (tid == 0) {
+      bulk::wait(&full[st], (uint32_t)((it >> 1) & 1));
+      if (next_issued) bulk::wait(&full[st ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+    }
+    return;
+  }
+  if (update) block_sum<kBT>(rr, 0.0, partial);
+}
+
 // ------------------------------------------------------- levels 1, 2 (bricks)
 template <int D>
 __device__ inline int64_t lidx(const int* __restrict__ nbr, int b, int x, int y, int z) {
@@ -1251,7 +1449,18 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   // down (with update: finish the previous CG iteration into r2, which becomes r)
   const bool one = c->mg_sweeps0 == 1;
   if (part & 1) {
-    if (one) {
+    c->npart_head = nd;
+    if (c->mg_bulk && c->bulk_grid > 0) {
+      const int g = nd < c->bulk_grid ? nd : c->bulk_grid;
+      c->npart_head = g;
+      if (one)
+        k0_head_bulk<T, true><<<g, kBT, bulk_smem<T>(), st>>>(c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd,
+                                                             c->q, c->partial, c->ds, update, e0, r1, c->dp);
+      else
+        k0_head_bulk<T, false><<<g, kBT, bulk_smem<T>(), st>>>(c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x,
+                                                              c->pd, c->q, c->partial, c->ds, update, e0, r1, c->dp);
+      MAC_COUNT(c);
+    } else if (one) {
       k0_pre_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
                                              c->ds, update, r1, c->dp); MAC_COUNT(c);
     } else {
@@ -1326,6 +1535,17 @@ int mg_configure(Ctx* c) {
   c->smem_optin = dyn64 < dyn32 ? dyn64 : dyn32;
   rc = check(cudaFuncSetAttribute(kd_coarse_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn64));
   if (!rc) rc = check(cudaFuncSetAttribute(kd_coarse_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn32));
+  // the prefetching first kernel: as many blocks as fit on all SMs at once
+  int nsm = 0, occ = 0;
+  if (!rc) rc = check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  if (c->mg_float) {
+    if (!rc) rc = check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k0_head_bulk<float, true>, kBT,
+                                                                      bulk_smem<float>()));
+  } else {
+    if (!rc) rc = check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k0_head_bulk<double, true>, kBT,
+                                                                      bulk_smem<double>()));
+  }
+  c->bulk_grid = rc ? 0 : nsm * occ;
   return rc;
 }
 

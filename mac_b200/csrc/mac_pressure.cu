@@ -675,7 +675,7 @@ static void precondition(Ctx* c) {
 // Convergence test after the update the V-cycle's first kernel applied (its
 // partial r.r are in c->partial).
 void cg_finish_update(Ctx* c) {
-  k_fin_rr<<<1, 1024, 0, c->stream>>>(c->partial, c->ndom_host, c->ds, c->prm.rtol * c->prm.rtol,
+  k_fin_rr<<<1, 1024, 0, c->stream>>>(c->partial, c->npart_head, c->ds, c->prm.rtol * c->prm.rtol,
                                       c->prm.max_iters); MAC_COUNT(c);
 }
 

@@ -537,10 +537,11 @@ int mac_set_learned_smoothing(void* ctx, double omega) {
   return MAC_OK;
 }
 
-int mac_set_multigrid(void* ctx, int sweeps0) {
+int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   CTX_OR_FAIL();
-  if (sweeps0 != 1 && sweeps0 != 2) return MAC_ERR_INVALID;
+  if ((sweeps0 != 1 && sweeps0 != 2) || (prefetch != 0 && prefetch != 1)) return MAC_ERR_INVALID;
   c->mg_sweeps0 = sweeps0;
+  c->mg_bulk = prefetch;
   return MAC_OK;
 }
 

@@ -136,7 +136,7 @@ def load(path: str = LIB_PATH):
     lib.mac_unet_launch_count.argtypes = [vp, _P(i64)]
     lib.mac_set_preconditioner_net.argtypes = [vp, vp]
     lib.mac_set_learned_smoothing.argtypes = [vp, f64]
-    lib.mac_set_multigrid.argtypes = [vp, i32]
+    lib.mac_set_multigrid.argtypes = [vp, i32, i32]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
     lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
     _lib = lib
@@ -440,9 +440,11 @@ class Context:
     def set_learned_smoothing(self, omega):
         self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
 
-    def set_multigrid(self, sweeps0):
-        """Jacobi sweeps before and after the coarse correction on the finest level (1 or 2)."""
-        self._check(self.lib.mac_set_multigrid(self.h, int(sweeps0)), "mac_set_multigrid")
+    def set_multigrid(self, sweeps0=2, prefetch=True):
+        """Jacobi sweeps before and after the coarse correction on the finest
+        level (1 or 2); prefetch: the V-cycle's first kernel prefetches bricks
+        with asynchronous bulk copies."""
+        self._check(self.lib.mac_set_multigrid(self.h, int(sweeps0), 1 if prefetch else 0), "mac_set_multigrid")
 
     # ---- drop-in CSC solver
     def csc_solve(self, offset, indice, value, b):

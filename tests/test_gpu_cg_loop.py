@@ -74,3 +74,24 @@ def test_zero_rhs_takes_no_iteration(pool64, solver):
     assert st["iterations"] == 0
     ex = got.exists.astype(bool)
     assert np.all(got.f64["p"][ex] == 0.0)
+
+
+@pytest.mark.parametrize("solver,sweeps", [("mixed", 1), ("mixed", 2), ("mgpcg64", 2)])
+def test_prefetching_first_kernel_matches_one_block_per_brick(pool64, solver, sweeps):
+    """The V-cycle's first kernel run as resident blocks prefetching bricks
+    with asynchronous bulk copies computes what the one-block-per-brick kernel
+    computes (only the r.r partials are summed in another grouping): the same
+    iteration count within one and the same pressure within 1e-10."""
+    out = []
+    for prefetch in (True, False):
+        with _ctx(pool64, solver, 1e-10, 500, sweeps) as ctx:
+            ctx.set_multigrid(sweeps, prefetch)
+            ctx.upload(pool64)
+            ctx.project(0)
+            st = ctx.stats()
+            got = ctx.download()
+        ex = got.exists.astype(bool)
+        out.append((st["iterations"], got.f64["p"][ex].copy()))
+    (i1, p1), (i0, p0) = out
+    assert abs(i1 - i0) <= 1, (i1, i0)
+    assert np.linalg.norm(p1 - p0) / np.linalg.norm(p0) <= 1e-10
