@@ -229,7 +229,7 @@ def _peaks():
         return {}
 
 
-def poisson_solves(dev, mg_sweeps=2, prefetch=True, reps=3):
+def poisson_solves(dev, mg_sweeps=2, prefetch=False, reps=3):
     """Standalone pressure solve of the 128^3 pool + 12 spheres world (solid box,
     face speeds uniform in [-1, 1]) to a relative residual of 1e-10: device time
     of one projection and of its solve (system set-up + CG iterations), per
@@ -305,6 +305,57 @@ def poisson_solves(dev, mg_sweeps=2, prefetch=True, reps=3):
     return res
 
 
+def learned_evaluation(dev, mg_sweeps=2, prefetch=False, sizes=(128, 256), rtol=1e-8):
+    """The learned preconditioner's evaluation: the pool + 12 spheres world at
+    128^3 and 256^3 (radii scaled with the box) solved to a relative residual
+    of 1e-8 with plain FP64 MG-PCG, the mixed form and the learned + mixed
+    form: device ms of the projection (median of 2 after one warm-up), CG
+    iterations, network iterations and whether MG-PCG took over."""
+    import torch
+    from mac_b200.gpu import Context
+    from mac_b200.state import pool_spheres_world
+    from mac_b200.unet import UNet
+    from mac_b200.world import setup_passes
+    if not os.path.exists(WEIGHTS):
+        return None
+    net = UNet(dev)
+    net.load(WEIGHTS)
+    out = {"rtol": rtol}
+    for n in sizes:
+        s = setup_passes(pool_spheres_world(n, r_range=(6.0 * n / 128, 20.0 * n / 128)))
+        row = {}
+        for solver in ("mgpcg64", "mixed", "learned_mixed"):
+            with Context(s.params, max_bricks=int(s.nbricks * 1.2) + 64, max_particles=1024, solver=solver,
+                         rtol=rtol, max_iters=1000, device=dev) as ctx:
+                ctx.set_multigrid(mg_sweeps, prefetch)
+                ctx.set_preconditioner(net)
+                stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+                times = []
+                for r in range(3):
+                    ctx.upload(s)
+                    ctx.sync()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ctx.project(0)
+                    e1.record(stream)
+                    e1.synchronize()
+                    if r:
+                        times.append(e0.elapsed_time(e1))
+                st = ctx.stats()
+            row[solver] = {"project_ms": round(float(np.median(times)), 3), "iterations": int(st["iterations"]),
+                           "relres": st["relres"]}
+            if solver.startswith("learned"):
+                row[solver].update({"learned_iterations": int(st["learned_iterations"]),
+                                    "fallback_to_mgpcg": bool(st["fallbacks"])})
+        row["unknowns"] = int(st["unknowns"])
+        row["speedup_vs_mgpcg64"] = {f: round(row["mgpcg64"]["project_ms"] / row[f]["project_ms"], 3)
+                                     for f in ("mixed", "learned_mixed")}
+        out[f"pool{n}"] = row
+        log(f"[learned eval] {n}^3: {row}")
+    net.close()
+    return out
+
+
 SOLVER_NAMES = {"mgpcg64": "plain FP64 MG-PCG", "mixed": "FP32 MG in FP64 PCG", "cg64": "FP64 Jacobi-PCG",
                 "learned": "learned preconditioner in FP64 flexible CG (FP64 MG-PCG fall-back)",
                 "learned_mixed": "learned preconditioner in FP64 flexible CG (FP32 MG fall-back)"}
@@ -329,7 +380,7 @@ def solver_forms(args, dev, params, host, wl, steps=5, warmup=2):
     for form in forms:
         with Context(params, max_bricks=wl[8], max_particles=wl[9], solver=form, rtol=1e-8, max_iters=1000,
                      device=dev, div_check=True) as ctx:
-            ctx.set_multigrid(args.mg_sweeps, not args.no_prefetch)
+            ctx.set_multigrid(args.mg_sweeps, args.prefetch)
             if form.startswith("learned"):
                 ctx.set_preconditioner(net)
             ctx.upload(None, host)
@@ -380,7 +431,7 @@ def run_ours(args, rank, world, local_rank):
     log(f"[rank {rank}] world built in {time.perf_counter() - t0:.1f}s: {s.nbricks} bricks, {s.nparticles} particles")
     ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
                   device=dev, div_check=True, warm_start=args.warm_start)
-    ctx.set_multigrid(args.mg_sweeps, not args.no_prefetch)
+    ctx.set_multigrid(args.mg_sweeps, args.prefetch)
     if args.solver.startswith("learned"):
         from mac_b200.unet import UNet
         net_main = UNet(dev)
@@ -494,7 +545,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"jet {wl[0]}x{wl[1]}x{wl[2]} h={wl[3]} inflow r={wl[4]:g} w={wl[5]}, pool depth "
                                f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
                    "solver": SOLVER_NAMES[args.solver], "mg_sweeps0": args.mg_sweeps,
-                   "mg_prefetch": not args.no_prefetch,
+                   "mg_prefetch": args.prefetch,
                    "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
@@ -510,7 +561,8 @@ def run_ours(args, rank, world, local_rank):
         out["solver_forms"] = solver_forms(args, dev, params, host, wl)
     del host
     if rank == 0 and not args.no_poisson:
-        out["poisson"] = poisson_solves(dev, args.mg_sweeps, not args.no_prefetch)
+        out["poisson"] = poisson_solves(dev, args.mg_sweeps, args.prefetch)
+        out["learned_evaluation"] = learned_evaluation(dev, args.mg_sweeps, args.prefetch)
     return out
 
 
@@ -529,8 +581,8 @@ def main():
     ap.add_argument("--mg-sweeps", type=int, choices=[1, 2], default=2,
                     help="Jacobi sweeps before and after the coarse correction on the finest multigrid level")
     ap.add_argument("--no-forms", action="store_true", help="skip stepping the jet with every solver form")
-    ap.add_argument("--no-prefetch", action="store_true",
-                    help="run the V-cycle's first kernel one block per brick instead of prefetching bricks")
+    ap.add_argument("--prefetch", action="store_true",
+                    help="run the V-cycle's first kernel as resident blocks prefetching bricks with bulk copies")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

@@ -185,7 +185,7 @@ struct Ctx {
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
   int mg_sweeps0 = 2;         // Jacobi sweeps before and after the coarse correction at level 0 (1 or 2)
-  int mg_bulk = 1;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
+  int mg_bulk = 0;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
   int bulk_grid = 0;          // its grid (blocks resident on all SMs at once)
   int npart_head = 0;         // partial sums the V-cycle's first kernel left (its grid)
   // learned preconditioner (flexible CG): the network and the previous z

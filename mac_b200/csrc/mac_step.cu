@@ -215,16 +215,18 @@ static int csc_solve_cg(Ctx* c, const double* hb, double* hx) {
 // ---- general (non-symmetric) matrices: Jacobi-preconditioned BiCGStab on
 // the row-major copy built at factorisation. A x is a row-wise product, so
 // every y_i is summed in a fixed order.
+// y = A x with scal[0] += w0.y and, with yy, scal[1] += y.y (formed from the
+// value just computed: y is never read back).
 __global__ void k_csr_spmv_dot(int n, const int* __restrict__ off, const int* __restrict__ ind,
                                const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
-                               const double* __restrict__ w0, const double* __restrict__ w1, double* scal) {
+                               const double* __restrict__ w0, int yy, double* scal) {
   double a0 = 0, a1 = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double s = 0;
     for (int k = off[i]; k < off[i + 1]; ++k) s += val[k] * x[ind[k]];
     y[i] = s;
     a0 += w0[i] * s;
-    if (w1) a1 += w1[i] * s;
+    if (yy) a1 += s * s;
   }
   for (int o = 16; o > 0; o >>= 1) {
     a0 += __shfl_down_sync(0xffffffffu, a0, o);
@@ -232,7 +234,7 @@ __global__ void k_csr_spmv_dot(int n, const int* __restrict__ off, const int* __
   }
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(scal, a0);
-    if (w1) atomicAdd(scal + 1, a1);
+    if (yy) atomicAdd(scal + 1, a1);
   }
 }
 
@@ -322,14 +324,14 @@ static int csc_solve_bicgstab(Ctx* c, const double* hb, double* hx) {
     first = false;
     k_bicg_vec<<<g, 256, 0, st>>>(n, 1, b, x, r, rh, p, v, y, s, z, t, dinv, scal, 0, beta, omega); MAC_COUNT(c);
     cudaMemsetAsync(scal, 0, 64, st);
-    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, y, v, rh, nullptr, scal); MAC_COUNT(c);
+    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, y, v, rh, 0, scal); MAC_COUNT(c);
     if ((rc = read())) return rc;
     const double rhv = hs[0];
     if (cg_breakdown(rhv)) break;
     alpha = rho / rhv;
     cudaMemsetAsync(scal, 0, 64, st);
     k_bicg_vec<<<g, 256, 0, st>>>(n, 2, b, x, r, rh, p, v, y, s, z, t, dinv, scal, alpha, 0, 0); MAC_COUNT(c);
-    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, z, t, s, t, scal); MAC_COUNT(c);
+    k_csr_spmv_dot<<<g, 256, 0, st>>>(n, c->csr_off, c->csr_ind, c->csr_val, z, t, s, 1, scal); MAC_COUNT(c);
     if ((rc = read())) return rc;
     const double ts = hs[0], tt = hs[1], ss = hs[2];
     ++it;

@@ -440,7 +440,7 @@ class Context:
     def set_learned_smoothing(self, omega):
         self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
 
-    def set_multigrid(self, sweeps0=2, prefetch=True):
+    def set_multigrid(self, sweeps0=2, prefetch=False):
         """Jacobi sweeps before and after the coarse correction on the finest
         level (1 or 2); prefetch: the V-cycle's first kernel prefetches bricks
         with asynchronous bulk copies."""

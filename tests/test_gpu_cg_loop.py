@@ -25,18 +25,20 @@ def pool64():
     return setup_passes(pool_spheres_world(N, r_range=(6.0 * N / 128, 20.0 * N / 128)))
 
 
-def _ctx(s, solver, rtol, max_iters, sweeps=2):
+def _ctx(s, solver, rtol, max_iters, sweeps=2, prefetch=False):
     from mac_b200.gpu import Context
     c = Context(s.params, max_bricks=int(s.nbricks * 1.2) + 64, max_particles=1024, solver=solver, rtol=rtol,
                 max_iters=max_iters)
-    c.set_multigrid(sweeps)
+    c.set_multigrid(sweeps, prefetch)
     return c
 
 
-@pytest.mark.parametrize("solver,sweeps", [("mixed", 2), ("mgpcg64", 2), ("cg64", 2), ("mixed", 1), ("mgpcg64", 1)])
+@pytest.mark.parametrize("solver,sweeps,prefetch", [("mixed", 2, False), ("mgpcg64", 2, False), ("cg64", 2, False),
+                                                    ("mixed", 1, False), ("mgpcg64", 1, False), ("mixed", 2, True),
+                                                    ("mixed", 1, True)])
 @pytest.mark.parametrize("cap", [1, 2, 5])
-def test_iteration_cap_is_exact(pool64, solver, sweeps, cap):
-    with _ctx(pool64, solver, 1e-14, cap, sweeps) as ctx:
+def test_iteration_cap_is_exact(pool64, solver, sweeps, prefetch, cap):
+    with _ctx(pool64, solver, 1e-14, cap, sweeps, prefetch) as ctx:
         ctx.upload(pool64)
         ctx.project(0, allow_not_converged=True)
         st = ctx.stats()
