@@ -230,6 +230,8 @@ static int create(const mac_params* p, Ctx** out) {
         double d = ax * c->dp.ih2[0] + ay * c->dp.ih2[1] + az * c->dp.ih2[2];
         c->dp.dtab[ax + 3 * ay + 9 * az] = d > 0 ? 1.0 / d : 0.0;
       }
+  c->dp.mgw1 = c->dp.mgw2 = 0.9;  // multigrid smoother (mac_set_smoother)
+  c->dp.mgws = 0.9;
   c->dp.cfl = p->cfl_factor;
   c->dp.dt_min = p->dt_min;
   c->dp.dt_max = p->dt_max;

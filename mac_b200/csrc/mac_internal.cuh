@@ -103,6 +103,9 @@ struct Params {
   // inverse diagonal of the level-0 operator by active faces per axis
   // (index ax + 3 ay + 9 az, each 0..2); 0 when no face is active
   double dtab[27];
+  // multigrid smoother: weights of the two Jacobi sweeps before and after each
+  // coarse correction, and of the single sweep of the one-sweep finest level
+  double mgw1, mgw2, mgws;
 };
 
 // Dense grid over the bounding box of the domain bricks (one cell per brick).
@@ -184,6 +187,7 @@ struct Ctx {
   void* mg_w[kLevels] = {};   // [4][cells]: left-face weights x,y,z and Dirichlet diagonal
   void* mg_dinv[kLevels] = {};
   int mg_float = 0;
+  double mg_scale = 0.6;      // coarse-operator scale of the Galerkin products
   int mg_sweeps0 = 2;         // Jacobi sweeps before and after the coarse correction at level 0 (1 or 2)
   int mg_bulk = 0;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
   int bulk_grid = 0;          // its grid (blocks resident on all SMs at once)

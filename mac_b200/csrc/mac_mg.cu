@@ -1,7 +1,7 @@
 // Multigrid preconditioner of the pressure solve.
 //
 // Hierarchy (Galerkin products with piecewise-constant transfer, each level's
-// operator scaled by kCoarseScale; stored as three left-face weights, the
+// operator scaled by the context's coarse scale; stored as three left-face weights, the
 // diagonal, its inverse and the Dirichlet part of the diagonal per cell):
 //   level 0  the fine cells of every brick that holds an in-domain cell
 //            (8^3 per brick; operator from the per-cell face classes),
@@ -23,11 +23,13 @@
 
 namespace mac {
 
-// Jacobi weight (the V-cycle stays positive definite for omega < 1) and the
-// per-level scale of the Galerkin operator (piecewise-constant transfer
-// over-weights the coarse operator; 0.6 was the best of 0.4-0.7 on pool masks).
-constexpr double kOmega = 0.9;
-constexpr double kCoarseScale = 0.6;
+// Smoother weights and the per-level scale of the Galerkin operator
+// (piecewise-constant transfer over-weights the coarse operator) come from the
+// context (Params::mgw1/mgw2/mgws, Ctx::mg_scale; mac_set_smoother). Two
+// sweeps with weights w1, w2 damp the error of an eigenvalue lambda of D^-1 A
+// (in (0, 2] here: the operators are diagonally dominant) by
+// (1 - w1 lambda)(1 - w2 lambda); the V-cycle stays symmetric positive
+// definite while that product stays inside (-1, 1) on (0, 2].
 constexpr int kCoarsestSweeps = 40;
 
 // Level-1 parent of level-0 cell n (pool index).
@@ -84,7 +86,8 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
   __shared__ uint16_t sm[kCells];
-  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const T om = (T)P.mgw1, om2 = (T)P.mgw2, c0 = (T)(P.mgw1 + P.mgw2 - P.mgw1 * P.mgw2);
+  const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   const double al = update ? ds->alpha : 0.0;
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
@@ -121,11 +124,11 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
     if (m & kDomainBit) {
       int si = s1_of(o);
       T dinv = (T)P.dtab[active_index(m)];
-      T s = (T)(2.0 - kOmega) * (T)rv[k];
+      T s = 0;
 #pragma unroll
       for (int f = 0; f < 6; ++f)
         if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
-      out = om * dinv * s;
+      out = dinv * (c0 * (T)rv[k] + om2 * s);
     }
     e[c] = out;
   }
@@ -202,7 +205,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
-  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const T om = (T)(FIRST ? P.mgw1 : P.mgw2), ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   uint16_t mk[kCPT];
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];    // e = w D^-1 r of the brick and its face halo
   __shared__ T res[kCells];
-  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const T om = (T)P.mgws, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   const double al = update ? ds->alpha : 0.0;
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];
-  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const T om = (T)P.mgws, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   uint16_t mk[kCPT];
@@ -459,7 +462,7 @@ __global__ void __launch_bounds__(kBT) k0_head_bulk(const int* __restrict__ dbl,
   T* sr = reinterpret_cast<T*>(smem + 2 * kBulkStage);  // w D^-1 r (brick and face halo)
   T* res = sr + kS1;                                     // RESTRICT: the brick's residual
   const int tid = threadIdx.x;
-  const T om = (T)kOmega, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  const T om = (T)(RESTRICT ? P.mgws : P.mgw1), om2 = (T)P.mgw2, c0 = (T)(P.mgw1 + P.mgw2 - P.mgw1 * P.mgw2), ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   const double al = update ? ds->alpha : 0.0;
   const uint32_t bytes = update ? (uint32_t)kBulkStage : (uint32_t)(kBulkVec + kCells * 2);
   auto issue = [&](int j, int st) {
@@ -566,11 +569,11 @@ __global__ void __launch_bounds__(kBT) k0_head_bulk(const int* __restrict__ dbl,
         if (m & kDomainBit) {
           const int si = s1_of(o);
           const T dinv = (T)P.dtab[active_index(m)];
-          T s = (T)(2.0 - kOmega) * (T)rv[k];
+          T s = 0;
 #pragma unroll
           for (int f = 0; f < 6; ++f)
             if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
-          out = om * dinv * s;
+          out = dinv * (c0 * (T)rv[k] + om2 * s);
         }
         e[c] = out;
       }
@@ -682,7 +685,7 @@ __device__ inline T apply_l(const T* __restrict__ e, const T* __restrict__ w, si
 template <class T, int D>
 __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
-                                              T* __restrict__ e, const int32_t* __restrict__ done) {
+                                              T* __restrict__ e, T w1, T w2, const int32_t* __restrict__ done) {
   if (solve_done(done)) return;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
@@ -714,13 +717,13 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
     dr[a] = w[4 * ncap + jr];
     rr[a] = r[jr];
   }
-  T s = (T)(2.0 - kOmega) * r[i];
+  T s = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    if (wl[a] != 0) s += wl[a] * (T)kOmega * dl[a] * rl[a];
-    if (wr[a] != 0) s += wr[a] * (T)kOmega * dr[a] * rr[a];
+    if (wl[a] != 0) s += wl[a] * w1 * dl[a] * rl[a];
+    if (wr[a] != 0) s += wr[a] * w1 * dr[a] * rr[a];
   }
-  e[i] = (T)kOmega * dinv * s;
+  e[i] = dinv * ((w1 + w2 - w1 * w2) * r[i] + w2 * s);
 }
 
 // Sum over aligned groups of 8 lanes; the result is valid in the group's first lane.
@@ -779,7 +782,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
                                                  const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                  const T* __restrict__ r, const T* __restrict__ e,
                                                  const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3,
-                                                 const int32_t* __restrict__ done) {
+                                                 T om, const int32_t* __restrict__ done) {
   if (solve_done(done)) return;
   constexpr int N = D * D * D;
   constexpr int H = D / 2;
@@ -844,7 +847,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     if (wl[a] != 0) s -= wl[a] * vl[a];
     if (wr[a] != 0) s -= wr[a] * vr[a];
   }
-  eout[i] = ecc + (T)kOmega * dinv * (r[i] - s);
+  eout[i] = ecc + om * dinv * (r[i] - s);
 }
 
 // ------------------------------------------------------------ dense levels
@@ -857,6 +860,7 @@ struct DView {
   T* e2;
   T* r;
   T* w;  // [6][n]
+  T w1, w2;  // smoother weights of the two sweeps
   __device__ int64_t at(int x, int y, int z) const { return x + (int64_t)nx * (y + (int64_t)ny * z); }
 };
 
@@ -895,16 +899,16 @@ __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
   int c[3] = {x, y, z};
   int dim[3] = {L.nx, L.ny, L.nz};
   int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  T s = (T)(2.0 - kOmega) * L.r[i];
+  T s = 0;
   for (int a = 0; a < 3; ++a) {
     T wl = L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) s += wl * (T)kOmega * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
+    if (wl != 0 && c[a] > 0) s += wl * L.w1 * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
     if (c[a] + 1 < dim[a]) {
       T wr = L.w[a * n + i + stride[a]];
-      if (wr != 0) s += wr * (T)kOmega * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
+      if (wr != 0) s += wr * L.w1 * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
     }
   }
-  L.e[i] = (T)kOmega * dinv * s;
+  L.e[i] = dinv * ((L.w1 + L.w2 - L.w1 * L.w2) * L.r[i] + L.w2 * s);
 }
 
 // One thread per (coarse cell, child), the 8 children on adjacent lanes.
@@ -967,7 +971,7 @@ __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__
       }
     }
   }
-  eout[i] = ec + (T)kOmega * dinv * (L.r[i] - s);
+  eout[i] = ec + (WITH_COARSE ? L.w1 : L.w2) * dinv * (L.r[i] - s);
 }
 
 // ------------------------------------------- coarse V-cycle in one block
@@ -983,7 +987,8 @@ struct DenseSet {
 // coarser level's correction, on a cnx x cny grid) is added to every e first
 // when given.
 template <class T>
-__device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce, int cnx, int cny, bool first) {
+__device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce, int cnx, int cny, bool first,
+                           T om) {
   const int n = (int)L.n;  // block-solved levels hold a few thousand cells: 32-bit index math
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const T* __restrict__ w = L.w;
@@ -996,7 +1001,7 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce
       continue;
     }
     if (first) {
-      eout[i] = (T)kOmega * dinv * r[i];
+      eout[i] = om * dinv * r[i];
       continue;
     }
     const int xy = qdiv(i, nx, rnx);
@@ -1027,7 +1032,7 @@ __device__ void blk_jacobi(const DView<T>& L, const T* ein, T* eout, const T* ce
         }
       }
     }
-    eout[i] = ec + (T)kOmega * dinv * (r[i] - s);
+    eout[i] = ec + om * dinv * (r[i] - s);
   }
 }
 
@@ -1173,9 +1178,9 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
   // down
   for (int l = lo; l < hi - 1; ++l) {
     const DView<T>& L = SL[l];
-    blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true);
+    blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true, L.w1);
     __syncthreads();
-    blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false);
+    blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false, L.w2);
     __syncthreads();
     swapped ^= 1u << l;
     blk_restrict(L, cur(l), SL[l + 1]);
@@ -1203,10 +1208,10 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
       if (i < n && p == 0) cur(l)[i] = (double)L.w[4 * L.n + i] == 0 ? (T)0 : (T)s;
       __syncthreads();
     } else {
-      blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true);
+      blk_jacobi(L, cur(l), cur(l), (const T*)nullptr, 0, 0, true, L.w1);
       __syncthreads();
       for (int s = 1; s < kCoarsestSweeps; ++s) {
-        blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false);
+        blk_jacobi(L, cur(l), oth(l), (const T*)nullptr, 0, 0, false, (s & 1) ? L.w2 : L.w1);
         __syncthreads();
         swapped ^= 1u << l;
       }
@@ -1215,9 +1220,9 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
   // up
   for (int l = hi - 2; l >= lo; --l) {
     const DView<T>& L = SL[l];
-    blk_jacobi(L, cur(l), oth(l), cur(l + 1), SL[l + 1].nx, SL[l + 1].ny, false);
+    blk_jacobi(L, cur(l), oth(l), cur(l + 1), SL[l + 1].nx, SL[l + 1].ny, false, L.w1);
     __syncthreads();
-    blk_jacobi(L, oth(l), cur(l), (const T*)nullptr, 0, 0, false);
+    blk_jacobi(L, oth(l), cur(l), (const T*)nullptr, 0, 0, false, L.w2);
     __syncthreads();
   }
   if (use_smem || cur(lo) != G.L[lo].e) blk_copy(G.L[lo].e, cur(lo), SL[lo].n);
@@ -1227,7 +1232,7 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
 // Level-1 weights from the level-0 face classes (Galerkin, piecewise constant).
 template <class T>
 __global__ void kw_l1(const int* __restrict__ dbl, int nd, const uint16_t* __restrict__ fmask, T* w, size_t ncap1,
-                      Params P) {
+                      Params P, double scale) {
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= (int64_t)nd * 64) return;
   int b = dbl[g >> 6];
@@ -1245,14 +1250,14 @@ __global__ void kw_l1(const int* __restrict__ dbl, int nd, const uint16_t* __res
       if (lc[a] == 0 && (m & (1u << (2 * a)))) wl[a] += P.ih2[a];
   }
   size_t i = (size_t)b * 64 + o;
-  for (int a = 0; a < 3; ++a) w[a * ncap1 + i] = (T)(kCoarseScale * wl[a]);
-  w[5 * ncap1 + i] = (T)(kCoarseScale * dd);
+  for (int a = 0; a < 3; ++a) w[a * ncap1 + i] = (T)(scale * wl[a]);
+  w[5 * ncap1 + i] = (T)(scale * dd);
 }
 
 // Brick level D -> D/2 (D = 4), or D = 2 -> dense level 3 at the brick position.
 template <class T, int D>
 __global__ void kw_coarsen(const int* __restrict__ dbl, int nd, const int* __restrict__ bkey, const T* __restrict__ wf,
-                           size_t ncapf, T* wc, size_t ncapc, DenseGrid g3) {
+                           size_t ncapf, T* wc, size_t ncapc, DenseGrid g3, double scale) {
   constexpr int H = D / 2;
   int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= (int64_t)nd * H * H * H) return;
@@ -1269,8 +1274,8 @@ __global__ void kw_coarsen(const int* __restrict__ dbl, int nd, const int* __res
   }
   size_t i = D == 2 ? (size_t)g3.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])
                     : (size_t)b * H * H * H + o;
-  for (int a = 0; a < 3; ++a) wc[a * ncapc + i] = (T)(kCoarseScale * wl[a]);
-  wc[5 * ncapc + i] = (T)(kCoarseScale * dd);
+  for (int a = 0; a < 3; ++a) wc[a * ncapc + i] = (T)(scale * wl[a]);
+  wc[5 * ncapc + i] = (T)(scale * dd);
 }
 
 template <class T, int D>
@@ -1294,7 +1299,7 @@ __global__ void kw_diag(const int* __restrict__ dbl, int nd, const int* __restri
 }
 
 template <class T>
-__global__ void kwd_coarsen(DView<T> F, DView<T> C) {
+__global__ void kwd_coarsen(DView<T> F, DView<T> C, double scale) {
   int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= C.n) return;
   int X = (int)(I % C.nx), Y = (int)((I / C.nx) % C.ny), Z = (int)(I / ((int64_t)C.nx * C.ny));
@@ -1308,8 +1313,8 @@ __global__ void kwd_coarsen(DView<T> F, DView<T> C) {
     for (int a = 0; a < 3; ++a)
       if (lc[a] == 0) wl[a] += (double)F.w[a * F.n + i];
   }
-  for (int a = 0; a < 3; ++a) C.w[a * C.n + I] = (T)(kCoarseScale * wl[a]);
-  C.w[5 * C.n + I] = (T)(kCoarseScale * dd);
+  for (int a = 0; a < 3; ++a) C.w[a * C.n + I] = (T)(scale * wl[a]);
+  C.w[5 * C.n + I] = (T)(scale * dd);
 }
 
 template <class T>
@@ -1343,6 +1348,8 @@ static DView<T> dview(Ctx* c, int l) {
   v.e2 = v.e + d.n;
   v.r = v.e + 2 * d.n;
   v.w = v.e + 3 * d.n;
+  v.w1 = (T)c->dp.mgw1;
+  v.w2 = (T)c->dp.mgw2;
   return v;
 }
 
@@ -1407,12 +1414,13 @@ static int mg_setup_t(Ctx* c) {
   rc = check(cudaMemsetAsync(w1, 0, ncap1 * 6 * sizeof(T), st));
   if (!rc) rc = check(cudaMemsetAsync(w2, 0, ncap2 * 6 * sizeof(T), st));
   if (rc) return rc;
-  kw_l1<T><<<g1, 256, 0, st>>>(c->dbl, nd, c->fmask, w1, ncap1, c->dp); MAC_COUNT(c);
-  kw_coarsen<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->bkey, w1, ncap1, w2, ncap2, c->g3); MAC_COUNT(c);
-  kw_coarsen<T, 2><<<g3, 256, 0, st>>>(c->dbl, nd, c->bkey, w2, ncap2, d3.w, (size_t)d3.n, c->g3); MAC_COUNT(c);
+  const double sc = c->mg_scale;
+  kw_l1<T><<<g1, 256, 0, st>>>(c->dbl, nd, c->fmask, w1, ncap1, c->dp, sc); MAC_COUNT(c);
+  kw_coarsen<T, 4><<<g2, 256, 0, st>>>(c->dbl, nd, c->bkey, w1, ncap1, w2, ncap2, c->g3, sc); MAC_COUNT(c);
+  kw_coarsen<T, 2><<<g3, 256, 0, st>>>(c->dbl, nd, c->bkey, w2, ncap2, d3.w, (size_t)d3.n, c->g3, sc); MAC_COUNT(c);
   for (int l = 0; l + 1 < c->ndense; ++l) {
     DView<T> F = dview<T>(c, l), C = dview<T>(c, l + 1);
-    kwd_coarsen<T><<<grid_for(C.n, 256), 256, 0, st>>>(F, C); MAC_COUNT(c);
+    kwd_coarsen<T><<<grid_for(C.n, 256), 256, 0, st>>>(F, C, sc); MAC_COUNT(c);
   }
   kw_diag<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1); MAC_COUNT(c);
   kw_diag<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2); MAC_COUNT(c);
@@ -1476,9 +1484,10 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   if (!one) {
     k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
   }
-  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1, dn); MAC_COUNT(c);
+  const T sw1 = (T)c->dp.mgw1, sw2 = (T)c->dp.mgw2;
+  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
   kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
-  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2, dn); MAC_COUNT(c);
+  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
   kl_restrict<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
@@ -1502,12 +1511,14 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
     kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
   // up
-  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, dn); MAC_COUNT(c);
+  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
+                                            dn); MAC_COUNT(c);
   kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
-                                             dn); MAC_COUNT(c);
-  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, dn); MAC_COUNT(c);
+                                             sw2, dn); MAC_COUNT(c);
+  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
+                                            dn); MAC_COUNT(c);
   kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
-                                             dn); MAC_COUNT(c);
+                                             sw2, dn); MAC_COUNT(c);
   if (one) {
     k0_post_one<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
     return;

@@ -547,6 +547,26 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   return MAC_OK;
 }
 
+int mac_set_smoother(void* ctx, double w1, double w2, double w_single, double coarse_scale) {
+  CTX_OR_FAIL();
+  if (!(w1 > 0 && w1 < 2 && w2 > 0 && w2 < 2 && w_single > 0 && w_single < 1 && coarse_scale > 0 &&
+        coarse_scale <= 1))
+    return MAC_ERR_INVALID;
+  // two sweeps damp lambda in (0, 2] by (1 - w1 lambda)(1 - w2 lambda): keep it inside (-1, 1)
+  for (int k = 1; k <= 200; ++k) {
+    const double l = 0.01 * k, f = (1 - w1 * l) * (1 - w2 * l);
+    if (!(f > -1 && f < 1)) return MAC_ERR_INVALID;
+  }
+  c->dp.mgw1 = w1;
+  c->dp.mgw2 = w2;
+  c->dp.mgws = w_single;
+  if (coarse_scale != c->mg_scale) {
+    c->mg_scale = coarse_scale;
+    c->system_ready = false;
+  }
+  return MAC_OK;
+}
+
 int mac_csc_factorize(void* ctx, int n, const int* offset, const int* indice, const double* value) {
   CTX_OR_FAIL();
   if (n < 0 || (n > 0 && (!offset || !indice || !value))) return MAC_ERR_INVALID;

@@ -69,7 +69,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
            "mac_unet_make_dataset", "mac_unet_make_dataset_ext", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
-           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_unet_set_loss", "mac_unet_time_forward"]
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_set_smoother", "mac_unet_set_loss", "mac_unet_time_forward"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -137,6 +137,7 @@ def load(path: str = LIB_PATH):
     lib.mac_set_preconditioner_net.argtypes = [vp, vp]
     lib.mac_set_learned_smoothing.argtypes = [vp, f64]
     lib.mac_set_multigrid.argtypes = [vp, i32, i32]
+    lib.mac_set_smoother.argtypes = [vp, f64, f64, f64, f64]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
     lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
     _lib = lib
@@ -439,6 +440,11 @@ class Context:
 
     def set_learned_smoothing(self, omega):
         self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
+
+    def set_smoother(self, w1=0.9, w2=0.9, w_single=0.9, coarse_scale=0.6):
+        """Multigrid smoother weights and coarse-operator scale (mac_set_smoother)."""
+        self._check(self.lib.mac_set_smoother(self.h, float(w1), float(w2), float(w_single), float(coarse_scale)),
+                    "mac_set_smoother")
 
     def set_multigrid(self, sweeps0=2, prefetch=False):
         """Jacobi sweeps before and after the coarse correction on the finest
