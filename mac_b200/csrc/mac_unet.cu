@@ -597,6 +597,7 @@ __global__ void k_adam(float* p, const float* __restrict__ g, float* mo, float* 
                        float b1, float b2, float eps, float bc1, float bc2) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const float gi = g[i];
+    if (!isfinite(gi)) continue;  // a degenerate batch leaves the parameter as it is
     const float m1 = b1 * mo[i] + (1.0f - b1) * gi;
     const float v1 = b2 * ve[i] + (1.0f - b2) * gi * gi;
     mo[i] = m1;

@@ -6,7 +6,8 @@
 Training pairs (residual, exact error) come from plain FP64 CG iterates on
 random fluid masks (a pool z < 0.4 size plus 12 spheres of radius 3..10 cells
 at size 64, solid box) and on size^3 patches of jet states (--jet-masks: the
-32x32x64 jet every 5 steps of its first 100 from the first init, and
+32x32x64 jet every 5 steps of its first 100 from the first init, at twice
+its resolution, and
 patches centred on the free surface of the 256x256x512 jet after its first
 init and 10 steps, both stepped on the device), generated on the device by
 mac_unet_make_dataset[_ext]; the network is trained with Adam by the device's
@@ -60,8 +61,20 @@ def surface_cells(s):
     return np.stack([x, y, z], axis=1) + lo
 
 
+MIN_FLUID = 4096  # a patch with fewer fluid cells is solved exactly within the snapshots: left out
+
+
+def upsample2(m):
+    """Each cell of a mask as 2x2x2 cells."""
+    return m.repeat(2, axis=0).repeat(2, axis=1).repeat(2, axis=2)
+
+
 def jet_masks(n_big, size, device=0, seed=7):
-    """Patches of jet states for the training set (module docstring)."""
+    """Patches of jet states for the training set (module docstring). The
+    32x32x64 jet's states are taken at twice the resolution (each cell as 2^3
+    cells, the size^3 window over the fluid's bottom), so that the patch holds
+    a problem of the training set's size; patches with fewer than MIN_FLUID
+    fluid cells are left out."""
     from .gpu import Context
     from .state import jet_world
     from .world import first_init
@@ -74,7 +87,10 @@ def jet_masks(n_big, size, device=0, seed=7):
             ctx.step()
             if k % 5 == 0:
                 st = ctx.download()
-                out.append(state_mask(st, (-1 - (size - 34) // 2, -1 - (size - 34) // 2, -1), size))
+                h = size // 2
+                m = upsample2(state_mask(st, (-1 - (h - 34) // 2, -1 - (h - 34) // 2, -1), h))
+                if int((m == 1).sum()) >= MIN_FLUID:
+                    out.append(m)
     s = jet_world(256, 256, 512, h=0.01, r_inflow=24.0, w_inflow=2.0, pool_depth=122, dt_max=0.01, seed=seed)
     with Context(s.params, max_bricks=40000, max_particles=80_000_000, solver="mixed", rtol=1e-8,
                  device=device) as ctx:
@@ -85,7 +101,9 @@ def jet_masks(n_big, size, device=0, seed=7):
         st = ctx.download()
     surf = surface_cells(st)
     for c in surf[rng.choice(len(surf), n_big, replace=False)]:
-        out.append(state_mask(st, c - size // 2, size))
+        m = state_mask(st, c - size // 2, size)
+        if int((m == 1).sum()) >= MIN_FLUID:
+            out.append(m)
     return np.stack(out)
 
 

@@ -97,3 +97,25 @@ def test_prefetching_first_kernel_matches_one_block_per_brick(pool64, solver, sw
     (i1, p1), (i0, p0) = out
     assert abs(i1 - i0) <= 1, (i1, i0)
     assert np.linalg.norm(p1 - p0) / np.linalg.norm(p0) <= 1e-10
+
+
+def test_smoother_settings(pool64):
+    """mac_set_smoother: weights whose two-sweep damping leaves (-1, 1) on
+    (0, 2] are refused; other weights and coarse scales change the iteration
+    count, not the answer (pressure within 1e-9 of the default settings' at a
+    relative residual of 1e-12)."""
+    from mac_b200.gpu import MacError
+    out = []
+    for w1, w2, scale in ((0.9, 0.9, 0.6), (0.5617, 1.3895, 0.6), (0.548, 1.025, 0.7)):
+        with _ctx(pool64, "mixed", 1e-12, 500) as ctx:
+            ctx.set_smoother(w1, w2, 0.9, scale)
+            ctx.upload(pool64)
+            ctx.project(0)
+            got = ctx.download()
+            out.append((ctx.stats()["iterations"], got.f64["p"][got.exists.astype(bool)].copy()))
+    for its, p in out[1:]:
+        assert np.linalg.norm(p - out[0][1]) / np.linalg.norm(out[0][1]) <= 1e-9
+    with _ctx(pool64, "mixed", 1e-12, 500) as ctx:
+        for bad in ((1.2, 1.2, 0.9, 0.6), (0.9, 0.9, 1.0, 0.6), (0.9, 0.9, 0.9, 1.5), (0.0, 0.9, 0.9, 0.6)):
+            with pytest.raises(MacError):
+                ctx.set_smoother(*bad)
