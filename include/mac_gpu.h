@@ -298,6 +298,11 @@ int mac_unet_launch_count(void* net, int64_t* count);
 /* Device time of one forward pass (mean over reps, CUDA events) on an n x d x h x w
  * grid and its algorithmic FLOPs (2 taps cin cout per output cell, unpadded channels). */
 int mac_unet_time_forward(void* net, int n, int d, int h, int w, int reps, double* ms, double* flops);
+/* Kernel of the forward 3x3x3 convolutions: 1 (default) stages each tile's input
+ * box with its halo in shared memory once and runs the 27 taps from it; 0 gathers
+ * every tap's operand separately (the kernel the backward pass shares). Both
+ * accumulate in the same order. */
+int mac_unet_set_conv(void* net, int staged);
 
 /* Attaches a network (mac_unet_create) as the preconditioner of the
  * MAC_SOLVER_LEARNED* solvers; NULL detaches it. The context does not own it. */

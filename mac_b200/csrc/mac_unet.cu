@@ -248,6 +248,153 @@ __global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
   if (warp == 0) umma::tmem_dealloc(tmem, TCOLS);
 }
 
+// ------------------------------------- forward 3x3x3 convolution, staged tile
+// A CTA computes a tile of 8 (x) x 16 (y) x 1 (z) output voxels (M = 128).
+// Its input box with a one-voxel halo, 10 x 18 x 3 voxels x KC channels, is
+// gathered from global memory once (concatenation and nearest upsampling of
+// the sources folded into the gather, zero outside the grid) into the
+// no-swizzle K-major layout [channel group g][z][y][x] x 16 bytes. For tap
+// (dz, dy, dx) the A operand is then the same box seen from another start
+// address: core matrix j (output row y = j, x = 0..7: eight consecutive
+// 16-byte rows) starts at ((g*3 + 1+dz)*18 + 1+dy + j)*10 + 1+dx, so the
+// M-adjacent core matrices lie SBO = 160 bytes apart and the K-adjacent ones
+// LBO = 8640 bytes apart, and the 27 taps need no further gathering. The
+// weights of a chunk of taps are staged K-major beside the box; one thread
+// issues every tcgen05.mma of the chunk (taps in order, K in steps of 16)
+// into the tensor-memory accumulator and commits to an mbarrier (bounded
+// wait); the epilogue is k_conv's (bias, ReLU, BF16 or FP32 store). The
+// accumulation visits taps and K steps in k_conv's order.
+constexpr int kBoxX = 10, kBoxY = 18, kBoxZ = 3, kBoxVox = kBoxX * kBoxY * kBoxZ;
+constexpr int kConvWChunk = 65536;  // bytes of weights staged at a time
+
+template <int KC, int NC>
+__host__ __device__ constexpr int tile_taps() {
+  return (kConvWChunk / (NC * KC * 2)) < 27 ? (kConvWChunk / (NC * KC * 2)) : 27;
+}
+template <int KC, int NC>
+__host__ __device__ constexpr int tile_smem() {
+  return KC * kBoxVox * 2 + tile_taps<KC, NC>() * NC * KC * 2 + 128;
+}
+
+template <int KC, int NC>
+__global__ void __launch_bounds__(128) k_conv_tile(ConvArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  constexpr int BOX_BYTES = KC * kBoxVox * 2;
+  constexpr int TB = tile_taps<KC, NC>();
+  constexpr uint32_t LBO_A = kBoxVox * 16, SBO_A = kBoxX * 16;
+  constexpr uint32_t SBO_B = (KC / 8) * 128;
+  constexpr uint32_t TCOLS = NC < 32 ? 32 : NC;
+  constexpr uint32_t IDESC = umma::idesc_bf16(128, NC, 0, 0);
+  uint8_t* box = smem;
+  uint8_t* wbuf = smem + BOX_BYTES;
+  uint64_t* done = reinterpret_cast<uint64_t*>(wbuf + TB * NC * KC * 2);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tx = (a.w + 7) / 8, ty = (a.h + 15) / 16;
+  int bid = blockIdx.x;
+  const int x0 = (bid % tx) * 8;
+  bid /= tx;
+  const int y0 = (bid % ty) * 16;
+  bid /= ty;
+  const int z0 = bid % a.d, n = bid / a.d;
+  if (tid == 0) {
+    umma::mbar_init(done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) umma::tmem_alloc(tslot, TCOLS);
+  // the input box, once
+  for (int i = tid; i < (KC / 8) * kBoxVox; i += 128) {
+    const int g = i / kBoxVox, vox = i - g * kBoxVox;
+    const int bx = vox % kBoxX, by = (vox / kBoxX) % kBoxY, bz = vox / (kBoxX * kBoxY);
+    const int x = x0 - 1 + bx, y = y0 - 1 + by, z = z0 - 1 + bz;
+    uint4 val = make_uint4(0, 0, 0, 0);
+    if (x >= 0 && x < a.w && y >= 0 && y < a.h && z >= 0 && z < a.d)
+      val = gather8(a.s1, a.s2, g, n, z, y, x, a.d, a.h, a.w);
+    *reinterpret_cast<uint4*>(box + (size_t)i * 16) = val;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  bool ok = true;
+  int phase = 0;
+  for (int t0 = 0; t0 < 27; t0 += TB) {
+    const int nt = 27 - t0 < TB ? 27 - t0 : TB;
+    // weights of taps t0 .. t0+nt-1: rows = output channels, K-major
+    for (int i = tid; i < nt * NC * (KC / 8); i += 128) {
+      const int tt = i / (NC * (KC / 8)), rem = i - tt * NC * (KC / 8);
+      const int row = rem / (KC / 8), c = rem % (KC / 8);
+      const uint4 val = ldg16(a.wt + ((size_t)(t0 + tt) * NC + row) * KC + c * 8);
+      *reinterpret_cast<uint4*>(wbuf + (size_t)tt * NC * KC * 2 + (row >> 3) * SBO_B + c * 128 + (row & 7) * 16) =
+          val;
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t abase = umma::smem_addr(box), bbase = umma::smem_addr(wbuf);
+      for (int tt = 0; tt < nt; ++tt) {
+        int dz, dy, dx;
+        tap_offset(t0 + tt, 27, dz, dy, dx);
+        const uint32_t at = abase + (uint32_t)((((1 + dz) * kBoxY + 1 + dy) * kBoxX + 1 + dx) * 16);
+        const uint32_t bt = bbase + (uint32_t)(tt * NC * KC * 2);
+#pragma unroll
+        for (int ks = 0; ks < KC / 16; ++ks)
+          umma::mma(tmem, umma::desc(at + ks * 2 * LBO_A, LBO_A, SBO_A), umma::desc(bt + ks * 256, 128, SBO_B),
+                    IDESC, (t0 + tt > 0 || ks > 0) ? 1u : 0u);
+      }
+      umma::commit(done);
+    }
+    // the next chunk overwrites the weights only after these MMAs completed
+    if (!umma::mbar_wait(done, (uint32_t)(phase & 1))) ok = false;
+    ++phase;
+    umma::fence_after_sync();
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+  }
+  const int m = tid;  // TMEM lane = tile row: x = m & 7, y = m >> 3
+  const int x = x0 + (m & 7), y = y0 + (m >> 3);
+  const bool valid = x < a.w && y < a.h;
+  const size_t v = (((size_t)n * a.d + z0) * a.h + y) * a.w + x;
+  if (ok) {
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c0 = 0; c0 < NC; c0 += 16) {
+      float f[16];
+      umma::tmem_ld16(trow + c0, f);
+      if (!valid) continue;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        if (a.bias) f[i] += a.bias[c0 + i];
+        if (a.relu) f[i] = fmaxf(f[i], 0.0f);
+      }
+      if (a.f32) {
+        if (c0 == 0) a.f32[v] = f[0];
+        continue;
+      }
+      uint4 pk[2];
+      uint32_t* w32 = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        __nv_bfloat162 b2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+        w32[i] = *reinterpret_cast<uint32_t*>(&b2);
+      }
+      bf16* dst;
+      if (c0 < a.c1)
+        dst = a.d1 + v * a.c1 + c0;
+      else
+        dst = a.d2 + v * (NC - a.c1) + (c0 - a.c1);
+      reinterpret_cast<uint4*>(dst)[0] = pk[0];
+      reinterpret_cast<uint4*>(dst)[1] = pk[1];
+    }
+  } else if (tid == 0) {
+    atomicExch(a.err, 1);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, TCOLS);
+}
+
 // ------------------------------------------------ weight gradient (K = voxels)
 // dW[tap][co][ci] += sum_v in[v + off(tap)][ci] * (g * gate)[v][co]; a CTA owns
 // 16 (tap, 8-channel group) row blocks = 128 GEMM rows and a range of voxels.
@@ -795,6 +942,27 @@ static void conv_t(const ConvArgs& a, cudaStream_t st) {
   k_conv<KC, NC, MODE><<<(unsigned)((V + 127) / 128), 128, smem, st>>>(a);
 }
 
+template <int KC, int NC>
+static void conv_tile_t(const ConvArgs& a, cudaStream_t st) {
+  const int smem = tile_smem<KC, NC>();
+  cudaFuncSetAttribute(k_conv_tile<KC, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const long tiles = (long)a.n * a.d * ((a.h + 15) / 16) * ((a.w + 7) / 8);
+  k_conv_tile<KC, NC><<<(unsigned)tiles, 128, smem, st>>>(a);
+}
+
+// Forward 3x3x3 convolutions through the staged-tile kernel.
+static int conv_tile(int kc, int nc, const ConvArgs& a, cudaStream_t st) {
+  if (kc == 16 && nc == 16) conv_tile_t<16, 16>(a, st);
+  else if (kc == 16 && nc == 32) conv_tile_t<16, 32>(a, st);
+  else if (kc == 32 && nc == 32) conv_tile_t<32, 32>(a, st);
+  else if (kc == 32 && nc == 64) conv_tile_t<32, 64>(a, st);
+  else if (kc == 64 && nc == 64) conv_tile_t<64, 64>(a, st);
+  else if (kc == 64 && nc == 32) conv_tile_t<64, 32>(a, st);
+  else if (kc == 32 && nc == 16) conv_tile_t<32, 16>(a, st);
+  else return MAC_ERR_INVALID;
+  return MAC_OK;
+}
+
 template <int MODE>
 static int conv_mode(int kc, int nc, const ConvArgs& a, cudaStream_t st) {
   if (kc == 16 && nc == 16) conv_t<16, 16, MODE>(a, st);
@@ -868,6 +1036,7 @@ struct Net {
   double* loss_hist = nullptr;
   int loss_cap = 0;
   long launches = 0;
+  int staged_conv = 1;  // forward 3x3x3 convolutions through k_conv_tile (0: k_conv)
 };
 
 static size_t level_vox(const Net& t, int l) {
@@ -953,6 +1122,7 @@ static int fwd(Net& t, int l, int lvl, Src s1, Src s2, bf16* dst, float* f32, cu
   a.f32 = f32;
   a.relu = kLayers[l].relu;
   ++t.launches;
+  if (t.staged_conv && a.taps == 27) return conv_tile(kLayers[l].cin, kLayers[l].cout, a, st);
   return conv_mode<0>(kLayers[l].cin, kLayers[l].cout, a, st);
 }
 
@@ -1499,6 +1669,13 @@ int mac_unet_train(void* net, int steps, int batch, float lr, uint64_t seed, flo
   if (!t) return MAC_ERR_INVALID;
   cudaSetDevice(t->device);
   return mac::unet::train(*t, steps, batch, lr, seed, losses, 0);
+}
+
+int mac_unet_set_conv(void* net, int staged) {
+  Net* t = (Net*)net;
+  if (!t || (staged != 0 && staged != 1)) return MAC_ERR_INVALID;
+  t->staged_conv = staged;
+  return MAC_OK;
 }
 
 int mac_unet_time_forward(void* net, int n, int d, int h, int w, int reps, double* ms, double* flops) {

@@ -69,7 +69,8 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
            "mac_unet_make_dataset", "mac_unet_make_dataset_ext", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
-           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_set_smoother", "mac_unet_set_loss", "mac_unet_time_forward"]
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_set_smoother", "mac_unet_set_loss", "mac_unet_time_forward",
+           "mac_unet_set_conv"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
 
@@ -140,6 +141,7 @@ def load(path: str = LIB_PATH):
     lib.mac_set_smoother.argtypes = [vp, f64, f64, f64, f64]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
     lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
+    lib.mac_unet_set_conv.argtypes = [vp, i32]
     _lib = lib
     return lib
 

@@ -55,6 +55,10 @@ class UNet:
         self._check(self.lib.mac_unet_set_params(self.h, p.ctypes.data_as(_P(ctypes.c_float)), float(tscale)),
                     "mac_unet_set_params")
 
+    def set_conv(self, staged=True):
+        """Forward 3x3x3 convolutions through the staged-tile kernel (True) or the per-tap gather."""
+        self._check(self.lib.mac_unet_set_conv(self.h, 1 if staged else 0), "mac_unet_set_conv")
+
     def forward(self, r, mask):
         r = _f32(r)
         m = np.ascontiguousarray(mask, dtype=np.int8)

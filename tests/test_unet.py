@@ -193,3 +193,34 @@ def test_training_lowers_the_loss(unet):
     losses = unet.train(80, batch=8, lr=1e-3, seed=9)
     assert np.all(np.isfinite(losses))
     assert losses[-10:].mean() < 0.8 * losses[:10].mean(), (losses[:10].mean(), losses[-10:].mean())
+
+
+def _box_problem(n, d, h, w, seed):
+    rng = np.random.default_rng(seed)
+    m = np.where(rng.random((n, d, h, w)) < 0.7, 1, 0).astype(np.int8)
+    m[:, :, :2, :] = -1
+    r = np.where(m == 1, rng.standard_normal((n, d, h, w)), 0.0).astype(np.float32)
+    return r, m
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(2, 16, 16, 16), (1, 12, 20, 28), (1, 8, 36, 44), (1, 64, 64, 64)])
+def test_staged_tile_forward_matches_per_tap_gather(unet, shape):
+    """The forward pass with its 3x3x3 convolutions on the staged-tile kernel
+    (one input box per 8 x 16 x 1 tile, taps as descriptor offsets) against the
+    per-tap gather kernel: the same accumulation order, so the same output,
+    on grids whose quarter-resolution levels leave partial tiles; and both
+    within the oracle's tolerance."""
+    p = _random_params(31).astype(np.float32)
+    unet.set_params(p, 0.5)
+    r, m = _box_problem(*shape, seed=32)
+    try:
+        unet.set_conv(False)
+        ref = unet.forward(r, m)
+    finally:
+        unet.set_conv(True)
+    got = unet.forward(r, m)
+    assert np.array_equal(got, ref), _rel(got, ref)
+    if shape[1] <= 16:
+        want = U.Net(p, 0.5).correction(r, m)
+        assert _rel(got, want) <= 2e-2, _rel(got, want)
