@@ -328,7 +328,8 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch);
  * over-weights them). Two sweeps damp an error component of eigenvalue lambda
  * of D^-1 A (in (0, 2]) by (1 - w1 lambda)(1 - w2 lambda); weights for which
  * that leaves (-1, 1) anywhere on (0, 2] are refused (MAC_ERR_INVALID), as they
- * would break the preconditioner's definiteness. Defaults 0.9, 0.9, 0.9, 0.6. */
+ * would break the preconditioner's definiteness. Defaults 0.5711, 1.8216 (the
+ * reciprocals of the degree-2 Chebyshev roots on [0.3, 2]), 0.9, 0.6. */
 int mac_set_smoother(void* ctx, double w1, double w2, double w_single, double coarse_scale);
 
 /* ---- allocation-free CSC solve (no counterpart in the reference) ----

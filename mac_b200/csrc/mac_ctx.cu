@@ -230,7 +230,12 @@ static int create(const mac_params* p, Ctx** out) {
         double d = ax * c->dp.ih2[0] + ay * c->dp.ih2[1] + az * c->dp.ih2[2];
         c->dp.dtab[ax + 3 * ay + 9 * az] = d > 0 ? 1.0 / d : 0.0;
       }
-  c->dp.mgw1 = c->dp.mgw2 = 0.9;  // multigrid smoother (mac_set_smoother)
+  // multigrid smoother (mac_set_smoother): the two sweep weights are the
+  // reciprocals of the degree-2 Chebyshev roots on [0.3, 2] (the spectrum of
+  // D^-1 A lies in (0, 2]); they took the 256^3 pool at 1e-8 from 17 to 15
+  // CG iterations against two sweeps at 0.9
+  c->dp.mgw1 = 0.5711;
+  c->dp.mgw2 = 1.8216;
   c->dp.mgws = 0.9;
   c->dp.cfl = p->cfl_factor;
   c->dp.dt_min = p->dt_min;

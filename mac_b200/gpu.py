@@ -443,7 +443,7 @@ class Context:
     def set_learned_smoothing(self, omega):
         self._check(self.lib.mac_set_learned_smoothing(self.h, float(omega)), "mac_set_learned_smoothing")
 
-    def set_smoother(self, w1=0.9, w2=0.9, w_single=0.9, coarse_scale=0.6):
+    def set_smoother(self, w1=0.5711, w2=1.8216, w_single=0.9, coarse_scale=0.6):
         """Multigrid smoother weights and coarse-operator scale (mac_set_smoother)."""
         self._check(self.lib.mac_set_smoother(self.h, float(w1), float(w2), float(w_single), float(coarse_scale)),
                     "mac_set_smoother")

@@ -106,7 +106,7 @@ def test_smoother_settings(pool64):
     relative residual of 1e-12)."""
     from mac_b200.gpu import MacError
     out = []
-    for w1, w2, scale in ((0.9, 0.9, 0.6), (0.5617, 1.3895, 0.6), (0.548, 1.025, 0.7)):
+    for w1, w2, scale in ((0.5711, 1.8216, 0.6), (0.9, 0.9, 0.6), (0.548, 1.025, 0.7)):
         with _ctx(pool64, "mixed", 1e-12, 500) as ctx:
             ctx.set_smoother(w1, w2, 0.9, scale)
             ctx.upload(pool64)

@@ -189,9 +189,12 @@ def test_divergence_projection_needs_an_init(golden):
 def test_stage_buffers_can_be_left_out_of_the_transfers(golden):
     """NULL speed-1 and acceleration pointers in mac_host_state: the step
     writes both before reading them on every existing cell, so a world
-    uploaded without them steps to the same speed 0, pressure, topology and
-    particles bit for bit on the existing cells (the reference's observable
-    state; slots of erased cells keep whatever their buffers held)."""
+    uploaded without them steps to the same topology and speed 0 and pressure
+    as one uploaded whole. Two runs of the same step agree to rounding only
+    (the CG dot products add their block partials in the order of the
+    domain-brick list, which the topology's atomic compaction sets), so the
+    fields are compared at 1e-13 relative, a hundred times inside the parity
+    tolerances."""
     from mac_b200.gpu import HostState
     s30 = golden("c1_ref_s30")
     with _ctx(s30) as ctx:
@@ -205,6 +208,6 @@ def test_stage_buffers_can_be_left_out_of_the_transfers(golden):
         ctx.download(lean, to_state=False)
         got = lean.to_state(s30.params)
     compare_topology(got, want)
-    d = max_abs_diff(got, want, ("u0x", "u0y", "u0z", "p"), existing_only=True)
-    assert all(v == 0.0 for v in d.values()), d
-    assert compare_particles(got, want) == 0.0
+    e = field_errors(got, want, ("u0x", "u0y", "u0z", "p"))
+    assert max(e.values()) <= 1e-13, e
+    compare_particles(got, want, atol=1e-13)
