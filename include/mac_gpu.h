@@ -321,14 +321,20 @@ int mac_set_learned_smoothing(void* ctx, double omega);
  * vectors with asynchronous bulk copies; 0 (default, measured faster on the
  * 256^3 pool and the 256x256x512 jet) runs one block per brick. */
 int mac_set_multigrid(void* ctx, int sweeps0, int prefetch);
+/* Launch of the pressure solve's CG-loop kernels (the V-cycle, SpMV, vector
+ * updates and scalar finishers): on = 1 (default) launches each with
+ * programmatic stream serialisation, so its blocks are scheduled while the
+ * previous kernel drains and wait on the device for its completion; 0 uses
+ * plain stream order. The results are bit-identical either way. */
+int mac_set_dependent_launch(void* ctx, int on);
 /* The multigrid's smoother and coarse operators: weights w1, w2 of the two
  * Jacobi sweeps before and after each coarse correction (on every level), the
  * weight of the single finest-level sweep (mac_set_multigrid(ctx, 1, .)), and
  * the scale of the Galerkin coarse operators (piecewise-constant transfer
  * over-weights them). Two sweeps damp an error component of eigenvalue lambda
- * of D^-1 A (in (0, 2]) by (1 - w1 lambda)(1 - w2 lambda); weights for which
- * that leaves (-1, 1) anywhere on (0, 2] are refused (MAC_ERR_INVALID), as they
- * would break the preconditioner's definiteness. Defaults 0.5711, 1.8216 (the
+ * of D^-1 A (in (0, 2]) by (1 - w1 lambda)(1 - w2 lambda); weights outside
+ * (0, 4), or for which that leaves (-1, 1) anywhere on (0, 2], are refused
+ * (MAC_ERR_INVALID), as they would break the preconditioner's definiteness. Defaults 0.5711, 1.8216 (the
  * reciprocals of the degree-2 Chebyshev roots on [0.3, 2]), 0.9, 0.6. */
 int mac_set_smoother(void* ctx, double w1, double w2, double w_single, double coarse_scale);
 

@@ -196,8 +196,11 @@ struct Ctx {
   void* unet = nullptr;
   double* zold = nullptr;
   double learned_omega = 0.8;
-  int* dbl = nullptr;          // bricks holding an in-domain cell
+  int* dbl = nullptr;          // bricks holding an in-domain cell, by brick coordinates (x fastest)
   int ndom_host = 0;
+  int* dbl_map = nullptr;      // ordering scratch: one slot per brick of the domain's bounding box
+  int64_t dbl_map_n = 0;
+  int* dbl_cnt = nullptr;      // ordering scratch: per-block counts, then offsets
   DenseGrid g3{};
   DenseDesc dense[kMaxDense] = {};
   int ndense = 0;
@@ -229,6 +232,7 @@ struct Ctx {
   int* eb_work = nullptr;      // boundary-condition extrapolation: colour counts and cursors
   long long launches = 0;      // kernels launched by this context
   struct Prof* prof = nullptr; // per-phase event timing (null when off)
+  int pdl = 1;                 // CG-loop kernels launched with programmatic stream serialisation
 };
 
 void prof_begin(Ctx* c, int phase);
@@ -237,6 +241,40 @@ void prof_end(Ctx* c, int phase);
 // Every kernel launch is followed by MAC_COUNT(c) so the context can report
 // how many of its kernels ran (mac_launch_count).
 #define MAC_COUNT(ctx) (++(ctx)->launches)
+
+// ------------------------------------------------- programmatic dependent launch
+// The CG loop runs some twenty dependent kernels per iteration, many of them a
+// few microseconds long, so the gap between two of them (the next grid's
+// launch and its blocks' ramp-up after the previous grid's last block) is a
+// large part of the iteration. Launched with programmatic stream
+// serialisation, a kernel's blocks may be scheduled once every block of the
+// previous kernel has started (pdl_entry's trigger), and they wait in
+// griddepcontrol.wait until that kernel has completed and its writes are
+// visible. A kernel launched this way calls pdl_entry() as its first
+// statement, on every path: it reads nothing before the wait, and since each
+// kernel of the chain waits for its predecessor's completion before it can
+// complete itself, completion stays ordered along the whole stream. The wait
+// ends because the previous grid depends on nothing that comes after it.
+// Without the launch attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... P, class... A>
+inline void launch_k(const Ctx* c, void (*k)(P...), dim3 grid, dim3 block, size_t smem, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = c->pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+}
 
 // ---------------------------------------------------------------- helpers
 __host__ __device__ inline unsigned long long pack_key(int x, int y, int z) {

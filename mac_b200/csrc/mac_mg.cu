@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
                                               const double* __restrict__ p, const double* __restrict__ q,
                                               double* partial, const Scalars* ds, int update, T* __restrict__ e,
                                               Params P) {
+  pdl_entry();
   if (solve_done(&ds->done)) return;
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
@@ -141,6 +142,7 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P,
                                                    const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T res[kCells];
@@ -202,6 +204,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P,
                                                const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict
     const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
     const double* __restrict__ rin, double* __restrict__ rout, double* __restrict__ x, const double* __restrict__ p,
     const double* __restrict__ q, double* partial, const Scalars* ds, int update, T* __restrict__ r1, Params P) {
+  pdl_entry();
   if (solve_done(&ds->done)) return;
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];    // e = w D^-1 r of the brick and its face halo
@@ -348,6 +352,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
     const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
     const double* __restrict__ r, const T* __restrict__ e1, double* __restrict__ z, double* partial, Params P,
     const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];
@@ -454,6 +459,7 @@ __global__ void __launch_bounds__(kBT) k0_head_bulk(const int* __restrict__ dbl,
                                                     const double* __restrict__ p, const double* __restrict__ q,
                                                     double* partial, Scalars* ds, int update, T* __restrict__ e,
                                                     T* __restrict__ r1, Params P) {
+  pdl_entry();
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ int64_t sb[6];
   __shared__ __align__(8) uint64_t full[2];
@@ -686,6 +692,7 @@ template <class T, int D>
 __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
                                               T* __restrict__ e, T w1, T w2, const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
@@ -743,6 +750,7 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
                                                    const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                    const T* __restrict__ r, const T* __restrict__ e, T* __restrict__ rc,
                                                    DenseGrid g3, const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   constexpr int H = D / 2;
   constexpr int N = D * D * D;
@@ -783,6 +791,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
                                                  const T* __restrict__ r, const T* __restrict__ e,
                                                  const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3,
                                                  T om, const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   constexpr int N = D * D * D;
   constexpr int H = D / 2;
@@ -885,6 +894,7 @@ __device__ inline T dense_apply(const DView<T>& L, const T* e, int64_t i, int x,
 // Device-wide dense kernels for level 3.
 template <class T>
 __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
@@ -914,6 +924,7 @@ __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
 // One thread per (coarse cell, child), the 8 children on adjacent lanes.
 template <class T>
 __global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t I = g >> 3;
@@ -935,6 +946,7 @@ __global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ 
 template <class T, bool WITH_COARSE>
 __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__ eout, DView<T> C,
                           const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
@@ -1144,6 +1156,7 @@ template <class T>
 __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem, const double* __restrict__ inv,
                                                         const int* __restrict__ inv_ok,
                                                         const int32_t* __restrict__ done) {
+  pdl_entry();
   if (solve_done(done)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // Level descriptors live in shared memory (one copy per block); which of a
@@ -1462,18 +1475,18 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
       const int g = nd < c->bulk_grid ? nd : c->bulk_grid;
       c->npart_head = g;
       if (one)
-        k0_head_bulk<T, true><<<g, kBT, bulk_smem<T>(), st>>>(c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd,
-                                                             c->q, c->partial, c->ds, update, e0, r1, c->dp);
+        launch_k(c, k0_head_bulk<T, true>, g, kBT, bulk_smem<T>(), c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd,
+                 c->q, c->partial, c->ds, update, e0, r1, c->dp);
       else
-        k0_head_bulk<T, false><<<g, kBT, bulk_smem<T>(), st>>>(c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x,
-                                                              c->pd, c->q, c->partial, c->ds, update, e0, r1, c->dp);
+        launch_k(c, k0_head_bulk<T, false>, g, kBT, bulk_smem<T>(), c->dbl, nd, c->nbr, c->fmask, c->r, c->r2, c->x,
+                 c->pd, c->q, c->partial, c->ds, update, e0, r1, c->dp);
       MAC_COUNT(c);
     } else if (one) {
-      k0_pre_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
-                                             c->ds, update, r1, c->dp); MAC_COUNT(c);
+      launch_k(c, k0_pre_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
+               c->ds, update, r1, c->dp); MAC_COUNT(c);
     } else {
-      k0_pre<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
-                                    update, e0, c->dp); MAC_COUNT(c);
+      launch_k(c, k0_pre<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
+               update, e0, c->dp); MAC_COUNT(c);
     }
     if (update) {
       std::swap(c->r, c->r2);
@@ -1482,51 +1495,51 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   }
   if (!(part & 2)) return;
   if (!one) {
-    k0_restrict<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
+    launch_k(c, k0_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
   }
   const T sw1 = (T)c->dp.mgw1, sw2 = (T)c->dp.mgw2;
-  kl_pre<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
-  kl_restrict<T, 4><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
-  kl_pre<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
-  kl_restrict<T, 2><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
     DView<T> d4 = dview<T>(c, 1);
-    kd_pre<T><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, dn); MAC_COUNT(c);
-    kd_restrict<T><<<grid_for(8 * d4.n, 256), 256, 0, st>>>(d3, d4, dn); MAC_COUNT(c);
+    launch_k(c, kd_pre<T>, grid_for(d3.n, 256), 256, 0, d3, dn); MAC_COUNT(c);
+    launch_k(c, kd_restrict<T>, grid_for(8 * d4.n, 256), 256, 0, d3, d4, dn); MAC_COUNT(c);
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
     S.lo = 1;
     S.hi = c->ndense;
     int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
-    kd_coarse_block<T><<<1, 1024, use_smem ? c->dense_smem : 0, st>>>(S, use_smem, c->coarse_inv, c->coarse_ok,
-                                                                      dn); MAC_COUNT(c);
-    kd_jacobi<T, true><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
-    kd_jacobi<T, false><<<grid_for(d3.n, 256), 256, 0, st>>>(d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
+    launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv, c->coarse_ok,
+             dn); MAC_COUNT(c);
+    launch_k(c, kd_jacobi<T, true>, grid_for(d3.n, 256), 256, 0, d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
+    launch_k(c, kd_jacobi<T, false>, grid_for(d3.n, 256), 256, 0, d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
   } else {
     DenseSet<T> S;
     S.L[0] = d3;
     S.lo = 0;
     S.hi = 1;
-    kd_coarse_block<T><<<1, 1024, 0, st>>>(S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
+    launch_k(c, kd_coarse_block<T>, 1, 1024, 0, S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
   // up
-  kl_jacobi<T, 2, true><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
-                                            dn); MAC_COUNT(c);
-  kl_jacobi<T, 2, false><<<g2, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
-                                             sw2, dn); MAC_COUNT(c);
-  kl_jacobi<T, 4, true><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
-                                            dn); MAC_COUNT(c);
-  kl_jacobi<T, 4, false><<<g1, 256, 0, st>>>(c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
-                                             sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
+           dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
+           sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 4, true>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
+           dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
+           sw2, dn); MAC_COUNT(c);
   if (one) {
-    k0_post_one<T><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
+    launch_k(c, k0_post_one<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
     return;
   }
-  k0_post<T, true><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
-                                       dn); MAC_COUNT(c);
-  k0_post<T, false><<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
-                                        c->dp, dn); MAC_COUNT(c);
+  launch_k(c, k0_post<T, true>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
+           dn); MAC_COUNT(c);
+  launch_k(c, k0_post<T, false>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
+           c->dp, dn); MAC_COUNT(c);
 }
 
 void mg_vcycle(Ctx* c, int update, int part) {

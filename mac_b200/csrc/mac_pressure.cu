@@ -73,6 +73,7 @@ int alloc_solver(Ctx* c) {
 void free_solver(Ctx* c) {
   cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->r2); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
+  cudaFree(c->dbl_map); cudaFree(c->dbl_cnt);
   cudaFree(c->zold);
   cudaFree(c->coarse_inv);
   cudaFree(c->coarse_ok);
@@ -177,6 +178,104 @@ __global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ blist, co
     }
   }
   (void)cnt;
+}
+
+// ------------------------------------------------ canonical domain-brick order
+// k_fmask appends the domain bricks in whatever order its blocks finish, and
+// the CG adds its per-block partial sums in the order of that list, so without
+// a fixed order two runs of the same step differ in the last bits. The list is
+// rewritten in the order of the bricks' coordinates (x fastest, then y, z):
+// each brick is scattered to its slot in the bounding box (no two share one),
+// and the occupied slots are compacted in slot order.
+constexpr int kOrderBlock = 1024;
+constexpr int64_t kOrderMaxSlots = (int64_t)1 << 26;  // larger boxes keep the appended order
+
+__global__ void k_order_scatter(const int* __restrict__ dbl, int nd, const int* __restrict__ bkey, DenseGrid g,
+                                int* __restrict__ map) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  int b = dbl[i];
+  map[g.index(bkey[3 * b], bkey[3 * b + 1], bkey[3 * b + 2])] = b;
+}
+
+__global__ void __launch_bounds__(kOrderBlock) k_order_count(const int* __restrict__ map, int64_t n,
+                                                             int* __restrict__ cnt) {
+  int64_t i = (int64_t)blockIdx.x * kOrderBlock + threadIdx.x;
+  int k = __syncthreads_count(i < n && map[i] >= 0);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = k;
+}
+
+// Exclusive prefix sum of nb block counts in place, one block: each thread
+// sums a contiguous run, the run totals are scanned through shared memory.
+__global__ void __launch_bounds__(kOrderBlock) k_order_scan(int* cnt, int nb) {
+  __shared__ int tot[kOrderBlock];
+  const int per = (nb + kOrderBlock - 1) / kOrderBlock;
+  const int lo = threadIdx.x * per, hi = min(nb, lo + per);
+  int s = 0;
+  for (int j = lo; j < hi; ++j) s += cnt[j];
+  tot[threadIdx.x] = s;
+  __syncthreads();
+  for (int d = 1; d < kOrderBlock; d <<= 1) {
+    int v = threadIdx.x >= d ? tot[threadIdx.x - d] : 0;
+    __syncthreads();
+    tot[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = tot[threadIdx.x] - s;
+  for (int j = lo; j < hi; ++j) {
+    int v = cnt[j];
+    cnt[j] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(kOrderBlock) k_order_write(const int* __restrict__ map, int64_t n,
+                                                             const int* __restrict__ off, int* __restrict__ dbl) {
+  __shared__ int wsum[kOrderBlock / 32];
+  int64_t i = (int64_t)blockIdx.x * kOrderBlock + threadIdx.x;
+  int b = i < n ? map[i] : -1;
+  unsigned bal = __ballot_sync(0xffffffffu, b >= 0);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(bal);
+  __syncthreads();
+  int before = 0;
+  for (int k = 0; k < w; ++k) before += wsum[k];
+  if (b >= 0) dbl[off[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = b;
+}
+
+static int order_domain_bricks(Ctx* c) {
+  const int* bb = c->hs->bbox;
+  const int nd = c->ndom_host;
+  if (nd <= 1) return MAC_OK;
+  DenseGrid g;
+  g.x0 = bb[0];
+  g.y0 = bb[1];
+  g.z0 = bb[2];
+  g.nx = bb[3] - bb[0] + 1;
+  g.ny = bb[4] - bb[1] + 1;
+  g.nz = bb[5] - bb[2] + 1;
+  const int64_t n = (int64_t)g.nx * g.ny * g.nz;
+  if (g.nx < 1 || g.ny < 1 || g.nz < 1 || n > kOrderMaxSlots) return MAC_OK;
+  const int64_t nb = (n + kOrderBlock - 1) / kOrderBlock;
+  if (n > c->dbl_map_n) {
+    cudaFree(c->dbl_map);
+    cudaFree(c->dbl_cnt);
+    c->dbl_map = nullptr;
+    c->dbl_cnt = nullptr;
+    c->dbl_map_n = 0;
+    int rc = check(cudaMalloc((void**)&c->dbl_map, sizeof(int) * n));
+    if (!rc) rc = check(cudaMalloc((void**)&c->dbl_cnt, sizeof(int) * nb));
+    if (rc) return rc;
+    c->dbl_map_n = n;
+  }
+  cudaStream_t st = c->stream;
+  int rc = check(cudaMemsetAsync(c->dbl_map, 0xff, sizeof(int) * n, st));
+  if (rc) return rc;
+  k_order_scatter<<<(nd + 255) / 256, 256, 0, st>>>(c->dbl, nd, c->bkey, g, c->dbl_map); MAC_COUNT(c);
+  k_order_count<<<(unsigned)nb, kOrderBlock, 0, st>>>(c->dbl_map, n, c->dbl_cnt); MAC_COUNT(c);
+  k_order_scan<<<1, kOrderBlock, 0, st>>>(c->dbl_cnt, (int)nb); MAC_COUNT(c);
+  k_order_write<<<(unsigned)nb, kOrderBlock, 0, st>>>(c->dbl_map, n, c->dbl_cnt, c->dbl); MAC_COUNT(c);
+  return check(cudaGetLastError());
 }
 
 __global__ void k_setup_reset(Scalars* ds) {
@@ -331,6 +430,7 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
                                                      const double* __restrict__ pold, double* __restrict__ pnew,
                                                      double* __restrict__ q, double* partial, Params P,
                                                      const Scalars* ds, int first) {
+  pdl_entry();
   if (ds->done) return;
   __shared__ int64_t sb[6];
   __shared__ double sp[kS1];  // the new direction on the brick and its face halo
@@ -381,6 +481,7 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
 }
 
 __global__ void k_fin_alpha(const double* partial, int nblk, Scalars* ds) {
+  pdl_entry();
   if (ds->done) return;
   double pq, unused;
   sum_partials(partial, nblk, &pq, &unused);
@@ -394,6 +495,7 @@ __global__ void k_fin_alpha(const double* partial, int nblk, Scalars* ds) {
 __global__ void __launch_bounds__(512) k_axpy(const int* __restrict__ dbl, double* __restrict__ x,
                                               double* __restrict__ r, const double* __restrict__ p,
                                               const double* __restrict__ q, double* partial, const Scalars* ds) {
+  pdl_entry();
   if (ds->done) return;
   double a = ds->alpha;
   int64_t c = (int64_t)dbl[blockIdx.x] * kCells + threadIdx.x;
@@ -404,6 +506,7 @@ __global__ void __launch_bounds__(512) k_axpy(const int* __restrict__ dbl, doubl
 }
 
 __global__ void k_fin_rr(const double* partial, int nblk, Scalars* ds, double rtol2, int max_iters) {
+  pdl_entry();
   if (ds->done) return;
   double rr, unused;
   sum_partials(partial, nblk, &rr, &unused);
@@ -436,6 +539,7 @@ __global__ void k_fin_rr_initial(const double* partial, int nblk, Scalars* ds, d
 
 // beta = rz_new / rz
 __global__ void k_fin_beta(const double* partial, int nblk, Scalars* ds, int first) {
+  pdl_entry();
   if (ds->done) return;
   double rz, unused;
   sum_partials(partial, nblk, &rz, &unused);
@@ -449,6 +553,7 @@ __global__ void k_fin_beta(const double* partial, int nblk, Scalars* ds, int fir
 __global__ void __launch_bounds__(512) k_jacobi_prec(const int* __restrict__ dbl, const uint16_t* __restrict__ fmask,
                                                      const double* __restrict__ r, double* __restrict__ z,
                                                      double* partial, Params P) {
+  pdl_entry();
   int64_t c = (int64_t)dbl[blockIdx.x] * kCells + threadIdx.x;
   uint16_t m = fmask[c];
   double v = (m & kDomainBit) ? r[c] * P.dtab[active_index(m)] : 0.0;
@@ -655,6 +760,7 @@ int setup_system(Ctx* c) {
   if (rc) return rc;
   c->ndom_host = c->hs->ndom;
   c->stats.unknowns = c->hs->nunknown;
+  if ((rc = order_domain_bricks(c))) return rc;
   if (c->ndom_host > 0 && c->prm.solver != MAC_SOLVER_CG_FP64) {
     rc = mg_setup(c);
     if (rc) return rc;
@@ -666,7 +772,7 @@ int setup_system(Ctx* c) {
 
 static void precondition(Ctx* c) {
   if (c->prm.solver == MAC_SOLVER_CG_FP64) {
-    k_jacobi_prec<<<c->ndom_host, 512, 0, c->stream>>>(c->dbl, c->fmask, c->r, c->z, c->partial, c->dp); MAC_COUNT(c);
+    launch_k(c, k_jacobi_prec, c->ndom_host, 512, 0, c->dbl, c->fmask, c->r, c->z, c->partial, c->dp); MAC_COUNT(c);
   } else {
     mg_vcycle(c, 0, 3);
   }
@@ -675,8 +781,8 @@ static void precondition(Ctx* c) {
 // Convergence test after the update the V-cycle's first kernel applied (its
 // partial r.r are in c->partial).
 void cg_finish_update(Ctx* c) {
-  k_fin_rr<<<1, 1024, 0, c->stream>>>(c->partial, c->npart_head, c->ds, c->prm.rtol * c->prm.rtol,
-                                      c->prm.max_iters); MAC_COUNT(c);
+  launch_k(c, k_fin_rr, 1, 1024, 0, c->partial, c->npart_head, c->ds, c->prm.rtol * c->prm.rtol,
+           c->prm.max_iters); MAC_COUNT(c);
 }
 
 int project(Ctx* c, int ib) {
@@ -771,20 +877,20 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
       prof_end(c, PH_VCYCLE);
       prof_begin(c, PH_CGVEC);
       if (!learned) {
-        k_fin_beta<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, first); MAC_COUNT(c);
+        launch_k(c, k_fin_beta, 1, 1024, 0, c->partial, nd, c->ds, first); MAC_COUNT(c);
       }
       prof_end(c, PH_CGVEC);
       prof_begin(c, PH_SPMV);
       std::swap(c->pd, c->pd2);  // pd2: previous direction, pd: new one
-      k_update_spmv<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
-                                        first); MAC_COUNT(c);
+      launch_k(c, k_update_spmv, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
+               first); MAC_COUNT(c);
       prof_end(c, PH_SPMV);
       first = 0;
       prof_begin(c, PH_CGVEC);
-      k_fin_alpha<<<1, 1024, 0, st>>>(c->partial, nd, c->ds); MAC_COUNT(c);
+      launch_k(c, k_fin_alpha, 1, 1024, 0, c->partial, nd, c->ds); MAC_COUNT(c);
       if (!fold) {
-        k_axpy<<<nd, 512, 0, st>>>(c->dbl, c->x, c->r, c->pd, c->q, c->partial, c->ds); MAC_COUNT(c);
-        k_fin_rr<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2, c->prm.max_iters); MAC_COUNT(c);
+        launch_k(c, k_axpy, nd, 512, 0, c->dbl, c->x, c->r, c->pd, c->q, c->partial, c->ds); MAC_COUNT(c);
+        launch_k(c, k_fin_rr, 1, 1024, 0, c->partial, nd, c->ds, rtol2, c->prm.max_iters); MAC_COUNT(c);
       }
       prof_end(c, PH_CGVEC);
       if (fold) {

@@ -547,9 +547,16 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   return MAC_OK;
 }
 
+int mac_set_dependent_launch(void* ctx, int on) {
+  CTX_OR_FAIL();
+  if (on != 0 && on != 1) return MAC_ERR_INVALID;
+  c->pdl = on;
+  return MAC_OK;
+}
+
 int mac_set_smoother(void* ctx, double w1, double w2, double w_single, double coarse_scale) {
   CTX_OR_FAIL();
-  if (!(w1 > 0 && w1 < 2 && w2 > 0 && w2 < 2 && w_single > 0 && w_single < 1 && coarse_scale > 0 &&
+  if (!(w1 > 0 && w1 < 4 && w2 > 0 && w2 < 4 && w_single > 0 && w_single < 1 && coarse_scale > 0 &&
         coarse_scale <= 1))
     return MAC_ERR_INVALID;
   // two sweeps damp lambda in (0, 2] by (1 - w1 lambda)(1 - w2 lambda): keep it inside (-1, 1)

@@ -116,6 +116,7 @@ def test_smoother_settings(pool64):
     for its, p in out[1:]:
         assert np.linalg.norm(p - out[0][1]) / np.linalg.norm(out[0][1]) <= 1e-9
     with _ctx(pool64, "mixed", 1e-12, 500) as ctx:
-        for bad in ((1.2, 1.2, 0.9, 0.6), (0.9, 0.9, 1.0, 0.6), (0.9, 0.9, 0.9, 1.5), (0.0, 0.9, 0.9, 0.6)):
+        for bad in ((1.2, 1.2, 0.9, 0.6), (0.9, 0.9, 1.0, 0.6), (0.9, 0.9, 0.9, 1.5), (0.0, 0.9, 0.9, 0.6),
+                    (0.3, 4.0, 0.9, 0.6)):
             with pytest.raises(MacError):
                 ctx.set_smoother(*bad)
