@@ -448,8 +448,6 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         ctx.step()
     ctx.sync()
-    ctx.set_profiling(True)
-    ctx.profile()  # reset
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -474,12 +472,30 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     launches = ctx.launches() - l0
+    sec, total_fluid_steps = reduce_over_ranks(ms / 1e3, fluid_steps, f"cuda:{dev}")
+    value = total_fluid_steps / sec
+
+    # Per-phase times for the rooflines, from further steps of the same run
+    # with an event pair around each phase. The events sit between kernels the
+    # CG loop otherwise chains with programmatic dependent launches, so these
+    # steps run slightly slower than the timed ones: the phase figures are
+    # conservative.
+    prof_steps = max(1, min(args.steps, 5))
+    ctx.set_profiling(True)
+    ctx.profile()  # reset
+    it0 = ctx.stats()["total_iterations"]
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(prof_steps):
+        ctx.step()
+    p1.record(stream)
+    p1.synchronize()
+    prof_ms_per_step = p0.elapsed_time(p1) / prof_steps
     prof = ctx.profile()
     ctx.set_profiling(False)
     st = ctx.stats()
     cg_iterations = st["total_iterations"] - it0
-    sec, total_fluid_steps = reduce_over_ranks(ms / 1e3, fluid_steps, f"cuda:{dev}")
-    value = total_fluid_steps / sec
 
     # e2e through the C-ABI with pinned host buffers: upload, step, download per step
     nb, npart = ctx.sizes()
@@ -553,7 +569,8 @@ def run_ours(args, rank, world, local_rank):
                    "live_bricks": st["live_bricks"], "cg_iters_per_solve_last": st["iterations"],
                    "cg_iters_mean": float(np.mean(iters)) if iters else None},
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clk, "roofline": roofline,
-        "phases_ms": phases, "phase_rooflines": {k: {"gbs": round(v["gbs"], 1), "avg_ms": round(v["avg_ms"], 4)}
+        "phases_ms": phases, "phase_steps": prof_steps, "phase_ms_per_step": round(prof_ms_per_step, 3),
+        "phase_rooflines": {k: {"gbs": round(v["gbs"], 1), "avg_ms": round(v["avg_ms"], 4)}
                                                  for k, v in rl.items()},
     }
     ctx.close()
