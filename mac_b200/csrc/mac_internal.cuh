@@ -114,6 +114,15 @@ struct DenseGrid {
   __host__ __device__ int64_t index(int bx, int by, int bz) const {
     return (int64_t)(bx - x0) + (int64_t)nx * ((int64_t)(by - y0) + (int64_t)ny * (bz - z0));
   }
+  __host__ __device__ bool contains(int bx, int by, int bz) const {
+    return (unsigned)(bx - x0) < (unsigned)nx && (unsigned)(by - y0) < (unsigned)ny && (unsigned)(bz - z0) < (unsigned)nz;
+  }
+  // index of a brick's dense cell; 0 for a brick outside the box (a live
+  // brick without in-domain cells next to a domain brick: its value is read
+  // but enters nothing, since the face weight to it is zero)
+  __host__ __device__ int64_t index_or0(int bx, int by, int bz) const {
+    return contains(bx, by, bz) ? index(bx, by, bz) : 0;
+  }
 };
 
 constexpr int kMaxDense = 12;
@@ -192,6 +201,12 @@ struct Ctx {
   int mg_bulk = 0;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
   int bulk_grid = 0;          // its grid (blocks resident on all SMs at once)
   int npart_head = 0;         // partial sums the V-cycle's first kernel left (its grid)
+  int mg_fused = 1;           // levels 1-3 of the V-cycle in two cooperative kernels
+  int kc_blocks_per_sm = 0;   // their blocks per SM (0: as many as fit)
+  int kc_grid = 0;            // their grid for the current system (0: one kernel per phase)
+  int kc_per = 0;             // domain bricks per block
+  unsigned* kc_bar = nullptr; // their grid barrier: arrival count, generation
+  int nsm = 0;
   // learned preconditioner (flexible CG): the network and the previous z
   void* unet = nullptr;
   double* zold = nullptr;
