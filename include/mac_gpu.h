@@ -327,14 +327,6 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch);
  * previous kernel drains and wait on the device for its completion; 0 uses
  * plain stream order. The results are bit-identical either way. */
 int mac_set_dependent_launch(void* ctx, int on);
-/* The V-cycle's levels 1-3 (brick levels 1 and 2, the dense level 3): on = 1
- * (default) runs their sweeps, restrictions and prolongations as two
- * cooperative kernels with grid barriers between the phases, each block
- * keeping its domain bricks' tables in shared memory; 0 launches one kernel
- * per phase. blocks_per_sm: blocks of the cooperative kernels per SM, 1..8,
- * 0 (default) as many as fit. The results are bit-identical either way; a
- * grid barrier that waits too long ends the solve with MAC_ERR_TIMEOUT. */
-int mac_set_coarse_fusion(void* ctx, int on, int blocks_per_sm);
 /* The multigrid's smoother and coarse operators: weights w1, w2 of the two
  * Jacobi sweeps before and after each coarse correction (on every level), the
  * weight of the single finest-level sweep (mac_set_multigrid(ctx, 1, .)), and

@@ -201,12 +201,6 @@ struct Ctx {
   int mg_bulk = 0;            // 1: the V-cycle's first kernel prefetches bricks with cp.async.bulk
   int bulk_grid = 0;          // its grid (blocks resident on all SMs at once)
   int npart_head = 0;         // partial sums the V-cycle's first kernel left (its grid)
-  int mg_fused = 1;           // levels 1-3 of the V-cycle in two cooperative kernels
-  int kc_blocks_per_sm = 0;   // their blocks per SM (0: as many as fit)
-  int kc_grid = 0;            // their grid for the current system (0: one kernel per phase)
-  int kc_per = 0;             // domain bricks per block
-  unsigned* kc_bar = nullptr; // their grid barrier: arrival count, generation
-  int nsm = 0;
   // learned preconditioner (flexible CG): the network and the previous z
   void* unet = nullptr;
   double* zold = nullptr;

@@ -1241,420 +1241,6 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
   if (use_smem || cur(lo) != G.L[lo].e) blk_copy(G.L[lo].e, cur(lo), SL[lo].n);
 }
 
-// ---------------------------------------- levels 1-3 in two cooperative kernels
-// The coarse part of a V-cycle is a dozen sweeps, restrictions and
-// prolongations over a few hundred thousand values each. As separate kernels
-// each costs its grid's launch and ramp-up plus a chain of dependent loads
-// (domain list -> brick table -> data) before any arithmetic: 5-17 us apiece
-// for a few microseconds of memory traffic. kc_down (levels 1 and 2 pre-smoothed
-// and restricted, level 3 likewise when the block solve starts at level 4) and
-// kc_up (the matching post-sweeps with their prolongations) run the same
-// phases as resident blocks separated by grid barriers: each block owns a
-// fixed run of domain bricks, reads their brick tables into shared memory once
-// and keeps them for every phase. Each phase computes exactly what the
-// separate kernel computes for the same cells, in the same operation order,
-// so the result is bit-identical to the unfused V-cycle.
-
-// Grid barrier for a cooperative launch (every block resident). Thread 0 of
-// each block arrives with a release fence; the last arrival resets the count
-// and advances the generation; the others poll it with acquire loads, at
-// most kBarPolls times, after which they record kErrTimeout and set the
-// solve's done flag, so every later kernel of the solve returns at once and
-// the solve reports MAC_ERR_TIMEOUT instead of hanging.
-struct GridBar {
-  unsigned count;
-  unsigned gen;
-};
-constexpr long long kBarPolls = 1ll << 22;  // ~0.3 s with the 64 ns sleep between polls
-
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__device__ inline void grid_bar(GridBar* gb, int* err, int32_t* stop) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned g = ld_acquire_gpu(&gb->gen);
-    __threadfence();
-    if (atomicAdd(&gb->count, 1u) == gridDim.x - 1) {
-      atomicExch(&gb->count, 0u);
-      __threadfence();
-      st_release_gpu(&gb->gen, g + 1);
-    } else {
-      long long k = 0;
-      while (ld_acquire_gpu(&gb->gen) == g) {
-        if (++k > kBarPolls) {
-          atomicOr(err, kErrTimeout);
-          atomicExch(stop, 1);
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-}
-
-template <class T>
-struct CoarseArgs {
-  const int* dbl;
-  int nd;
-  int per;  // domain bricks per block
-  const int* nbr;
-  const int* bkey;
-  const T* w1;
-  const T* w2;
-  size_t ncap1, ncap2;
-  T *r1, *e1, *e1b, *r2, *e2, *e2b;
-  DView<T> d3, d4;
-  int dense;  // levels 3 (and 4 in the block solve) dense: level 3 smoothed here
-  DenseGrid g3;
-  T sw1, sw2;
-  const int32_t* done;
-  int32_t* stop;  // the same flag, set when a barrier wait runs out
-  GridBar* bar;
-  int* err;
-};
-
-// The block's brick tables: tab[7 j + k] as load_lbricks, for the block's
-// bricks j = 0 .. per-1 (domain-list positions blockIdx.x * per + j); sdi the
-// dense level-3 index of each table brick.
-template <class T>
-__device__ inline int kc_load_tables(const CoarseArgs<T>& A, int* tab, int64_t* sdi) {
-  const int j0 = blockIdx.x * A.per;
-  const int nown = max(0, min(A.per, A.nd - j0));
-  for (int t = threadIdx.x; t < 7 * nown; t += blockDim.x) {
-    const int j = t / 7, k = t - 7 * j;
-    const int b = A.dbl[j0 + j];
-    int v;
-    if (k == 0) {
-      v = b;
-    } else {
-      const int f = k - 1, d = (f & 1) ? 1 : -1, ax = f >> 1;
-      v = A.nbr[(size_t)b * kNbr + nbr_index(ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0)];
-    }
-    tab[t] = v;
-    sdi[t] = v < 0 ? 0 : A.g3.index_or0(A.bkey[3 * v], A.bkey[3 * v + 1], A.bkey[3 * v + 2]);
-  }
-  return nown;
-}
-
-// kl_pre's cell computation (two sweeps from zero) at cell o of table brick sb.
-template <class T, int D>
-__device__ inline void kc_pre_cell(const int* sb, int o, const T* __restrict__ w, size_t ncap,
-                                   const T* __restrict__ r, T* __restrict__ e, T w1, T w2) {
-  constexpr int N = D * D * D;
-  const int b = sb[0];
-  const size_t i = (size_t)b * N + o;
-  const T dinv = w[4 * ncap + i];
-  if (dinv == 0) {
-    e[i] = (T)0;
-    return;
-  }
-  const int x = o % D, y = (o / D) % D, z = o / (D * D);
-  int64_t n[6];
-  lnbrs<D>(sb, x, y, z, n);
-  T wl[3], wr[3], dl[3], dr[3], rl[3], rr[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
-    const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
-    wl[a] = w[a * ncap + i];
-    dl[a] = w[4 * ncap + jl];
-    rl[a] = r[jl];
-    wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr];
-    dr[a] = w[4 * ncap + jr];
-    rr[a] = r[jr];
-  }
-  T s = 0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (wl[a] != 0) s += wl[a] * w1 * dl[a] * rl[a];
-    if (wr[a] != 0) s += wr[a] * w1 * dr[a] * rr[a];
-  }
-  e[i] = dinv * ((w1 + w2 - w1 * w2) * r[i] + w2 * s);
-}
-
-template <class T, int D>
-__device__ inline void kc_pre(const int* tab, int nown, const T* __restrict__ w, size_t ncap,
-                              const T* __restrict__ r, T* __restrict__ e, T w1, T w2) {
-  constexpr int N = D * D * D;
-  for (int t = threadIdx.x; t < nown * N; t += blockDim.x)
-    kc_pre_cell<T, D>(tab + 7 * (t / N), t % N, w, ncap, r, e, w1, w2);
-}
-
-// kl_restrict's computation over the block's bricks (8 children of a coarse
-// cell on 8 adjacent lanes; every lane of a warp runs the same trip count).
-template <class T, int D>
-__device__ inline void kc_restrict(const int* tab, const int64_t* sdi, int nown, const T* __restrict__ w,
-                                   size_t ncap, const T* __restrict__ r, const T* __restrict__ e,
-                                   T* __restrict__ rc) {
-  constexpr int H = D / 2;
-  constexpr int N = D * D * D;
-  const int total = nown * N;
-  const int span = (total + 31) & ~31;
-  for (int t = threadIdx.x; t < span; t += blockDim.x) {
-    const bool live = t < total;
-    T v = 0;
-    int p = 0;
-    const int* sb = tab + 7 * (live ? t / N : 0);
-    if (live) {
-      const int b = sb[0];
-      const int o = t % N;
-      p = o >> 3;
-      const int k = o & 7;
-      const int X = p % H, Y = (p / H) % H, Z = p / (H * H);
-      const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-      const size_t i = (size_t)b * N + x + D * y + D * D * z;
-      if (w[4 * ncap + i] != 0) {
-        int64_t n[6];
-        lnbrs<D>(sb, x, y, z, n);
-        v = r[i] - apply_l<T, D>(e, w, ncap, n, i, e[i]);
-      }
-    }
-    v = sum8(v);
-    if (live && (t & 7) == 0) {
-      if (D == 2) rc[sdi[7 * (t / N)]] = (T)v;
-      else rc[(size_t)sb[0] * H * H * H + p] = (T)v;
-    }
-  }
-}
-
-// kl_jacobi's computation at cell o of table brick j.
-template <class T, int D, bool WITH_COARSE>
-__device__ inline void kc_jacobi_cell(const int* sb, const int64_t* sd, int o, const T* __restrict__ w,
-                                      size_t ncap, const T* __restrict__ r, const T* __restrict__ e,
-                                      const T* __restrict__ ec, T* __restrict__ eout, T om) {
-  constexpr int N = D * D * D;
-  constexpr int H = D / 2;
-  const int b = sb[0];
-  const size_t i = (size_t)b * N + o;
-  const T dinv = w[4 * ncap + i];
-  if (dinv == 0) {
-    eout[i] = (T)0;
-    return;
-  }
-  const int x = o % D, y = (o / D) % D, z = o / (D * D);
-  auto ev = [&](int k, int lx, int ly, int lz) -> T {
-    const int nb = sb[k];
-    T v = e[(size_t)nb * N + lx + D * ly + D * D * lz];
-    if (WITH_COARSE) {
-      if (D == 2) v += ec[sd[k]];
-      else v += ec[(size_t)nb * H * H * H + (lx >> 1) + H * (ly >> 1) + H * H * (lz >> 1)];
-    }
-    return v;
-  };
-  T wl[3], wr[3], vl[3], vr[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const int c[3] = {x, y, z};
-    int pl[3] = {x, y, z}, pr[3] = {x, y, z};
-    int kl = 0, kr = 0;
-    if (c[a] > 0) pl[a] = c[a] - 1;
-    else { kl = 1 + 2 * a; pl[a] = D - 1; }
-    if (c[a] < D - 1) pr[a] = c[a] + 1;
-    else { kr = 2 + 2 * a; pr[a] = 0; }
-    const bool hl = sb[kl] >= 0, hr = sb[kr] >= 0;
-    if (!hl) { kl = 0; pl[0] = x; pl[1] = y; pl[2] = z; }
-    if (!hr) { kr = 0; pr[0] = x; pr[1] = y; pr[2] = z; }
-    wl[a] = w[a * ncap + i];
-    vl[a] = ev(kl, pl[0], pl[1], pl[2]);
-    wr[a] = hr ? w[a * ncap + (size_t)sb[kr] * N + pr[0] + D * pr[1] + D * D * pr[2]] : (T)0;
-    vr[a] = ev(kr, pr[0], pr[1], pr[2]);
-  }
-  const T ecc = ev(0, x, y, z);
-  T s = w[3 * ncap + i] * ecc;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (wl[a] != 0) s -= wl[a] * vl[a];
-    if (wr[a] != 0) s -= wr[a] * vr[a];
-  }
-  eout[i] = ecc + om * dinv * (r[i] - s);
-}
-
-template <class T, int D, bool WITH_COARSE>
-__device__ inline void kc_jacobi(const int* tab, const int64_t* sdi, int nown, const T* __restrict__ w,
-                                 size_t ncap, const T* __restrict__ r, const T* __restrict__ e,
-                                 const T* __restrict__ ec, T* __restrict__ eout, T om) {
-  constexpr int N = D * D * D;
-  for (int t = threadIdx.x; t < nown * N; t += blockDim.x) {
-    const int j = t / N;
-    kc_jacobi_cell<T, D, WITH_COARSE>(tab + 7 * j, sdi + 7 * j, t % N, w, ncap, r, e, ec, eout, om);
-  }
-}
-
-// The dense level-3 kernels' computations, grid-strided.
-template <class T>
-__device__ inline void kc_dense_pre(const DView<T>& L) {
-  const int64_t n = L.n;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const T dinv = L.w[4 * n + i];
-    if (dinv == 0) {
-      L.e[i] = (T)0;
-      continue;
-    }
-    int x, y, z;
-    coords3(i, L.nx, L.ny, L.n, x, y, z);
-    const int c[3] = {x, y, z};
-    const int dim[3] = {L.nx, L.ny, L.nz};
-    const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-    T s = 0;
-    for (int a = 0; a < 3; ++a) {
-      T wl = L.w[a * n + i];
-      if (wl != 0 && c[a] > 0) s += wl * L.w1 * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
-      if (c[a] + 1 < dim[a]) {
-        T wr = L.w[a * n + i + stride[a]];
-        if (wr != 0) s += wr * L.w1 * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
-      }
-    }
-    L.e[i] = dinv * ((L.w1 + L.w2 - L.w1 * L.w2) * L.r[i] + L.w2 * s);
-  }
-}
-
-template <class T>
-__device__ inline void kc_dense_restrict(const DView<T>& F, const DView<T>& C) {
-  const int64_t total = 8 * C.n, stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < total; g0 += stride) {
-    const int64_t g = g0 + threadIdx.x;
-    const int64_t I = g >> 3;
-    const int k = (int)(g & 7);
-    T s = 0;
-    if (I < C.n) {
-      int X, Y, Z;
-      coords3(I, C.nx, C.ny, C.n, X, Y, Z);
-      const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-      if (x < F.nx && y < F.ny && z < F.nz) {
-        const int64_t i = F.at(x, y, z);
-        if (F.w[4 * F.n + i] != 0) s = F.r[i] - dense_apply(F, F.e, i, x, y, z, F.e[i]);
-      }
-    }
-    s = sum8(s);
-    if (I < C.n && k == 0) C.r[I] = (T)s;
-  }
-}
-
-template <class T, bool WITH_COARSE>
-__device__ inline void kc_dense_jacobi(const DView<T>& L, const T* __restrict__ ein, T* __restrict__ eout,
-                                       const DView<T>& C) {
-  const int64_t n = L.n;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const T dinv = L.w[4 * n + i];
-    if (dinv == 0) {
-      eout[i] = (T)0;
-      continue;
-    }
-    int x, y, z;
-    coords3(i, L.nx, L.ny, L.n, x, y, z);
-    auto ev = [&](int64_t j, int xx, int yy, int zz) -> T {
-      T v = ein[j];
-      if (WITH_COARSE) v += C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
-      return v;
-    };
-    const int c[3] = {x, y, z};
-    const int dim[3] = {L.nx, L.ny, L.nz};
-    const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-    const T ec = ev(i, x, y, z);
-    T s = L.w[3 * n + i] * ec;
-    for (int a = 0; a < 3; ++a) {
-      int p[3] = {x, y, z};
-      T wl = L.w[a * n + i];
-      if (wl != 0 && c[a] > 0) {
-        p[a] = c[a] - 1;
-        s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
-      }
-      if (c[a] + 1 < dim[a]) {
-        T wr = L.w[a * n + i + stride[a]];
-        if (wr != 0) {
-          p[a] = c[a] + 1;
-          s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
-        }
-      }
-    }
-    eout[i] = ec + (WITH_COARSE ? L.w1 : L.w2) * dinv * (L.r[i] - s);
-  }
-}
-
-constexpr int kCoarseThreads = 256;
-
-// Down: level 1 pre-sweeps, restriction to level 2, level 2 pre-sweeps,
-// restriction to level 3 (dense), and with dense = 1 level 3's pre-sweeps and
-// restriction to level 4.
-template <class T>
-__global__ void __launch_bounds__(kCoarseThreads, 4) kc_down(CoarseArgs<T> A) {
-  if (solve_done(A.done)) return;  // set before this launch: the same in every block
-  extern __shared__ __align__(16) unsigned char kc_smem[];
-  int64_t* sdi = (int64_t*)kc_smem;
-  int* tab = (int*)(sdi + 7 * A.per);
-  const int nown = kc_load_tables(A, tab, sdi);
-  __syncthreads();
-  kc_pre<T, 4>(tab, nown, A.w1, A.ncap1, A.r1, A.e1, A.sw1, A.sw2);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_restrict<T, 4>(tab, sdi, nown, A.w1, A.ncap1, A.r1, A.e1, A.r2);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_pre<T, 2>(tab, nown, A.w2, A.ncap2, A.r2, A.e2, A.sw1, A.sw2);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_restrict<T, 2>(tab, sdi, nown, A.w2, A.ncap2, A.r2, A.e2, A.d3.r);
-  if (A.dense) {
-    grid_bar(A.bar, A.err, A.stop);
-    kc_dense_pre(A.d3);
-    grid_bar(A.bar, A.err, A.stop);
-    kc_dense_restrict(A.d3, A.d4);
-  }
-}
-
-// Up: with dense = 1 level 3's two post-sweeps (the first adding level 4's
-// correction), then level 2's (the first adding level 3's) and level 1's (the
-// first adding level 2's).
-template <class T>
-__global__ void __launch_bounds__(kCoarseThreads, 4) kc_up(CoarseArgs<T> A) {
-  if (solve_done(A.done)) return;
-  extern __shared__ __align__(16) unsigned char kc_smem[];
-  int64_t* sdi = (int64_t*)kc_smem;
-  int* tab = (int*)(sdi + 7 * A.per);
-  const int nown = kc_load_tables(A, tab, sdi);
-  __syncthreads();
-  if (A.dense) {
-    kc_dense_jacobi<T, true>(A.d3, A.d3.e, A.d3.e2, A.d4);
-    grid_bar(A.bar, A.err, A.stop);
-    kc_dense_jacobi<T, false>(A.d3, A.d3.e2, A.d3.e, A.d4);
-    grid_bar(A.bar, A.err, A.stop);
-  }
-  kc_jacobi<T, 2, true>(tab, sdi, nown, A.w2, A.ncap2, A.r2, A.e2, A.d3.e, A.e2b, A.sw1);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_jacobi<T, 2, false>(tab, sdi, nown, A.w2, A.ncap2, A.r2, A.e2b, nullptr, A.e2, A.sw2);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_jacobi<T, 4, true>(tab, sdi, nown, A.w1, A.ncap1, A.r1, A.e1, A.e2, A.e1b, A.sw1);
-  grid_bar(A.bar, A.err, A.stop);
-  kc_jacobi<T, 4, false>(tab, sdi, nown, A.w1, A.ncap1, A.r1, A.e1b, nullptr, A.e1, A.sw2);
-}
-
-template <class T>
-static size_t kc_smem_bytes(int per) {
-  return (size_t)per * 7 * (sizeof(int64_t) + sizeof(int));
-}
-constexpr int kCoarseMaxPer = 256;  // domain bricks per block at most (21.5 KB of tables)
-
-template <class T>
-static void kc_launch(Ctx* c, void (*k)(CoarseArgs<T>), const CoarseArgs<T>& A) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(c->kc_grid);
-  cfg.blockDim = dim3(kCoarseThreads);
-  cfg.dynamicSmemBytes = kc_smem_bytes<T>(c->kc_per);
-  cfg.stream = c->stream;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeCooperative;
-  at[0].val.cooperative = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k, A);
-}
-
 // ------------------------------------------------------------ weights setup
 // Level-1 weights from the level-0 face classes (Galerkin, piecewise constant).
 template <class T>
@@ -1856,27 +1442,6 @@ static int mg_setup_t(Ctx* c) {
     kwd_diag<T><<<grid_for(L.n, 256), 256, 0, st>>>(L); MAC_COUNT(c);
   }
   kd_coarsest_inverse<T><<<1, 1024, 0, st>>>(dview<T>(c, c->ndense - 1), c->coarse_inv, c->coarse_ok); MAC_COUNT(c);
-  // fused coarse levels: every block resident, each owning at most
-  // kCoarseMaxPer domain bricks; else the one-kernel-per-phase V-cycle
-  c->kc_grid = 0;
-  c->kc_per = 0;
-  if (c->mg_fused && nd > 0 && c->nsm > 0) {
-    const size_t smem = kc_smem_bytes<T>(kCoarseMaxPer);
-    int od = 0, ou = 0;
-    rc = check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, kc_down<T>, kCoarseThreads, smem));
-    if (!rc) rc = check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ou, kc_up<T>, kCoarseThreads, smem));
-    if (rc) return rc;
-    int occ = od < ou ? od : ou;
-    if (c->kc_blocks_per_sm > 0 && c->kc_blocks_per_sm < occ) occ = c->kc_blocks_per_sm;
-    const int grid = c->nsm * occ;
-    const int per = grid > 0 ? (nd + grid - 1) / grid : 0;
-    if (grid > 0 && per <= kCoarseMaxPer) {
-      c->kc_grid = grid;
-      c->kc_per = per;
-    }
-    rc = check(cudaMemsetAsync(c->kc_bar, 0, 2 * sizeof(unsigned), st));
-    if (rc) return rc;
-  }
   return check(cudaGetLastError());
 }
 
@@ -1933,78 +1498,40 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
     launch_k(c, k0_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
   }
   const T sw1 = (T)c->dp.mgw1, sw2 = (T)c->dp.mgw2;
-  if (c->kc_grid > 0) {
-    CoarseArgs<T> A;
-    A.dbl = c->dbl;
-    A.nd = nd;
-    A.per = c->kc_per;
-    A.nbr = c->nbr;
-    A.bkey = c->bkey;
-    A.w1 = w1;
-    A.w2 = w2;
-    A.ncap1 = ncap1;
-    A.ncap2 = ncap2;
-    A.r1 = r1;
-    A.e1 = e1;
-    A.e1b = e1b;
-    A.r2 = r2;
-    A.e2 = e2;
-    A.e2b = e2b;
-    A.d3 = d3;
-    A.dense = c->ndense > 1 ? 1 : 0;
-    A.d4 = A.dense ? dview<T>(c, 1) : d3;
-    A.g3 = G;
-    A.sw1 = sw1;
-    A.sw2 = sw2;
-    A.done = dn;
-    A.stop = &c->ds->done;
-    A.bar = (GridBar*)c->kc_bar;
-    A.err = &c->ds->err;
-    kc_launch(c, kc_down<T>, A); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
+  // dense level 3 on the device, levels 4.. in one block
+  if (c->ndense > 1) {
+    DView<T> d4 = dview<T>(c, 1);
+    launch_k(c, kd_pre<T>, grid_for(d3.n, 256), 256, 0, d3, dn); MAC_COUNT(c);
+    launch_k(c, kd_restrict<T>, grid_for(8 * d4.n, 256), 256, 0, d3, d4, dn); MAC_COUNT(c);
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
-    S.lo = A.dense ? 1 : 0;
+    S.lo = 1;
     S.hi = c->ndense;
-    const int use_smem = A.dense && c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
-    launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv,
-             c->coarse_ok, dn); MAC_COUNT(c);
-    kc_launch(c, kc_up<T>, A); MAC_COUNT(c);
+    int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
+    launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv, c->coarse_ok,
+             dn); MAC_COUNT(c);
+    launch_k(c, kd_jacobi<T, true>, grid_for(d3.n, 256), 256, 0, d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
+    launch_k(c, kd_jacobi<T, false>, grid_for(d3.n, 256), 256, 0, d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
   } else {
-    launch_k(c, kl_pre<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
-    launch_k(c, kl_restrict<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
-    launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
-    launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
-    // dense level 3 on the device, levels 4.. in one block
-    if (c->ndense > 1) {
-      DView<T> d4 = dview<T>(c, 1);
-      launch_k(c, kd_pre<T>, grid_for(d3.n, 256), 256, 0, d3, dn); MAC_COUNT(c);
-      launch_k(c, kd_restrict<T>, grid_for(8 * d4.n, 256), 256, 0, d3, d4, dn); MAC_COUNT(c);
-      DenseSet<T> S;
-      for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
-      S.lo = 1;
-      S.hi = c->ndense;
-      int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
-      launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv, c->coarse_ok,
-               dn); MAC_COUNT(c);
-      launch_k(c, kd_jacobi<T, true>, grid_for(d3.n, 256), 256, 0, d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
-      launch_k(c, kd_jacobi<T, false>, grid_for(d3.n, 256), 256, 0, d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
-    } else {
-      DenseSet<T> S;
-      S.L[0] = d3;
-      S.lo = 0;
-      S.hi = 1;
-      launch_k(c, kd_coarse_block<T>, 1, 1024, 0, S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
-    }
-    // up
-    launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
-             dn); MAC_COUNT(c);
-    launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
-             sw2, dn); MAC_COUNT(c);
-    launch_k(c, kl_jacobi<T, 4, true>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
-             dn); MAC_COUNT(c);
-    launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
-             sw2, dn); MAC_COUNT(c);
+    DenseSet<T> S;
+    S.L[0] = d3;
+    S.lo = 0;
+    S.hi = 1;
+    launch_k(c, kd_coarse_block<T>, 1, 1024, 0, S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
+  // up
+  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
+           dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
+           sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 4, true>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
+           dn); MAC_COUNT(c);
+  launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
+           sw2, dn); MAC_COUNT(c);
   if (one) {
     launch_k(c, k0_post_one<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
     return;
@@ -2043,7 +1570,6 @@ int mg_configure(Ctx* c) {
                                                                       bulk_smem<double>()));
   }
   c->bulk_grid = rc ? 0 : nsm * occ;
-  c->nsm = rc ? 0 : nsm;
   return rc;
 }
 

@@ -49,8 +49,6 @@ int alloc_solver(Ctx* c) {
   A(dalloc(&c->coarse_inv, 64 * 64));
   A(dalloc(&c->coarse_ok, 1));
   if (rc == MAC_OK) A(check(cudaMemset(c->coarse_ok, 0, sizeof(int))));
-  A(dalloc(&c->kc_bar, 2));
-  if (rc == MAC_OK) A(check(cudaMemset(c->kc_bar, 0, 2 * sizeof(unsigned))));
   c->npartial = 2 * c->cap_bricks + 64;
   A(dalloc(&c->partial, c->npartial));
   c->mg_float = c->prm.solver == MAC_SOLVER_MGPCG_MIXED || c->prm.solver == MAC_SOLVER_LEARNED_MIXED;
@@ -75,7 +73,7 @@ int alloc_solver(Ctx* c) {
 void free_solver(Ctx* c) {
   cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->r2); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
-  cudaFree(c->dbl_map); cudaFree(c->dbl_cnt); cudaFree(c->kc_bar);
+  cudaFree(c->dbl_map); cudaFree(c->dbl_cnt);
   cudaFree(c->zold);
   cudaFree(c->coarse_inv);
   cudaFree(c->coarse_ok);

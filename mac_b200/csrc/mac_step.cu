@@ -547,15 +547,6 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   return MAC_OK;
 }
 
-int mac_set_coarse_fusion(void* ctx, int on, int blocks_per_sm) {
-  CTX_OR_FAIL();
-  if ((on != 0 && on != 1) || blocks_per_sm < 0 || blocks_per_sm > 8) return MAC_ERR_INVALID;
-  c->mg_fused = on;
-  c->kc_blocks_per_sm = blocks_per_sm;
-  c->system_ready = false;  // the grid is chosen with the system
-  return MAC_OK;
-}
-
 int mac_set_dependent_launch(void* ctx, int on) {
   CTX_OR_FAIL();
   if (on != 0 && on != 1) return MAC_ERR_INVALID;

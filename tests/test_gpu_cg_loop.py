@@ -120,22 +120,3 @@ def test_smoother_settings(pool64):
                     (0.3, 4.0, 0.9, 0.6)):
             with pytest.raises(MacError):
                 ctx.set_smoother(*bad)
-
-
-@pytest.mark.parametrize("solver,sweeps", [("mixed", 2), ("mgpcg64", 2), ("mixed", 1)])
-def test_fused_coarse_levels_change_no_bit(pool64, solver, sweeps):
-    """Levels 1-3 of the V-cycle as two cooperative kernels (default, with as
-    many blocks as fit and with one block per SM, which gives each block more
-    bricks) and as one kernel per phase: the same iterations and the same
-    pressure bit for bit."""
-    out = []
-    for fused, per_sm in ((True, 0), (True, 1), (False, 0)):
-        with _ctx(pool64, solver, 1e-10, 500, sweeps) as ctx:
-            ctx.set_coarse_fusion(fused, per_sm)
-            ctx.upload(pool64)
-            ctx.project(0)
-            got = ctx.download()
-            out.append((ctx.stats()["iterations"], got.f64["p"][got.exists.astype(bool)].copy()))
-    for its, p in out[1:]:
-        assert its == out[0][0]
-        assert np.array_equal(p, out[0][1])

@@ -212,10 +212,9 @@ def test_stage_buffers_can_be_left_out_of_the_transfers(golden):
 STEP_FIELDS = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
 
 
-def _steps(state, n, solver, dependent_launch=True, fused=True):
+def _steps(state, n, solver, dependent_launch=True):
     with _ctx(state, solver=solver, rtol=1e-8) as ctx:
         ctx.set_dependent_launch(dependent_launch)
-        ctx.set_coarse_fusion(fused)
         ctx.upload(state)
         for _ in range(n):
             ctx.step()
@@ -239,14 +238,12 @@ def test_steps_are_reproducible(golden, solver):
     assert compare_particles(a, b) == 0.0
 
 
-def test_launch_forms_change_no_bit(golden):
+def test_dependent_launch_changes_no_bit(golden):
     """The CG loop's kernels launched with programmatic stream serialisation
-    and the V-cycle's coarse levels fused into cooperative kernels (the
-    defaults) give the same world as plain stream order and one kernel per
-    multigrid phase."""
+    (the default) and in plain stream order give the same world."""
     s30 = golden("c1_ref_s30")
     a, ia = _steps(s30, 3, "mixed", dependent_launch=True)
-    b, ib = _steps(s30, 3, "mixed", dependent_launch=False, fused=False)
+    b, ib = _steps(s30, 3, "mixed", dependent_launch=False)
     assert ia == ib
     compare_topology(a, b)
     d = max_abs_diff(a, b, STEP_FIELDS, existing_only=True)
