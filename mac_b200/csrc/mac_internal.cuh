@@ -269,6 +269,13 @@ __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+// A kernel's prologue before pdl_entry() may load what the previous kernel
+// does not write: the launch order makes a kernel start only after every
+// block of the previous kernel has passed its own wait, i.e. after the kernel
+// before that has completed. So the prologue may read static data (brick
+// tables, face masks, multigrid weights) and whatever the kernels two or more
+// launches back wrote; it writes nothing to global memory, and every thread
+// reaches pdl_entry() before it may return.
 
 template <class... P, class... A>
 inline void launch_k(const Ctx* c, void (*k)(P...), dim3 grid, dim3 block, size_t smem, A&&... args) {

@@ -82,16 +82,20 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
                                               const double* __restrict__ p, const double* __restrict__ q,
                                               double* partial, const Scalars* ds, int update, T* __restrict__ e,
                                               Params P) {
-  pdl_entry();
-  if (solve_done(&ds->done)) return;
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
   __shared__ uint16_t sm[kCells];
   const T om = (T)P.mgw1, om2 = (T)P.mgw2, c0 = (T)(P.mgw1 + P.mgw2 - P.mgw1 * P.mgw2);
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
-  const double al = update ? ds->alpha : 0.0;
+  // prologue (static): brick, face neighbours, face masks
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  uint16_t mk[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
+  pdl_entry();
+  if (solve_done(&ds->done)) return;
+  const double al = update ? ds->alpha : 0.0;
   double rv[kCPT];
   double rr = 0;
 #pragma unroll
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
       rr += v * v;
     }
     rv[k] = v;
-    const uint16_t m = fmask[c];
+    const uint16_t m = mk[k];
     sm[o] = m;
     sr[s1_of(o)] = om * (T)P.dtab[active_index(m)] * (T)v;
   }
@@ -142,12 +146,12 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P,
                                                    const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T res[kCells];
   __shared__ T se[kS1];
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  // prologue: brick, face neighbours, face masks (static) and r (written by
+  // the V-cycle's first kernel, two launches back)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   uint16_t mk[kCPT];
@@ -158,6 +162,8 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
     mk[k] = fmask[c];
     rk[k] = r[c];
   }
+  pdl_entry();
+  if (solve_done(done)) return;
   __syncthreads();
   stage_arr(se, e, b, sb);
   __syncthreads();
@@ -204,11 +210,11 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P,
                                                const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];  // e (plus the coarse correction when FIRST) with face halo
   const T om = (T)(FIRST ? P.mgw1 : P.mgw2), ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
+  // prologue: brick, face neighbours, face masks (static), r and, when FIRST,
+  // the brick's pre-smoothed e (both written many launches back)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
   uint16_t mk[kCPT];
@@ -219,11 +225,13 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
     mk[k] = fmask[c];
     rk[k] = r[c];
   }
+  T v[4];
+  if (FIRST) load4(e + (int64_t)b * kCells + 4 * threadIdx.x, v);
+  pdl_entry();
+  if (solve_done(done)) return;
   if (FIRST) {
     // the brick: cells 4t..4t+3 of one row share two level-1 parents
     const int o4 = 4 * threadIdx.x;
-    T v[4];
-    load4(e + (int64_t)b * kCells + o4, v);
     const int p0 = parent_off(o4);
     const T c0 = e1[(size_t)b * 64 + p0], c1 = e1[(size_t)b * 64 + p0 + 1];
     __syncthreads();
@@ -692,37 +700,47 @@ template <class T, int D>
 __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
                                               T* __restrict__ e, T w1, T w2, const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
+  // prologue (static): the brick tables, the cell's weights and its
+  // neighbours' inverse diagonals
   load_lbricks<D>(dbl, nd, nbr, sbr);
   __syncthreads();
-  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (int64_t)nd * N) return;
-  const int* sb = sbr + 7 * (threadIdx.x / N);
-  int b = sb[0];
-  int o = (int)(g % N);
-  size_t i = (size_t)b * N + o;
-  T dinv = w[4 * ncap + i];
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = g < (int64_t)nd * N;
+  size_t i = 0;
+  T dinv = 0;
+  int64_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};
+  T wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0}, dl[3] = {0, 0, 0}, dr[3] = {0, 0, 0};
+  if (live) {
+    const int* sb = sbr + 7 * (threadIdx.x / N);
+    const int o = (int)(g % N);
+    i = (size_t)sb[0] * N + o;
+    dinv = w[4 * ncap + i];
+    const int x = o % D, y = (o / D) % D, z = o / (D * D);
+    int64_t n[6];
+    lnbrs<D>(sb, x, y, z, n);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      jl[a] = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
+      jr[a] = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+      wl[a] = w[a * ncap + i];
+      dl[a] = w[4 * ncap + jl[a]];
+      wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr[a]];
+      dr[a] = w[4 * ncap + jr[a]];
+    }
+  }
+  pdl_entry();
+  if (!live || solve_done(done)) return;
   if (dinv == 0) {
     e[i] = (T)0;
     return;
   }
-  int x = o % D, y = (o / D) % D, z = o / (D * D);
-  int64_t n[6];
-  lnbrs<D>(sb, x, y, z, n);
-  T wl[3], wr[3], dl[3], dr[3], rl[3], rr[3];
+  T rl[3], rr[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int64_t jl = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
-    const int64_t jr = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
-    wl[a] = w[a * ncap + i];
-    dl[a] = w[4 * ncap + jl];
-    rl[a] = r[jl];
-    wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr];
-    dr[a] = w[4 * ncap + jr];
-    rr[a] = r[jr];
+    rl[a] = r[jl[a]];
+    rr[a] = r[jr[a]];
   }
   T s = 0;
 #pragma unroll
@@ -750,18 +768,21 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
                                                    const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                    const T* __restrict__ r, const T* __restrict__ e, T* __restrict__ rc,
                                                    DenseGrid g3, const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   constexpr int H = D / 2;
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
+  // prologue: the brick tables and weights (static) and the cell's residual
+  // (written two or more launches back)
   load_lbricks<D>(dbl, nd, nbr, sbr);
   __syncthreads();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = g < (int64_t)nd * N;  // nd * N is a multiple of 8: groups are whole
   const int* sb = sbr + 7 * (threadIdx.x / N);
-  T v = 0;
   int b = 0, p = 0;
+  bool act = false;
+  size_t i = 0;
+  int64_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};
+  T wd = 0, ri = 0, wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0};
   if (live) {
     b = sb[0];
     const int o = (int)(g % N);
@@ -769,12 +790,40 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
     const int k = o & 7;
     const int X = p % H, Y = (p / H) % H, Z = p / (H * H);
     const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-    const size_t i = (size_t)b * N + x + D * y + D * D * z;
-    if (w[4 * ncap + i] != 0) {
+    i = (size_t)b * N + x + D * y + D * D * z;
+    act = w[4 * ncap + i] != 0;
+    if (act) {
       int64_t n[6];
       lnbrs<D>(sb, x, y, z, n);
-      v = r[i] - apply_l<T, D>(e, w, ncap, n, i, e[i]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        jl[a] = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
+        jr[a] = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+        wl[a] = w[a * ncap + i];
+        wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr[a]];
+      }
+      wd = w[3 * ncap + i];
+      ri = r[i];
     }
+  }
+  pdl_entry();
+  if (solve_done(done)) return;
+  T v = 0;
+  if (act) {
+    // r - M e in apply_l's order
+    T el[3], er[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      el[a] = e[jl[a]];
+      er[a] = e[jr[a]];
+    }
+    T s = wd * e[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (wl[a] != 0) s -= wl[a] * el[a];
+      if (wr[a] != 0) s -= wr[a] * er[a];
+    }
+    v = ri - s;
   }
   v = sum8(v);
   if (live && (threadIdx.x & 7) == 0) {
@@ -791,12 +840,13 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
                                                  const T* __restrict__ r, const T* __restrict__ e,
                                                  const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3,
                                                  T om, const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   constexpr int N = D * D * D;
   constexpr int H = D / 2;
   __shared__ int sbr[7 * LBricks<D>::BPB];
   __shared__ int64_t sdi[7 * LBricks<D>::BPB];  // D = 2: dense level-3 index of each table brick
+  // prologue: brick tables and weights (static), r, and with the coarse
+  // correction this level's e (both written two or more launches back; e
+  // without it is the previous launch's output and waits)
   load_lbricks<D>(dbl, nd, nbr, sbr);
   __syncthreads();
   if (WITH_COARSE && D == 2) {
@@ -806,32 +856,22 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     }
     __syncthreads();
   }
-  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (int64_t)nd * N) return;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = g < (int64_t)nd * N;
   const int* sb = sbr + 7 * (threadIdx.x / N);
-  int b = sb[0];
-  int o = (int)(g % N);
-  size_t i = (size_t)b * N + o;
-  T dinv = w[4 * ncap + i];
-  if (dinv == 0) {
-    eout[i] = (T)0;
-    return;
-  }
+  const int o = live ? (int)(g % N) : 0;
+  const size_t i = live ? (size_t)sb[0] * N + o : 0;
   const int x = o % D, y = (o / D) % D, z = o / (D * D);
-  // e plus the coarse correction at local cell (lx, ly, lz) of the brick in
-  // table slot k (0 = this brick)
-  auto ev = [&](int k, int lx, int ly, int lz) -> T {
-    const int nb = sb[k];
-    T v = e[(size_t)nb * N + lx + D * ly + D * D * lz];
-    if (WITH_COARSE) {
-      if (D == 2) v += ec[sdi[7 * (threadIdx.x / N) + k]];
-      else v += ec[(size_t)nb * H * H * H + (lx >> 1) + H * (ly >> 1) + H * H * (lz >> 1)];
-    }
-    return v;
-  };
-  // the six neighbours: slot and local coordinates (an absent neighbour reads
-  // this cell and drops out through its zero weight)
-  T wl[3], wr[3], vl[3], vr[3];
+  // stencil points: 0 = the cell, 1 + 2a / 2 + 2a = its -/+ neighbour on axis
+  // a (an absent neighbour is the cell itself and drops out through its zero
+  // weight); slot in the brick table and local coordinates
+  int ks[7], lx[7], ly[7], lz[7];
+  ks[0] = 0;
+  lx[0] = x;
+  ly[0] = y;
+  lz[0] = z;
+  T wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0}, ev[7] = {0, 0, 0, 0, 0, 0, 0};
+  T dinv = 0, wd = 0, ri = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int c[3] = {x, y, z};
@@ -844,19 +884,52 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     const bool hl = sb[kl] >= 0, hr = sb[kr] >= 0;
     if (!hl) { kl = 0; pl[0] = x; pl[1] = y; pl[2] = z; }
     if (!hr) { kr = 0; pr[0] = x; pr[1] = y; pr[2] = z; }
-    wl[a] = w[a * ncap + i];
-    vl[a] = ev(kl, pl[0], pl[1], pl[2]);
-    wr[a] = hr ? w[a * ncap + (size_t)sb[kr] * N + pr[0] + D * pr[1] + D * D * pr[2]] : (T)0;
-    vr[a] = ev(kr, pr[0], pr[1], pr[2]);
+    ks[1 + 2 * a] = kl;
+    lx[1 + 2 * a] = pl[0];
+    ly[1 + 2 * a] = pl[1];
+    lz[1 + 2 * a] = pl[2];
+    ks[2 + 2 * a] = kr;
+    lx[2 + 2 * a] = pr[0];
+    ly[2 + 2 * a] = pr[1];
+    lz[2 + 2 * a] = pr[2];
+    if (live) {
+      wl[a] = w[a * ncap + i];
+      wr[a] = hr ? w[a * ncap + (size_t)sb[kr] * N + pr[0] + D * pr[1] + D * D * pr[2]] : (T)0;
+    }
   }
-  T ecc = ev(0, x, y, z);
-  T s = w[3 * ncap + i] * ecc;
+  if (live) {
+    dinv = w[4 * ncap + i];
+    wd = w[3 * ncap + i];
+    ri = r[i];
+    if (WITH_COARSE) {
+#pragma unroll
+      for (int q = 0; q < 7; ++q) ev[q] = e[(size_t)sb[ks[q]] * N + lx[q] + D * ly[q] + D * D * lz[q]];
+    }
+  }
+  pdl_entry();
+  if (!live || solve_done(done)) return;
+  if (dinv == 0) {
+    eout[i] = (T)0;
+    return;
+  }
+  // e plus the coarse correction at each stencil point
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    const int nb = sb[ks[q]];
+    if (WITH_COARSE) {
+      if (D == 2) ev[q] += ec[sdi[7 * (threadIdx.x / N) + ks[q]]];
+      else ev[q] += ec[(size_t)nb * H * H * H + (lx[q] >> 1) + H * (ly[q] >> 1) + H * H * (lz[q] >> 1)];
+    } else {
+      ev[q] = e[(size_t)nb * N + lx[q] + D * ly[q] + D * D * lz[q]];
+    }
+  }
+  T s = wd * ev[0];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    if (wl[a] != 0) s -= wl[a] * vl[a];
-    if (wr[a] != 0) s -= wr[a] * vr[a];
+    if (wl[a] != 0) s -= wl[a] * ev[1 + 2 * a];
+    if (wr[a] != 0) s -= wr[a] * ev[2 + 2 * a];
   }
-  eout[i] = ecc + om * dinv * (r[i] - s);
+  eout[i] = ev[0] + om * dinv * (ri - s);
 }
 
 // ------------------------------------------------------------ dense levels
@@ -894,29 +967,40 @@ __device__ inline T dense_apply(const DView<T>& L, const T* e, int64_t i, int x,
 // Device-wide dense kernels for level 3.
 template <class T>
 __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
+  // prologue (static): the cell's and its neighbours' weights and inverse diagonals
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < L.n;
+  const int64_t n = L.n;
+  T dinv = 0, wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0}, dl[3] = {0, 0, 0}, dr[3] = {0, 0, 0};
+  bool hl[3] = {false, false, false}, hr[3] = {false, false, false};
+  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  if (live) {
+    dinv = L.w[4 * n + i];
+    int x, y, z;
+    coords3(i, L.nx, L.ny, L.n, x, y, z);
+    const int c[3] = {x, y, z};
+    const int dim[3] = {L.nx, L.ny, L.nz};
+    for (int a = 0; a < 3; ++a) {
+      wl[a] = L.w[a * n + i];
+      hl[a] = wl[a] != 0 && c[a] > 0;
+      if (hl[a]) dl[a] = L.w[4 * n + i - stride[a]];
+      if (c[a] + 1 < dim[a]) {
+        wr[a] = L.w[a * n + i + stride[a]];
+        hr[a] = wr[a] != 0;
+        if (hr[a]) dr[a] = L.w[4 * n + i + stride[a]];
+      }
+    }
+  }
   pdl_entry();
-  if (solve_done(done)) return;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= L.n) return;
-  int64_t n = L.n;
-  T dinv = L.w[4 * n + i];
+  if (!live || solve_done(done)) return;
   if (dinv == 0) {
     L.e[i] = (T)0;
     return;
   }
-  int x, y, z;
-  coords3(i, L.nx, L.ny, L.n, x, y, z);
-  int c[3] = {x, y, z};
-  int dim[3] = {L.nx, L.ny, L.nz};
-  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
   T s = 0;
   for (int a = 0; a < 3; ++a) {
-    T wl = L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) s += wl * L.w1 * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
-    if (c[a] + 1 < dim[a]) {
-      T wr = L.w[a * n + i + stride[a]];
-      if (wr != 0) s += wr * L.w1 * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
-    }
+    if (hl[a]) s += wl[a] * L.w1 * dl[a] * L.r[i - stride[a]];
+    if (hr[a]) s += wr[a] * L.w1 * dr[a] * L.r[i + stride[a]];
   }
   L.e[i] = dinv * ((L.w1 + L.w2 - L.w1 * L.w2) * L.r[i] + L.w2 * s);
 }
@@ -924,20 +1008,50 @@ __global__ void kd_pre(DView<T> L, const int32_t* __restrict__ done) {
 // One thread per (coarse cell, child), the 8 children on adjacent lanes.
 template <class T>
 __global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
+  // prologue: weights (static) and the fine residual (written two launches back)
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t I = g >> 3;
   const int k = (int)(g & 7);
-  T s = 0;
+  const int64_t n = F.n;
+  bool act = false;
+  int64_t i = 0;
+  int c[3] = {0, 0, 0};
+  const int dim[3] = {F.nx, F.ny, F.nz};
+  const int64_t stride[3] = {1, F.nx, (int64_t)F.nx * F.ny};
+  T wd = 0, ri = 0, wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0};
   if (I < C.n) {
     int X, Y, Z;
     coords3(I, C.nx, C.ny, C.n, X, Y, Z);
-    const int x = 2 * X + (k & 1), y = 2 * Y + ((k >> 1) & 1), z = 2 * Z + (k >> 2);
-    if (x < F.nx && y < F.ny && z < F.nz) {
-      const int64_t i = F.at(x, y, z);
-      if (F.w[4 * F.n + i] != 0) s = F.r[i] - dense_apply(F, F.e, i, x, y, z, F.e[i]);
+    c[0] = 2 * X + (k & 1);
+    c[1] = 2 * Y + ((k >> 1) & 1);
+    c[2] = 2 * Z + (k >> 2);
+    if (c[0] < F.nx && c[1] < F.ny && c[2] < F.nz) {
+      i = F.at(c[0], c[1], c[2]);
+      act = F.w[4 * n + i] != 0;
+      if (act) {
+        wd = F.w[3 * n + i];
+        ri = F.r[i];
+        for (int a = 0; a < 3; ++a) {
+          wl[a] = F.w[a * n + i];
+          if (c[a] + 1 < dim[a]) wr[a] = F.w[a * n + i + stride[a]];
+        }
+      }
     }
+  }
+  pdl_entry();
+  if (solve_done(done)) return;
+  T s = 0;
+  if (act) {
+    // r - M e in dense_apply's order
+    const T* e = F.e;
+    T m = wd * e[i];
+    for (int a = 0; a < 3; ++a) {
+      if (wl[a] != 0 && c[a] > 0) m -= wl[a] * e[i - stride[a]];
+      if (c[a] + 1 < dim[a]) {
+        if (wr[a] != 0) m -= wr[a] * e[i + stride[a]];
+      }
+    }
+    s = ri - m;
   }
   s = sum8(s);
   if (I < C.n && k == 0) C.r[I] = (T)s;
@@ -946,44 +1060,71 @@ __global__ void kd_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ 
 template <class T, bool WITH_COARSE>
 __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__ eout, DView<T> C,
                           const int32_t* __restrict__ done) {
+  // prologue: weights (static), r, and with the coarse correction this
+  // level's e (written three launches back); without it e is the previous
+  // launch's output and waits
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < L.n;
+  const int64_t n = L.n;
+  int c[3] = {0, 0, 0};
+  const int dim[3] = {L.nx, L.ny, L.nz};
+  const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+  T dinv = 0, wd = 0, ri = 0, wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0};
+  bool hl[3] = {false, false, false}, hr[3] = {false, false, false};
+  T vc = 0, vl[3] = {0, 0, 0}, vr[3] = {0, 0, 0};
+  if (live) {
+    coords3(i, L.nx, L.ny, L.n, c[0], c[1], c[2]);
+    dinv = L.w[4 * n + i];
+    wd = L.w[3 * n + i];
+    ri = L.r[i];
+    for (int a = 0; a < 3; ++a) {
+      wl[a] = L.w[a * n + i];
+      hl[a] = wl[a] != 0 && c[a] > 0;
+      if (c[a] + 1 < dim[a]) {
+        wr[a] = L.w[a * n + i + stride[a]];
+        hr[a] = wr[a] != 0;
+      }
+    }
+    if (WITH_COARSE) {
+      vc = ein[i];
+      for (int a = 0; a < 3; ++a) {
+        if (hl[a]) vl[a] = ein[i - stride[a]];
+        if (hr[a]) vr[a] = ein[i + stride[a]];
+      }
+    }
+  }
   pdl_entry();
-  if (solve_done(done)) return;
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= L.n) return;
-  int64_t n = L.n;
-  T dinv = L.w[4 * n + i];
+  if (!live || solve_done(done)) return;
   if (dinv == 0) {
     eout[i] = (T)0;
     return;
   }
-  int x, y, z;
-  coords3(i, L.nx, L.ny, L.n, x, y, z);
-  auto ev = [&](int64_t j, int xx, int yy, int zz) -> T {
-    T v = ein[j];
-    if (WITH_COARSE) v += C.e[C.at(xx >> 1, yy >> 1, zz >> 1)];
-    return v;
-  };
-  int c[3] = {x, y, z};
-  int dim[3] = {L.nx, L.ny, L.nz};
-  int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  T ec = ev(i, x, y, z);
-  T s = L.w[3 * n + i] * ec;
-  for (int a = 0; a < 3; ++a) {
-    int p[3] = {x, y, z};
-    T wl = L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) {
-      p[a] = c[a] - 1;
-      s -= wl * ev(i - stride[a], p[0], p[1], p[2]);
-    }
-    if (c[a] + 1 < dim[a]) {
-      T wr = L.w[a * n + i + stride[a]];
-      if (wr != 0) {
-        p[a] = c[a] + 1;
-        s -= wr * ev(i + stride[a], p[0], p[1], p[2]);
+  // e plus the coarse correction at the cell and its coupled neighbours
+  auto cc = [&](int xx, int yy, int zz) -> T { return C.e[C.at(xx >> 1, yy >> 1, zz >> 1)]; };
+  if (WITH_COARSE) {
+    vc += cc(c[0], c[1], c[2]);
+    for (int a = 0; a < 3; ++a) {
+      int p[3] = {c[0], c[1], c[2]};
+      if (hl[a]) {
+        p[a] = c[a] - 1;
+        vl[a] += cc(p[0], p[1], p[2]);
       }
+      p[a] = c[a] + 1;
+      if (hr[a]) vr[a] += cc(p[0], p[1], p[2]);
+    }
+  } else {
+    vc = ein[i];
+    for (int a = 0; a < 3; ++a) {
+      if (hl[a]) vl[a] = ein[i - stride[a]];
+      if (hr[a]) vr[a] = ein[i + stride[a]];
     }
   }
-  eout[i] = ec + (WITH_COARSE ? L.w1 : L.w2) * dinv * (L.r[i] - s);
+  T s = wd * vc;
+  for (int a = 0; a < 3; ++a) {
+    if (hl[a]) s -= wl[a] * vl[a];
+    if (hr[a]) s -= wr[a] * vr[a];
+  }
+  eout[i] = vc + (WITH_COARSE ? L.w1 : L.w2) * dinv * (ri - s);
 }
 
 // ------------------------------------------- coarse V-cycle in one block
@@ -1156,8 +1297,6 @@ template <class T>
 __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_smem, const double* __restrict__ inv,
                                                         const int* __restrict__ inv_ok,
                                                         const int32_t* __restrict__ done) {
-  pdl_entry();
-  if (solve_done(done)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // Level descriptors live in shared memory (one copy per block); which of a
   // level's two correction buffers is current is a bit in a register.
@@ -1178,11 +1317,30 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
     }
   }
   __syncthreads();
+  // prologue: the levels' weights (static since the set-up) into shared
+  // memory and this thread's entries of the coarsest inverse, while the
+  // previous kernel still runs; the residual of level lo is that kernel's
+  // output and is copied after the wait
   if (use_smem) {
-    for (int l = lo; l < hi; ++l) {
-      blk_copy(SL[l].w, G.L[l].w, 6 * SL[l].n);
-      if (l == lo) blk_copy(SL[l].r, G.L[l].r, SL[l].n);
+    for (int l = lo; l < hi; ++l) blk_copy(SL[l].w, G.L[l].w, 6 * SL[l].n);
+  }
+  const bool exact = *inv_ok && SL[hi - 1].n <= 64;
+  double iv[4] = {0.0, 0.0, 0.0, 0.0};
+  if (exact) {
+    const int n = (int)SL[hi - 1].n;
+    const int i = threadIdx.x >> 4, p = threadIdx.x & 15;
+    if (i < n) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = p + 16 * q;
+        if (j < n) iv[q] = inv[i * 64 + j];
+      }
     }
+  }
+  pdl_entry();
+  if (solve_done(done)) return;
+  if (use_smem) {
+    blk_copy(SL[lo].r, G.L[lo].r, SL[lo].n);
     __syncthreads();
   }
   unsigned swapped = 0;
@@ -1203,7 +1361,7 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
   {
     const int l = hi - 1;
     const DView<T>& L = SL[l];
-    if (*inv_ok && L.n <= 64) {
+    if (exact) {
       // row i of inv r by the 16 lanes i*16..i*16+15 (j = lane part + 16 q),
       // summed over the lanes with shuffles; the block holds 1024 threads
       const int n = (int)L.n;
@@ -1213,7 +1371,7 @@ __global__ void __launch_bounds__(1024) kd_coarse_block(DenseSet<T> G, int use_s
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int j = p + 16 * q;
-          if (j < n) s += inv[i * 64 + j] * (double)L.r[j];
+          if (j < n) s += iv[q] * (double)L.r[j];
         }
       }
 #pragma unroll

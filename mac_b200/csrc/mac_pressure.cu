@@ -430,15 +430,13 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
                                                      const double* __restrict__ pold, double* __restrict__ pnew,
                                                      double* __restrict__ q, double* partial, Params P,
                                                      const Scalars* ds, int first) {
-  pdl_entry();
-  if (ds->done) return;
   __shared__ int64_t sb[6];
   __shared__ double sp[kS1];  // the new direction on the brick and its face halo
+  // prologue: brick, face neighbours and face masks (static), the brick's z
+  // (the preconditioner's output, two launches back) and p_old (16-byte
+  // vector loads); only beta comes from the previous launch
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  const double be = first ? 0.0 : ds->beta;
-  // the cells' face masks and the brick's z and p_old (16-byte vector loads)
-  // are in flight before the barrier the halo staging waits on
   uint16_t mk[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
@@ -446,6 +444,9 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   double vz[4], vp[4] = {0.0, 0.0, 0.0, 0.0};
   load4(z + (int64_t)b * kCells + o4, vz);
   if (!first) load4(pold + (int64_t)b * kCells + o4, vp);
+  pdl_entry();
+  if (ds->done) return;
+  const double be = first ? 0.0 : ds->beta;
   __syncthreads();
   // p = z (first) or z + beta p_old, on the brick and its face halo
   if (first) stage_h1_halo(sp, sb, [&](int64_t i) { return z[i]; });
