@@ -432,6 +432,8 @@ def run_ours(args, rank, world, local_rank):
     ctx = Context(s.params, max_bricks=wl[8], max_particles=wl[9], solver=args.solver, rtol=1e-8, max_iters=1000,
                   device=dev, div_check=True, warm_start=args.warm_start)
     ctx.set_multigrid(args.mg_sweeps, args.prefetch)
+    ctx.set_dependent_launch(not args.no_dependent_launch)
+    ctx.set_concurrent_binning(not args.no_concurrent_binning)
     if args.solver.startswith("learned"):
         from mac_b200.unet import UNet
         net_main = UNet(dev)
@@ -562,6 +564,8 @@ def run_ours(args, rank, world, local_rank):
                                f"{wl[6]}, 8 particles/fluid cell, LayerMax 4, CFL 0.5",
                    "solver": SOLVER_NAMES[args.solver], "mg_sweeps0": args.mg_sweeps,
                    "mg_prefetch": args.prefetch,
+                   "dependent_launch": not args.no_dependent_launch,
+                   "concurrent_binning": not args.no_concurrent_binning,
                    "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
@@ -600,6 +604,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip stepping the jet with every solver form")
     ap.add_argument("--prefetch", action="store_true",
                     help="run the V-cycle's first kernel as resident blocks prefetching bricks with bulk copies")
+    ap.add_argument("--no-dependent-launch", action="store_true",
+                    help="launch the CG loop's kernels in plain stream order")
+    ap.add_argument("--no-concurrent-binning", action="store_true",
+                    help="bin the particles inside the move instead of on a second stream during RK2-TVD")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

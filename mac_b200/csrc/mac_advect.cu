@@ -912,16 +912,12 @@ int acc_zero(Ctx* c) {
   return check(cudaGetLastError());
 }
 
-int move_particles(Ctx* c) {
+int bin_particles(Ctx* c, cudaStream_t st) {
   if (c->np_host == 0 || c->nlive_host == 0) return MAC_OK;
-  cudaStream_t st = c->stream;
-  size_t cap = (size_t)c->cap_bricks * kCells;
-  int64_t np = c->np_host;
-  int stray = (int)c->cap_bricks;
+  const int64_t np = c->np_host;
+  const int stray = (int)c->cap_bricks;
   int g = grid_for(np, 256);
   if (g > 148 * 16) g = 148 * 16;
-  unsigned long long* bad = &c->ds->bad_reads;
-  prof_begin(c, PH_MOVE);
   int rc = check(cudaMemsetAsync(c->bcount, 0, sizeof(int) * (c->cap_bricks + 1), st));
   if (!rc) rc = check(cudaMemsetAsync(c->bcursor, 0, sizeof(int) * (c->cap_bricks + 1) * kCells, st));
   if (rc) return rc;
@@ -934,14 +930,31 @@ int move_particles(Ctx* c) {
   std::swap(c->px, c->px2);
   std::swap(c->py, c->py2);
   std::swap(c->pz, c->pz2);
+  return check(cudaGetLastError());
+}
+
+int move_binned(Ctx* c) {
+  if (c->np_host == 0 || c->nlive_host == 0) return MAC_OK;
+  cudaStream_t st = c->stream;
+  const size_t cap = (size_t)c->cap_bricks * kCells;
+  const int stray = (int)c->cap_bricks;
+  unsigned long long* bad = &c->ds->bad_reads;
   k_move_binned<<<c->nlive_host, 256, 0, st>>>(c->px, c->py, c->pz, c->blist, c->bkey, c->nbr, c->boff, c->hkeys,
                                                c->hval, c->hcap, c->lay, c->f64 + U0X * cap, c->f64 + U0Y * cap,
                                                c->f64 + U0Z * cap, c->dp, c->ds, bad); MAC_COUNT(c);
   k_move_stray<<<4, 256, 0, st>>>(c->px, c->py, c->pz, c->boff, stray, c->nbr, c->hkeys, c->hval, c->hcap, c->lay,
                                   c->f64 + U0X * cap, c->f64 + U0Y * cap, c->f64 + U0Z * cap, c->dp, c->ds,
                                   bad); MAC_COUNT(c);
-  prof_end(c, PH_MOVE);
   return check(cudaGetLastError());
+}
+
+int move_particles(Ctx* c) {
+  if (c->np_host == 0 || c->nlive_host == 0) return MAC_OK;
+  prof_begin(c, PH_MOVE);
+  int rc = bin_particles(c, c->stream);
+  if (!rc) rc = move_binned(c);
+  prof_end(c, PH_MOVE);
+  return rc;
 }
 
 }  // namespace mac

@@ -197,6 +197,9 @@ static void free_all(Ctx* c) {
   if (c->hs_lag) cudaFreeHost(c->hs_lag);
   for (cudaEvent_t e : c->ev_lag)
     if (e) cudaEventDestroy(e);
+  if (c->ev_topo) cudaEventDestroy(c->ev_topo);
+  if (c->ev_bins) cudaEventDestroy(c->ev_bins);
+  if (c->side) cudaStreamDestroy(c->side);
   cudaFree(c->csc_off); cudaFree(c->csc_ind); cudaFree(c->csc_val); cudaFree(c->csc_vec);
   cudaFree(c->csr_off); cudaFree(c->csr_ind); cudaFree(c->csr_val); cudaFree(c->eb_work);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -260,6 +263,9 @@ static int create(const mac_params* p, Ctx** out) {
   int rc = MAC_OK;
   auto A = [&](int r) { if (rc == MAC_OK) rc = r; };
   A(check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)));
+  A(check(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)));
+  A(check(cudaEventCreateWithFlags(&c->ev_topo, cudaEventDisableTiming)));
+  A(check(cudaEventCreateWithFlags(&c->ev_bins, cudaEventDisableTiming)));
   A(dalloc(&c->bkey, 3 * c->cap_bricks));
   A(dalloc(&c->lay, nc));
   A(dalloc(&c->type, nc));

@@ -242,6 +242,11 @@ struct Ctx {
   long long launches = 0;      // kernels launched by this context
   struct Prof* prof = nullptr; // per-phase event timing (null when off)
   int pdl = 1;                 // CG-loop kernels launched with programmatic stream serialisation
+  // particle binning on a second stream, overlapping the step's projections
+  int bin_side = 1;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_topo = nullptr;  // the topology is done (the binning may start)
+  cudaEvent_t ev_bins = nullptr;  // the binning is done (the move may start)
 };
 
 void prof_begin(Ctx* c, int phase);
@@ -542,6 +547,11 @@ int topology_stage(Ctx* c);
 int setup_system(Ctx* c);
 int extrapolate(Ctx* c);
 int move_particles(Ctx* c);
+// The move's two halves: binning the particles by brick and cell on stream st
+// (into the second particle buffers, which then become the current ones), and
+// the RK4 move of the binned particles on the context's stream.
+int bin_particles(Ctx* c, cudaStream_t st);
+int move_binned(Ctx* c);
 int alloc_solver(Ctx* c);
 void free_solver(Ctx* c);
 int mg_setup(Ctx* c);

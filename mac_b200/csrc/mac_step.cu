@@ -72,15 +72,44 @@ static int step_b(Ctx* c) {
   return rk_all(c);
 }
 
-// One step of test/TestJetDEau_Basic.cpp:434-441.
+// One step of test/TestJetDEau_Basic.cpp:434-441. The particles do not move
+// between the topology and the move, so their binning by brick and cell runs
+// on a second stream from the end of the topology, overlapping RK2-TVD (whose
+// projections are latency-bound and leave memory bandwidth free) and the
+// extrapolation; the context's stream waits for it before the move, and on
+// every early return, since the binning swaps the current particle buffers.
 static int step(Ctx* c) {
   if (c->dp.pipeline == 1) return step_b(c);
   int rc = topology_rebuild(c, false);
   if (rc) return rc;
+  bool side = false;
+  if (c->bin_side && c->np_host > 0 && c->nlive_host > 0) {
+    rc = check(cudaEventRecord(c->ev_topo, c->stream));
+    if (!rc) rc = check(cudaStreamWaitEvent(c->side, c->ev_topo, 0));
+    if (!rc) rc = bin_particles(c, c->side);
+    if (!rc) rc = check(cudaEventRecord(c->ev_bins, c->side));
+    if (rc) return rc;
+    side = true;
+  }
+  auto join = [&]() -> int { return side ? check(cudaStreamWaitEvent(c->stream, c->ev_bins, 0)) : MAC_OK; };
   int ode = rk2tvd(c);
-  if (ode && ode != MAC_ERR_NOT_CONVERGED) return ode;
-  if ((rc = extrapolate(c))) return rc;
-  if ((rc = move_particles(c))) return rc;
+  if (ode && ode != MAC_ERR_NOT_CONVERGED) {
+    join();
+    return ode;
+  }
+  if ((rc = extrapolate(c))) {
+    join();
+    return rc;
+  }
+  if ((rc = join())) return rc;
+  if (side) {
+    prof_begin(c, PH_MOVE);
+    rc = move_binned(c);
+    prof_end(c, PH_MOVE);
+  } else {
+    rc = move_particles(c);
+  }
+  if (rc) return rc;
   k_advance_time<<<1, 1, 0, c->stream>>>(c->ds); MAC_COUNT(c);
   rc = check(cudaGetLastError());
   return rc ? rc : ode;
@@ -544,6 +573,13 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   if ((sweeps0 != 1 && sweeps0 != 2) || (prefetch != 0 && prefetch != 1)) return MAC_ERR_INVALID;
   c->mg_sweeps0 = sweeps0;
   c->mg_bulk = prefetch;
+  return MAC_OK;
+}
+
+int mac_set_concurrent_binning(void* ctx, int on) {
+  CTX_OR_FAIL();
+  if (on != 0 && on != 1) return MAC_ERR_INVALID;
+  c->bin_side = on;
   return MAC_OK;
 }
 

@@ -212,9 +212,10 @@ def test_stage_buffers_can_be_left_out_of_the_transfers(golden):
 STEP_FIELDS = ("u0x", "u0y", "u0z", "u1x", "u1y", "u1z", "ax", "ay", "az", "p")
 
 
-def _steps(state, n, solver, dependent_launch=True):
+def _steps(state, n, solver, dependent_launch=True, concurrent_binning=True):
     with _ctx(state, solver=solver, rtol=1e-8) as ctx:
         ctx.set_dependent_launch(dependent_launch)
+        ctx.set_concurrent_binning(concurrent_binning)
         ctx.upload(state)
         for _ in range(n):
             ctx.step()
@@ -238,13 +239,17 @@ def test_steps_are_reproducible(golden, solver):
     assert compare_particles(a, b) == 0.0
 
 
-def test_dependent_launch_changes_no_bit(golden):
+@pytest.mark.parametrize("dependent_launch,concurrent_binning", [(False, True), (True, False), (False, False)])
+def test_launch_forms_change_no_bit(golden, dependent_launch, concurrent_binning):
     """The CG loop's kernels launched with programmatic stream serialisation
-    (the default) and in plain stream order give the same world."""
+    and the particle binning on a second stream during RK2-TVD (the defaults)
+    give the same world, particles included, as plain stream order and the
+    binning inside the move."""
     s30 = golden("c1_ref_s30")
-    a, ia = _steps(s30, 3, "mixed", dependent_launch=True)
-    b, ib = _steps(s30, 3, "mixed", dependent_launch=False)
+    a, ia = _steps(s30, 3, "mixed")
+    b, ib = _steps(s30, 3, "mixed", dependent_launch, concurrent_binning)
     assert ia == ib
     compare_topology(a, b)
     d = max_abs_diff(a, b, STEP_FIELDS, existing_only=True)
     assert all(v == 0.0 for v in d.values()), d
+    assert compare_particles(a, b) == 0.0
