@@ -328,9 +328,9 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch);
  * plain stream order. The results are bit-identical either way. */
 int mac_set_dependent_launch(void* ctx, int on);
 /* mac_step (pipeline A): on = 1 (default) bins the particles by brick and cell
- * on a second stream of the context right after the topology, overlapping
- * RK2-TVD and the extrapolation (the particles do not move in between); 0
- * bins them in the move itself. The results are bit-identical either way.
+ * on a second stream of the context, started when the first projection's CG
+ * loop begins and overlapping the rest of RK2-TVD and the extrapolation (the
+ * particles do not move in between); 0 bins them in the move itself. The results are bit-identical either way.
  * With 1, the "move" phase of mac_get_profile holds the RK4 move alone. */
 int mac_set_concurrent_binning(void* ctx, int on);
 /* The multigrid's smoother and coarse operators: weights w1, w2 of the two

@@ -948,6 +948,17 @@ int move_binned(Ctx* c) {
   return check(cudaGetLastError());
 }
 
+int launch_side_binning(Ctx* c) {
+  if (!c->bin_pending) return MAC_OK;
+  c->bin_pending = 0;
+  int rc = check(cudaEventRecord(c->ev_topo, c->stream));
+  if (!rc) rc = check(cudaStreamWaitEvent(c->side, c->ev_topo, 0));
+  if (!rc) rc = bin_particles(c, c->side);
+  if (!rc) rc = check(cudaEventRecord(c->ev_bins, c->side));
+  if (!rc) c->bin_launched = 1;
+  return rc;
+}
+
 int move_particles(Ctx* c) {
   if (c->np_host == 0 || c->nlive_host == 0) return MAC_OK;
   prof_begin(c, PH_MOVE);

@@ -262,8 +262,13 @@ static int create(const mac_params* p, Ctx** out) {
   size_t nc = (size_t)c->cap_bricks * kCells;
   int rc = MAC_OK;
   auto A = [&](int r) { if (rc == MAC_OK) rc = r; };
-  A(check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)));
-  A(check(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)));
+  // the context's stream at the highest priority, the side stream (particle
+  // binning beside the solve) at the lowest: the block scheduler serves the
+  // solve's kernels first and the binning fills what they leave
+  int prio_low = 0, prio_high = 0;
+  A(check(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)));
+  A(check(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_high)));
+  A(check(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_low)));
   A(check(cudaEventCreateWithFlags(&c->ev_topo, cudaEventDisableTiming)));
   A(check(cudaEventCreateWithFlags(&c->ev_bins, cudaEventDisableTiming)));
   A(dalloc(&c->bkey, 3 * c->cap_bricks));

@@ -244,6 +244,8 @@ struct Ctx {
   int pdl = 1;                 // CG-loop kernels launched with programmatic stream serialisation
   // particle binning on a second stream, overlapping the step's projections
   int bin_side = 1;
+  int bin_pending = 0;   // the step wants its binning started beside the first solve
+  int bin_launched = 0;  // it was: the context's stream must wait on ev_bins
   cudaStream_t side = nullptr;
   cudaEvent_t ev_topo = nullptr;  // the topology is done (the binning may start)
   cudaEvent_t ev_bins = nullptr;  // the binning is done (the move may start)
@@ -552,6 +554,9 @@ int move_particles(Ctx* c);
 // the RK4 move of the binned particles on the context's stream.
 int bin_particles(Ctx* c, cudaStream_t st);
 int move_binned(Ctx* c);
+// Starts the pending binning on the side stream (once per step, at the first
+// projection's CG loop, where the device is latency-bound).
+int launch_side_binning(Ctx* c);
 int alloc_solver(Ctx* c);
 void free_solver(Ctx* c);
 int mg_setup(Ctx* c);

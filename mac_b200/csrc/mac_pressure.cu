@@ -831,6 +831,8 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
       k_residual<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
       k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
     }
+    // a step's particle binning runs beside this solve's iterations
+    if ((rc = launch_side_binning(c))) return rc;
     int first = 1;
     // Learned preconditioner: flexible CG until it stalls (the residual norm
     // falls by less than 2x over kStallWindow iterations, or kLearnedMax

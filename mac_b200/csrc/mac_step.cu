@@ -74,24 +74,23 @@ static int step_b(Ctx* c) {
 
 // One step of test/TestJetDEau_Basic.cpp:434-441. The particles do not move
 // between the topology and the move, so their binning by brick and cell runs
-// on a second stream from the end of the topology, overlapping RK2-TVD (whose
-// projections are latency-bound and leave memory bandwidth free) and the
-// extrapolation; the context's stream waits for it before the move, and on
-// every early return, since the binning swaps the current particle buffers.
+// on a second stream, started when the first projection's CG loop begins
+// (its iterations are latency-bound and leave memory bandwidth free) and
+// overlapping the rest of RK2-TVD and the extrapolation; the context's stream
+// waits for it before the move, and on every early return, since the binning
+// swaps the current particle buffers.
 static int step(Ctx* c) {
   if (c->dp.pipeline == 1) return step_b(c);
   int rc = topology_rebuild(c, false);
   if (rc) return rc;
-  bool side = false;
-  if (c->bin_side && c->np_host > 0 && c->nlive_host > 0) {
-    rc = check(cudaEventRecord(c->ev_topo, c->stream));
-    if (!rc) rc = check(cudaStreamWaitEvent(c->side, c->ev_topo, 0));
-    if (!rc) rc = bin_particles(c, c->side);
-    if (!rc) rc = check(cudaEventRecord(c->ev_bins, c->side));
-    if (rc) return rc;
-    side = true;
-  }
-  auto join = [&]() -> int { return side ? check(cudaStreamWaitEvent(c->stream, c->ev_bins, 0)) : MAC_OK; };
+  c->bin_pending = c->bin_side && c->np_host > 0 && c->nlive_host > 0 ? 1 : 0;
+  c->bin_launched = 0;
+  auto join = [&]() -> int {
+    c->bin_pending = 0;
+    if (!c->bin_launched) return MAC_OK;
+    c->bin_launched = 0;
+    return check(cudaStreamWaitEvent(c->stream, c->ev_bins, 0));
+  };
   int ode = rk2tvd(c);
   if (ode && ode != MAC_ERR_NOT_CONVERGED) {
     join();
@@ -101,8 +100,9 @@ static int step(Ctx* c) {
     join();
     return rc;
   }
+  const bool binned = c->bin_launched != 0;
   if ((rc = join())) return rc;
-  if (side) {
+  if (binned) {
     prof_begin(c, PH_MOVE);
     rc = move_binned(c);
     prof_end(c, PH_MOVE);
