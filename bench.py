@@ -433,7 +433,7 @@ def run_ours(args, rank, world, local_rank):
                   device=dev, div_check=True, warm_start=args.warm_start)
     ctx.set_multigrid(args.mg_sweeps, args.prefetch)
     ctx.set_dependent_launch(not args.no_dependent_launch)
-    ctx.set_concurrent_binning(not args.no_concurrent_binning)
+    ctx.set_concurrent_binning(args.concurrent_binning)
     if args.solver.startswith("learned"):
         from mac_b200.unet import UNet
         net_main = UNet(dev)
@@ -565,7 +565,7 @@ def run_ours(args, rank, world, local_rank):
                    "solver": SOLVER_NAMES[args.solver], "mg_sweeps0": args.mg_sweeps,
                    "mg_prefetch": args.prefetch,
                    "dependent_launch": not args.no_dependent_launch,
-                   "concurrent_binning": not args.no_concurrent_binning,
+                   "concurrent_binning": args.concurrent_binning,
                    "rtol": 1e-8, "initial_guess": "last pressure" if args.warm_start else "zero",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state > 3 GB)",
@@ -606,8 +606,8 @@ def main():
                     help="run the V-cycle's first kernel as resident blocks prefetching bricks with bulk copies")
     ap.add_argument("--no-dependent-launch", action="store_true",
                     help="launch the CG loop's kernels in plain stream order")
-    ap.add_argument("--no-concurrent-binning", action="store_true",
-                    help="bin the particles inside the move instead of on a second stream during RK2-TVD")
+    ap.add_argument("--concurrent-binning", action="store_true",
+                    help="bin the particles on a second stream during RK2-TVD instead of inside the move")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the standalone 128^3 pressure-solve timing")
     ap.add_argument("--warm-start", action="store_true",

@@ -327,12 +327,20 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch);
  * previous kernel drains and wait on the device for its completion; 0 uses
  * plain stream order. The results are bit-identical either way. */
 int mac_set_dependent_launch(void* ctx, int on);
-/* mac_step (pipeline A): on = 1 (default) bins the particles by brick and cell
- * on a second stream of the context, started when the first projection's CG
- * loop begins and overlapping the rest of RK2-TVD and the extrapolation (the
- * particles do not move in between); 0 bins them in the move itself. The results are bit-identical either way.
- * With 1, the "move" phase of mac_get_profile holds the RK4 move alone. */
+/* mac_step (pipeline A): on = 1 bins the particles by brick and cell on a
+ * second stream of the context, started when the first projection's CG loop
+ * begins and overlapping the rest of RK2-TVD and the extrapolation (the
+ * particles do not move in between); 0 (default) bins them in the move
+ * itself. The results are bit-identical either way. On the 256x256x512 jet
+ * the binning's memory traffic slows the solve by about what it saves, so the
+ * default keeps one stream. With 1, the "move" phase of mac_get_profile holds
+ * the RK4 move alone. */
 int mac_set_concurrent_binning(void* ctx, int on);
+/* The multigrid's dense levels (level 3, one cell per brick, and its
+ * coarsenings): levels of more than max_cells cells (at least 64) run as
+ * device-wide sweep kernels, the rest in one 1024-thread block that solves the
+ * coarsest exactly. Default 1024. */
+int mac_set_coarse_block(void* ctx, int max_cells);
 /* The multigrid's smoother and coarse operators: weights w1, w2 of the two
  * Jacobi sweeps before and after each coarse correction (on every level), the
  * weight of the single finest-level sweep (mac_set_multigrid(ctx, 1, .)), and

@@ -216,6 +216,8 @@ struct Ctx {
   void* dense_buf = nullptr;   // dense levels: 9 arrays (e, e2, r, 6 weights) per cell
   size_t dense_bytes = 0;
   size_t dense_smem = 0;
+  int dense_lo = 1;              // first dense level of the one-block coarse solve
+  int blk_max_cells = 1024;      // the largest level it takes; larger ones run device-wide
   double* coarse_inv = nullptr;  // [64][64] inverse of the coarsest dense level
   int* coarse_ok = nullptr;      // 1 when coarse_inv is valid
   int smem_optin = 0;
@@ -242,8 +244,9 @@ struct Ctx {
   long long launches = 0;      // kernels launched by this context
   struct Prof* prof = nullptr; // per-phase event timing (null when off)
   int pdl = 1;                 // CG-loop kernels launched with programmatic stream serialisation
-  // particle binning on a second stream, overlapping the step's projections
-  int bin_side = 1;
+  // particle binning on a second stream, overlapping the step's first
+  // projection (measured no faster on the 256x256x512 jet: off by default)
+  int bin_side = 0;
   int bin_pending = 0;   // the step wants its binning started beside the first solve
   int bin_launched = 0;  // it was: the context's stream must wait on ev_bins
   cudaStream_t side = nullptr;

@@ -1563,9 +1563,14 @@ static int dense_layout(Ctx* c) {
     if (rc) return rc;
     c->dense_bytes = need + need / 4;
   }
-  // smem staging of the block-solved levels (1..): 9 arrays per cell
+  // levels above blk_max_cells run as device-wide sweeps (level 3 always);
+  // the rest go to the one-block solve, staged in shared memory (9 arrays per
+  // cell) when they fit
+  int lo = 1;
+  while (lo < nl - 1 && c->dense[lo].n > c->blk_max_cells) ++lo;
+  c->dense_lo = lo;
   int64_t cells = 0;
-  for (int l = 1; l < nl; ++l) cells += c->dense[l].n;
+  for (int l = lo; l < nl; ++l) cells += c->dense[l].n;
   c->dense_smem = (size_t)cells * 9 * ts;
   return check(cudaMemsetAsync(c->dense_buf, 0, (size_t)off * 9 * ts, c->stream));
 }
@@ -1662,18 +1667,25 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
-    DView<T> d4 = dview<T>(c, 1);
-    launch_k(c, kd_pre<T>, grid_for(d3.n, 256), 256, 0, d3, dn); MAC_COUNT(c);
-    launch_k(c, kd_restrict<T>, grid_for(8 * d4.n, 256), 256, 0, d3, d4, dn); MAC_COUNT(c);
+    // dense levels 0 .. lo-1 device-wide, lo .. in one block
+    const int lo = c->dense_lo;
+    for (int l = 0; l < lo; ++l) {
+      const DView<T> L = dview<T>(c, l), C = dview<T>(c, l + 1);
+      launch_k(c, kd_pre<T>, grid_for(L.n, 256), 256, 0, L, dn); MAC_COUNT(c);
+      launch_k(c, kd_restrict<T>, grid_for(8 * C.n, 256), 256, 0, L, C, dn); MAC_COUNT(c);
+    }
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
-    S.lo = 1;
+    S.lo = lo;
     S.hi = c->ndense;
     int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
     launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv, c->coarse_ok,
              dn); MAC_COUNT(c);
-    launch_k(c, kd_jacobi<T, true>, grid_for(d3.n, 256), 256, 0, d3, d3.e, d3.e2, d4, dn); MAC_COUNT(c);
-    launch_k(c, kd_jacobi<T, false>, grid_for(d3.n, 256), 256, 0, d3, d3.e2, d3.e, d4, dn); MAC_COUNT(c);
+    for (int l = lo - 1; l >= 0; --l) {
+      const DView<T> L = dview<T>(c, l), C = dview<T>(c, l + 1);
+      launch_k(c, kd_jacobi<T, true>, grid_for(L.n, 256), 256, 0, L, L.e, L.e2, C, dn); MAC_COUNT(c);
+      launch_k(c, kd_jacobi<T, false>, grid_for(L.n, 256), 256, 0, L, L.e2, L.e, C, dn); MAC_COUNT(c);
+    }
   } else {
     DenseSet<T> S;
     S.L[0] = d3;

@@ -576,6 +576,14 @@ int mac_set_multigrid(void* ctx, int sweeps0, int prefetch) {
   return MAC_OK;
 }
 
+int mac_set_coarse_block(void* ctx, int max_cells) {
+  CTX_OR_FAIL();
+  if (max_cells < 64) return MAC_ERR_INVALID;
+  c->blk_max_cells = max_cells;
+  c->system_ready = false;  // the level split is made with the system
+  return MAC_OK;
+}
+
 int mac_set_concurrent_binning(void* ctx, int on) {
   CTX_OR_FAIL();
   if (on != 0 && on != 1) return MAC_ERR_INVALID;

@@ -69,7 +69,7 @@ EXPORTS = ["mac_default_params", "mac_ctx_create", "mac_ctx_destroy", "mac_get_s
            "mac_unet_create", "mac_unet_destroy", "mac_unet_nparams", "mac_unet_init", "mac_unet_get_params",
            "mac_unet_set_params", "mac_unet_forward", "mac_unet_loss_grad", "mac_unet_adam_step",
            "mac_unet_make_dataset", "mac_unet_make_dataset_ext", "mac_unet_get_sample", "mac_unet_train", "mac_unet_launch_count",
-           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_set_dependent_launch", "mac_set_concurrent_binning", "mac_set_smoother", "mac_unet_set_loss", "mac_unet_time_forward",
+           "mac_set_preconditioner_net", "mac_set_learned_smoothing", "mac_set_multigrid", "mac_set_dependent_launch", "mac_set_concurrent_binning", "mac_set_coarse_block", "mac_set_smoother", "mac_unet_set_loss", "mac_unet_time_forward",
            "mac_unet_set_conv"]
 PHASES = ["topology", "forces", "setup", "divergence", "spmv", "cg_vector", "vcycle", "gradient", "extrapolate",
           "move"]
@@ -140,6 +140,7 @@ def load(path: str = LIB_PATH):
     lib.mac_set_multigrid.argtypes = [vp, i32, i32]
     lib.mac_set_dependent_launch.argtypes = [vp, i32]
     lib.mac_set_concurrent_binning.argtypes = [vp, i32]
+    lib.mac_set_coarse_block.argtypes = [vp, i32]
     lib.mac_set_smoother.argtypes = [vp, f64, f64, f64, f64]
     lib.mac_unet_set_loss.argtypes = [vp, i32]
     lib.mac_unet_time_forward.argtypes = [vp, i32, i32, i32, i32, i32, _P(f64), _P(f64)]
@@ -461,9 +462,14 @@ class Context:
         (default on) or in plain stream order; bit-identical results."""
         self._check(self.lib.mac_set_dependent_launch(self.h, 1 if on else 0), "mac_set_dependent_launch")
 
+    def set_coarse_block(self, max_cells=1024):
+        """Dense multigrid levels above max_cells cells as device-wide sweeps,
+        the rest in the one-block coarse solve."""
+        self._check(self.lib.mac_set_coarse_block(self.h, int(max_cells)), "mac_set_coarse_block")
+
     def set_concurrent_binning(self, on=True):
-        """Particle binning on a second stream during RK2-TVD (default) or
-        inside the move; bit-identical results."""
+        """Particle binning on a second stream during RK2-TVD or inside the
+        move (the default); bit-identical results."""
         self._check(self.lib.mac_set_concurrent_binning(self.h, 1 if on else 0), "mac_set_concurrent_binning")
 
     # ---- drop-in CSC solver

@@ -120,3 +120,21 @@ def test_smoother_settings(pool64):
                     (0.3, 4.0, 0.9, 0.6)):
             with pytest.raises(MacError):
                 ctx.set_smoother(*bad)
+
+
+@pytest.mark.parametrize("max_cells", [64, 1 << 30])
+def test_coarse_block_split(pool64, max_cells):
+    """Dense multigrid levels moved between the device-wide sweeps and the
+    one-block coarse solve (every dense level but the coarsest device-wide,
+    or all in the block): the same solve to within the tolerance, with about
+    the same number of iterations."""
+    out = []
+    for mc in (1024, max_cells):
+        with _ctx(pool64, "mixed", 1e-12, 500) as ctx:
+            ctx.set_coarse_block(mc)
+            ctx.upload(pool64)
+            ctx.project(0)
+            got = ctx.download()
+            out.append((ctx.stats()["iterations"], got.f64["p"][got.exists.astype(bool)].copy()))
+    assert abs(out[1][0] - out[0][0]) <= 2, (out[0][0], out[1][0])
+    assert np.linalg.norm(out[1][1] - out[0][1]) / np.linalg.norm(out[0][1]) <= 1e-9
