@@ -437,9 +437,13 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   // vector loads); only beta comes from the previous launch
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  // the stencil pass gives each thread a z-run of four cells of one (x, y)
+  // column, cells (t & 63) + 256 (t >> 6) + 64 k, so a cell's z neighbours
+  // inside the run come from registers instead of shared memory
+  const int ob = (threadIdx.x & 63) + 256 * (threadIdx.x >> 6);
   uint16_t mk[kCPT];
 #pragma unroll
-  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
+  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + ob + 64 * k];
   const int o4 = 4 * threadIdx.x;
   double vz[4], vp[4] = {0.0, 0.0, 0.0, 0.0};
   load4(z + (int64_t)b * kCells + o4, vz);
@@ -455,24 +459,31 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
 #pragma unroll
   for (int k = 0; k < 4; ++k) sp[si4 + k] = first ? vz[k] : vz[k] + be * vp[k];
   __syncthreads();
+  const int si0 = s1_of(ob);
+  double pcs[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) pcs[k] = sp[si0 + 100 * k];
   double pq = 0;
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    int o = threadIdx.x + kBT * k;
-    int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = mk[k];
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
+    const uint16_t m = mk[k];
     if (!(m & kDomainBit)) {
       pnew[c] = 0.0;
       q[c] = 0.0;
       continue;
     }
-    int si = s1_of(o);
-    double pc = sp[si];
+    const int si = si0 + 100 * k;
+    const double pc = pcs[k];
     double s = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) s += P.ih2[f >> 1] * pc;
-      if (m & (1u << f)) s -= P.ih2[f >> 1] * sp[si + s1_off(f)];
+      if (m & (1u << f)) {
+        const double pn = f == 4 ? (k > 0 ? pcs[k - 1] : sp[si - 100])
+                                 : (f == 5 ? (k < kCPT - 1 ? pcs[k + 1] : sp[si + 100]) : sp[si + s1_off(f)]);
+        s -= P.ih2[f >> 1] * pn;
+      }
     }
     pnew[c] = pc;
     q[c] = s;
