@@ -462,6 +462,20 @@ __device__ inline void load4(const float* p, V* v) {
   v[0] = (V)a.x; v[1] = (V)a.y; v[2] = (V)a.z; v[3] = (V)a.w;
 }
 
+// Stencil passes over a staged brick give thread t the z-run of four cells
+// (t & 63) + 256 (t >> 6) + 64 k, k = 0..3, of one (x, y) column: the loads
+// and stores of each k stay coalesced, and a cell's z neighbours inside the
+// run are the thread's own staged values (v[k -+ 1]) rather than shared-memory
+// reads; zrun_nbr gives the face-f neighbour of run cell k at staging slot si.
+static_assert(kCPT == 4, "z-runs of four cells");
+__device__ inline int zrun_base() { return (threadIdx.x & 63) + 256 * (threadIdx.x >> 6); }
+template <class S>
+__device__ inline S zrun_nbr(const S* s, const S* v, int si, int k, int f) {
+  if (f == 4) return k > 0 ? v[k - 1] : s[si - 100];
+  if (f == 5) return k < kCPT - 1 ? v[k + 1] : s[si + 100];
+  return s[si + s1_off(f)];
+}
+
 // The face halos of a brick staging: s[slot] = val(global index), 0 where the
 // neighbour brick is absent; all three loads are issued before any store.
 template <class S, class F>

@@ -154,11 +154,14 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   // the V-cycle's first kernel, two launches back)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  // the stencil pass takes a z-run of four cells of one column per thread
+  // (cells zrun_base() + 64 k): z neighbours inside the run from registers
+  const int ob = zrun_base();
   uint16_t mk[kCPT];
   double rk[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    const int64_t c = (int64_t)b * kCells + threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
     mk[k] = fmask[c];
     rk[k] = r[c];
   }
@@ -167,23 +170,26 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   __syncthreads();
   stage_arr(se, e, b, sb);
   __syncthreads();
+  const int si0 = s1_of(ob);
+  T ecs[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) ecs[k] = se[si0 + 100 * k];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    int o = threadIdx.x + kBT * k;
-    uint16_t m = mk[k];
+    const uint16_t m = mk[k];
     T v = 0;
     if (m & kDomainBit) {
-      int si = s1_of(o);
-      T ec = se[si];
+      const int si = si0 + 100 * k;
+      const T ec = ecs[k];
       T me = 0;
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
         if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
-        if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
+        if (m & (1u << f)) me -= ih2[f >> 1] * zrun_nbr(se, ecs, si, k, f);
       }
       v = (T)rk[k] - me;
     }
-    res[o] = v;
+    res[ob + 64 * k] = v;
   }
   __syncthreads();
   int o = threadIdx.x;
@@ -217,11 +223,12 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
   // the brick's pre-smoothed e (both written many launches back)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  const int ob = zrun_base();  // the stencil pass's z-run (cells ob + 64 k)
   uint16_t mk[kCPT];
   double rk[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    const int64_t c = (int64_t)b * kCells + threadIdx.x + kBT * k;
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
     mk[k] = fmask[c];
     rk[k] = r[c];
   }
@@ -246,24 +253,27 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
     stage_arr(se, e, b, sb);
   }
   __syncthreads();
+  const int si0 = s1_of(ob);
+  T eps[kCPT];
+#pragma unroll
+  for (int k = 0; k < kCPT; ++k) eps[k] = se[si0 + 100 * k];
   double rz = 0;
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    int o = threadIdx.x + kBT * k;
-    int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = mk[k];
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
+    const uint16_t m = mk[k];
     if (!(m & kDomainBit)) {
       if (FIRST) eout[c] = (T)0;
       else z[c] = 0.0;
       continue;
     }
-    int si = s1_of(o);
-    T epc = se[si];
+    const int si = si0 + 100 * k;
+    const T epc = eps[k];
     T me = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) me += ih2[f >> 1] * epc;
-      if (m & (1u << f)) me -= ih2[f >> 1] * se[si + s1_off(f)];
+      if (m & (1u << f)) me -= ih2[f >> 1] * zrun_nbr(se, eps, si, k, f);
     }
     double rc = rk[k];
     T out = epc + om * (T)P.dtab[active_index(m)] * ((T)rc - me);

@@ -437,10 +437,7 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   // vector loads); only beta comes from the previous launch
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  // the stencil pass gives each thread a z-run of four cells of one (x, y)
-  // column, cells (t & 63) + 256 (t >> 6) + 64 k, so a cell's z neighbours
-  // inside the run come from registers instead of shared memory
-  const int ob = (threadIdx.x & 63) + 256 * (threadIdx.x >> 6);
+  const int ob = zrun_base();  // the stencil pass's z-run (cells ob + 64 k)
   uint16_t mk[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + ob + 64 * k];
@@ -479,11 +476,7 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       if (m & (1u << (8 + f))) s += P.ih2[f >> 1] * pc;
-      if (m & (1u << f)) {
-        const double pn = f == 4 ? (k > 0 ? pcs[k - 1] : sp[si - 100])
-                                 : (f == 5 ? (k < kCPT - 1 ? pcs[k + 1] : sp[si + 100]) : sp[si + s1_off(f)]);
-        s -= P.ih2[f >> 1] * pn;
-      }
+      if (m & (1u << f)) s -= P.ih2[f >> 1] * zrun_nbr(sp, pcs, si, k, f);
     }
     pnew[c] = pc;
     q[c] = s;
