@@ -84,24 +84,27 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
                                               Params P) {
   __shared__ int64_t sb[6];
   __shared__ T sr[kS1];  // w D^-1 r of the brick and its face halo
-  __shared__ uint16_t sm[kCells];
   const T om = (T)P.mgw1, om2 = (T)P.mgw2, c0 = (T)(P.mgw1 + P.mgw2 - P.mgw1 * P.mgw2);
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
-  // prologue (static): brick, face neighbours, face masks
+  // prologue (static): brick, face neighbours, face masks; each thread takes
+  // the z-run of four cells ob + 64 k (its z neighbours' staged values then
+  // come from registers in the stencil pass)
   int b = dbl[blockIdx.x];
   load_face_bases(nbr, b, sb);
+  const int ob = zrun_base();
   uint16_t mk[kCPT];
 #pragma unroll
-  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + threadIdx.x + kBT * k];
+  for (int k = 0; k < kCPT; ++k) mk[k] = fmask[(int64_t)b * kCells + ob + 64 * k];
   pdl_entry();
   if (solve_done(&ds->done)) return;
   const double al = update ? ds->alpha : 0.0;
+  const int si0 = s1_of(ob);
   double rv[kCPT];
+  T srv[kCPT];
   double rr = 0;
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    const int o = threadIdx.x + kBT * k;
-    const int64_t c = (int64_t)b * kCells + o;
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
     double v = rin[c];
     if (update) {
       v = v - al * q[c];
@@ -110,9 +113,8 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
       rr += v * v;
     }
     rv[k] = v;
-    const uint16_t m = mk[k];
-    sm[o] = m;
-    sr[s1_of(o)] = om * (T)P.dtab[active_index(m)] * (T)v;
+    srv[k] = om * (T)P.dtab[active_index(mk[k])] * (T)v;
+    sr[si0 + 100 * k] = srv[k];
   }
   __syncthreads();
   stage_h1_halo(sr, sb, [&](int64_t i) {
@@ -122,17 +124,16 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
-    int o = threadIdx.x + kBT * k;
-    int64_t c = (int64_t)b * kCells + o;
-    uint16_t m = sm[o];
+    const int64_t c = (int64_t)b * kCells + ob + 64 * k;
+    const uint16_t m = mk[k];
     T out = 0;
     if (m & kDomainBit) {
-      int si = s1_of(o);
-      T dinv = (T)P.dtab[active_index(m)];
+      const int si = si0 + 100 * k;
+      const T dinv = (T)P.dtab[active_index(m)];
       T s = 0;
 #pragma unroll
       for (int f = 0; f < 6; ++f)
-        if (m & (1u << f)) s += ih2[f >> 1] * sr[si + s1_off(f)];
+        if (m & (1u << f)) s += ih2[f >> 1] * zrun_nbr(sr, srv, si, k, f);
       out = dinv * (c0 * (T)rv[k] + om2 * s);
     }
     e[c] = out;
