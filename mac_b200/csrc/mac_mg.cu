@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
   const bool live = g < (int64_t)nd * N;
   size_t i = 0;
   T dinv = 0;
-  int64_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};
+  uint32_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};  // cell indices of a level (below 2^32: 64 per brick)
   T wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0}, dl[3] = {0, 0, 0}, dr[3] = {0, 0, 0};
   if (live) {
     const int* sb = sbr + 7 * (threadIdx.x / N);
@@ -733,8 +733,8 @@ __global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int n
     lnbrs<D>(sb, x, y, z, n);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      jl[a] = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
-      jr[a] = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+      jl[a] = (uint32_t)(n[2 * a] < 0 ? (int64_t)i : n[2 * a]);
+      jr[a] = (uint32_t)(n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1]);
       wl[a] = w[a * ncap + i];
       dl[a] = w[4 * ncap + jl[a]];
       wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr[a]];
@@ -792,7 +792,7 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
   int b = 0, p = 0;
   bool act = false;
   size_t i = 0;
-  int64_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};
+  uint32_t jl[3] = {0, 0, 0}, jr[3] = {0, 0, 0};  // cell indices of a level (below 2^32)
   T wd = 0, ri = 0, wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0};
   if (live) {
     b = sb[0];
@@ -808,8 +808,8 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
       lnbrs<D>(sb, x, y, z, n);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        jl[a] = n[2 * a] < 0 ? (int64_t)i : n[2 * a];
-        jr[a] = n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1];
+        jl[a] = (uint32_t)(n[2 * a] < 0 ? (int64_t)i : n[2 * a]);
+        jr[a] = (uint32_t)(n[2 * a + 1] < 0 ? (int64_t)i : n[2 * a + 1]);
         wl[a] = w[a * ncap + i];
         wr[a] = n[2 * a + 1] < 0 ? (T)0 : w[a * ncap + jr[a]];
       }
@@ -875,14 +875,21 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
   const int x = o % D, y = (o / D) % D, z = o / (D * D);
   // stencil points: 0 = the cell, 1 + 2a / 2 + 2a = its -/+ neighbour on axis
   // a (an absent neighbour is the cell itself and drops out through its zero
-  // weight); slot in the brick table and local coordinates
-  int ks[7], lx[7], ly[7], lz[7];
-  ks[0] = 0;
-  lx[0] = x;
-  ly[0] = y;
-  lz[0] = z;
+  // weight): their cell indices ei in this level and, with the coarse
+  // correction, ci in the coarser one (32-bit: below 64 cells a brick)
+  uint32_t ei[7], ci[7];
   T wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0}, ev[7] = {0, 0, 0, 0, 0, 0, 0};
   T dinv = 0, wd = 0, ri = 0;
+  const int jt = 7 * (threadIdx.x / N);  // this brick's row in the tables
+  auto point = [&](int q, int k, int px, int py, int pz) {
+    const int nb = sb[k];
+    ei[q] = (uint32_t)((size_t)nb * N + px + D * py + D * D * pz);
+    if (WITH_COARSE) {
+      if (D == 2) ci[q] = (uint32_t)sdi[jt + k];
+      else ci[q] = (uint32_t)((size_t)nb * H * H * H + (px >> 1) + H * (py >> 1) + H * H * (pz >> 1));
+    }
+  };
+  point(0, 0, x, y, z);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int c[3] = {x, y, z};
@@ -895,17 +902,11 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     const bool hl = sb[kl] >= 0, hr = sb[kr] >= 0;
     if (!hl) { kl = 0; pl[0] = x; pl[1] = y; pl[2] = z; }
     if (!hr) { kr = 0; pr[0] = x; pr[1] = y; pr[2] = z; }
-    ks[1 + 2 * a] = kl;
-    lx[1 + 2 * a] = pl[0];
-    ly[1 + 2 * a] = pl[1];
-    lz[1 + 2 * a] = pl[2];
-    ks[2 + 2 * a] = kr;
-    lx[2 + 2 * a] = pr[0];
-    ly[2 + 2 * a] = pr[1];
-    lz[2 + 2 * a] = pr[2];
     if (live) {
+      point(1 + 2 * a, kl, pl[0], pl[1], pl[2]);
+      point(2 + 2 * a, kr, pr[0], pr[1], pr[2]);
       wl[a] = w[a * ncap + i];
-      wr[a] = hr ? w[a * ncap + (size_t)sb[kr] * N + pr[0] + D * pr[1] + D * D * pr[2]] : (T)0;
+      wr[a] = hr ? w[a * ncap + ei[2 + 2 * a]] : (T)0;
     }
   }
   if (live) {
@@ -914,7 +915,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
     ri = r[i];
     if (WITH_COARSE) {
 #pragma unroll
-      for (int q = 0; q < 7; ++q) ev[q] = e[(size_t)sb[ks[q]] * N + lx[q] + D * ly[q] + D * D * lz[q]];
+      for (int q = 0; q < 7; ++q) ev[q] = e[ei[q]];
     }
   }
   pdl_entry();
@@ -926,13 +927,8 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
   // e plus the coarse correction at each stencil point
 #pragma unroll
   for (int q = 0; q < 7; ++q) {
-    const int nb = sb[ks[q]];
-    if (WITH_COARSE) {
-      if (D == 2) ev[q] += ec[sdi[7 * (threadIdx.x / N) + ks[q]]];
-      else ev[q] += ec[(size_t)nb * H * H * H + (lx[q] >> 1) + H * (ly[q] >> 1) + H * H * (lz[q] >> 1)];
-    } else {
-      ev[q] = e[(size_t)nb * N + lx[q] + D * ly[q] + D * D * lz[q]];
-    }
+    if (WITH_COARSE) ev[q] += ec[ci[q]];
+    else ev[q] = e[ei[q]];
   }
   T s = wd * ev[0];
 #pragma unroll
