@@ -1134,150 +1134,6 @@ __global__ void kd_jacobi(DView<T> L, const T* __restrict__ ein, T* __restrict__
   eout[i] = vc + (WITH_COARSE ? L.w1 : L.w2) * dinv * (ri - s);
 }
 
-// ---------------------------------- dense levels: fused pre/restrict and post
-// The device-wide dense levels (level 3 and, on large domains, level 4) hold
-// at most a few tens of thousands of cells, all in L2, so recomputing a
-// neighbour's sweep is cheaper than a kernel boundary: kd_pre_restrict forms
-// the two pre-sweeps from zero at a fine cell and its six neighbours and
-// restricts the residual (one launch instead of kd_pre + kd_restrict), and
-// kd_post applies both post-sweeps, the first recomputed at the cell's six
-// neighbours (one launch instead of two kd_jacobi). Every value is formed by
-// the same expression, in the same order, as in the separate kernels.
-
-// kd_pre's value at cell i (coordinates c): two sweeps from zero.
-template <class T>
-__device__ inline T dense_pre_e(const DView<T>& L, int64_t i, const int* c) {
-  const int64_t n = L.n;
-  const T dinv = L.w[4 * n + i];
-  if (dinv == 0) return (T)0;
-  const int dim[3] = {L.nx, L.ny, L.nz};
-  const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  T s = 0;
-  for (int a = 0; a < 3; ++a) {
-    const T wl = L.w[a * n + i];
-    if (wl != 0 && c[a] > 0) s += wl * L.w1 * L.w[4 * n + i - stride[a]] * L.r[i - stride[a]];
-    if (c[a] + 1 < dim[a]) {
-      const T wr = L.w[a * n + i + stride[a]];
-      if (wr != 0) s += wr * L.w1 * L.w[4 * n + i + stride[a]] * L.r[i + stride[a]];
-    }
-  }
-  return dinv * ((L.w1 + L.w2 - L.w1 * L.w2) * L.r[i] + L.w2 * s);
-}
-
-template <class T>
-__global__ void kd_pre_restrict(DView<T> F, DView<T> C, const int32_t* __restrict__ done) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t I = g >> 3;
-  const int k = (int)(g & 7);
-  pdl_entry();
-  if (solve_done(done)) return;
-  const int64_t n = F.n;
-  T s = 0;
-  if (I < C.n) {
-    int X, Y, Z;
-    coords3(I, C.nx, C.ny, C.n, X, Y, Z);
-    const int c[3] = {2 * X + (k & 1), 2 * Y + ((k >> 1) & 1), 2 * Z + (k >> 2)};
-    if (c[0] < F.nx && c[1] < F.ny && c[2] < F.nz) {
-      const int64_t i = F.at(c[0], c[1], c[2]);
-      const T ei = dense_pre_e(F, i, c);
-      F.e[i] = ei;
-      if (F.w[4 * n + i] != 0) {
-        // r - M e in dense_apply's order, neighbours' e recomputed
-        const int dim[3] = {F.nx, F.ny, F.nz};
-        const int64_t stride[3] = {1, F.nx, (int64_t)F.nx * F.ny};
-        T m = F.w[3 * n + i] * ei;
-        for (int a = 0; a < 3; ++a) {
-          int p[3] = {c[0], c[1], c[2]};
-          const T wl = F.w[a * n + i];
-          if (wl != 0 && c[a] > 0) {
-            p[a] = c[a] - 1;
-            m -= wl * dense_pre_e(F, i - stride[a], p);
-          }
-          if (c[a] + 1 < dim[a]) {
-            const T wr = F.w[a * n + i + stride[a]];
-            if (wr != 0) {
-              p[a] = c[a] + 1;
-              m -= wr * dense_pre_e(F, i + stride[a], p);
-            }
-          }
-        }
-        s = F.r[i] - m;
-      }
-    }
-  }
-  s = sum8(s);
-  if (I < C.n && k == 0) C.r[I] = (T)s;
-}
-
-// kd_jacobi<true>'s value at cell j (coordinates c): the first post-sweep,
-// the coarse correction added to every e it reads.
-template <class T>
-__device__ inline T dense_post1(const DView<T>& L, const DView<T>& C, int64_t j, const int* c) {
-  const int64_t n = L.n;
-  const T dinv = L.w[4 * n + j];
-  if (dinv == 0) return (T)0;
-  auto ev = [&](int64_t q, int xx, int yy, int zz) -> T { return L.e[q] + C.e[C.at(xx >> 1, yy >> 1, zz >> 1)]; };
-  const int dim[3] = {L.nx, L.ny, L.nz};
-  const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-  const T ec = ev(j, c[0], c[1], c[2]);
-  T s = L.w[3 * n + j] * ec;
-  for (int a = 0; a < 3; ++a) {
-    int p[3] = {c[0], c[1], c[2]};
-    const T wl = L.w[a * n + j];
-    if (wl != 0 && c[a] > 0) {
-      p[a] = c[a] - 1;
-      s -= wl * ev(j - stride[a], p[0], p[1], p[2]);
-    }
-    if (c[a] + 1 < dim[a]) {
-      const T wr = L.w[a * n + j + stride[a]];
-      if (wr != 0) {
-        p[a] = c[a] + 1;
-        s -= wr * ev(j + stride[a], p[0], p[1], p[2]);
-      }
-    }
-  }
-  return ec + L.w1 * dinv * (L.r[j] - s);
-}
-
-// Both post-sweeps: L.e <- second sweep of (first sweep of L.e + P C.e).
-template <class T>
-__global__ void kd_post(DView<T> L, DView<T> C, const int32_t* __restrict__ done) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = i < L.n;
-  int c[3] = {0, 0, 0};
-  if (live) coords3(i, L.nx, L.ny, L.n, c[0], c[1], c[2]);
-  pdl_entry();
-  if (!live || solve_done(done)) return;
-  const int64_t n = L.n;
-  const T dinv = L.w[4 * n + i];
-  T out = 0;
-  if (dinv != 0) {
-    // kd_jacobi<false> on the recomputed first sweep
-    const int dim[3] = {L.nx, L.ny, L.nz};
-    const int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
-    const T ec = dense_post1(L, C, i, c);
-    T s = L.w[3 * n + i] * ec;
-    for (int a = 0; a < 3; ++a) {
-      int p[3] = {c[0], c[1], c[2]};
-      const T wl = L.w[a * n + i];
-      if (wl != 0 && c[a] > 0) {
-        p[a] = c[a] - 1;
-        s -= wl * dense_post1(L, C, i - stride[a], p);
-      }
-      if (c[a] + 1 < dim[a]) {
-        const T wr = L.w[a * n + i + stride[a]];
-        if (wr != 0) {
-          p[a] = c[a] + 1;
-          s -= wr * dense_post1(L, C, i + stride[a], p);
-        }
-      }
-    }
-    out = ec + L.w2 * dinv * (L.r[i] - s);
-  }
-  // every block reads L.e at its cells' neighbours: write the result to e2
-  L.e2[i] = out;
-}
-
 // ------------------------------------------- coarse V-cycle in one block
 // Levels lo..hi-1 of the dense hierarchy, staged in shared memory when they
 // fit (else worked on in global memory); __syncthreads separates the sweeps.
@@ -1817,13 +1673,13 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
   launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
-  T* d3c = d3.e;  // level 3's correction for level 2's first post-sweep
   if (c->ndense > 1) {
     // dense levels 0 .. lo-1 device-wide, lo .. in one block
     const int lo = c->dense_lo;
     for (int l = 0; l < lo; ++l) {
       const DView<T> L = dview<T>(c, l), C = dview<T>(c, l + 1);
-      launch_k(c, kd_pre_restrict<T>, grid_for(8 * C.n, 256), 256, 0, L, C, dn); MAC_COUNT(c);
+      launch_k(c, kd_pre<T>, grid_for(L.n, 256), 256, 0, L, dn); MAC_COUNT(c);
+      launch_k(c, kd_restrict<T>, grid_for(8 * C.n, 256), 256, 0, L, C, dn); MAC_COUNT(c);
     }
     DenseSet<T> S;
     for (int l = 0; l < c->ndense; ++l) S.L[l] = dview<T>(c, l);
@@ -1832,15 +1688,11 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
     int use_smem = c->dense_smem <= (size_t)c->smem_optin ? 1 : 0;
     launch_k(c, kd_coarse_block<T>, 1, 1024, use_smem ? c->dense_smem : 0, S, use_smem, c->coarse_inv, c->coarse_ok,
              dn); MAC_COUNT(c);
-    // up: kd_post leaves each device-wide level's correction in its e2 (it
-    // reads e at its cells' neighbours); the block leaves level lo's in e
     for (int l = lo - 1; l >= 0; --l) {
-      const DView<T> L = dview<T>(c, l);
-      DView<T> C = dview<T>(c, l + 1);
-      if (l + 1 < lo) C.e = C.e2;
-      launch_k(c, kd_post<T>, grid_for(L.n, 256), 256, 0, L, C, dn); MAC_COUNT(c);
+      const DView<T> L = dview<T>(c, l), C = dview<T>(c, l + 1);
+      launch_k(c, kd_jacobi<T, true>, grid_for(L.n, 256), 256, 0, L, L.e, L.e2, C, dn); MAC_COUNT(c);
+      launch_k(c, kd_jacobi<T, false>, grid_for(L.n, 256), 256, 0, L, L.e2, L.e, C, dn); MAC_COUNT(c);
     }
-    d3c = d3.e2;
   } else {
     DenseSet<T> S;
     S.L[0] = d3;
@@ -1849,7 +1701,7 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
     launch_k(c, kd_coarse_block<T>, 1, 1024, 0, S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
   // up
-  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3c, e2b, G, sw1,
+  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
            dn); MAC_COUNT(c);
   launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
            sw2, dn); MAC_COUNT(c);
