@@ -586,19 +586,36 @@ __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist,
   __syncthreads();
   int o = threadIdx.x;
   int64_t c = (int64_t)b * kCells + o;
-  if (lay[c] == kMissing) return;
-  bool dc = is_fluid(type[c]);
-  double pc = dc ? x[c] : (pdir ? dir_or_zero(pdir[c]) : 0.0);
-  pres[c] = pc;
-  uint8_t fl = flags[c];
+  // every load a cell may need is issued before any is tested (a missing
+  // neighbour brick reads the cell itself), so no load waits on another
+  int64_t nn[3];
+  int8_t ln[3];
+  uint8_t tn[3];
+  double xn[3];
   double* U[3] = {ux, uy, uz};
+  const int8_t lc = lay[c];
+  const uint8_t tc = type[c], fl = flags[c];
+  const double xc = x[c];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
-    int64_t n = nb0(sb, c, o, 2 * i);
-    bool nexists = n >= 0 && lay[n] != kMissing;
-    bool dn = nexists && is_fluid(type[n]);
+    nn[i] = nb0(sb, c, o, 2 * i);
+    const int64_t m = nn[i] >= 0 ? nn[i] : c;
+    ln[i] = lay[m];
+    tn[i] = type[m];
+    xn[i] = x[m];
+  }
+  if (lc == kMissing) return;
+  const bool dc = is_fluid(tc);
+  const double pc = dc ? xc : (pdir ? dir_or_zero(pdir[c]) : 0.0);
+  pres[c] = pc;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int64_t n = nn[i];
+    const bool nexists = n >= 0 && ln[i] != kMissing;
+    const bool dn = nexists && is_fluid(tn[i]);
     if (!(dc || dn)) continue;
     if (fl & (1u << i)) continue;
-    double pn = nexists ? (dn ? x[n] : (pdir ? dir_or_zero(pdir[n]) : 0.0)) : (n >= 0 ? pres[n] : 0.0);
+    const double pn = nexists ? (dn ? xn[i] : (pdir ? dir_or_zero(pdir[n]) : 0.0)) : (n >= 0 ? pres[n] : 0.0);
     double gr = pc * P.ih[i];
     gr -= pn * P.ih[i];
     U[i][c] = U[i][c] - gr;
