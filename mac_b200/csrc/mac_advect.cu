@@ -301,11 +301,6 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
                                                      double* fz, int L) {
   double* const F[3] = {fx, fy, fz};
   __shared__ int sn[kNbr];
-  // the layers of the brick and the cells its faces' stencils reach (local
-  // coordinates -2..8 on every axis), staged once per brick that can write
-  constexpr int kE = 11;
-  __shared__ int8_t sl[kE * kE * kE];
-  auto lay_at = [&](int x, int y, int z) -> int8_t { return sl[(x + 2) + kE * (y + 2) + kE * kE * (z + 2)]; };
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
     int b = blist[bi];
     if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
@@ -316,24 +311,17 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
       if (nb >= 0) near |= lmask[nb];
     }
     const bool skip = !(near & layer_bit(L));
-    if (!skip) {
-      for (int t = threadIdx.x; t < kE * kE * kE; t += blockDim.x) {
-        const int x = t % kE - 2, y = (t / kE) % kE - 2, z = t / (kE * kE) - 2;
-        sl[t] = lay_i(lay, cidx(sn, x, y, z));
-      }
-      __syncthreads();
-    }
     for (int o = skip ? kCells : threadIdx.x; o < kCells; o += blockDim.x) {
       int64_t c = (int64_t)b * kCells + o;
-      int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
-      int8_t lB = lay_at(x, y, z);
+      int8_t lB = lay[c];
       if (lB < 0) continue;  // c must exist with a layer
+      int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
       uint8_t fl = flags[c];
       for (int i = 0; i < 3; ++i) {
         if (fl & (1u << i)) continue;  // non-forced Set on a const face does nothing
         int a[3] = {x, y, z};
         a[i] -= 1;
-        int8_t lA = lay_at(a[0], a[1], a[2]);
+        int8_t lA = lay_i(lay, cidx(sn, a[0], a[1], a[2]));
         bool vA = lA >= 0;
         bool write = (vA && lA == L && lB >= L) || (lB == L && (!vA || lA >= L));
         if (!write) continue;
@@ -347,7 +335,7 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
                 if (!vA) continue;
                 int m[3] = {x, y, z};
                 m[i] -= 2;
-                int8_t l = lay_at(m[0], m[1], m[2]);
+                int8_t l = lay_i(lay, cidx(sn, m[0], m[1], m[2]));
                 if (l >= 0 && l < L) {
                   ++n;
                   val += rdv(Ui, cidx(sn, a[0], a[1], a[2]));
@@ -355,10 +343,11 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
               } else {
                 int m[3] = {x, y, z};
                 m[i] += 1;
-                int8_t l = lay_at(m[0], m[1], m[2]);
+                int64_t mi = cidx(sn, m[0], m[1], m[2]);
+                int8_t l = lay_i(lay, mi);
                 if (l >= 0 && l < L) {
                   ++n;
-                  val += rdv(Ui, cidx(sn, m[0], m[1], m[2]));
+                  val += rdv(Ui, mi);
                 }
               }
             } else {
@@ -366,11 +355,12 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
               m4[j] += s;
               int m3[3] = {m4[0], m4[1], m4[2]};
               m3[i] -= 1;
-              int8_t l4 = lay_at(m4[0], m4[1], m4[2]);
-              int8_t l3 = lay_at(m3[0], m3[1], m3[2]);
+              int64_t i4 = cidx(sn, m4[0], m4[1], m4[2]);
+              int8_t l4 = lay_i(lay, i4);
+              int8_t l3 = lay_i(lay, cidx(sn, m3[0], m3[1], m3[2]));
               if (l3 >= 0 && l4 >= 0 && (l3 < L || l4 < L)) {
                 ++n;
-                val += rdv(Ui, cidx(sn, m4[0], m4[1], m4[2]));
+                val += rdv(Ui, i4);
               }
             }
           }
