@@ -151,20 +151,35 @@ __global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ blist, co
   __syncthreads();
   int o = threadIdx.x;
   int64_t c = (int64_t)b * kCells + o;
+  // every load is issued before any is tested (a missing neighbour brick
+  // reads the cell itself)
+  const int8_t lc = lay[c];
+  const uint8_t tc = type[c], fc = flags[c];
+  int64_t nn[6];
+  int8_t ln[6];
+  uint8_t fn[6], tn[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    nn[f] = nb0(sb, c, o, f);
+    const int64_t q = nn[f] < 0 ? c : nn[f];
+    ln[f] = lay[q];
+    fn[f] = flags[q];
+    tn[f] = type[q];
+  }
   uint16_t m = 0;
-  if (lay[c] != kMissing && is_fluid(type[c])) {
+  if (lc != kMissing && is_fluid(tc)) {
     m = kDomainBit;
+#pragma unroll
     for (int f = 0; f < 6; ++f) {
       int ax = f >> 1;
-      int64_t n = nb0(sb, c, o, f);
-      if (n < 0 || lay[n] == kMissing) {
+      if (nn[f] < 0 || ln[f] == kMissing) {
         m |= (uint16_t)(1u << (8 + f));  // missing neighbour: Dirichlet
         continue;
       }
-      bool neumann = (f & 1) ? ((flags[n] >> ax) & 1) : ((flags[c] >> ax) & 1);
+      bool neumann = (f & 1) ? ((fn[f] >> ax) & 1) : ((fc >> ax) & 1);
       if (neumann) continue;
       m |= (uint16_t)(1u << (8 + f));
-      if (is_fluid(type[n])) m |= (uint16_t)(1u << f);
+      if (is_fluid(tn[f])) m |= (uint16_t)(1u << f);
     }
   }
   fmask[c] = m;
@@ -352,19 +367,29 @@ __global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ dbl,
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
-    if (!(fmask[c] & kDomainBit)) {
+    // the mask and all six speeds are loaded before either is tested (a
+    // missing neighbour brick reads the cell itself)
+    const uint16_t m = fmask[c];
+    const double* U[3] = {ux, uy, uz};
+    int64_t nn[3];
+    double uc[3], un[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      nn[i] = nb0(sb, c, o, 2 * i + 1);
+      uc[i] = U[i][c];
+      un[i] = U[i][nn[i] < 0 ? c : nn[i]];
+    }
+    if (!(m & kDomainBit)) {
       rhs[c] = 0.0;
       x[c] = 0.0;
       r[c] = 0.0;
       continue;
     }
-    const double* U[3] = {ux, uy, uz};
     double d = 0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      d -= U[i][c] * P.ih[i];
-      int64_t n = nb0(sb, c, o, 2 * i + 1);
-      d += (n < 0 ? 0.0 : U[i][n]) * P.ih[i];
+      d -= uc[i] * P.ih[i];
+      d += (nn[i] < 0 ? 0.0 : un[i]) * P.ih[i];
     }
     if (pdir) {
       double sum = 0;
@@ -636,14 +661,22 @@ __global__ void __launch_bounds__(kBT) k_divmax(const int* __restrict__ dbl, con
   for (int k = 0; k < kCPT; ++k) {
     int o = threadIdx.x + kBT * k;
     int64_t c = (int64_t)b * kCells + o;
-    if (!(fmask[c] & kDomainBit)) continue;
+    const uint16_t m = fmask[c];
     const double* U[3] = {ux, uy, uz};
+    int64_t nn[3];
+    double uc[3], un[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      nn[i] = nb0(sb, c, o, 2 * i + 1);
+      uc[i] = U[i][c];
+      un[i] = U[i][nn[i] < 0 ? c : nn[i]];
+    }
+    if (!(m & kDomainBit)) continue;
     double d = 0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      d -= U[i][c] * P.ih[i];
-      int64_t n = nb0(sb, c, o, 2 * i + 1);
-      d += (n < 0 ? 0.0 : U[i][n]) * P.ih[i];
+      d -= uc[i] * P.ih[i];
+      d += (nn[i] < 0 ? 0.0 : un[i]) * P.ih[i];
     }
     mx = fmax(mx, fabs(d));
   }
