@@ -313,24 +313,15 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ bli
     const bool skip = !(near & layer_bit(L));
     for (int o = skip ? kCells : threadIdx.x; o < kCells; o += blockDim.x) {
       int64_t c = (int64_t)b * kCells + o;
-      int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
-      // the cell's layer and flags and its -x, -y, -z neighbours' layers are
-      // loaded before any of them is tested
-      const int8_t lB = lay[c];
-      const uint8_t fl = flags[c];
-      int8_t lAs[3];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        int a[3] = {x, y, z};
-        a[i] -= 1;
-        lAs[i] = lay_i(lay, cidx(sn, a[0], a[1], a[2]));
-      }
+      int8_t lB = lay[c];
       if (lB < 0) continue;  // c must exist with a layer
+      int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
+      uint8_t fl = flags[c];
       for (int i = 0; i < 3; ++i) {
         if (fl & (1u << i)) continue;  // non-forced Set on a const face does nothing
         int a[3] = {x, y, z};
         a[i] -= 1;
-        int8_t lA = lAs[i];
+        int8_t lA = lay_i(lay, cidx(sn, a[0], a[1], a[2]));
         bool vA = lA >= 0;
         bool write = (vA && lA == L && lB >= L) || (lB == L && (!vA || lA >= L));
         if (!write) continue;
