@@ -411,11 +411,19 @@ __global__ void k_bfs_level(const int* __restrict__ blist, const int* __restrict
       if (l != kMissing && l != kEmpty) continue;
       int x = o & 7, y = (o >> 3) & 7, z = o >> 6;
       int8_t want = (int8_t)(L - 1);
-      bool hit = lay_at(lay, nbr, b, x - 1, y, z) == want || lay_at(lay, nbr, b, x, y - 1, z) == want ||
-                 lay_at(lay, nbr, b, x, y, z - 1) == want;
-      if (!ring && !hit)
-        hit = lay_at(lay, nbr, b, x + 1, y, z) == want || lay_at(lay, nbr, b, x, y + 1, z) == want ||
-              lay_at(lay, nbr, b, x, y, z + 1) == want;
+      // all neighbour layers are loaded before any is compared (no load waits
+      // on another's test); a neighbour being set to L by this launch never
+      // equals L - 1, so reading its old or new layer is the same
+      const int8_t lm[3] = {lay_at(lay, nbr, b, x - 1, y, z), lay_at(lay, nbr, b, x, y - 1, z),
+                            lay_at(lay, nbr, b, x, y, z - 1)};
+      int8_t lp[3] = {kMissing, kMissing, kMissing};
+      if (!ring) {
+        lp[0] = lay_at(lay, nbr, b, x + 1, y, z);
+        lp[1] = lay_at(lay, nbr, b, x, y + 1, z);
+        lp[2] = lay_at(lay, nbr, b, x, y, z + 1);
+      }
+      bool hit = lm[0] == want || lm[1] == want || lm[2] == want;
+      if (!ring && !hit) hit = lp[0] == want || lp[1] == want || lp[2] == want;
       if (hit) {
         lay[c] = (int8_t)L;
         const uint8_t t = type[c];
