@@ -206,6 +206,7 @@ struct Ctx {
   double* zold = nullptr;
   double learned_omega = 0.8;
   int* dbl = nullptr;          // bricks holding an in-domain cell, by brick coordinates (x fastest)
+  int* drow = nullptr;         // per domain brick: pool index and six face neighbours (8 ints)
   int ndom_host = 0;
   int* dbl_map = nullptr;      // ordering scratch: one slot per brick of the domain's bounding box
   int64_t dbl_map_n = 0;
@@ -384,6 +385,20 @@ __device__ inline void load_face_bases(const int* __restrict__ nbr, int b, int64
     int nb = nbr[(size_t)b * kNbr + idx[threadIdx.x]];
     sb[threadIdx.x] = nb < 0 ? -1 : (int64_t)nb * kCells;
   }
+}
+
+// A domain brick's row of the brick rows built with the solve's domain list:
+// its pool index and its -x, +x, -y, +y, -z, +z face neighbours (-1 absent),
+// 8 ints. One load round gives a block its brick and face bases (threads 0..5
+// stage them, in load_face_bases' order), where the list and the neighbour
+// table take two.
+__device__ inline int load_drow(const int* __restrict__ drow, int64_t* sb) {
+  const int* row = drow + 8 * (size_t)blockIdx.x;
+  if (threadIdx.x < 6) {
+    const int nb = row[1 + threadIdx.x];
+    sb[threadIdx.x] = nb < 0 ? -1 : (int64_t)nb * kCells;
+  }
+  return row[0];
 }
 
 // Index of the face-f neighbour of cell c (slot o of its brick), -1 if its brick is absent.

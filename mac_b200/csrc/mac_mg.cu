@@ -76,7 +76,7 @@ __device__ inline void coords3(int64_t i, int nx, int ny, int64_t n, int& x, int
 // so a block staging its face halos reads the old r of its neighbours and
 // forms their new r on the fly with the same expression.
 template <class T>
-__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const int* __restrict__ drow,
                                               const uint16_t* __restrict__ fmask, const double* __restrict__ rin,
                                               double* __restrict__ rout, double* __restrict__ x,
                                               const double* __restrict__ p, const double* __restrict__ q,
@@ -89,8 +89,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
   // prologue (static): brick, face neighbours, face masks; each thread takes
   // the z-run of four cells ob + 64 k (its z neighbours' staged values then
   // come from registers in the stencil pass)
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   const int ob = zrun_base();
   uint16_t mk[kCPT];
 #pragma unroll
@@ -143,7 +142,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre(const in
 
 // res = r - M e on the brick, summed over 2x2x2 children into level 1.
 template <class T>
-__global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ drow,
                                                    const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P,
                                                    const int32_t* __restrict__ done) {
@@ -153,8 +152,7 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ dbl, 
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   // prologue: brick, face neighbours, face masks (static) and r (written by
   // the V-cycle's first kernel, two launches back)
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   // the stencil pass takes a z-run of four cells of one column per thread
   // (cells zrun_base() + 64 k): z neighbours inside the run from registers
   const int ob = zrun_base();
@@ -212,7 +210,7 @@ __device__ inline int parent_off(int off) { return ((off & 7) >> 1) + 4 * (((off
 // preconditioned residual z and the block's partial r.z. The cells' r and
 // face masks are loaded first, so they are in flight during the staging.
 template <class T, bool FIRST>
-__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const int* __restrict__ drow,
                                                const uint16_t* __restrict__ fmask, const double* __restrict__ r,
                                                const T* __restrict__ e, const T* __restrict__ e1, T* __restrict__ eout,
                                                double* __restrict__ z, double* partial, Params P,
@@ -222,8 +220,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
   const T om = (T)(FIRST ? P.mgw1 : P.mgw2), ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   // prologue: brick, face neighbours, face masks (static), r and, when FIRST,
   // the brick's pre-smoothed e (both written many launches back)
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   const int ob = zrun_base();  // the stencil pass's z-run (cells ob + 64 k)
   uint16_t mk[kCPT];
   double rk[kCPT];
@@ -641,24 +638,12 @@ struct LBricks {
 // sbr[7 * j + k]: local brick j's pool index (k = 0) and its face neighbours
 // -x, +x, -y, +y, -z, +z (k = 1..6), -1 when absent or past the list.
 template <int D>
-__device__ inline void load_lbricks(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr, int* sbr) {
+__device__ inline void load_lbricks(const int* __restrict__ drow, int nd, int* sbr) {
   constexpr int BPB = LBricks<D>::BPB;
   for (int t = threadIdx.x; t < 7 * BPB; t += blockDim.x) {
     const int j = t / 7, k = t % 7;
     const int gb = blockIdx.x * BPB + j;
-    int v = -1;
-    if (gb < nd) {
-      const int b = dbl[gb];
-      if (k == 0) {
-        v = b;
-      } else {
-        const int f = k - 1;
-        const int d = (f & 1) ? 1 : -1;
-        const int ax = f >> 1;
-        v = nbr[(size_t)b * kNbr + nbr_index(ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0)];
-      }
-    }
-    sbr[t] = v;
+    sbr[t] = gb < nd ? drow[8 * (size_t)gb + k] : -1;
   }
 }
 
@@ -708,14 +693,14 @@ __device__ inline T apply_l(const T* __restrict__ e, const T* __restrict__ w, si
 }
 
 template <class T, int D>
-__global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(256) kl_pre(const int* __restrict__ drow, int nd,
                                               const T* __restrict__ w, size_t ncap, const T* __restrict__ r,
                                               T* __restrict__ e, T w1, T w2, const int32_t* __restrict__ done) {
   constexpr int N = D * D * D;
   __shared__ int sbr[7 * LBricks<D>::BPB];
   // prologue (static): the brick tables, the cell's weights and its
   // neighbours' inverse diagonals
-  load_lbricks<D>(dbl, nd, nbr, sbr);
+  load_lbricks<D>(drow, nd, sbr);
   __syncthreads();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = g < (int64_t)nd * N;
@@ -775,7 +760,7 @@ __device__ inline V sum8(V v) {
 // (brick-local), D = 2 writes the dense level 3 at the brick's position. One
 // thread per fine cell, the 8 children of a coarse cell on 8 adjacent lanes.
 template <class T, int D>
-__global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ drow, int nd,
                                                    const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                    const T* __restrict__ r, const T* __restrict__ e, T* __restrict__ rc,
                                                    DenseGrid g3, const int32_t* __restrict__ done) {
@@ -784,7 +769,7 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
   __shared__ int sbr[7 * LBricks<D>::BPB];
   // prologue: the brick tables and weights (static) and the cell's residual
   // (written two or more launches back)
-  load_lbricks<D>(dbl, nd, nbr, sbr);
+  load_lbricks<D>(drow, nd, sbr);
   __syncthreads();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = g < (int64_t)nd * N;  // nd * N is a multiple of 8: groups are whole
@@ -846,7 +831,7 @@ __global__ void __launch_bounds__(256) kl_restrict(const int* __restrict__ dbl, 
 // One Jacobi sweep at a brick level, optionally adding the coarse correction
 // first (D = 4: from level 2 bricks; D = 2: from the dense level 3).
 template <class T, int D, bool WITH_COARSE>
-__global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ drow, int nd,
                                                  const int* __restrict__ bkey, const T* __restrict__ w, size_t ncap,
                                                  const T* __restrict__ r, const T* __restrict__ e,
                                                  const T* __restrict__ ec, T* __restrict__ eout, DenseGrid g3,
@@ -858,7 +843,7 @@ __global__ void __launch_bounds__(256) kl_jacobi(const int* __restrict__ dbl, in
   // prologue: brick tables and weights (static), r, and with the coarse
   // correction this level's e (both written two or more launches back; e
   // without it is the previous launch's output and waits)
-  load_lbricks<D>(dbl, nd, nbr, sbr);
+  load_lbricks<D>(drow, nd, sbr);
   __syncthreads();
   if (WITH_COARSE && D == 2) {
     for (int t = threadIdx.x; t < 7 * LBricks<D>::BPB; t += blockDim.x) {
@@ -1655,7 +1640,7 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
       launch_k(c, k0_pre_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
                c->ds, update, r1, c->dp); MAC_COUNT(c);
     } else {
-      launch_k(c, k0_pre<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
+      launch_k(c, k0_pre<T>, nd, kBT, 0, c->drow, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
                update, e0, c->dp); MAC_COUNT(c);
     }
     if (update) {
@@ -1665,13 +1650,13 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   }
   if (!(part & 2)) return;
   if (!one) {
-    launch_k(c, k0_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
+    launch_k(c, k0_restrict<T>, nd, kBT, 0, c->drow, c->fmask, c->r, e0, r1, c->dp, dn); MAC_COUNT(c);
   }
   const T sw1 = (T)c->dp.mgw1, sw2 = (T)c->dp.mgw2;
-  launch_k(c, kl_pre<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
-  launch_k(c, kl_restrict<T, 4>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
-  launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
-  launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 4>, g1, 256, 0, c->drow, nd, w1, ncap1, r1, e1, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 4>, g1, 256, 0, c->drow, nd, c->bkey, w1, ncap1, r1, e1, r2, G, dn); MAC_COUNT(c);
+  launch_k(c, kl_pre<T, 2>, g2, 256, 0, c->drow, nd, w2, ncap2, r2, e2, sw1, sw2, dn); MAC_COUNT(c);
+  launch_k(c, kl_restrict<T, 2>, g2, 256, 0, c->drow, nd, c->bkey, w2, ncap2, r2, e2, d3.r, G, dn); MAC_COUNT(c);
   // dense level 3 on the device, levels 4.. in one block
   if (c->ndense > 1) {
     // dense levels 0 .. lo-1 device-wide, lo .. in one block
@@ -1701,21 +1686,21 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
     launch_k(c, kd_coarse_block<T>, 1, 1024, 0, S, 0, c->coarse_inv, c->coarse_ok, dn); MAC_COUNT(c);
   }
   // up
-  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
+  launch_k(c, kl_jacobi<T, 2, true>, g2, 256, 0, c->drow, nd, c->bkey, w2, ncap2, r2, e2, d3.e, e2b, G, sw1,
            dn); MAC_COUNT(c);
-  launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->dbl, nd, c->nbr, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
+  launch_k(c, kl_jacobi<T, 2, false>, g2, 256, 0, c->drow, nd, c->bkey, w2, ncap2, r2, e2b, nullptr, e2, G,
            sw2, dn); MAC_COUNT(c);
-  launch_k(c, kl_jacobi<T, 4, true>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
+  launch_k(c, kl_jacobi<T, 4, true>, g1, 256, 0, c->drow, nd, c->bkey, w1, ncap1, r1, e1, e2, e1b, G, sw1,
            dn); MAC_COUNT(c);
-  launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->dbl, nd, c->nbr, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
+  launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->drow, nd, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
            sw2, dn); MAC_COUNT(c);
   if (one) {
     launch_k(c, k0_post_one<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
     return;
   }
-  launch_k(c, k0_post<T, true>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
+  launch_k(c, k0_post<T, true>, nd, kBT, 0, c->drow, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,
            dn); MAC_COUNT(c);
-  launch_k(c, k0_post<T, false>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
+  launch_k(c, k0_post<T, false>, nd, kBT, 0, c->drow, c->fmask, c->r, e0b, nullptr, nullptr, c->z, c->partial,
            c->dp, dn); MAC_COUNT(c);
 }
 

@@ -46,6 +46,7 @@ int alloc_solver(Ctx* c) {
   A(dalloc(&c->pd2, nc));
   A(dalloc(&c->q, nc));
   A(dalloc(&c->dbl, c->cap_bricks));
+  A(dalloc(&c->drow, (size_t)c->cap_bricks * 8));
   A(dalloc(&c->coarse_inv, 64 * 64));
   A(dalloc(&c->coarse_ok, 1));
   if (rc == MAC_OK) A(check(cudaMemset(c->coarse_ok, 0, sizeof(int))));
@@ -73,7 +74,7 @@ int alloc_solver(Ctx* c) {
 void free_solver(Ctx* c) {
   cudaFree(c->fmask); cudaFree(c->x); cudaFree(c->b); cudaFree(c->r); cudaFree(c->r2); cudaFree(c->z); cudaFree(c->pd);
   cudaFree(c->q); cudaFree(c->pd2); cudaFree(c->partial); cudaFree(c->dbl); cudaFree(c->dense_buf);
-  cudaFree(c->dbl_map); cudaFree(c->dbl_cnt);
+  cudaFree(c->dbl_map); cudaFree(c->dbl_cnt); cudaFree(c->drow);
   cudaFree(c->zold);
   cudaFree(c->coarse_inv);
   cudaFree(c->coarse_ok);
@@ -256,6 +257,21 @@ __global__ void __launch_bounds__(kOrderBlock) k_order_write(const int* __restri
   int before = 0;
   for (int k = 0; k < w; ++k) before += wsum[k];
   if (b >= 0) dbl[off[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u))] = b;
+}
+
+__global__ void k_drow(const int* __restrict__ dbl, int nd, const int* __restrict__ nbr, int* __restrict__ drow) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 8 * (int64_t)nd) return;
+  const int k = (int)(t & 7);
+  const int b = dbl[t >> 3];
+  int v = -1;
+  if (k == 0) {
+    v = b;
+  } else if (k < 7) {
+    const int f = k - 1, d = (f & 1) ? 1 : -1, ax = f >> 1;
+    v = nbr[(size_t)b * kNbr + nbr_index(ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0)];
+  }
+  drow[t] = v;
 }
 
 static int order_domain_bricks(Ctx* c) {
@@ -450,7 +466,7 @@ __global__ void __launch_bounds__(kBT) k_residual(const int* __restrict__ dbl, c
 
 // p = z + beta p (first: p = z), then q = M p and the partial p.q; the
 // neighbours' new p is formed on the fly so p is read once and written once.
-__global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ drow,
                                                      const uint16_t* __restrict__ fmask, const double* __restrict__ z,
                                                      const double* __restrict__ pold, double* __restrict__ pnew,
                                                      double* __restrict__ q, double* partial, Params P,
@@ -460,8 +476,7 @@ __global__ void __launch_bounds__(kBT) k_update_spmv(const int* __restrict__ dbl
   // prologue: brick, face neighbours and face masks (static), the brick's z
   // (the preconditioner's output, two launches back) and p_old (16-byte
   // vector loads); only beta comes from the previous launch
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   const int ob = zrun_base();  // the stencil pass's z-run (cells ob + 64 k)
   uint16_t mk[kCPT];
 #pragma unroll
@@ -816,6 +831,9 @@ int setup_system(Ctx* c) {
   c->ndom_host = c->hs->ndom;
   c->stats.unknowns = c->hs->nunknown;
   if ((rc = order_domain_bricks(c))) return rc;
+  if (c->ndom_host > 0) {
+    k_drow<<<grid_for(8 * (int64_t)c->ndom_host, 256), 256, 0, st>>>(c->dbl, c->ndom_host, c->nbr, c->drow); MAC_COUNT(c);
+  }
   if (c->ndom_host > 0 && c->prm.solver != MAC_SOLVER_CG_FP64) {
     rc = mg_setup(c);
     if (rc) return rc;
@@ -939,7 +957,7 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
       prof_end(c, PH_CGVEC);
       prof_begin(c, PH_SPMV);
       std::swap(c->pd, c->pd2);  // pd2: previous direction, pd: new one
-      launch_k(c, k_update_spmv, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
+      launch_k(c, k_update_spmv, nd, kBT, 0, c->drow, c->fmask, c->z, c->pd2, c->pd, c->q, c->partial, c->dp, c->ds,
                first); MAC_COUNT(c);
       prof_end(c, PH_SPMV);
       first = 0;
