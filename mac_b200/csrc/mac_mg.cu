@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 1) k0_post(const in
 // in k0_pre.
 template <class T>
 __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict(
-    const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
+    const int* __restrict__ drow, const uint16_t* __restrict__ fmask,
     const double* __restrict__ rin, double* __restrict__ rout, double* __restrict__ x, const double* __restrict__ p,
     const double* __restrict__ q, double* partial, const Scalars* ds, int update, T* __restrict__ r1, Params P) {
   pdl_entry();
@@ -304,8 +304,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict
   __shared__ T res[kCells];
   const T om = (T)P.mgws, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   const double al = update ? ds->alpha : 0.0;
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   double rv[kCPT];
   uint16_t mk[kCPT];
   double rr = 0;
@@ -365,7 +364,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 16 : 12) k0_pre_restrict
 // in FP64 with the block's partial r.z.
 template <class T>
 __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
-    const int* __restrict__ dbl, const int* __restrict__ nbr, const uint16_t* __restrict__ fmask,
+    const int* __restrict__ drow, const uint16_t* __restrict__ fmask,
     const double* __restrict__ r, const T* __restrict__ e1, double* __restrict__ z, double* partial, Params P,
     const int32_t* __restrict__ done) {
   pdl_entry();
@@ -373,8 +372,7 @@ __global__ void __launch_bounds__(kBT, sizeof(T) == 4 ? 12 : 1) k0_post_one(
   __shared__ int64_t sb[6];
   __shared__ T se[kS1];
   const T om = (T)P.mgws, ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   uint16_t mk[kCPT];
   double rk[kCPT];
 #pragma unroll
@@ -1637,7 +1635,7 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
                  c->pd, c->q, c->partial, c->ds, update, e0, r1, c->dp);
       MAC_COUNT(c);
     } else if (one) {
-      launch_k(c, k0_pre_restrict<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
+      launch_k(c, k0_pre_restrict<T>, nd, kBT, 0, c->drow, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial,
                c->ds, update, r1, c->dp); MAC_COUNT(c);
     } else {
       launch_k(c, k0_pre<T>, nd, kBT, 0, c->drow, c->fmask, c->r, c->r2, c->x, c->pd, c->q, c->partial, c->ds,
@@ -1695,7 +1693,7 @@ static void mg_vcycle_t(Ctx* c, int update, int part) {
   launch_k(c, kl_jacobi<T, 4, false>, g1, 256, 0, c->drow, nd, c->bkey, w1, ncap1, r1, e1b, nullptr, e1, G,
            sw2, dn); MAC_COUNT(c);
   if (one) {
-    launch_k(c, k0_post_one<T>, nd, kBT, 0, c->dbl, c->nbr, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
+    launch_k(c, k0_post_one<T>, nd, kBT, 0, c->drow, c->fmask, c->r, e1, c->z, c->partial, c->dp, dn); MAC_COUNT(c);
     return;
   }
   launch_k(c, k0_post<T, true>, nd, kBT, 0, c->drow, c->fmask, c->r, e0, e1, e0b, nullptr, nullptr, c->dp,

@@ -368,15 +368,14 @@ __global__ void __launch_bounds__(512) k_dirichlet(const int* __restrict__ blist
 // With Dirichlet air pressures (pdir non-null, the viscous projection of
 // src/Algorithms_Solve_Pressure_Dirichlet.h:178-188), a cell next to a
 // Dirichlet cell first takes div -= sum over those neighbours of p_D / h_i^2.
-__global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_divergence(const int* __restrict__ drow,
                                                     const uint16_t* __restrict__ fmask, const double* __restrict__ ux,
                                                     const double* __restrict__ uy, const double* __restrict__ uz,
                                                     const double* __restrict__ pres, double* __restrict__ rhs,
                                                     double* __restrict__ x, double* __restrict__ r, int warm,
                                                     double* partial, Params P, const double* __restrict__ pdir) {
   __shared__ int64_t sb[6];
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   __syncthreads();
   double bb = 0;
 #pragma unroll
@@ -441,13 +440,12 @@ __device__ inline double apply0(const double* __restrict__ v, const uint16_t* __
 }
 
 // r = rhs - M x for a warm start, with the block's partial r.r
-__global__ void __launch_bounds__(kBT) k_residual(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_residual(const int* __restrict__ drow,
                                                   const uint16_t* __restrict__ fmask, const double* __restrict__ rhs,
                                                   const double* __restrict__ x, double* __restrict__ r,
                                                   double* partial, Params P) {
   __shared__ int64_t sb[6];
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   __syncthreads();
   double rr = 0;
 #pragma unroll
@@ -663,13 +661,12 @@ __global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist,
 }
 
 // max |div| over domain cells (the check of src/Algorithms_Solve_Pressure.h:208-219)
-__global__ void __launch_bounds__(kBT) k_divmax(const int* __restrict__ dbl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(kBT) k_divmax(const int* __restrict__ drow,
                                                 const uint16_t* __restrict__ fmask, const double* __restrict__ ux,
                                                 const double* __restrict__ uy, const double* __restrict__ uz, Params P,
                                                 Scalars* ds) {
   __shared__ int64_t sb[6];
-  int b = dbl[blockIdx.x];
-  load_face_bases(nbr, b, sb);
+  const int b = load_drow(drow, sb);
   __syncthreads();
   double mx = 0;
 #pragma unroll
@@ -895,12 +892,12 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
       k_dirichlet<<<c->nlive_host, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, D[0], D[1], D[2], pdir,
                                                  c->dp); MAC_COUNT(c);
     }
-    k_divergence<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,
+    k_divergence<<<nd, kBT, 0, st>>>(c->drow, c->fmask, U[0], U[1], U[2], c->f64 + (size_t)PRES * cap, c->b,
                                      c->x, c->r, warm, c->partial, c->dp, pdir); MAC_COUNT(c);
     prof_end(c, PH_DIVERGENCE);
     k_fin_bnorm<<<1, 1024, 0, st>>>(c->partial, nd, c->ds); MAC_COUNT(c);
     if (warm) {
-      k_residual<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
+      k_residual<<<nd, kBT, 0, st>>>(c->drow, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
       k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
     }
     // a step's particle binning runs beside this solve's iterations
@@ -999,7 +996,7 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
           // MG-PCG from the current x: true residual, fresh directions
           learned = false;
           c->stats.fallbacks += 1;
-          k_residual<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
+          k_residual<<<nd, kBT, 0, st>>>(c->drow, c->fmask, c->b, c->x, c->r, c->partial, c->dp); MAC_COUNT(c);
           k_fin_rr_initial<<<1, 1024, 0, st>>>(c->partial, nd, c->ds, rtol2); MAC_COUNT(c);
           first = 1;
         }
@@ -1026,7 +1023,7 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
   }
   if (c->prm.div_check && nd > 0) {
     k_zero_div<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
-    k_divmax<<<nd, kBT, 0, st>>>(c->dbl, c->nbr, c->fmask, U[0], U[1], U[2], c->dp, c->ds); MAC_COUNT(c);
+    k_divmax<<<nd, kBT, 0, st>>>(c->drow, c->fmask, U[0], U[1], U[2], c->dp, c->ds); MAC_COUNT(c);
     rc = read_scalars(c);
     if (rc) return rc;
     unsigned long long bits = c->hs->div_bits;
