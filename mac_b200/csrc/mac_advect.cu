@@ -151,7 +151,7 @@ __device__ inline double face_accel(const Stage& S, uint8_t fl, int x, int y, in
 // The speed field read by the stencils is staged per brick; the kernels write
 // other arrays only, so no block reads what another writes.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_forces(const int* __restrict__ lrow, int nlive,
+__global__ void __launch_bounds__(256) k_forces(const int* __restrict__ blist, int nlive, const int* __restrict__ nbr,
                                                 const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
                                                 const uint8_t* __restrict__ flags, double* f64, size_t cap,
                                                 int ib, Params P, const Scalars* __restrict__ ds) {
@@ -161,7 +161,8 @@ __global__ void __launch_bounds__(256) k_forces(const int* __restrict__ lrow, in
   const double* U[3];
   for (int i = 0; i < 3; ++i) U[i] = f64 + (size_t)((MODE == 2 ? 1 : (MODE == 1 ? 0 : ib)) * 3 + i) * cap;
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
-    const int b = load_lrow(lrow, bi, sn);
+    int b = blist[bi];
+    if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
     stage_forces(S, U, sn, lay, type);
     __syncthreads();
@@ -195,8 +196,8 @@ __global__ void __launch_bounds__(256) k_forces(const int* __restrict__ lrow, in
 // the forces of speed field U, through the non-forced Set, for every existing
 // cell (src/Algorithms_Gravity.h:15-28, src/Algorithms_Convection.h:18-37,
 // src/Algorithms_Viscosity.h:24-30).
-__global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ lrow, int nlive,
-                                                    const int8_t* __restrict__ lay,
+__global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ blist, int nlive,
+                                                    const int* __restrict__ nbr, const int8_t* __restrict__ lay,
                                                     const uint8_t* __restrict__ type, const uint8_t* __restrict__ flags,
                                                     const double* __restrict__ ux, const double* __restrict__ uy,
                                                     const double* __restrict__ uz, double* ax, double* ay, double* az,
@@ -206,7 +207,8 @@ __global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ lrow
   const double* U[3] = {ux, uy, uz};
   double* A[3] = {ax, ay, az};
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
-    const int b = load_lrow(lrow, bi, sn);
+    int b = blist[bi];
+    if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
     stage_forces(S, U, sn, lay, type);
     __syncthreads();
@@ -225,10 +227,9 @@ __global__ void __launch_bounds__(256) k_forces_add(const int* __restrict__ lrow
 
 int forces_add(Ctx* c, const double* const* U) {
   if (c->nlive_host == 0) return MAC_OK;
-  if (int rc = ensure_lrow(c)) return rc;
   size_t cap = (size_t)c->cap_bricks * kCells;
   prof_begin(c, PH_FORCES);
-  k_forces_add<<<c->nlive_host, 256, 0, c->stream>>>(c->lrow, c->nlive_host, c->lay, c->type, c->flags,
+  k_forces_add<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
                                                      U[0], U[1], U[2], c->f64 + AX * cap, c->f64 + AY * cap,
                                                      c->f64 + AZ * cap, c->dp); MAC_COUNT(c);
   prof_end(c, PH_FORCES);
@@ -237,23 +238,21 @@ int forces_add(Ctx* c, const double* const* U) {
 
 int forces(Ctx* c, int ib) {
   if (c->nlive_host == 0) return MAC_OK;
-  if (int rc = ensure_lrow(c)) return rc;
   size_t cap = (size_t)c->cap_bricks * kCells;
-  k_forces<0><<<c->nlive_host, 256, 0, c->stream>>>(c->lrow, c->nlive_host, c->lay, c->type, c->flags,
+  k_forces<0><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
                                                     c->f64, cap, ib, c->dp, c->ds); MAC_COUNT(c);
   return check(cudaGetLastError());
 }
 
 int rk_stage(Ctx* c, int stage) {
   if (c->nlive_host == 0) return MAC_OK;
-  if (int rc = ensure_lrow(c)) return rc;
   size_t cap = (size_t)c->cap_bricks * kCells;
   prof_begin(c, PH_FORCES);
   if (stage == 1) {
-    k_forces<1><<<c->nlive_host, 256, 0, c->stream>>>(c->lrow, c->nlive_host, c->lay, c->type, c->flags,
+    k_forces<1><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
                                                       c->f64, cap, 0, c->dp, c->ds); MAC_COUNT(c);
   } else {
-    k_forces<2><<<c->nlive_host, 256, 0, c->stream>>>(c->lrow, c->nlive_host, c->lay, c->type, c->flags,
+    k_forces<2><<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->type, c->flags,
                                                       c->f64, cap, 1, c->dp, c->ds); MAC_COUNT(c);
   }
   prof_end(c, PH_FORCES);
@@ -296,14 +295,15 @@ __global__ void __launch_bounds__(256) k_layer_mask(const int* __restrict__ blis
 // A face of a cell in brick b is written at level L only when its cell or the
 // cell behind it (-e_i) has layer L, so only when b or one of its -x, -y, -z
 // face neighbours holds a layer-L cell; other bricks are skipped whole.
-__global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ lrow, int nlive,
+__global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ blist, int nlive, const int* __restrict__ nbr,
                                                      const int8_t* __restrict__ lay, const uint8_t* __restrict__ flags,
                                                      const uint32_t* __restrict__ lmask, double* fx, double* fy,
                                                      double* fz, int L) {
   double* const F[3] = {fx, fy, fz};
   __shared__ int sn[kNbr];
   for (int bi = blockIdx.x; bi < nlive; bi += gridDim.x) {
-    const int b = load_lrow(lrow, bi, sn);
+    int b = blist[bi];
+    if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
     __syncthreads();
     uint32_t near = lmask[b];
     for (int i = 0; i < 3; ++i) {
@@ -377,11 +377,10 @@ __global__ void __launch_bounds__(256) k_extrapolate(const int* __restrict__ lro
 // pipeline B).
 int extrapolate_field(Ctx* c, double* const* F) {
   if (c->nlive_host == 0) return MAC_OK;
-  if (int rc = ensure_lrow(c)) return rc;
   prof_begin(c, PH_EXTRAPOLATE);
   k_layer_mask<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->lay, c->lmask); MAC_COUNT(c);
   for (int L = 1; L <= c->dp.layer_max + 1; ++L) {
-    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->lrow, c->nlive_host, c->lay, c->flags, c->lmask,
+    k_extrapolate<<<c->nlive_host, 256, 0, c->stream>>>(c->blist, c->nlive_host, c->nbr, c->lay, c->flags, c->lmask,
                                                         F[0], F[1], F[2], L); MAC_COUNT(c);
   }
   prof_end(c, PH_EXTRAPOLATE);
@@ -678,8 +677,8 @@ __global__ void k_bin_scatter(const double* __restrict__ px, const double* __res
 // the particles binned to one brick: the brick's speed field with a two-cell
 // halo (12^3 cells from up to 27 bricks) is staged in shared memory and the
 // 96 stencil reads of each particle's RK4 come from there.
-__global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, double* pz, const int* __restrict__ lrow,
-                                                     const int* __restrict__ bkey,
+__global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, double* pz,
+                                                     const int* __restrict__ blist, const int* __restrict__ bkey,
                                                      const int* __restrict__ nbr, const int64_t* __restrict__ off,
                                                      const unsigned long long* __restrict__ hk, const int* __restrict__ hv,
                                                      int64_t hcap, const int8_t* __restrict__ lay,
@@ -688,9 +687,10 @@ __global__ void __launch_bounds__(256) k_move_binned(double* px, double* py, dou
                                                      const Scalars* __restrict__ ds, unsigned long long* bad_count) {
   __shared__ double s[3 * kStageComp];
   __shared__ int sn[kNbr];
-  const int b = load_lrow(lrow, blockIdx.x, sn);
+  int b = blist[blockIdx.x];
   int64_t p0 = off[b], p1 = off[b + 1];
   if (p0 == p1) return;
+  if (threadIdx.x < kNbr) sn[threadIdx.x] = nbr[(size_t)b * kNbr + threadIdx.x];
   __syncthreads();
   const double* U[3] = {ux, uy, uz};
   int ox = bkey[3 * b] * 8 - 2, oy = bkey[3 * b + 1] * 8 - 2, oz = bkey[3 * b + 2] * 8 - 2;
@@ -939,9 +939,7 @@ int move_binned(Ctx* c) {
   const size_t cap = (size_t)c->cap_bricks * kCells;
   const int stray = (int)c->cap_bricks;
   unsigned long long* bad = &c->ds->bad_reads;
-  int rc = ensure_lrow(c);
-  if (rc) return rc;
-  k_move_binned<<<c->nlive_host, 256, 0, st>>>(c->px, c->py, c->pz, c->lrow, c->bkey, c->nbr, c->boff, c->hkeys,
+  k_move_binned<<<c->nlive_host, 256, 0, st>>>(c->px, c->py, c->pz, c->blist, c->bkey, c->nbr, c->boff, c->hkeys,
                                                c->hval, c->hcap, c->lay, c->f64 + U0X * cap, c->f64 + U0Y * cap,
                                                c->f64 + U0Z * cap, c->dp, c->ds, bad); MAC_COUNT(c);
   k_move_stray<<<4, 256, 0, st>>>(c->px, c->py, c->pz, c->boff, stray, c->nbr, c->hkeys, c->hval, c->hcap, c->lay,

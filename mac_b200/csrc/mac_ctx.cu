@@ -187,7 +187,7 @@ static void free_all(Ctx* c) {
   cudaFree(c->depth); cudaFree(c->pkeep); cudaFree(c->u2);
   for (int k = 0; k < 2; ++k)
     for (int i = 0; i < 3; ++i) { cudaFree(c->pbuf[k][i]); cudaFree(c->pbuf2[k][i]); }
-  cudaFree(c->nbr); cudaFree(c->lrow); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
+  cudaFree(c->nbr); cudaFree(c->blist); cudaFree(c->blist2); cudaFree(c->freelist); cudaFree(c->alive);
   cudaFree(c->hkeys); cudaFree(c->hval); cudaFree(c->newslots);
   cudaFree(c->px); cudaFree(c->py); cudaFree(c->pz); cudaFree(c->pending);
   cudaFree(c->px2); cudaFree(c->py2); cudaFree(c->pz2); cudaFree(c->pbrick);
@@ -290,7 +290,6 @@ static int create(const mac_params* p, Ctx** out) {
       }
   }
   A(dalloc(&c->nbr, kNbr * c->cap_bricks));
-  A(dalloc(&c->lrow, (size_t)32 * c->cap_bricks));
   A(dalloc(&c->blist, c->cap_bricks));
   A(dalloc(&c->blist2, c->cap_bricks));
   A(dalloc(&c->freelist, c->cap_bricks));

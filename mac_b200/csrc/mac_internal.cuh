@@ -207,8 +207,6 @@ struct Ctx {
   double learned_omega = 0.8;
   int* dbl = nullptr;          // bricks holding an in-domain cell, by brick coordinates (x fastest)
   int* drow = nullptr;         // per domain brick: pool index and six face neighbours (8 ints)
-  int* lrow = nullptr;         // per live brick (list order): pool index and its 27 neighbours (32 ints)
-  int lrow_ok = 0;             // lrow matches the current live list and neighbour table
   int ndom_host = 0;
   int* dbl_map = nullptr;      // ordering scratch: one slot per brick of the domain's bounding box
   int64_t dbl_map_n = 0;
@@ -402,29 +400,6 @@ __device__ inline int load_drow(const int* __restrict__ drow, int64_t* sb) {
   }
   return row[0];
 }
-
-// A live brick's row of the live-brick rows (list position bi): its pool index
-// then its 27 neighbours in nbr_index order (-1 absent), 32 ints. One load
-// round gives a block its brick and neighbour row (threads 0..26 stage it in
-// sn), where the live list and the neighbour table take two.
-__device__ inline int load_lrow(const int* __restrict__ lrow, int bi, int* sn) {
-  const int* row = lrow + 32 * (size_t)bi;
-  if (threadIdx.x < kNbr) sn[threadIdx.x] = row[1 + threadIdx.x];
-  return row[0];
-}
-// The same row's six face neighbours as load_face_bases stages them.
-__device__ inline int load_lrow_faces(const int* __restrict__ lrow, int bi, int64_t* sb) {
-  const int* row = lrow + 32 * (size_t)bi;
-  if (threadIdx.x < 6) {
-    const int f = threadIdx.x, d = (f & 1) ? 1 : -1, ax = f >> 1;
-    const int nb = row[1 + nbr_index(ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0)];
-    sb[f] = nb < 0 ? -1 : (int64_t)nb * kCells;
-  }
-  return row[0];
-}
-// Builds the live-brick rows if the live list or the neighbour table changed
-// since they were last built (one launch on the context's stream).
-int ensure_lrow(Ctx* c);
 
 // Index of the face-f neighbour of cell c (slot o of its brick), -1 if its brick is absent.
 __device__ inline int64_t nb0(const int64_t* sb, int64_t c, int o, int f) {

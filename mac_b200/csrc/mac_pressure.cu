@@ -140,13 +140,14 @@ __device__ inline void sum_partials(const double* partial, int nblk, double* s0,
 // sign +1 looks at the neighbour's left face, sign -1 at the cell's own. Bricks
 // with an in-domain cell are collected into the domain brick list, and their
 // key bounds into the scalars.
-__global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ lrow,
+__global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ blist, const int* __restrict__ nbr,
                                                const int* __restrict__ bkey, const int8_t* __restrict__ lay,
                                                const uint8_t* __restrict__ type, const uint8_t* __restrict__ flags,
                                                uint16_t* fmask, int* dbl, Scalars* ds) {
   __shared__ int64_t sb[6];
   __shared__ int cnt;
-  const int b = load_lrow_faces(lrow, blockIdx.x, sb);
+  int b = blist[blockIdx.x];
+  load_face_bases(nbr, b, sb);
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
   int o = threadIdx.x;
@@ -612,13 +613,14 @@ __global__ void __launch_bounds__(512) k_jacobi_prec(const int* __restrict__ dbl
 // non-forced Set (const faces keep their value).
 __device__ inline double dir_or_zero(double q) { return q == q ? q : 0.0; }
 
-__global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ lrow,
+__global__ void __launch_bounds__(512) k_gradient(const int* __restrict__ blist, const int* __restrict__ nbr,
                                                   const int8_t* __restrict__ lay, const uint8_t* __restrict__ type,
                                                   const uint8_t* __restrict__ flags, const double* __restrict__ x,
                                                   double* __restrict__ pres, double* ux, double* uy, double* uz,
                                                   Params P, const double* __restrict__ pdir) {
   __shared__ int64_t sb[6];
-  const int b = load_lrow_faces(lrow, blockIdx.x, sb);
+  int b = blist[blockIdx.x];
+  load_face_bases(nbr, b, sb);
   __syncthreads();
   int o = threadIdx.x;
   int64_t c = (int64_t)b * kCells + o;
@@ -819,8 +821,7 @@ int setup_system(Ctx* c) {
   prof_begin(c, PH_SETUP);
   k_setup_reset<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   if (n > 0) {
-    if (int e = ensure_lrow(c)) return e;
-    k_fmask<<<n, 512, 0, st>>>(c->lrow, c->bkey, c->lay, c->type, c->flags, c->fmask, c->dbl, c->ds); MAC_COUNT(c);
+    k_fmask<<<n, 512, 0, st>>>(c->blist, c->nbr, c->bkey, c->lay, c->type, c->flags, c->fmask, c->dbl, c->ds); MAC_COUNT(c);
   }
   int rc = read_scalars(c);
   if (rc) return rc;
@@ -1016,8 +1017,7 @@ int project_field(Ctx* c, double* const* U, const double* const* D) {
   int n = c->nlive_host;
   if (n > 0) {
     prof_begin(c, PH_GRADIENT);
-    if ((rc = ensure_lrow(c))) return rc;
-    k_gradient<<<n, 512, 0, st>>>(c->lrow, c->lay, c->type, c->flags, c->x, c->f64 + (size_t)PRES * cap,
+    k_gradient<<<n, 512, 0, st>>>(c->blist, c->nbr, c->lay, c->type, c->flags, c->x, c->f64 + (size_t)PRES * cap,
                                   U[0], U[1], U[2], c->dp, pdir); MAC_COUNT(c);
     prof_end(c, PH_GRADIENT);
   }

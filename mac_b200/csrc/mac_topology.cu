@@ -649,24 +649,6 @@ __global__ void k_dt_finalize(Params P, Scalars* ds) {
   ds->dt = dt;
 }
 
-// The live-brick rows: row bi holds blist[bi] and its 27 neighbours.
-__global__ void k_lrow(const int* __restrict__ blist, const int* __restrict__ nbr, int* __restrict__ lrow,
-                       const Scalars* __restrict__ ds) {
-  const int64_t n = 32 * (int64_t)ds->nlive;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(t & 31);
-    const int b = blist[t >> 5];
-    lrow[t] = k == 0 ? b : (k <= kNbr ? nbr[(size_t)b * kNbr + k - 1] : -1);
-  }
-}
-
-int ensure_lrow(Ctx* c) {
-  if (c->lrow_ok) return MAC_OK;
-  k_lrow<<<kTopoBlocks, 256, 0, c->stream>>>(c->blist, c->nbr, c->lrow, c->ds); MAC_COUNT(c);
-  c->lrow_ok = 1;
-  return check(cudaGetLastError());
-}
-
 // ------------------------------------------------------------ drivers
 int rebuild_index(Ctx* c) {
   cudaStream_t st = c->stream;
@@ -674,13 +656,11 @@ int rebuild_index(Ctx* c) {
   k_hash_insert_live<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->ds); MAC_COUNT(c);
   k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
   c->system_ready = false;
-  c->lrow_ok = 0;
-  return ensure_lrow(c);
+  return check(cudaGetLastError());
 }
 
 static void alloc_new(Ctx* c) {
   cudaStream_t st = c->stream;
-  c->lrow_ok = 0;  // the live list grows
   k_alloc_bricks<<<kTopoBlocks, 256, 0, st>>>(c->newslots, c->hkeys, c->hval, c->bkey, c->blist, c->freelist,
                                                c->lay, c->type, c->flags, c->f64, c->depth, c->u2,
                                                (size_t)c->cap_bricks * kCells, c->cap_bricks, c->ds); MAC_COUNT(c);
@@ -769,7 +749,6 @@ int topo_update_layer(Ctx* c) {
   alloc_new(c);
   k_after_alloc<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   k_build_nbr<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->bkey, c->hkeys, c->hval, c->hcap, c->nbr, c->ds); MAC_COUNT(c);
-  c->lrow_ok = 0;
   if (c->dp.depth_mode) {
     k_depth_seed<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->nbr, c->lay, c->depth, c->ds); MAC_COUNT(c);
   }
@@ -789,7 +768,6 @@ int topo_delete(Ctx* c) {
   cudaStream_t st = c->stream;
   k_delete<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->lay, c->flags, c->alive, c->ds); MAC_COUNT(c);
   k_compact<<<kTopoBlocks, 256, 0, st>>>(c->blist, c->blist2, c->freelist, c->alive, c->ds); MAC_COUNT(c);
-  c->lrow_ok = 0;
   k_compact_done<<<1, 1, 0, st>>>(c->ds); MAC_COUNT(c);
   int* t = c->blist;
   c->blist = c->blist2;
