@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ drow,
                                                    const T* __restrict__ e, T* __restrict__ r1, Params P,
                                                    const int32_t* __restrict__ done) {
   __shared__ int64_t sb[6];
-  __shared__ T res[kCells];
   __shared__ T se[kS1];
   const T ih2[3] = {(T)P.ih2[0], (T)P.ih2[1], (T)P.ih2[2]};
   // prologue: brick, face neighbours, face masks (static) and r (written by
@@ -173,10 +172,11 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ drow,
   T ecs[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) ecs[k] = se[si0 + 100 * k];
+  T v[kCPT];
 #pragma unroll
   for (int k = 0; k < kCPT; ++k) {
     const uint16_t m = mk[k];
-    T v = 0;
+    v[k] = 0;
     if (m & kDomainBit) {
       const int si = si0 + 100 * k;
       const T ec = ecs[k];
@@ -186,18 +186,22 @@ __global__ void __launch_bounds__(kBT) k0_restrict(const int* __restrict__ drow,
         if (m & (1u << (8 + f))) me += ih2[f >> 1] * ec;
         if (m & (1u << f)) me -= ih2[f >> 1] * zrun_nbr(se, ecs, si, k, f);
       }
-      v = (T)rk[k] - me;
+      v[k] = (T)rk[k] - me;
     }
-    res[ob + 64 * k] = v;
   }
-  __syncthreads();
-  int o = threadIdx.x;
-  if (o < 64) {
-    int X = o & 3, Y = (o >> 2) & 3, Z = o >> 4;
-    int base = 2 * X + 16 * Y + 128 * Z;
-    T s = res[base] + res[base + 1] + res[base + 8] + res[base + 9] + res[base + 64] + res[base + 65] +
-          res[base + 72] + res[base + 73];
-    r1[(size_t)b * 64 + o] = s;
+  // the 2x2x2 children of a level-1 cell: z pairs inside the thread's run,
+  // x pairs on lanes t, t ^ 1 and y pairs on lanes t, t ^ 8 (x = t & 7,
+  // y = (t >> 3) & 7); the lane with x and y even holds the sums
+  T s0 = v[0] + v[1], s1 = v[2] + v[3];
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 8);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 8);
+  const int x = threadIdx.x & 7, y = (threadIdx.x >> 3) & 7, zh = threadIdx.x >> 6;
+  if (!((x | y) & 1)) {
+    const size_t base = (size_t)b * 64 + (x >> 1) + 4 * (y >> 1) + 16 * (2 * zh);
+    r1[base] = s0;
+    r1[base + 16] = s1;
   }
 }
 
