@@ -1607,7 +1607,6 @@ int mg_setup(Ctx* c) { return c->mg_float ? mg_setup_t<float>(c) : mg_setup_t<do
 // part: 1 = the head (first kernel, with update the convergence test), 2 = the rest.
 template <class T>
 static void mg_vcycle_t(Ctx* c, int update, int part) {
-  cudaStream_t st = c->stream;
   int nd = c->ndom_host;
   size_t ncap1 = (size_t)c->cap_bricks * 64, ncap2 = (size_t)c->cap_bricks * 8;
   T* e0 = (T*)c->mg_e[0];

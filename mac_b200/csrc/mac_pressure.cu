@@ -145,10 +145,8 @@ __global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ blist, co
                                                const uint8_t* __restrict__ type, const uint8_t* __restrict__ flags,
                                                uint16_t* fmask, int* dbl, Scalars* ds) {
   __shared__ int64_t sb[6];
-  __shared__ int cnt;
   int b = blist[blockIdx.x];
   load_face_bases(nbr, b, sb);
-  if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
   int o = threadIdx.x;
   int64_t c = (int64_t)b * kCells + o;
@@ -193,7 +191,6 @@ __global__ void __launch_bounds__(512) k_fmask(const int* __restrict__ blist, co
       atomicMax(&ds->bbox[3 + a], bkey[3 * b + a]);
     }
   }
-  (void)cnt;
 }
 
 // ------------------------------------------------ canonical domain-brick order
