@@ -12,6 +12,9 @@ extrapolation, RK4 particle move.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The timed steps run without per-phase events; the phase times and rooflines
+in the line come from a few further, profiled steps of the same run.
+
 --impl reference times the reference's own code (compiled from its headers into
 oracle/_ref/mac_ref; its solver stand-in is FP64 Jacobi-CG at 1e-8) on the
 host cores, one single-threaded process per core, each on a bounded sub-box of
