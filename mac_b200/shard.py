@@ -113,7 +113,7 @@ def _pack(state: State, sel: np.ndarray):
     return keys, np.concatenate(parts, axis=1) if len(keys) else np.zeros((0, 0), np.uint8)
 
 
-def _unpack(state: State, rows: np.ndarray, keys: np.ndarray, blob: np.ndarray) -> None:
+def _unpack(state: State, rows: np.ndarray, blob: np.ndarray) -> None:
     col = 0
     for f in GHOST_FIELDS:
         a = _field(state, f)
@@ -181,7 +181,7 @@ def exchange_ghosts(local: LocalSlab, plan: SlabPlan, group=None) -> int:
         rows = np.array([index.get(tuple(int(v) for v in kk), -1) for kk in k], dtype=np.int64)
         ok = rows >= 0
         if ok.any():
-            _unpack(st, rows[ok], k[ok], blobs_in[p][ok])
+            _unpack(st, rows[ok], blobs_in[p][ok])
             written += int(ok.sum())
     return written
 
